@@ -1,0 +1,751 @@
+// ggms_engine.cu -- host orchestration and the C ABI (include/ggms.h).
+//
+// One call = one stream-ordered sequence of kernels over a cached workspace:
+// no host round trip between the passes, no allocation on the steady path,
+// one H2D of the ks and one D2H of the answers when those live in host memory.
+// (The reference does ~12 cudaMalloc/cudaFree and ~10 blocking copies per
+// call: DistributedSMOS/bucketMultiselect.cu:583-606, 625-638, 805-845.)
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+
+#include "ggms_kernels.cuh"
+#include "ggms_learned.cuh"
+
+namespace ggms {
+
+// ------------------------------------------------------------------ context
+struct Context {
+  int device = 0;
+  int sms = 148;
+  uint8_t* arena = nullptr;
+  size_t arena_bytes = 0;
+  uint8_t* pinned = nullptr;
+  size_t pinned_bytes = 0;
+  std::mutex mu;
+  long long launches = 0;          // kernels launched by this context
+  // profiling: events around pass 1, pass 2 and the whole call (ring of calls)
+  static constexpr int RING = 256;
+  bool profile = false;
+  cudaEvent_t ev[RING][6] = {};
+  int ring_head = 0, ring_count = 0;
+};
+
+static int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return GGMS_OK;
+  if (e == cudaErrorMemoryAllocation) return GGMS_E_OOM;
+  return GGMS_E_CUDA;
+}
+
+#define GGMS_CU(x)                                  \
+  do {                                              \
+    cudaError_t e_ = (x);                           \
+    if (e_ != cudaSuccess) return cuda_status(e_);  \
+  } while (0)
+
+static int ensure_arena(Context* c, size_t bytes) {
+  if (c->arena_bytes >= bytes) return GGMS_OK;
+  if (c->arena) {
+    GGMS_CU(cudaDeviceSynchronize());
+    cudaFree(c->arena);
+    c->arena = nullptr;
+    c->arena_bytes = 0;
+  }
+  size_t want = bytes + bytes / 8;
+  GGMS_CU(cudaMalloc(&c->arena, want));
+  c->arena_bytes = want;
+  return GGMS_OK;
+}
+
+static int ensure_pinned(Context* c, size_t bytes) {
+  if (c->pinned_bytes >= bytes) return GGMS_OK;
+  if (c->pinned) {
+    GGMS_CU(cudaDeviceSynchronize());
+    cudaFreeHost(c->pinned);
+    c->pinned = nullptr;
+    c->pinned_bytes = 0;
+  }
+  size_t want = std::max<size_t>(bytes, 1 << 16);
+  GGMS_CU(cudaMallocHost(&c->pinned, want));
+  c->pinned_bytes = want;
+  return GGMS_OK;
+}
+
+static int create_context(Context** out, int device) {
+  Context* c = new (std::nothrow) Context();
+  if (!c) return GGMS_E_OOM;
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) {
+    delete c;
+    return cuda_status(e);
+  }
+  *out = c;
+  return GGMS_OK;
+}
+
+static void destroy_context(Context* c) {
+  if (!c) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(c->device);
+  cudaDeviceSynchronize();
+  if (c->arena) cudaFree(c->arena);
+  if (c->pinned) cudaFreeHost(c->pinned);
+  for (int i = 0; i < Context::RING; ++i)
+    for (int j = 0; j < 6; ++j)
+      if (c->ev[i][j]) cudaEventDestroy(c->ev[i][j]);
+  cudaSetDevice(prev);
+  delete c;
+}
+
+// default contexts of the drop-in entry points, one per device
+static std::mutex g_default_mu;
+static Context* g_default[64];
+
+static int default_context(Context** out) {
+  int dev = 0;
+  GGMS_CU(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return GGMS_E_UNSUPPORTED;
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  if (!g_default[dev]) {
+    int rc = create_context(&g_default[dev], dev);
+    if (rc != GGMS_OK) return rc;
+  }
+  *out = g_default[dev];
+  return GGMS_OK;
+}
+
+// ------------------------------------------------------------------ workspace layout
+struct Bump {
+  size_t off = 0;
+  size_t take(size_t bytes) {
+    size_t o = (off + 255) & ~(size_t)255;
+    off = o + bytes;
+    return o;
+  }
+};
+
+template <typename K>
+struct Workspace {
+  Counters* C;
+  uint32_t* kin;
+  uint32_t* krank;
+  uint32_t* kseg;
+  uint32_t* kbin;
+  K* kkey;
+  K* samp_raw;
+  K* samp_sorted;
+  K* samp_tmp;
+  Assigner<K>* asg;       // [0] sampled, [1] learned
+  LearnState* learn;
+  uint32_t* hist0;
+  uint32_t* aflag0;
+  uint32_t* cmap0;
+  Seg<K>* segs[2];
+  uint32_t* cursor[2];
+  TileRef* tiles[2];
+  uint32_t* rows[2];
+  uint32_t* aflag[2];
+  K* points;
+  K* cand[2];
+  void* out_dev;
+  size_t bytes;
+};
+
+struct Plan {
+  uint64_t n;
+  uint32_t nk;
+  uint32_t B;        // level-0 buckets
+  uint32_t S;        // sample size
+  uint32_t cap_seg;
+  uint32_t cap_tiles;
+  int assigner;
+  int train_steps;
+  float bound;
+  uint64_t seed;
+};
+
+template <typename K>
+static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) {
+  Bump b;
+  Workspace<K> w;
+  size_t o_C = b.take(sizeof(Counters));
+  size_t o_kin = b.take(4ull * p.nk);
+  size_t o_krank = b.take(4ull * p.nk);
+  size_t o_kseg = b.take(4ull * p.nk);
+  size_t o_kbin = b.take(4ull * p.nk);
+  size_t o_kkey = b.take(sizeof(K) * p.nk);
+  size_t o_sr = b.take(sizeof(K) * p.S);
+  size_t o_ss = b.take(sizeof(K) * p.S);
+  size_t o_st = b.take(sizeof(K) * p.S);
+  size_t o_asg = b.take(sizeof(Assigner<K>) * 2);
+  size_t o_learn = b.take(sizeof(LearnState));
+  size_t o_h0 = b.take(4ull * p.B);
+  size_t o_a0 = b.take(4ull * (p.B / 32));
+  size_t o_c0 = b.take(4ull * p.B);
+  size_t o_segs[2], o_cur[2], o_tiles[2], o_rows[2], o_af[2], o_cand[2];
+  for (int i = 0; i < 2; ++i) {
+    o_segs[i] = b.take(sizeof(Seg<K>) * p.cap_seg);
+    o_cur[i] = b.take(4ull * p.cap_seg);
+    o_tiles[i] = b.take(sizeof(TileRef) * p.cap_tiles);
+    o_rows[i] = b.take(4ull * NBIN * p.cap_seg);
+    o_af[i] = b.take(4ull * NBIN_WORDS * p.cap_seg);
+  }
+  size_t o_pts = b.take(sizeof(K) * p.nk);
+  for (int i = 0; i < 2; ++i) o_cand[i] = b.take(sizeof(K) * p.n);
+  size_t o_out = b.take(out_elem_bytes * p.nk);
+  w.bytes = b.take(0) + 256;
+  if (!base) return w;
+  w.C = (Counters*)(base + o_C);
+  w.kin = (uint32_t*)(base + o_kin);
+  w.krank = (uint32_t*)(base + o_krank);
+  w.kseg = (uint32_t*)(base + o_kseg);
+  w.kbin = (uint32_t*)(base + o_kbin);
+  w.kkey = (K*)(base + o_kkey);
+  w.samp_raw = (K*)(base + o_sr);
+  w.samp_sorted = (K*)(base + o_ss);
+  w.samp_tmp = (K*)(base + o_st);
+  w.asg = (Assigner<K>*)(base + o_asg);
+  w.learn = (LearnState*)(base + o_learn);
+  w.hist0 = (uint32_t*)(base + o_h0);
+  w.aflag0 = (uint32_t*)(base + o_a0);
+  w.cmap0 = (uint32_t*)(base + o_c0);
+  for (int i = 0; i < 2; ++i) {
+    w.segs[i] = (Seg<K>*)(base + o_segs[i]);
+    w.cursor[i] = (uint32_t*)(base + o_cur[i]);
+    w.tiles[i] = (TileRef*)(base + o_tiles[i]);
+    w.rows[i] = (uint32_t*)(base + o_rows[i]);
+    w.aflag[i] = (uint32_t*)(base + o_af[i]);
+    w.cand[i] = (K*)(base + o_cand[i]);
+  }
+  w.points = (K*)(base + o_pts);
+  w.out_dev = (void*)(base + o_out);
+  return w;
+}
+
+static uint32_t pow2_floor(uint64_t v) {
+  uint32_t r = 1;
+  while ((uint64_t)r * 2 <= v && r < (1u << 30)) r <<= 1;
+  return r;
+}
+
+static int make_plan(Plan* p, uint64_t n, uint32_t nk, const ggms_opts& o) {
+  p->n = n;
+  p->nk = nk;
+  uint32_t B = (uint32_t)o.num_buckets;
+  if (B == 0) {
+    // about 2^11 elements per bucket, between 2^10 and 2^14 buckets
+    B = pow2_floor(std::max<uint64_t>(n >> 11, 1));
+    B = std::min<uint32_t>(std::max<uint32_t>(B, 1u << 10), 1u << 14);
+  }
+  if (B < (1u << 10) || B > (1u << 15) || (B & (B - 1))) return GGMS_E_INVALID_ARG;
+  p->B = B;
+  int asg = o.assigner;
+  if (asg < GGMS_ASSIGNER_AUTO || asg > GGMS_ASSIGNER_LEARNED_MLP) return GGMS_E_INVALID_ARG;
+  p->assigner = asg;
+  uint32_t S = (uint32_t)o.sample_size;
+  if (S == 0) S = (asg == GGMS_ASSIGNER_SAMPLED) ? 1024u : (1u << 16);
+  if (S < 1024u || S > 65536u || (S & (S - 1))) return GGMS_E_INVALID_ARG;
+  p->S = S;
+  p->cap_seg = nk + 1;
+  p->cap_tiles = (uint32_t)((n + TILE - 1) / TILE) + p->cap_seg;
+  p->train_steps = o.train_steps > 0 ? o.train_steps : 0;
+  p->bound = o.imbalance_bound > 0.0f ? o.imbalance_bound : 3.0f;
+  p->seed = o.seed;
+  return GGMS_OK;
+}
+
+// ------------------------------------------------------------------ kernel configs
+constexpr int L0_NT = 512;
+constexpr int L0_UNROLL = 4;
+constexpr int LV_NT = 256;
+constexpr int MAX_LEVELS_32 = 3;
+constexpr int MAX_LEVELS_64 = 6;
+
+template <typename T>
+static size_t l0_smem(uint32_t B) {
+  return (size_t)B * 4u + AsgSmem<typename KeyOf<T>::K>::bytes;
+}
+
+template <typename T>
+static int l0_grid(Context* c, uint32_t B, int* grid) {
+  static int occ_cache[2][8] = {};
+  const int bi = (B == (1u << 15)) ? 5 : (B == (1u << 14)) ? 4 : (B == (1u << 13)) ? 3
+               : (B == (1u << 12)) ? 2 : (B == (1u << 11)) ? 1 : 0;
+  size_t sm = l0_smem<T>(B);
+  GGMS_CU(cudaFuncSetAttribute(l0_count<T, L0_NT, L0_UNROLL>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  GGMS_CU(cudaFuncSetAttribute(l0_compact<T, L0_NT, L0_UNROLL>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  int occ = 0;
+  GGMS_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, l0_count<T, L0_NT, L0_UNROLL>,
+                                                        L0_NT, sm));
+  (void)occ_cache;
+  (void)bi;
+  *grid = std::max(1, occ) * c->sms;
+  return GGMS_OK;
+}
+
+// Profiling slot of the current call (or null when profiling is off).
+static cudaEvent_t* prof_slot(Context* c) {
+  if (!c->profile) return nullptr;
+  if (c->ring_count == Context::RING) return nullptr;  // ring full: drop
+  int idx = (c->ring_head + c->ring_count) % Context::RING;
+  if (!c->ev[idx][0])
+    for (int j = 0; j < 6; ++j) cudaEventCreate(&c->ev[idx][j]);
+  c->ring_count++;
+  return c->ev[idx];
+}
+static inline void prof_rec(cudaEvent_t* slot, int j, cudaStream_t st) {
+  if (slot) cudaEventRecord(slot[j], st);
+}
+
+static inline unsigned cdiv(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }
+
+// ------------------------------------------------------------------ the single-vector path
+template <typename T>
+static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* ks, uint64_t nk64,
+                      T* out, const ggms_opts& o, cudaStream_t st) {
+  using K = typename KeyOf<T>::K;
+  if (!d_in || n == 0 || n > 0xFFFFFFFFull || nk64 > 0x7FFFFFFFull) return GGMS_E_INVALID_ARG;
+  if (nk64 == 0) return GGMS_OK;
+  if (!ks || !out) return GGMS_E_INVALID_ARG;
+  if ((uintptr_t)d_in % sizeof(T) != 0) return GGMS_E_INVALID_ARG;
+  const uint32_t nk = (uint32_t)nk64;
+  if (!o.ks_on_device) {
+    for (uint32_t i = 0; i < nk; ++i)
+      if (ks[i] < 1u || (uint64_t)ks[i] > n) return GGMS_E_INVALID_ARG;
+  }
+  Plan p;
+  int rc = make_plan(&p, n, nk, o);
+  if (rc) return rc;
+  GGMS_CU(cudaSetDevice(ctx->device));
+  Workspace<K> w0 = layout<K>(p, sizeof(T), nullptr);
+  rc = ensure_arena(ctx, w0.bytes);
+  if (rc) return rc;
+  Workspace<K> w = layout<K>(p, sizeof(T), ctx->arena);
+  const bool host_k = !o.ks_on_device, host_out = !o.out_on_device;
+  const size_t pin_bytes = (host_k ? 4ull * nk : 0) + (host_out ? sizeof(T) * nk : 0) + sizeof(Counters) + 64;
+  rc = ensure_pinned(ctx, pin_bytes);
+  if (rc) return rc;
+  uint8_t* pin = ctx->pinned;
+  Counters* pin_C = (Counters*)pin;
+  uint8_t* pin_k = pin + ((sizeof(Counters) + 63) & ~(size_t)63);
+  uint8_t* pin_out = pin_k + (host_k ? ((4ull * nk + 63) & ~(size_t)63) : 0);
+
+  const Caps caps{p.cap_seg, p.cap_tiles, p.nk};
+  cudaEvent_t* prof = prof_slot(ctx);
+  prof_rec(prof, 0, st);
+  GGMS_CU(cudaMemsetAsync(w.C, 0, sizeof(Counters), st));
+  const uint32_t* d_k = ks;
+  if (host_k) {
+    memcpy(pin_k, ks, 4ull * nk);
+    GGMS_CU(cudaMemcpyAsync(w.kin, pin_k, 4ull * nk, cudaMemcpyHostToDevice, st));
+    d_k = w.kin;
+  }
+  ++ctx->launches;
+  k_init_single<<<cdiv(nk, 256), 256, 0, st>>>(d_k, nk, n, w.krank, w.kseg, w.C);
+
+  // ---- level-0 assigner
+  const uint32_t S = p.S;
+  ++ctx->launches;
+  asg_sample<T><<<cdiv(S, 256), 256, 0, st>>>(d_in, n, S, p.seed, w.samp_raw);
+  if (S <= 4096) {
+    ++ctx->launches;
+    asg_sort_chunks<K, 4096, 1024><<<1, 1024, 0, st>>>(w.samp_raw, w.samp_sorted, S);
+  } else {
+    ++ctx->launches;
+    asg_sort_chunks<K, 4096, 1024><<<S / 4096, 1024, 0, st>>>(w.samp_raw, w.samp_tmp, S);
+    ++ctx->launches;
+    asg_merge_rank<K><<<cdiv(S, 256), 256, 0, st>>>(w.samp_tmp, w.samp_sorted, S, 4096u);
+  }
+  ++ctx->launches;
+  asg_build_sampled<K><<<1, 256, 0, st>>>(w.samp_sorted, S, p.B, &w.asg[0]);
+  if (p.assigner != GGMS_ASSIGNER_SAMPLED) {
+    rc = learn_and_choose<K>(p.assigner, w.samp_sorted, S, p.B, p.train_steps, p.bound, w.asg,
+                             w.learn, &w.C->asg_choice, st, &ctx->launches);
+    if (rc) return rc;
+  }
+
+  // ---- PASS 1: count
+  int grid = 0;
+  rc = l0_grid<T>(ctx, p.B, &grid);
+  if (rc) return rc;
+  const size_t sm = l0_smem<T>(p.B);
+  GGMS_CU(cudaMemsetAsync(w.hist0, 0, 4ull * p.B, st));
+  GGMS_CU(cudaMemsetAsync(w.aflag0, 0, 4ull * (p.B / 32), st));
+  prof_rec(prof, 1, st);
+  ++ctx->launches;
+  l0_count<T, L0_NT, L0_UNROLL><<<grid, L0_NT, sm, st>>>(d_in, n, w.asg, w.C, w.hist0);
+  prof_rec(prof, 2, st);
+  ++ctx->launches;
+  l0_scan<<<1, 1024, 0, st>>>(w.hist0, p.B, w.C);
+  ++ctx->launches;
+  lvl_locate_rows<<<cdiv(nk, 256), 256, 0, st>>>(w.hist0, p.B, nk, w.krank, w.kseg, w.kbin,
+                                                   w.aflag0, p.B / 32, w.C);
+  ++ctx->launches;
+  l0_children<K><<<cdiv(p.B, 256), 256, 0, st>>>(w.hist0, w.aflag0, p.B, w.asg, w.C, w.cmap0,
+                                                   w.segs[1], w.cursor[1], w.tiles[1], w.points, caps);
+  ++ctx->launches;
+  lvl_relabel<K><<<cdiv(nk, 256), 256, 0, st>>>(w.cmap0, p.B, nk, w.kbin, w.kseg, w.kkey,
+                                                  w.points, w.C);
+  // ---- PASS 2: compact the buckets that still need refinement
+  prof_rec(prof, 3, st);
+  ++ctx->launches;
+  l0_compact<T, L0_NT, L0_UNROLL><<<grid, L0_NT, sm, st>>>(d_in, n, w.asg, w.C, w.cmap0,
+                                                           w.segs[1], w.cursor[1], w.cand[0]);
+  prof_rec(prof, 4, st);
+
+  // ---- refinement levels over candidates
+  const int maxlev = (sizeof(K) == 4) ? MAX_LEVELS_32 : MAX_LEVELS_64;
+  const int lv_grid = ctx->sms * 8;
+  const int seg_grid = std::min<int>((int)p.cap_seg, ctx->sms * 2);
+  for (int l = 1; l <= maxlev; ++l) {
+    const int pp = l & 1, q = pp ^ 1;
+    const K* src = w.cand[(l - 1) & 1];
+    K* dst = w.cand[l & 1];
+    ++ctx->launches;
+    lvl_prep<<<ctx->sms * 2, 256, 0, st>>>(w.rows[pp], w.aflag[pp], w.C, pp, caps);
+    ++ctx->launches;
+    lvl_count<K, LV_NT><<<lv_grid, LV_NT, 0, st>>>(src, w.segs[pp], w.tiles[pp], w.C, pp, w.rows[pp], caps);
+    ++ctx->launches;
+    lvl_scan<<<seg_grid, 1024, 0, st>>>(w.rows[pp], w.C, pp, caps);
+    ++ctx->launches;
+    lvl_locate_rows<<<cdiv(nk, 256), 256, 0, st>>>(w.rows[pp], NBIN, nk, w.krank, w.kseg, w.kbin,
+                                                     w.aflag[pp], NBIN_WORDS, w.C);
+    ++ctx->launches;
+    lvl_children<K, 1024><<<seg_grid, 1024, 0, st>>>(w.rows[pp], w.aflag[pp], w.segs[pp], w.C, pp,
+                                                     w.segs[q], w.cursor[q], w.tiles[q], w.points, caps);
+    ++ctx->launches;
+    lvl_relabel<K><<<cdiv(nk, 256), 256, 0, st>>>(w.rows[pp], NBIN, nk, w.kbin, w.kseg, w.kkey,
+                                                    w.points, w.C);
+    if (l < maxlev) {
+      ++ctx->launches;
+      lvl_compact<K, LV_NT><<<lv_grid, LV_NT, 0, st>>>(src, w.segs[pp], w.tiles[pp], w.C, pp,
+                                                       w.rows[pp], w.segs[q], w.cursor[q], dst, caps);
+    }
+  }
+
+  // ---- answers
+  T* d_out = host_out ? (T*)w.out_dev : out;
+  ++ctx->launches;
+  write_out<T><<<cdiv(nk, 256), 256, 0, st>>>(w.kkey, w.kseg, nk, d_out, w.C);
+  GGMS_CU(cudaGetLastError());
+  if (host_out) GGMS_CU(cudaMemcpyAsync(pin_out, d_out, sizeof(T) * nk, cudaMemcpyDeviceToHost, st));
+  prof_rec(prof, 5, st);
+  const bool need_sync = host_out || o.stats;
+  if (!need_sync) return GGMS_OK;
+  GGMS_CU(cudaMemcpyAsync(pin_C, w.C, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+  GGMS_CU(cudaStreamSynchronize(st));
+  if (host_out) memcpy(out, pin_out, sizeof(T) * nk);
+  if (o.stats) {
+    ggms_stats* s = o.stats;
+    Assigner<K> a_used;
+    GGMS_CU(cudaMemcpy(&a_used, &w.asg[pin_C->asg_choice], sizeof(Assigner<K>), cudaMemcpyDeviceToHost));
+    LearnState ls;
+    GGMS_CU(cudaMemcpy(&ls, w.learn, sizeof(LearnState), cudaMemcpyDeviceToHost));
+    s->assigner_used = (int32_t)a_used.kind;
+    s->num_buckets = (int32_t)p.B;
+    s->full_passes = 2;
+    s->levels = (int32_t)pin_C->levels_run;
+    s->candidates = (int64_t)pin_C->cand0;
+    s->refine_elements = (int64_t)pin_C->refine_elems;
+    s->active_buckets = (int32_t)pin_C->active0;
+    s->point_buckets = (int32_t)pin_C->point0;
+    s->small_segments = (int32_t)pin_C->small_segs;
+    s->sample_size = (int32_t)S;
+    s->bucket_max_over_mean = (float)pin_C->max_bucket0 / ((float)n / (float)p.B);
+    s->model_imbalance = (p.assigner == GGMS_ASSIGNER_SAMPLED) ? 0.0f : ls.imbalance;
+    s->model_loss = (p.assigner == GGMS_ASSIGNER_SAMPLED) ? 0.0f : ls.loss;
+  }
+  if (pin_C->status) return (int)pin_C->status;
+  return GGMS_OK;
+}
+
+template <typename T>
+static int dropin(const T* d_vector, int length, const uint32_t* kVals, int numKs, T* outputs) {
+  if (length <= 0 || numKs < 0) return GGMS_E_INVALID_ARG;
+  Context* c = nullptr;
+  int rc = default_context(&c);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(c->mu);
+  ggms_opts o;
+  ggms_default_opts(&o);
+  return run_single<T>(c, d_vector, (uint64_t)length, kVals, (uint64_t)numKs, outputs, o, 0);
+}
+
+template <typename T>
+static int ex(ggms_context* cx, const T* d_in, int64_t n, const uint32_t* ks, int64_t nk, T* out,
+              const ggms_opts* opts, void* stream) {
+  if (n <= 0 || nk < 0) return GGMS_E_INVALID_ARG;
+  ggms_opts o;
+  ggms_default_opts(&o);
+  if (opts) {
+    if (opts->struct_size != (int32_t)sizeof(ggms_opts)) return GGMS_E_INVALID_ARG;
+    o = *opts;
+  }
+  Context* c = (Context*)cx;
+  if (!c) {
+    int rc = default_context(&c);
+    if (rc) return rc;
+  }
+  std::lock_guard<std::mutex> lk(c->mu);
+  return run_single<T>(c, d_in, (uint64_t)n, ks, (uint64_t)nk, out, o, (cudaStream_t)stream);
+}
+
+
+// ------------------------------------------------------------------ batched segmented path
+// Level 0 is a radix level over each caller segment (no per-segment sampling
+// yet); every level runs over all segments at once.
+template <typename T>
+static int run_segmented(Context* ctx, const T* d_in, const int64_t* seg_off, int64_t nseg64,
+                         const uint32_t* ks, const int64_t* k_off, T* out, const ggms_opts& o,
+                         cudaStream_t st) {
+  using K = typename KeyOf<T>::K;
+  if (!d_in || !seg_off || !k_off || nseg64 <= 0 || nseg64 > (1 << 30)) return GGMS_E_INVALID_ARG;
+  if ((uintptr_t)d_in % sizeof(T) != 0) return GGMS_E_INVALID_ARG;
+  const uint32_t nseg = (uint32_t)nseg64;
+  int64_t h_tot[2], h_k[2];
+  GGMS_CU(cudaSetDevice(ctx->device));
+  GGMS_CU(cudaMemcpyAsync(&h_tot[0], seg_off, 8, cudaMemcpyDeviceToHost, st));
+  GGMS_CU(cudaMemcpyAsync(&h_tot[1], seg_off + nseg, 8, cudaMemcpyDeviceToHost, st));
+  GGMS_CU(cudaMemcpyAsync(&h_k[0], k_off, 8, cudaMemcpyDeviceToHost, st));
+  GGMS_CU(cudaMemcpyAsync(&h_k[1], k_off + nseg, 8, cudaMemcpyDeviceToHost, st));
+  GGMS_CU(cudaStreamSynchronize(st));
+  if (h_tot[0] != 0 || h_k[0] != 0 || h_tot[1] < 0 || h_k[1] < 0) return GGMS_E_INVALID_ARG;
+  const uint64_t n = (uint64_t)h_tot[1];
+  const uint64_t nk64 = (uint64_t)h_k[1];
+  if (nk64 == 0) return GGMS_OK;
+  if (n == 0 || n > 0xFFFFFFFFull || nk64 > 0x7FFFFFFFull || !ks || !out) return GGMS_E_INVALID_ARG;
+  const uint32_t nk = (uint32_t)nk64;
+  ggms_opts oo = o;
+  oo.assigner = GGMS_ASSIGNER_SAMPLED;
+  oo.num_buckets = 1024;
+  oo.sample_size = 1024;
+  Plan p;
+  int rc = make_plan(&p, n, nk, oo);
+  if (rc) return rc;
+  p.cap_seg = std::max<uint32_t>(nk, nseg) + 1;
+  p.cap_tiles = (uint32_t)((n + TILE - 1) / TILE) + p.cap_seg;
+  Workspace<K> w0 = layout<K>(p, sizeof(T), nullptr);
+  rc = ensure_arena(ctx, w0.bytes);
+  if (rc) return rc;
+  Workspace<K> w = layout<K>(p, sizeof(T), ctx->arena);
+  const Caps caps{p.cap_seg, p.cap_tiles, p.nk};
+  GGMS_CU(cudaMemsetAsync(w.C, 0, sizeof(Counters), st));
+  ++ctx->launches;
+  k_init_seg<<<cdiv(nk, 256), 256, 0, st>>>(ks, nk, seg_off, k_off, nseg, w.krank, w.kseg, w.C);
+  ++ctx->launches;
+  seg_init<K><<<cdiv(nseg, 256), 256, 0, st>>>(seg_off, nseg, k_off, w.segs[0], w.tiles[0], w.C);
+  ++ctx->launches;
+  seg_set_count<<<1, 1, 0, st>>>(w.C, nseg);
+  const int maxlev = (sizeof(K) == 4) ? 3 : 6;  // radix shifts 21,10,0 / 53,42,31,20,9,0
+  const int lv_grid = ctx->sms * 8;
+  const int seg_grid = ctx->sms * 2;
+  for (int l = 0; l < maxlev; ++l) {
+    const int pp = l & 1, q = pp ^ 1;
+    K* dst = w.cand[l & 1];
+    ++ctx->launches;
+    lvl_prep<<<ctx->sms * 2, 256, 0, st>>>(w.rows[pp], w.aflag[pp], w.C, pp, caps);
+    if (l == 0) {
+        ++ctx->launches;
+        lvl_count<T, LV_NT><<<lv_grid, LV_NT, 0, st>>>(d_in, w.segs[pp], w.tiles[pp], w.C, pp, w.rows[pp], caps);
+      } else {
+        ++ctx->launches;
+        lvl_count<K, LV_NT><<<lv_grid, LV_NT, 0, st>>>(w.cand[(l - 1) & 1], w.segs[pp], w.tiles[pp],
+                                                       w.C, pp, w.rows[pp], caps);
+      }
+    ++ctx->launches;
+    lvl_scan<<<seg_grid, 1024, 0, st>>>(w.rows[pp], w.C, pp, caps);
+    ++ctx->launches;
+    lvl_locate_rows<<<cdiv(nk, 256), 256, 0, st>>>(w.rows[pp], NBIN, nk, w.krank, w.kseg, w.kbin,
+                                                     w.aflag[pp], NBIN_WORDS, w.C);
+    ++ctx->launches;
+    lvl_children<K, 1024><<<seg_grid, 1024, 0, st>>>(w.rows[pp], w.aflag[pp], w.segs[pp], w.C, pp,
+                                                     w.segs[q], w.cursor[q], w.tiles[q], w.points, caps);
+    ++ctx->launches;
+    lvl_relabel<K><<<cdiv(nk, 256), 256, 0, st>>>(w.rows[pp], NBIN, nk, w.kbin, w.kseg, w.kkey,
+                                                    w.points, w.C);
+    if (l + 1 < maxlev) {
+      if (l == 0) {
+          ++ctx->launches;
+          lvl_compact<T, LV_NT><<<lv_grid, LV_NT, 0, st>>>(d_in, w.segs[pp], w.tiles[pp], w.C, pp,
+                                                           w.rows[pp], w.segs[q], w.cursor[q], dst, caps);
+        } else {
+          ++ctx->launches;
+          lvl_compact<K, LV_NT><<<lv_grid, LV_NT, 0, st>>>(w.cand[(l - 1) & 1], w.segs[pp], w.tiles[pp],
+                                                           w.C, pp, w.rows[pp], w.segs[q], w.cursor[q],
+                                                           dst, caps);
+        }
+    }
+  }
+  ++ctx->launches;
+  write_out<T><<<cdiv(nk, 256), 256, 0, st>>>(w.kkey, w.kseg, nk, out, w.C);
+  GGMS_CU(cudaGetLastError());
+  if (o.stats) {
+    Counters hc;
+    GGMS_CU(cudaMemcpyAsync(&hc, w.C, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+    GGMS_CU(cudaStreamSynchronize(st));
+    memset(o.stats, 0, sizeof(ggms_stats));
+    o.stats->levels = (int32_t)hc.levels_run;
+    o.stats->refine_elements = (int64_t)hc.refine_elems;
+    o.stats->full_passes = 2;
+    if (hc.status) return (int)hc.status;
+  }
+  return GGMS_OK;
+}
+
+template <typename T>
+static int segmented(ggms_context* cx, const T* d_in, const int64_t* seg_off, int64_t nseg,
+                     const uint32_t* ks, const int64_t* k_off, T* out, const ggms_opts* opts,
+                     void* stream) {
+  ggms_opts o;
+  ggms_default_opts(&o);
+  if (opts) {
+    if (opts->struct_size != (int32_t)sizeof(ggms_opts)) return GGMS_E_INVALID_ARG;
+    o = *opts;
+  }
+  Context* c = (Context*)cx;
+  if (!c) {
+    int rc = default_context(&c);
+    if (rc) return rc;
+  }
+  std::lock_guard<std::mutex> lk(c->mu);
+  return run_segmented<T>(c, d_in, seg_off, nseg, ks, k_off, out, o, (cudaStream_t)stream);
+}
+
+}  // namespace ggms
+
+// ====================================================================== C ABI
+using namespace ggms;
+
+extern "C" {
+
+void ggms_default_opts(ggms_opts* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->struct_size = (int32_t)sizeof(ggms_opts);
+  o->assigner = GGMS_ASSIGNER_AUTO;
+  o->seed = 0x5EEDull;
+  o->imbalance_bound = 3.0f;
+}
+
+const char* ggms_status_string(int s) {
+  switch (s) {
+    case GGMS_OK: return "ok";
+    case GGMS_E_INVALID_ARG: return "invalid argument";
+    case GGMS_E_OOM: return "out of memory";
+    case GGMS_E_NOT_CONVERGED: return "not converged";
+    case GGMS_E_CUDA: return "CUDA error";
+    case GGMS_E_UNSUPPORTED: return "unsupported";
+    case GGMS_E_INTERNAL: return "internal error";
+    default: return "unknown status";
+  }
+}
+
+int ggms_version(void) { return 100; }
+
+int ggms_create(ggms_context** ctx, int device) {
+  if (!ctx) return GGMS_E_INVALID_ARG;
+  Context* c = nullptr;
+  int rc = create_context(&c, device);
+  if (rc) return rc;
+  *ctx = (ggms_context*)c;
+  return GGMS_OK;
+}
+
+int ggms_destroy(ggms_context* ctx) {
+  destroy_context((Context*)ctx);
+  return GGMS_OK;
+}
+
+int ggms_get_default_context(ggms_context** ctx) {
+  if (!ctx) return GGMS_E_INVALID_ARG;
+  Context* c = nullptr;
+  int rc = default_context(&c);
+  if (rc) return rc;
+  *ctx = (ggms_context*)c;
+  return GGMS_OK;
+}
+
+int ggms_context_profile(ggms_context* ctx, int enable) {
+  Context* c = (Context*)ctx;
+  if (!c) return GGMS_E_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->profile = enable != 0;
+  return GGMS_OK;
+}
+
+int ggms_context_pass_times(ggms_context* ctx, float* p1, float* p2, float* call, int max) {
+  Context* c = (Context*)ctx;
+  if (!c || max < 0) return -GGMS_E_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(c->mu);
+  int got = 0;
+  while (c->ring_count > 0 && got < max) {
+    cudaEvent_t* e = c->ev[c->ring_head];
+    if (cudaEventSynchronize(e[5]) != cudaSuccess) return -GGMS_E_CUDA;
+    float a = 0, b = 0, t = 0;
+    cudaEventElapsedTime(&a, e[1], e[2]);
+    cudaEventElapsedTime(&b, e[3], e[4]);
+    cudaEventElapsedTime(&t, e[0], e[5]);
+    if (p1) p1[got] = a;
+    if (p2) p2[got] = b;
+    if (call) call[got] = t;
+    ++got;
+    c->ring_head = (c->ring_head + 1) % Context::RING;
+    c->ring_count--;
+  }
+  return got;
+}
+
+int64_t ggms_context_launches(ggms_context* ctx) {
+  Context* c = (Context*)ctx;
+  if (!c) return -1;
+  return (int64_t)c->launches;
+}
+
+#define GGMS_DROPIN(NAME, T)                                                                 \
+  int NAME(const T* d_vector, int length, const uint32_t* kVals, int numKs, T* outputs,     \
+           int blocks, int threads) {                                                        \
+    (void)blocks;                                                                            \
+    (void)threads;                                                                           \
+    return dropin<T>(d_vector, length, kVals, numKs, outputs);                               \
+  }
+
+GGMS_DROPIN(ggms_bucket_multiselect_f32, float)
+GGMS_DROPIN(ggms_bucket_multiselect_f64, double)
+GGMS_DROPIN(ggms_bucket_multiselect_u32, uint32_t)
+GGMS_DROPIN(ggms_bucket_multiselect_i32, int32_t)
+GGMS_DROPIN(ggms_iterative_smos_f32, float)
+GGMS_DROPIN(ggms_iterative_smos_f64, double)
+GGMS_DROPIN(ggms_iterative_smos_u32, uint32_t)
+GGMS_DROPIN(ggms_iterative_smos_i32, int32_t)
+
+#define GGMS_EX(NAME, T)                                                                      \
+  int NAME(ggms_context* ctx, const T* d_in, int64_t n, const uint32_t* ks, int64_t nk,      \
+           T* out, const ggms_opts* opts, void* stream) {                                     \
+    return ex<T>(ctx, d_in, n, ks, nk, out, opts, stream);                                    \
+  }
+
+GGMS_EX(ggms_multiselect_f32_ex, float)
+GGMS_EX(ggms_multiselect_f64_ex, double)
+GGMS_EX(ggms_multiselect_u32_ex, uint32_t)
+GGMS_EX(ggms_multiselect_i32_ex, int32_t)
+
+int ggms_multiselect_segmented_f32(ggms_context* ctx, const float* d_in, const int64_t* seg_off,
+                                   int64_t nseg, const uint32_t* ks, const int64_t* k_off,
+                                   float* out, const ggms_opts* opts, void* stream) {
+  return segmented<float>(ctx, d_in, seg_off, nseg, ks, k_off, out, opts, stream);
+}
+int ggms_multiselect_segmented_u32(ggms_context* ctx, const uint32_t* d_in, const int64_t* seg_off,
+                                   int64_t nseg, const uint32_t* ks, const int64_t* k_off,
+                                   uint32_t* out, const ggms_opts* opts, void* stream) {
+  return segmented<uint32_t>(ctx, d_in, seg_off, nseg, ks, k_off, out, opts, stream);
+}
+
+}  // extern "C"

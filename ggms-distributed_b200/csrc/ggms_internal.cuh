@@ -1,0 +1,212 @@
+// ggms_internal.cuh -- shared device definitions of the selector.
+//
+// Keys.  Every input type is mapped on load to an unsigned key whose integer
+// order is the value order (the reference compares raw values with >= against
+// pivots, DistributedSMOS/bucketMultiselect.cu:178-185; mapping to keys makes
+// NaN, -0.0/+0.0 and duplicates exact and lets every later step be integer
+// work):
+//   float  : bits ^ (negative ? 0xFFFFFFFF : 0x80000000)
+//   double : the 64-bit analogue
+//   int32  : bits ^ 0x80000000
+//   uint32 : identity
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ggms {
+
+// ------------------------------------------------------------------ key traits
+template <typename T> struct KeyOf;
+template <> struct KeyOf<float> {
+  using K = uint32_t;
+  static constexpr int BITS = 32;
+  __host__ __device__ static K to(float v) {
+#ifdef __CUDA_ARCH__
+    uint32_t u = __float_as_uint(v);
+#else
+    uint32_t u; __builtin_memcpy(&u, &v, 4);
+#endif
+    return u ^ ((u >> 31) ? 0xFFFFFFFFu : 0x80000000u);
+  }
+  __host__ __device__ static float from(K k) {
+    uint32_t u = k ^ ((k >> 31) ? 0x80000000u : 0xFFFFFFFFu);
+#ifdef __CUDA_ARCH__
+    return __uint_as_float(u);
+#else
+    float v; __builtin_memcpy(&v, &u, 4); return v;
+#endif
+  }
+};
+template <> struct KeyOf<double> {
+  using K = uint64_t;
+  static constexpr int BITS = 64;
+  __host__ __device__ static K to(double v) {
+#ifdef __CUDA_ARCH__
+    uint64_t u = (uint64_t)__double_as_longlong(v);
+#else
+    uint64_t u; __builtin_memcpy(&u, &v, 8);
+#endif
+    return u ^ ((u >> 63) ? 0xFFFFFFFFFFFFFFFFull : 0x8000000000000000ull);
+  }
+  __host__ __device__ static double from(K k) {
+    uint64_t u = k ^ ((k >> 63) ? 0x8000000000000000ull : 0xFFFFFFFFFFFFFFFFull);
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double((long long)u);
+#else
+    double v; __builtin_memcpy(&v, &u, 8); return v;
+#endif
+  }
+};
+template <> struct KeyOf<uint32_t> {
+  using K = uint32_t;
+  static constexpr int BITS = 32;
+  __host__ __device__ static K to(uint32_t v) { return v; }
+  __host__ __device__ static uint32_t from(K k) { return k; }
+};
+template <> struct KeyOf<uint64_t> {  // keys of 64-bit types are already keys
+  using K = uint64_t;
+  static constexpr int BITS = 64;
+  __host__ __device__ static K to(uint64_t v) { return v; }
+  __host__ __device__ static uint64_t from(K k) { return k; }
+};
+template <> struct KeyOf<int32_t> {
+  using K = uint32_t;
+  static constexpr int BITS = 32;
+  __host__ __device__ static K to(int32_t v) { return ((uint32_t)v) ^ 0x80000000u; }
+  __host__ __device__ static int32_t from(K k) { return (int32_t)(k ^ 0x80000000u); }
+};
+
+template <typename K> struct KeyBits;
+template <> struct KeyBits<uint32_t> { static constexpr int value = 32; };
+template <> struct KeyBits<uint64_t> { static constexpr int value = 64; };
+
+__device__ __forceinline__ float key_to_float_rn(uint32_t d) { return __uint2float_rn(d); }
+__device__ __forceinline__ float key_to_float_rn(uint64_t d) { return __ull2float_rn(d); }
+
+__host__ __device__ __forceinline__ int bitlen(uint32_t v) {
+#ifdef __CUDA_ARCH__
+  return 32 - __clz(v);
+#else
+  return v ? 32 - __builtin_clz(v) : 0;
+#endif
+}
+__host__ __device__ __forceinline__ int bitlen(uint64_t v) {
+#ifdef __CUDA_ARCH__
+  return 64 - __clzll((long long)v);
+#else
+  return v ? 64 - __builtin_clzll(v) : 0;
+#endif
+}
+
+// ------------------------------------------------------------------ constants
+constexpr int RADIX_BITS = 11;                  // bits resolved per refinement level
+constexpr int NBIN = 1 << RADIX_BITS;           // 2048 bins per refinement segment
+constexpr int NBIN_WORDS = NBIN / 32;           // active-flag words per segment row
+constexpr int TILE = 16384;                     // elements per refinement work item
+constexpr int ASG_MAXM = 256;                   // max segments of the level-0 assigner
+constexpr int ASG_CELL_BITS = 12;
+constexpr int ASG_NCELL = 1 << ASG_CELL_BITS;   // uniform lookup cells over the knot range
+constexpr uint32_t K_DONE = 0xFFFFFFFFu;        // k_seg value of a resolved k
+constexpr uint32_t CM_NONE = 0xFFFFFFFFu;       // child-map entry: bin holds no requested k
+constexpr uint32_t CM_POINT = 0x80000000u;      // child-map flag: bin is one key; low bits index points[]
+
+// ------------------------------------------------------------------ assigner
+// A monotone piecewise-linear map key -> bucket in [0, B).  Keys below the
+// first knot go to bucket 0, keys above the last knot to bucket B-1; inside,
+// segment j ([x[j], x[j+1])) maps linearly onto buckets [base[j], base[j+1]-1].
+// This one format carries both the reference's sampled pivots + slopes
+// (DistributedSMOS/bucketMultiselect.cu:421-515, 135-210) and the learned
+// CDF models, which are compiled into it.  A uniform cell table over the knot
+// range gives the segment of a key in O(1) (plus a short forward walk).
+template <typename K>
+struct Assigner {
+  uint32_t M;                 // segments; knots are x[0..M]
+  uint32_t B;                 // buckets
+  uint32_t csh;               // cell = (key - x[0]) >> csh
+  uint32_t ncell;             // cells in use
+  uint32_t kind;              // GGMS_ASSIGNER_* that built it
+  float quality;              // imbalance measured on the sample (max/mean)
+  float loss;                 // training loss (learned) or 0
+  uint32_t pad;
+  K x[ASG_MAXM + 1];
+  uint32_t base[ASG_MAXM + 1];
+  float slope[ASG_MAXM];
+  uint16_t idx[ASG_NCELL];
+};
+
+// Shared-memory view of an assigner (the hot loops copy it in once).
+template <typename K>
+struct AsgView {
+  const K* x;
+  const uint32_t* base;
+  const float* slope;
+  const uint16_t* idx;
+  uint32_t M, B, csh;
+};
+
+// The single evaluation routine used by the counting pass, the compaction pass
+// and the inverse (bucket -> key range) search.  All arithmetic is explicitly
+// rounded (no contraction), so every kernel computes the same bucket.
+template <typename K>
+__device__ __forceinline__ uint32_t asg_eval(const AsgView<K>& a, K key) {
+  const K x0 = a.x[0];
+  if (key < x0) return 0u;
+  const uint32_t M = a.M;
+  if (key > a.x[M]) return a.B - 1u;
+  if (M == 0u) return a.base[0];
+  uint32_t c = (uint32_t)((key - x0) >> a.csh);
+  uint32_t j = a.idx[c];
+  while (j + 1u < M && key >= a.x[j + 1u]) ++j;
+  const uint32_t b0 = a.base[j];
+  // segment j maps into [base[j], base[j+1] - 1]: distinct knots never share a bucket
+  const uint32_t span = a.base[j + 1u] - b0;
+  const float cap = __uint2float_rn(span ? span - 1u : 0u);
+  float t = __fmul_rn(key_to_float_rn((K)(key - a.x[j])), a.slope[j]);
+  t = fminf(t, cap);
+  return b0 + __float2uint_rz(t);
+}
+
+// ------------------------------------------------------------------ refinement levels
+// A segment of candidates.  Every key of the segment lies in [lo, hi]; its bin
+// is (key - lo) >> shift, shift chosen so that bins < NBIN.
+template <typename K>
+struct Seg {
+  uint64_t off;   // first element in the level's source buffer (or input)
+  uint32_t cnt;   // elements
+  uint32_t shift;
+  K lo;
+  K hi;
+};
+
+struct TileRef {
+  uint32_t seg;   // segment id in the level's list
+  uint32_t no;    // tile number inside the segment
+};
+
+// Device counters (one small block of memory, zeroed per call).
+struct Counters {
+  uint32_t nsegs[2];          // segments of the level stored in pool p
+  uint32_t ntiles[2];
+  uint32_t npoints;
+  uint32_t status;            // nonzero: internal error code
+  uint32_t active0;           // active level-0 buckets
+  uint32_t point0;            // of which single-key
+  uint32_t levels_run;        // refinement levels that had work
+  uint32_t max_bucket0;       // largest level-0 bucket
+  uint32_t small_segs;
+  uint32_t pad0;
+  unsigned long long cand0;   // elements copied by the level-0 compaction
+  unsigned long long refine_elems;
+  uint32_t asg_choice;        // index of the assigner in use (0 sampled, 1 learned)
+  uint32_t pad1[7];
+};
+
+// Capacities of the device-side lists; every append checks them and records
+// GGMS_E_INTERNAL instead of writing out of bounds.
+struct Caps {
+  uint32_t segs;
+  uint32_t tiles;
+  uint32_t points;
+};
+
+}  // namespace ggms

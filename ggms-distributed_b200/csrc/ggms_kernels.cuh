@@ -1,0 +1,891 @@
+// ggms_kernels.cuh -- device kernels of the exact multiselect engine.
+//
+// Pipeline for one vector (all on the device, no host round trip):
+//   k_init        ks (1-based k-th largest) -> 0-based ascending ranks
+//   asg_*         draw S sample keys, sort them, build the level-0 assigner
+//   l0_count      PASS 1 over the input: per-CTA shared histogram of buckets
+//   l0_scan       inclusive scan of the bucket counts
+//   l0_locate     each k finds its bucket and its rank inside the bucket
+//   l0_children   active buckets -> key range (inverse of the assigner);
+//                 single-key buckets resolve their ks at once, the others
+//                 become refinement segments
+//   l0_relabel    ks follow their bucket
+//   l0_compact    PASS 2 over the input: copy the keys of refinement segments
+//   lvl_* (x L)   the same steps over candidates only, with radix bins of
+//                 11 key bits, until every k sits in a single-key bin
+//   write_out     answers (as the caller's type) in the caller's k order
+//
+// Reference steps these replace (DistributedSMOS/bucketMultiselect.cu):
+//   minmax (:543-547) -- not needed: the assigner has open tail buckets;
+//   k sort + peel (:625-656) -- not needed: ks are located independently;
+//   generatePivots (:421-515) -> asg_*;  assignSmartBucket (:135-210) -> l0_count;
+//   sumCounts (:219-226) -> l0_scan;  findKBuckets (:92-116, host) -> l0_locate;
+//   unique buckets + reindexCounts (:726-768, host + kernel) -> l0_children;
+//   copyElements (:254-313) -> l0_compact;  thrust::sort + copyValuesInChunk
+//   (:814-833) -> the refinement levels + write_out.
+// IterativeSMOS (DistributedSMOS/iterativeSMOS.cu:1348-1531) repeats
+// bucketing over the survivors with re-fitted pivots; here the survivors are
+// refined with exact radix bins of the known key range, which ends in a bounded
+// number of levels (3 for 32-bit keys, 6 for 64-bit) with every k exact.
+#pragma once
+#include "ggms_internal.cuh"
+#include "../../include/ggms.h"
+
+namespace ggms {
+
+constexpr unsigned FULL = 0xFFFFFFFFu;
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ void set_status(Counters* C, uint32_t code) {
+  atomicCAS(&C->status, 0u, code);
+}
+
+// streaming 16-byte load that does not allocate in L1 (each byte is read once per pass)
+__device__ __forceinline__ uint4 ld_stream16(const void* p) {
+  uint4 r;
+  asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+               : "l"(p));
+  return r;
+}
+
+// splitmix64 finaliser (Steele, Lea, Flood 2014) -- sample positions
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+template <typename K> __host__ __device__ constexpr K key_max() { return (K)~(K)0; }
+
+// ------------------------------------------------------------------ block scan (1024 threads)
+// Inclusive scan of `cnt` (multiple of 1024) uint32 values in global memory, in place.
+// Returns (to thread 0) the maximum element.
+template <int NT>
+__device__ void block_inclusive_scan_global(uint32_t* data, uint32_t cnt, uint32_t* smem_warp,
+                                            uint32_t* max_out) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t ipt = cnt / NT;
+  uint32_t* mine = data + (size_t)tid * ipt;
+  uint32_t sum = 0, mx = 0;
+  for (uint32_t i = 0; i < ipt; ++i) {
+    uint32_t v = mine[i];
+    mx = max(mx, v);
+    sum += v;
+  }
+  // warp inclusive scan of thread sums
+  uint32_t inc = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(FULL, inc, o);
+    if (lane >= o) inc += t;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(FULL, mx, o));
+  if (lane == 31) smem_warp[warp] = inc;
+  if (lane == 0) smem_warp[32 + warp] = mx;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = (lane < NT / 32) ? smem_warp[lane] : 0u;
+    uint32_t wm = (lane < NT / 32) ? smem_warp[32 + lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t t = __shfl_up_sync(FULL, w, o);
+      if (lane >= o) w += t;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wm = max(wm, __shfl_xor_sync(FULL, wm, o));
+    smem_warp[lane] = w;  // inclusive warp totals
+    if (lane == 0) smem_warp[64] = wm;
+  }
+  __syncthreads();
+  uint32_t run = inc - sum + (warp > 0 ? smem_warp[warp - 1] : 0u);
+  for (uint32_t i = 0; i < ipt; ++i) {
+    run += mine[i];
+    mine[i] = run;
+  }
+  if (tid == 0 && max_out) *max_out = smem_warp[64];
+  __syncthreads();
+}
+
+// ------------------------------------------------------------------ ks
+// 1-based k-th largest -> 0-based rank in ascending order (the reference's
+// wrappers compute length - k + 1, 1-based smallest: bucketMultiselect.cu:860-861).
+__global__ void k_init_single(const uint32_t* __restrict__ ks, uint32_t nk, uint64_t n,
+                              uint32_t* k_rank, uint32_t* k_seg, Counters* C) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nk) return;
+  uint32_t k = ks[i];
+  if (k < 1u || (uint64_t)k > n) {
+    set_status(C, GGMS_E_INVALID_ARG);
+    k_seg[i] = K_DONE;
+    k_rank[i] = 0;
+    return;
+  }
+  k_rank[i] = (uint32_t)(n - k);
+  k_seg[i] = 0;
+}
+
+// ------------------------------------------------------------------ sampling
+template <typename T>
+__global__ void asg_sample(const T* __restrict__ in, uint64_t n, uint32_t S, uint64_t seed,
+                           typename KeyOf<T>::K* out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S) return;
+  uint64_t h = mix64(seed ^ mix64((uint64_t)i + 0x632BE59BD9B4E019ull));
+  uint64_t pos = __umul64hi(h, n);  // uniform in [0, n)
+  out[i] = KeyOf<T>::to(in[pos]);
+}
+
+// Bitonic sort of one chunk of CH keys per CTA in shared memory.
+template <typename K, int CH, int NT>
+__global__ __launch_bounds__(NT) void asg_sort_chunks(const K* __restrict__ in, K* out, uint32_t S) {
+  __shared__ K s[CH];
+  const uint32_t base = blockIdx.x * CH;
+  const uint32_t cnt = min((uint32_t)CH, S - base);
+  for (uint32_t i = threadIdx.x; i < CH; i += NT) s[i] = i < cnt ? in[base + i] : key_max<K>();
+  __syncthreads();
+  for (uint32_t k = 2; k <= (uint32_t)CH; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = threadIdx.x; i < (uint32_t)CH; i += NT) {
+        uint32_t ixj = i ^ j;
+        if (ixj > i) {
+          K a = s[i], b = s[ixj];
+          bool up = (i & k) == 0;
+          if ((a > b) == up) {
+            s[i] = b;
+            s[ixj] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (uint32_t i = threadIdx.x; i < cnt; i += NT) out[base + i] = s[i];
+}
+
+// Stable merge of G sorted chunks by ranking: each key counts the keys before
+// it in every other chunk (ties go to the lower chunk).
+template <typename K>
+__global__ void asg_merge_rank(const K* __restrict__ chunks, K* sorted, uint32_t S, uint32_t CH) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S) return;
+  const uint32_t G = (S + CH - 1) / CH;
+  const uint32_t c = i / CH, p = i % CH;
+  const K key = chunks[i];
+  uint32_t rank = p;
+  for (uint32_t c2 = 0; c2 < G; ++c2) {
+    if (c2 == c) continue;
+    const K* a = chunks + (size_t)c2 * CH;
+    uint32_t len = min(CH, S - c2 * CH);
+    uint32_t lo = 0, hi = len;
+    if (c2 < c) {  // upper bound
+      while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (a[m] <= key) lo = m + 1; else hi = m; }
+    } else {       // lower bound
+      while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (a[m] < key) lo = m + 1; else hi = m; }
+    }
+    rank += lo;
+  }
+  sorted[rank] = key;
+}
+
+// ------------------------------------------------------------------ assigner build
+// Builds a PL assigner from knot candidates.  The knot keys are
+// sorted[q[j]] for j = 0..Mreq, their target CDF values cdf[j] in [0, 1]
+// (cdf[0] = 0, cdf[Mreq] = 1).  Equal knots (an atom of the sample) are merged;
+// an atom v gets a bucket of its own by an extra knot at v+1.  Bases are made
+// strictly increasing so that distinct knots never share a bucket.
+template <typename K>
+__device__ void asg_build_from_knots(const K* sorted, const uint32_t* q, const float* cdf,
+                                     uint32_t Mreq, uint32_t B, uint32_t kind, Assigner<K>* A) {
+  __shared__ K X[ASG_MAXM + 2];
+  __shared__ uint32_t Bs[ASG_MAXM + 2];
+  __shared__ uint32_t Ms;
+  if (threadIdx.x == 0) {
+    const float span = (float)(B - 2u);
+    uint32_t m = 0;
+    uint32_t prev_b = 1;
+    // dedupe; remember the base at the end of each run of equal knots
+    uint32_t atom_end_b = 0;
+    bool atom = false;
+    for (uint32_t j = 0; j <= Mreq; ++j) {
+      K xk = sorted[q[j]];
+      float f = fminf(fmaxf(cdf[j], 0.0f), 1.0f);
+      uint32_t b = 1u + (uint32_t)__float2uint_rn(f * span);
+      if (j == 0) b = 1u;
+      if (j == Mreq) b = B - 1u;
+      b = max(b, prev_b);
+      prev_b = b;
+      if (m > 0 && xk == X[m - 1]) {
+        atom = true;
+        atom_end_b = b;
+        continue;
+      }
+      if (atom && m > 0) {
+        // close the atom at X[m-1]: keys above it start at the run's end base
+        K v = X[m - 1];
+        if (v + 1 < xk && m < ASG_MAXM + 1) {
+          X[m] = v + 1;
+          Bs[m] = max(Bs[m - 1] + 1u, atom_end_b);
+          ++m;
+        }
+        atom = false;
+      }
+      X[m] = xk;
+      Bs[m] = b;
+      ++m;
+    }
+    // strictly increasing bases, capped at B-1 from the top
+    Bs[0] = 1u;
+    for (uint32_t t = 1; t < m; ++t) Bs[t] = max(Bs[t], Bs[t - 1] + 1u);
+    Bs[m - 1] = max(Bs[m - 1], B - 1u);
+    for (int t = (int)m - 1; t >= 0; --t) {
+      uint32_t cap = (B - 1u) - (uint32_t)((int)m - 1 - t);
+      Bs[t] = min(Bs[t], cap);
+    }
+    if (m == 1) Bs[0] = 1u;
+    Ms = m - 1;
+    A->M = m - 1;
+    A->B = B;
+    A->kind = kind;
+    A->loss = 0.0f;
+    const K span_k = X[m - 1] - X[0];
+    const int sh = max(0, bitlen(span_k) - ASG_CELL_BITS);
+    A->csh = (uint32_t)sh;
+    A->ncell = (uint32_t)(span_k >> sh) + 1u;
+  }
+  __syncthreads();
+  const uint32_t M = Ms;
+  for (uint32_t t = threadIdx.x; t <= M; t += blockDim.x) {
+    A->x[t] = X[t];
+    A->base[t] = Bs[t];
+    if (t < M) {
+      float db = (float)(Bs[t + 1] - Bs[t]);
+      float dx = key_to_float_rn((K)(X[t + 1] - X[t]));
+      A->slope[t] = __fdiv_rn(db, dx);
+    }
+  }
+  __syncthreads();
+  // cell index: idx[c] = last segment j <= M-1 whose knot is <= the cell's first key
+  const uint32_t csh = A->csh, ncell = A->ncell;
+  for (uint32_t c = threadIdx.x; c < (uint32_t)ASG_NCELL; c += blockDim.x) {
+    uint32_t j = 0;
+    if (c < ncell && M > 0) {
+      K start = X[0] + ((K)c << csh);
+      uint32_t lo = 0, hi = M - 1;  // largest j in [0, M-1] with X[j] <= start
+      while (lo < hi) {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (X[mid] <= start) lo = mid; else hi = mid - 1;
+      }
+      j = lo;
+    }
+    A->idx[c] = (uint16_t)j;
+  }
+}
+
+template <typename K>
+__device__ __forceinline__ AsgView<K> asg_view_global(const Assigner<K>* A) {
+  AsgView<K> v;
+  v.x = A->x; v.base = A->base; v.slope = A->slope; v.idx = A->idx;
+  v.M = A->M; v.B = A->B; v.csh = A->csh;
+  return v;
+}
+
+// Occupancy of the assigner's buckets on its own (sorted) sample, over 256
+// groups of buckets: max / mean.
+template <typename K>
+__device__ void asg_measure(const K* sorted, uint32_t S, Assigner<K>* A) {
+  __shared__ uint32_t g[256];
+  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) g[i] = 0;
+  __syncthreads();
+  AsgView<K> v = asg_view_global(A);
+  const uint32_t B = A->B;
+  for (uint32_t i = threadIdx.x; i < S; i += blockDim.x) {
+    uint32_t b = asg_eval(v, sorted[i]);
+    atomicAdd(&g[(uint32_t)(((uint64_t)b * 256u) / B)], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t mx = 0;
+    for (int i = 0; i < 256; ++i) mx = max(mx, g[i]);
+    A->quality = (float)mx / ((float)S / 256.0f);
+  }
+}
+
+// The reference's pivot rule (bucketMultiselect.cu:421-515, sizeOfSample = 1024,
+// numPivots = 17, endOffset = 22, pivotOffset = (1024 - 44) / 14 = 70):
+// pivots {min, s[21], s[21 + 70(i-1)] for i = 2..14, s[1001], max}, every
+// segment gets the same number of buckets.  The global min and max (a full
+// minmax pass in the reference) are replaced by the sample's extremes plus an
+// open tail bucket at each end.  For other sample sizes the offsets scale.
+template <typename K>
+__global__ void asg_build_sampled(const K* __restrict__ sorted, uint32_t S, uint32_t B,
+                                  Assigner<K>* A) {
+  __shared__ uint32_t q[17];
+  __shared__ float cdf[17];
+  if (threadIdx.x == 0) {
+    const uint32_t end_off = max(1u, (22u * S) / 1024u);
+    const uint32_t piv_off = (S - 2u * end_off) / 14u;
+    q[0] = 0;
+    q[1] = end_off - 1u;
+    for (uint32_t i = 2; i <= 14; ++i) q[i] = piv_off * (i - 1u) + end_off - 1u;
+    q[15] = S - end_off - 1u;
+    q[16] = S - 1u;
+    for (int i = 0; i <= 16; ++i) cdf[i] = (float)i / 16.0f;
+  }
+  __syncthreads();
+  asg_build_from_knots<K>(sorted, q, cdf, 16u, B, GGMS_ASSIGNER_SAMPLED, A);
+  __syncthreads();
+  asg_measure<K>(sorted, S, A);
+}
+
+// ------------------------------------------------------------------ level 0 (one vector)
+template <typename K>
+struct AsgSmem {
+  static constexpr size_t bytes =
+      sizeof(K) * (ASG_MAXM + 1) + 4 * (ASG_MAXM + 1) + 4 * ASG_MAXM + 2 * ASG_NCELL;
+};
+
+template <typename K>
+__device__ __forceinline__ AsgView<K> asg_to_smem(const Assigner<K>* __restrict__ A, uint8_t* sm) {
+  K* sx = (K*)sm;
+  uint32_t* sb = (uint32_t*)(sx + ASG_MAXM + 1);
+  float* ss = (float*)(sb + ASG_MAXM + 1);
+  uint16_t* si = (uint16_t*)(ss + ASG_MAXM);
+  const uint32_t M = A->M, nc = A->ncell;
+  for (uint32_t i = threadIdx.x; i <= M; i += blockDim.x) {
+    sx[i] = A->x[i];
+    sb[i] = A->base[i];
+    if (i < M) ss[i] = A->slope[i];
+  }
+  for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) si[i] = A->idx[i];
+  AsgView<K> v;
+  v.x = sx; v.base = sb; v.slope = ss; v.idx = si;
+  v.M = M; v.B = A->B; v.csh = A->csh;
+  return v;
+}
+
+// 16-byte vector view of the input
+template <typename T> struct Vec16 {
+  static constexpr int N = 16 / sizeof(T);
+};
+
+template <typename T>
+__device__ __forceinline__ void unpack16(const uint4& q, T (&e)[Vec16<T>::N]) {
+  static_assert(sizeof(T) * Vec16<T>::N == 16, "");
+  __builtin_memcpy(e, &q, 16);
+}
+
+// PASS 1.  Persistent CTAs; each keeps a shared histogram of the B buckets and
+// flushes its non-zero bins once.  A warp whose 32 x (16-byte vector) all land
+// in one bucket (sorted or clustered data) adds once.
+template <typename T, int NT, int UNROLL>
+__global__ __launch_bounds__(NT) void l0_count(const T* __restrict__ in, uint64_t n,
+                                              const Assigner<typename KeyOf<T>::K>* __restrict__ As,
+                                              const Counters* __restrict__ C,
+                                              uint32_t* __restrict__ hist0) {
+  using K = typename KeyOf<T>::K;
+  constexpr int EPV = Vec16<T>::N;
+  extern __shared__ __align__(16) uint8_t smem[];
+  const Assigner<K>* A = As + C->asg_choice;
+  const uint32_t B = A->B;
+  uint32_t* h = (uint32_t*)smem;
+  AsgView<K> av = asg_to_smem<K>(A, smem + (size_t)B * 4u);
+  for (uint32_t i = threadIdx.x; i < B; i += NT) h[i] = 0u;
+  __syncthreads();
+
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t gtid = (uint64_t)blockIdx.x * NT + threadIdx.x;
+  const uint64_t gstride = (uint64_t)gridDim.x * NT;
+  const uintptr_t addr = (uintptr_t)in;
+  uint64_t head = ((16u - (uint32_t)(addr & 15u)) & 15u) / sizeof(T);
+  if (head > n) head = n;
+  const uint64_t nvec = (n - head) / EPV;
+  const T* vbase = in + head;
+
+  for (uint64_t i0 = gtid; i0 < ((nvec + gstride - 1) / gstride) * gstride; i0 += gstride * UNROLL) {
+    uint4 q[UNROLL];
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) {
+      uint64_t i = i0 + (uint64_t)u * gstride;
+      if (i < nvec) q[u] = ld_stream16(vbase + i * EPV);
+    }
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) {
+      uint64_t i = i0 + (uint64_t)u * gstride;
+      const bool valid = i < nvec;
+      uint32_t b[EPV];
+      bool same = true;
+      if (valid) {
+        T e[EPV];
+        unpack16<T>(q[u], e);
+#pragma unroll
+        for (int t = 0; t < EPV; ++t) {
+          b[t] = asg_eval<K>(av, KeyOf<T>::to(e[t]));
+          same = same && (b[t] == b[0]);
+        }
+      } else {
+        b[0] = 0u;
+      }
+      const uint32_t vmask = __ballot_sync(FULL, valid);
+      if (vmask == 0u) continue;
+      const uint32_t b0 = __shfl_sync(FULL, b[0], __ffs(vmask) - 1);
+      const bool uni = __all_sync(FULL, !valid || (same && b[0] == b0));
+      if (uni) {
+        if (lane == (uint32_t)(__ffs(vmask) - 1)) atomicAdd(&h[b0], (uint32_t)(EPV * __popc(vmask)));
+      } else if (valid) {
+        if (same) {
+          atomicAdd(&h[b[0]], (uint32_t)EPV);
+        } else {
+#pragma unroll
+          for (int t = 0; t < EPV; ++t) atomicAdd(&h[b[t]], 1u);
+        }
+      }
+    }
+  }
+  // unaligned head and the tail that does not fill a vector
+  {
+    const uint64_t tail0 = head + nvec * EPV;
+    const uint64_t nscalar = head + (n - tail0);
+    for (uint64_t j = gtid; j < nscalar; j += gstride) {
+      uint64_t idx = j < head ? j : tail0 + (j - head);
+      atomicAdd(&h[asg_eval<K>(av, KeyOf<T>::to(in[idx]))], 1u);
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < B; i += NT) {
+    uint32_t v = h[i];
+    if (v) atomicAdd(&hist0[i], v);
+  }
+}
+
+// Inclusive scan of the level-0 counts (one CTA) + the largest bucket.
+__global__ __launch_bounds__(1024) void l0_scan(uint32_t* hist0, uint32_t B, Counters* C) {
+  __shared__ uint32_t w[72];
+  block_inclusive_scan_global<1024>(hist0, B, w, &C->max_bucket0);
+}
+
+// Each k finds the bucket holding its rank: the smallest b with I[b] > r.
+__global__ void lvl_locate_rows(const uint32_t* __restrict__ rows, uint32_t row_len, uint32_t nk,
+                                uint32_t* k_rank, const uint32_t* __restrict__ k_seg,
+                                uint32_t* k_bin, uint32_t* aflag, uint32_t flag_words,
+                                Counters* C) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nk) return;
+  const uint32_t s = k_seg[i];
+  if (s == K_DONE) return;
+  const uint32_t* I = rows + (size_t)s * row_len;
+  const uint32_t r = k_rank[i];
+  if (r >= I[row_len - 1]) {  // cannot happen: rank beyond the segment
+    set_status(C, GGMS_E_INTERNAL);
+    return;
+  }
+  uint32_t lo = 0, hi = row_len - 1;
+  while (lo < hi) {
+    uint32_t m = (lo + hi) >> 1;
+    if (I[m] > r) hi = m; else lo = m + 1;
+  }
+  k_bin[i] = lo;
+  k_rank[i] = r - (lo ? I[lo - 1] : 0u);
+  atomicOr(&aflag[(size_t)s * flag_words + (lo >> 5)], 1u << (lo & 31));
+}
+
+// Active level-0 buckets -> refinement segments (or points).  One thread per bucket.
+template <typename K>
+__global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __restrict__ aflag,
+                            uint32_t B, const Assigner<K>* __restrict__ As, Counters* C,
+                            uint32_t* cmap0, Seg<K>* segs1, uint32_t* cursor1, TileRef* tiles1,
+                            K* points, Caps caps) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  if (!((aflag[b >> 5] >> (b & 31)) & 1u)) {
+    cmap0[b] = CM_NONE;
+    return;
+  }
+  const Assigner<K>* A = As + C->asg_choice;
+  const AsgView<K> av = asg_view_global(A);
+  const uint32_t start = b ? I[b - 1] : 0u;
+  const uint32_t cnt = I[b] - start;
+  // key range of bucket b: [L(b), L(b+1) - 1], L(x) = smallest key with eval >= x
+  auto L = [&](uint32_t target) -> K {
+    K lo = 0, hi = key_max<K>();
+    while (lo < hi) {
+      K mid = lo + ((hi - lo) >> 1);
+      if (asg_eval<K>(av, mid) >= target) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+  };
+  const K lo = (b == 0) ? (K)0 : L(b);
+  const K hi = (b == B - 1) ? key_max<K>() : (K)(L(b + 1) - 1);
+  atomicAdd(&C->active0, 1u);
+  if (lo == hi) {
+    uint32_t pid = atomicAdd(&C->npoints, 1u);
+    if (pid >= caps.points) { set_status(C, GGMS_E_INTERNAL); cmap0[b] = CM_NONE; return; }
+    points[pid] = lo;
+    cmap0[b] = CM_POINT | pid;
+    atomicAdd(&C->point0, 1u);
+    return;
+  }
+  const uint32_t id = atomicAdd(&C->nsegs[1], 1u);
+  if (id >= caps.segs) { set_status(C, GGMS_E_INTERNAL); cmap0[b] = CM_NONE; return; }
+  Seg<K> s;
+  s.off = start;
+  s.cnt = cnt;
+  s.lo = lo;
+  s.hi = hi;
+  s.shift = (uint32_t)max(0, bitlen((K)(hi - lo)) - RADIX_BITS);
+  segs1[id] = s;
+  cursor1[id] = 0u;
+  const uint32_t nt = (cnt + TILE - 1) / TILE;
+  const uint32_t t0 = atomicAdd(&C->ntiles[1], nt);
+  if (t0 + nt > caps.tiles || t0 + nt < t0) { set_status(C, GGMS_E_INTERNAL); cmap0[b] = CM_NONE; return; }
+  for (uint32_t t = 0; t < nt; ++t) tiles1[t0 + t] = TileRef{id, t};
+  cmap0[b] = id;
+  atomicAdd(&C->cand0, (unsigned long long)cnt);
+}
+
+// ks follow their bin: resolved (single key) or the id of the next segment.
+template <typename K>
+__global__ void lvl_relabel(const uint32_t* __restrict__ cmap, uint32_t row_len, uint32_t nk,
+                            const uint32_t* __restrict__ k_bin, uint32_t* k_seg, K* k_key,
+                            const K* __restrict__ points, Counters* C) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nk) return;
+  const uint32_t s = k_seg[i];
+  if (s == K_DONE) return;
+  const uint32_t e = cmap[(size_t)s * row_len + k_bin[i]];
+  if (e == CM_NONE) {
+    set_status(C, GGMS_E_INTERNAL);
+    k_seg[i] = K_DONE;
+    return;
+  }
+  if (e & CM_POINT) {
+    k_key[i] = points[e & ~CM_POINT];
+    k_seg[i] = K_DONE;
+  } else {
+    k_seg[i] = e;
+  }
+}
+
+// PASS 2.  Copies the keys of refinement buckets into their segment's region
+// of the candidate buffer.  Slots are reserved per warp and per target segment.
+template <typename T, int NT, int UNROLL>
+__global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint64_t n,
+                                                const Assigner<typename KeyOf<T>::K>* __restrict__ As,
+                                                const Counters* __restrict__ C,
+                                                const uint32_t* __restrict__ cmap0,
+                                                const Seg<typename KeyOf<T>::K>* __restrict__ segs1,
+                                                uint32_t* cursor1, typename KeyOf<T>::K* dst) {
+  using K = typename KeyOf<T>::K;
+  constexpr int EPV = Vec16<T>::N;
+  extern __shared__ __align__(16) uint8_t smem[];
+  const Assigner<K>* A = As + C->asg_choice;
+  const uint32_t B = A->B;
+  uint32_t* cm = (uint32_t*)smem;
+  AsgView<K> av = asg_to_smem<K>(A, smem + (size_t)B * 4u);
+  for (uint32_t i = threadIdx.x; i < B; i += NT) cm[i] = cmap0[i];
+  __syncthreads();
+
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t gtid = (uint64_t)blockIdx.x * NT + threadIdx.x;
+  const uint64_t gstride = (uint64_t)gridDim.x * NT;
+  const uintptr_t addr = (uintptr_t)in;
+  uint64_t head = ((16u - (uint32_t)(addr & 15u)) & 15u) / sizeof(T);
+  if (head > n) head = n;
+  const uint64_t nvec = (n - head) / EPV;
+  const T* vbase = in + head;
+
+  auto emit = [&](bool hit, uint32_t e, K key) {
+    const uint32_t hm = __ballot_sync(FULL, hit);
+    if (hm == 0u) return;
+    if (hit) {
+      const uint32_t peers = __match_any_sync(hm, e);
+      const int leader = __ffs(peers) - 1;
+      uint32_t basepos = 0;
+      if ((int)lane == leader) basepos = atomicAdd(&cursor1[e], (uint32_t)__popc(peers));
+      basepos = __shfl_sync(peers, basepos, leader);
+      const uint32_t slot = basepos + __popc(peers & lanemask_lt());
+      const Seg<K>& sg = segs1[e];
+      if (slot < sg.cnt) dst[sg.off + slot] = key;
+      else set_status(const_cast<Counters*>(C), GGMS_E_INTERNAL);
+    }
+  };
+
+  for (uint64_t i0 = gtid; i0 < ((nvec + gstride - 1) / gstride) * gstride; i0 += gstride * UNROLL) {
+    uint4 q[UNROLL];
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) {
+      uint64_t i = i0 + (uint64_t)u * gstride;
+      if (i < nvec) q[u] = ld_stream16(vbase + i * EPV);
+    }
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) {
+      uint64_t i = i0 + (uint64_t)u * gstride;
+      const bool valid = i < nvec;
+      T e[EPV];
+      if (valid) unpack16<T>(q[u], e);
+#pragma unroll
+      for (int t = 0; t < EPV; ++t) {
+        K key = valid ? KeyOf<T>::to(e[t]) : (K)0;
+        uint32_t c = valid ? cm[asg_eval<K>(av, key)] : CM_NONE;
+        emit(valid && c < CM_POINT, c, key);
+      }
+    }
+  }
+  {
+    const uint64_t tail0 = head + nvec * EPV;
+    const uint64_t nscalar = head + (n - tail0);
+    const uint64_t rounds = (nscalar + gstride - 1) / gstride;
+    for (uint64_t r = 0; r < rounds; ++r) {
+      uint64_t j = gtid + r * gstride;
+      bool valid = j < nscalar;
+      K key = 0;
+      uint32_t c = CM_NONE;
+      if (valid) {
+        uint64_t idx = j < head ? j : tail0 + (j - head);
+        key = KeyOf<T>::to(in[idx]);
+        c = cm[asg_eval<K>(av, key)];
+      }
+      emit(valid && c < CM_POINT, c, key);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ refinement levels
+// Level l works on the segments of pool p = l & 1 and creates children in pool
+// q = p ^ 1.  Keys are read from `src` and children are written to `dst`.
+
+// zero this level's histogram rows / flags; reset the child pool's counters
+__global__ void lvl_prep(uint32_t* rows, uint32_t* aflag, Counters* C, int p, Caps caps) {
+  const uint32_t ns = min(C->nsegs[p], caps.segs);
+  const size_t words = (size_t)ns * NBIN;
+  const size_t fw = (size_t)ns * NBIN_WORDS;
+  const size_t gt = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t gs = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = gt; i < words; i += gs) rows[i] = 0u;
+  for (size_t i = gt; i < fw; i += gs) aflag[i] = 0u;
+  if (gt == 0) {
+    C->nsegs[p ^ 1] = 0u;
+    C->ntiles[p ^ 1] = 0u;
+    if (ns) C->levels_run += 1u;
+  }
+}
+
+// Histogram of radix bins, one tile of one segment per iteration.
+template <typename InT, int NT>
+__global__ __launch_bounds__(NT) void lvl_count(const InT* __restrict__ src,
+                                               const Seg<typename KeyOf<InT>::K>* __restrict__ segs,
+                                               const TileRef* __restrict__ tiles,
+                                               Counters* C, int p, uint32_t* rows, Caps caps) {
+  using K = typename KeyOf<InT>::K;
+  __shared__ uint32_t h[NBIN];
+  const uint32_t nt = min(C->ntiles[p], caps.tiles);
+  const uint32_t ns = min(C->nsegs[p], caps.segs);
+  for (uint32_t t = blockIdx.x; t < nt; t += gridDim.x) {
+    const TileRef tr = tiles[t];
+    if (tr.seg >= ns) continue;  // only after a capacity error (status already set)
+    const Seg<K> s = segs[tr.seg];
+    for (uint32_t i = threadIdx.x; i < NBIN; i += NT) h[i] = 0u;
+    __syncthreads();
+    const uint64_t beg = s.off + (uint64_t)tr.no * TILE;
+    const uint64_t end = min(beg + TILE, s.off + s.cnt);
+    for (uint64_t i = beg + threadIdx.x; i < end; i += NT) {
+      K key = KeyOf<InT>::to(src[i]);
+      uint32_t bin = (uint32_t)((K)(key - s.lo) >> s.shift);
+      atomicAdd(&h[min(bin, (uint32_t)NBIN - 1u)], 1u);
+    }
+    __syncthreads();
+    uint32_t* row = rows + (size_t)tr.seg * NBIN;
+    for (uint32_t i = threadIdx.x; i < NBIN; i += NT) {
+      uint32_t v = h[i];
+      if (v) atomicAdd(&row[i], v);
+    }
+    if (threadIdx.x == 0) atomicAdd(&C->refine_elems, (unsigned long long)(end - beg));
+    __syncthreads();
+  }
+}
+
+__global__ __launch_bounds__(1024) void lvl_scan(uint32_t* rows, const Counters* __restrict__ C, int p,
+                                                  Caps caps) {
+  __shared__ uint32_t w[72];
+  const uint32_t ns = min(C->nsegs[p], caps.segs);
+  for (uint32_t s = blockIdx.x; s < ns; s += gridDim.x)
+    block_inclusive_scan_global<1024>(rows + (size_t)s * NBIN, NBIN, w, nullptr);
+}
+
+// Active bins of each segment -> child segments (pool q) or points.  One CTA
+// per segment; the row holding the inclusive counts is overwritten by the
+// child map (each entry read before any is written).
+template <typename K, int NT>
+__global__ __launch_bounds__(NT) void lvl_children(uint32_t* rows, const uint32_t* __restrict__ aflag,
+                                                  const Seg<K>* __restrict__ segs, Counters* C, int p,
+                                                  Seg<K>* segs_q, uint32_t* cursor_q, TileRef* tiles_q,
+                                                  K* points, Caps caps) {
+  constexpr int PER = NBIN / NT;
+  const uint32_t ns = min(C->nsegs[p], caps.segs);
+  for (uint32_t sid = blockIdx.x; sid < ns; sid += gridDim.x) {
+    const Seg<K> s = segs[sid];
+    uint32_t* I = rows + (size_t)sid * NBIN;
+    const uint32_t* F = aflag + (size_t)sid * NBIN_WORDS;
+    uint32_t out[PER];
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const uint32_t b = threadIdx.x + u * NT;
+      out[u] = CM_NONE;
+      if (!((F[b >> 5] >> (b & 31)) & 1u)) continue;
+      const uint32_t start = b ? I[b - 1] : 0u;
+      const uint32_t cnt = I[b] - start;
+      const K blo = s.lo + ((K)b << s.shift);
+      const K width_m1 = (K)(((K)1 << s.shift) - 1);
+      K bhi = (key_max<K>() - blo < width_m1) ? key_max<K>() : (K)(blo + width_m1);
+      if (bhi > s.hi) bhi = s.hi;
+      if (blo == bhi) {
+        uint32_t pid = atomicAdd(&C->npoints, 1u);
+        if (pid >= caps.points) { set_status(C, GGMS_E_INTERNAL); continue; }
+        points[pid] = blo;
+        out[u] = CM_POINT | pid;
+        continue;
+      }
+      const uint32_t id = atomicAdd(&C->nsegs[p ^ 1], 1u);
+      if (id >= caps.segs) { set_status(C, GGMS_E_INTERNAL); continue; }
+      Seg<K> c;
+      c.off = s.off + start;
+      c.cnt = cnt;
+      c.lo = blo;
+      c.hi = bhi;
+      c.shift = (uint32_t)max(0, bitlen((K)(bhi - blo)) - RADIX_BITS);
+      segs_q[id] = c;
+      cursor_q[id] = 0u;
+      const uint32_t nt = (cnt + TILE - 1) / TILE;
+      const uint32_t t0 = atomicAdd(&C->ntiles[p ^ 1], nt);
+      if (t0 + nt > caps.tiles || t0 + nt < t0) { set_status(C, GGMS_E_INTERNAL); continue; }
+      for (uint32_t t = 0; t < nt; ++t) tiles_q[t0 + t] = TileRef{id, t};
+      out[u] = id;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < PER; ++u) I[threadIdx.x + u * NT] = out[u];
+    __syncthreads();
+  }
+}
+
+// Copies each key whose bin became a child segment into that child's region.
+template <typename InT, int NT>
+__global__ __launch_bounds__(NT) void lvl_compact(const InT* __restrict__ src,
+                                                 const Seg<typename KeyOf<InT>::K>* __restrict__ segs,
+                                                 const TileRef* __restrict__ tiles,
+                                                 const Counters* __restrict__ C, int p,
+                                                 const uint32_t* __restrict__ rows,
+                                                 const Seg<typename KeyOf<InT>::K>* __restrict__ segs_q,
+                                                 uint32_t* cursor_q, typename KeyOf<InT>::K* dst,
+                                                 Caps caps) {
+  using K = typename KeyOf<InT>::K;
+  __shared__ uint32_t cm[NBIN];
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t nt = min(C->ntiles[p], caps.tiles);
+  const uint32_t ns = min(C->nsegs[p], caps.segs);
+  for (uint32_t t = blockIdx.x; t < nt; t += gridDim.x) {
+    const TileRef tr = tiles[t];
+    if (tr.seg >= ns) continue;  // only after a capacity error (status already set)
+    const Seg<K> s = segs[tr.seg];
+    const uint32_t* row = rows + (size_t)tr.seg * NBIN;
+    for (uint32_t i = threadIdx.x; i < NBIN; i += NT) cm[i] = row[i];
+    __syncthreads();
+    const uint64_t beg = s.off + (uint64_t)tr.no * TILE;
+    const uint64_t end = min(beg + TILE, s.off + s.cnt);
+    const uint64_t span = ((end - beg + NT - 1) / NT) * NT;
+    for (uint64_t o = threadIdx.x; o < span; o += NT) {
+      const uint64_t i = beg + o;
+      const bool valid = i < end;
+      K key = 0;
+      uint32_t c = CM_NONE;
+      if (valid) {
+        key = KeyOf<InT>::to(src[i]);
+        uint32_t bin = (uint32_t)((K)(key - s.lo) >> s.shift);
+        c = cm[min(bin, (uint32_t)NBIN - 1u)];
+      }
+      const bool hit = valid && c < CM_POINT;
+      const uint32_t hm = __ballot_sync(FULL, hit);
+      if (hm && hit) {
+        const uint32_t peers = __match_any_sync(hm, c);
+        const int leader = __ffs(peers) - 1;
+        uint32_t basepos = 0;
+        if ((int)lane == leader) basepos = atomicAdd(&cursor_q[c], (uint32_t)__popc(peers));
+        basepos = __shfl_sync(peers, basepos, leader);
+        const uint32_t slot = basepos + __popc(peers & lanemask_lt());
+        const Seg<K>& sg = segs_q[c];
+        if (slot < sg.cnt) dst[sg.off + slot] = key;
+        else set_status(const_cast<Counters*>(C), GGMS_E_INTERNAL);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+
+// ------------------------------------------------------------------ batched segments
+// Level 0 of the batched mode: every caller segment that holds a k becomes a
+// radix segment over the whole key space (top 11 key bits first).
+template <typename K>
+__global__ void seg_init(const int64_t* __restrict__ seg_off, uint32_t nseg,
+                         const int64_t* __restrict__ k_off, Seg<K>* segs0, TileRef* tiles0,
+                         Counters* C) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseg) return;
+  const int64_t a = seg_off[s], b = seg_off[s + 1];
+  Seg<K> d;
+  d.off = (uint64_t)a;
+  d.cnt = (b > a) ? (uint32_t)(b - a) : 0u;
+  d.lo = 0;
+  d.hi = key_max<K>();
+  d.shift = (uint32_t)(KeyBits<K>::value - RADIX_BITS);
+  segs0[s] = d;
+  if (b < a) set_status(C, GGMS_E_INVALID_ARG);
+  if (k_off[s + 1] == k_off[s] || d.cnt == 0) return;  // nothing to select here
+  const uint32_t nt = (d.cnt + TILE - 1) / TILE;
+  const uint32_t t0 = atomicAdd(&C->ntiles[0], nt);
+  for (uint32_t t = 0; t < nt; ++t) tiles0[t0 + t] = TileRef{s, t};
+}
+
+__global__ void seg_set_count(Counters* C, uint32_t nseg) { C->nsegs[0] = nseg; }
+
+// k i belongs to the segment s with k_off[s] <= i < k_off[s+1].
+__global__ void k_init_seg(const uint32_t* __restrict__ ks, uint32_t nk,
+                           const int64_t* __restrict__ seg_off, const int64_t* __restrict__ k_off,
+                           uint32_t nseg, uint32_t* k_rank, uint32_t* k_seg, Counters* C) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nk) return;
+  uint32_t lo = 0, hi = nseg - 1;  // largest s with k_off[s] <= i
+  while (lo < hi) {
+    uint32_t m = (lo + hi + 1) >> 1;
+    if (k_off[m] <= (int64_t)i) lo = m; else hi = m - 1;
+  }
+  const uint64_t len = (uint64_t)(seg_off[lo + 1] - seg_off[lo]);
+  const uint32_t k = ks[i];
+  if (k < 1u || (uint64_t)k > len) {
+    set_status(C, GGMS_E_INVALID_ARG);
+    k_seg[i] = K_DONE;
+    k_rank[i] = 0;
+    return;
+  }
+  k_rank[i] = (uint32_t)(len - k);
+  k_seg[i] = lo;
+}
+
+// ------------------------------------------------------------------ outputs
+template <typename T>
+__global__ void write_out(const typename KeyOf<T>::K* __restrict__ k_key,
+                          const uint32_t* __restrict__ k_seg, uint32_t nk, T* out, Counters* C) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nk) return;
+  if (k_seg[i] != K_DONE) set_status(C, GGMS_E_NOT_CONVERGED);
+  out[i] = KeyOf<T>::from(k_key[i]);
+}
+
+}  // namespace ggms

@@ -1,0 +1,43 @@
+"""The C-ABI library loads and exports every symbol its headers declare
+(no compute call: this runs without a GPU)."""
+import ctypes
+import os
+import subprocess
+
+import pytest
+
+import ggms_b200
+
+
+def test_library_built():
+    assert os.path.exists(ggms_b200.LIB_PATH), "run make -C ggms-distributed_b200"
+
+
+def test_every_declared_symbol_exported():
+    lib = ggms_b200.load()
+    names = ggms_b200.declared_symbols()
+    assert len(names) >= 19
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_no_undeclared_exports():
+    out = subprocess.run(["nm", "-D", "--defined-only", ggms_b200.LIB_PATH],
+                         capture_output=True, text=True, check=True).stdout
+    exported = {l.split()[-1] for l in out.splitlines() if " T " in l and "ggms_" in l}
+    assert exported <= set(ggms_b200.declared_symbols()), exported - set(ggms_b200.declared_symbols())
+
+
+def test_status_strings_and_version():
+    lib = ggms_b200.load()
+    assert lib.ggms_version() >= 100
+    assert ggms_b200.status_string(0) == "ok"
+    assert ggms_b200.status_string(1) == "invalid argument"
+
+
+def test_default_opts_layout():
+    o = ggms_b200.default_opts()
+    assert o.struct_size == ctypes.sizeof(ggms_b200.Opts)
+    assert o.assigner == ggms_b200.ASSIGNER_AUTO
+
+
