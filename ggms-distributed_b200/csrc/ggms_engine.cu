@@ -14,6 +14,7 @@
 
 #include "ggms_kernels.cuh"
 #include "ggms_learned.cuh"
+#include "../../include/ggms_diag.h"
 
 namespace ggms {
 
@@ -619,6 +620,104 @@ static int segmented(ggms_context* cx, const T* d_in, const int64_t* seg_off, in
   return run_segmented<T>(c, d_in, seg_off, nseg, ks, k_off, out, o, (cudaStream_t)stream);
 }
 
+
+// ------------------------------------------------------------------ diagnostics
+namespace diag {
+
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() { if (p) cudaFree(p); }
+};
+
+static int pl_gradient(const uint32_t* keys, int S, const float* theta, float* loss, float* grad,
+                       uint32_t* knots, int* Mout) {
+  if (!keys || S < 2 || !theta || !loss || !grad) return GGMS_E_INVALID_ARG;
+  DevBuf dk, da, dl, dt, dout;
+  GGMS_CU(cudaMalloc(&dk.p, 4ull * S));
+  GGMS_CU(cudaMalloc(&da.p, sizeof(Assigner<uint32_t>)));
+  GGMS_CU(cudaMalloc(&dl.p, sizeof(LearnState)));
+  GGMS_CU(cudaMalloc(&dt.p, 4ull * PL_M));
+  GGMS_CU(cudaMalloc(&dout.p, 4ull * (PL_M + 1)));
+  GGMS_CU(cudaMemcpy(dk.p, keys, 4ull * S, cudaMemcpyHostToDevice));
+  GGMS_CU(cudaMemcpy(dt.p, theta, 4ull * PL_M, cudaMemcpyHostToDevice));
+  auto* A = (Assigner<uint32_t>*)da.p;
+  auto* L = (LearnState*)dl.p;
+  pl_init_knots<uint32_t><<<1, 256>>>((const uint32_t*)dk.p, (uint32_t)S, 1u << 14, A);
+  Assigner<uint32_t> h;
+  GGMS_CU(cudaMemcpy(&h, A, sizeof(h), cudaMemcpyDeviceToHost));
+  pl_stats<uint32_t><<<(PL_M * 32 + 255) / 256, 256>>>((const uint32_t*)dk.p, (uint32_t)S, A, L);
+  float* dloss = (float*)dout.p;
+  float* dgrad = dloss + 1;
+  pl_grad_probe<<<1, 32>>>(L, (const float*)dt.p, h.M, (uint32_t)S, dloss, dgrad);
+  GGMS_CU(cudaDeviceSynchronize());
+  GGMS_CU(cudaMemcpy(loss, dloss, 4, cudaMemcpyDeviceToHost));
+  GGMS_CU(cudaMemcpy(grad, dgrad, 4ull * h.M, cudaMemcpyDeviceToHost));
+  if (knots) memcpy(knots, h.x, 4ull * (h.M + 1));
+  if (Mout) *Mout = (int)h.M;
+  return GGMS_OK;
+}
+
+static int mlp_gradient(const float* x, const float* t, const float* params, float* loss, float* grad) {
+  if (!x || !t || !params || !loss || !grad) return GGMS_E_INVALID_ARG;
+  DevBuf dx, dt, dp, dprobe;
+  GGMS_CU(cudaMalloc(&dx.p, 4ull * MLP_Q));
+  GGMS_CU(cudaMalloc(&dt.p, 4ull * MLP_Q));
+  GGMS_CU(cudaMalloc(&dp.p, 4ull * MLP_NP));
+  GGMS_CU(cudaMalloc(&dprobe.p, 4ull * (MLP_NP + 1)));
+  GGMS_CU(cudaMemcpy(dx.p, x, 4ull * MLP_Q, cudaMemcpyHostToDevice));
+  GGMS_CU(cudaMemcpy(dt.p, t, 4ull * MLP_Q, cudaMemcpyHostToDevice));
+  GGMS_CU(cudaMemcpy(dp.p, params, 4ull * MLP_NP, cudaMemcpyHostToDevice));
+  GGMS_CU(cudaFuncSetAttribute(mlp_train<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(MlpSmem)));
+  mlp_train<uint32_t><<<MLP_CTAS, MLP_NT, sizeof(MlpSmem)>>>(
+      nullptr, 0u, nullptr, nullptr, (float*)dp.p, 0u, 0.0f, (const float*)dx.p, (const float*)dt.p,
+      (float*)dprobe.p);
+  GGMS_CU(cudaDeviceSynchronize());
+  float* hp = (float*)malloc(4ull * (MLP_NP + 1));
+  if (!hp) return GGMS_E_OOM;
+  cudaError_t e = cudaMemcpy(hp, dprobe.p, 4ull * (MLP_NP + 1), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) {
+    memcpy(grad, hp, 4ull * MLP_NP);
+    *loss = hp[MLP_NP];
+  }
+  free(hp);
+  return cuda_status(e);
+}
+
+static int fit(const uint32_t* keys, int S, int kind, int steps, float* l0, float* l1, float* imb_m,
+               float* imb_s) {
+  if (!keys || S < 1024 || (kind != GGMS_ASSIGNER_LEARNED_PL && kind != GGMS_ASSIGNER_LEARNED_MLP))
+    return GGMS_E_INVALID_ARG;
+  DevBuf dk, da, dl, dc;
+  GGMS_CU(cudaMalloc(&dk.p, 4ull * S));
+  GGMS_CU(cudaMalloc(&da.p, 2 * sizeof(Assigner<uint32_t>)));
+  GGMS_CU(cudaMalloc(&dl.p, sizeof(LearnState)));
+  GGMS_CU(cudaMalloc(&dc.p, 4));
+  GGMS_CU(cudaMemcpy(dk.p, keys, 4ull * S, cudaMemcpyHostToDevice));
+  auto* As = (Assigner<uint32_t>*)da.p;
+  auto* L = (LearnState*)dl.p;
+  const uint32_t* k = (const uint32_t*)dk.p;
+  const uint32_t B = 1u << 14;
+  asg_build_sampled<uint32_t><<<1, 256>>>(k, (uint32_t)S, B, &As[0]);
+  long long launches = 0;
+  int rc = learn_and_choose<uint32_t>(kind, k, (uint32_t)S, B, steps, 1e30f, As, L, (uint32_t*)dc.p,
+                                      0, &launches);
+  if (rc) return rc;
+  GGMS_CU(cudaDeviceSynchronize());
+  LearnState hl;
+  Assigner<uint32_t> a0, a1;
+  GGMS_CU(cudaMemcpy(&hl, L, sizeof(hl), cudaMemcpyDeviceToHost));
+  GGMS_CU(cudaMemcpy(&a0, &As[0], sizeof(a0), cudaMemcpyDeviceToHost));
+  GGMS_CU(cudaMemcpy(&a1, &As[1], sizeof(a1), cudaMemcpyDeviceToHost));
+  if (l0) *l0 = (kind == GGMS_ASSIGNER_LEARNED_PL) ? hl.loss_init : -1.0f;
+  if (l1) *l1 = (kind == GGMS_ASSIGNER_LEARNED_PL) ? hl.loss : hl.mlp_loss;
+  if (imb_m) *imb_m = a1.quality;
+  if (imb_s) *imb_s = a0.quality;
+  return GGMS_OK;
+}
+
+}  // namespace diag
+
 }  // namespace ggms
 
 // ====================================================================== C ABI
@@ -746,6 +845,21 @@ int ggms_multiselect_segmented_u32(ggms_context* ctx, const uint32_t* d_in, cons
                                    int64_t nseg, const uint32_t* ks, const int64_t* k_off,
                                    uint32_t* out, const ggms_opts* opts, void* stream) {
   return segmented<uint32_t>(ctx, d_in, seg_off, nseg, ks, k_off, out, opts, stream);
+}
+
+int ggms_diag_pl_gradient(const uint32_t* keys, int S, const float* theta, float* loss, float* grad,
+                          uint32_t* knots, int* M) {
+  return diag::pl_gradient(keys, S, theta, loss, grad, knots, M);
+}
+
+int ggms_diag_mlp_gradient(const float* x, const float* t, const float* params, float* loss,
+                           float* grad) {
+  return diag::mlp_gradient(x, t, params, loss, grad);
+}
+
+int ggms_diag_fit(const uint32_t* keys, int S, int kind, int steps, float* l0, float* l1,
+                  float* imb_m, float* imb_s) {
+  return diag::fit(keys, S, kind, steps, l0, l1, imb_m, imb_s);
 }
 
 }  // extern "C"

@@ -26,6 +26,7 @@ namespace ggms {
 
 constexpr int PL_M = 256;        // segments of the learned PL model
 constexpr int MLP_H = 32;        // hidden width of the MLP model
+constexpr int MLP_NPARAM = 1153; // 32 + 32 + 32*32 + 32 + 32 + 1
 
 struct PLStats {                 // per segment, in double for a stable sum
   double n, su, su2, sy, syu, sy2;
@@ -44,11 +45,9 @@ struct LearnState {
   uint32_t steps;
   uint32_t choice;               // 1 learned accepted, 0 fell back to sampled
   uint32_t pad[2];
-  // MLP parameters and optimizer state (see ggms_mlp.cuh)
-  float w1[MLP_H], b1[MLP_H], w2[MLP_H * MLP_H], b2[MLP_H], w3[MLP_H], b3;
-  float mlp_loss_init;
+  // MLP parameters (see ggms_mlp.cuh)
+  float mlp_params[MLP_NPARAM + 3];
   float mlp_loss;
-  float x_scale;                 // 1 / (x_M - x_0) in key units, as float
 };
 
 __device__ __forceinline__ float softplusf(float x) {

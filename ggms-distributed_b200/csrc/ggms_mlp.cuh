@@ -1,15 +1,296 @@
-// ggms_mlp.cuh -- monotone 1-32-32-1 MLP CDF model (trained on the GPU).
+// ggms_mlp.cuh -- monotone 1-32-32-1 MLP CDF model, trained on the GPU.
+//
+//   x = (key - x_0) / (x_M - x_0)                    (key space, in [0, 1])
+//   h1 = tanh(w1 * x + c1)           w1 = softplus(V1) > 0     (32)
+//   h2 = tanh(W2 h1 + c2)            W2 = softplus(V2) > 0     (32 x 32)
+//   y  = sigmoid(w3 . h2 + c3)       w3 = softplus(V3) > 0
+// Positive weights and increasing activations make y non-decreasing in x, so
+// the compiled assigner is monotone.  Loss: mean (y_i - t_i)^2 over Q = 1024
+// training points at the quantiles of the self-drawn sample (t_i = rank / S).
+//
+// Training runs in ONE launch of one thread-block cluster (8 CTAs x 128
+// threads, one training point per thread): every step each CTA computes its
+// partial gradient (per-sample forward/backward, then the weight-gradient
+// contractions from shared memory), CTA 0 sums the eight partials through
+// distributed shared memory, applies Adam and the other CTAs read the new
+// parameters back the same way.  The trained model is evaluated at the knots
+// of the PL assigner format and compiled into it (pl_compile).
 #pragma once
+#include <cooperative_groups.h>
+
 #include "ggms_learned.cuh"
 
 namespace ggms {
 
+namespace cg = cooperative_groups;
+
+constexpr int MLP_CTAS = 8;
+constexpr int MLP_NT = 128;
+constexpr int MLP_Q = MLP_CTAS * MLP_NT;                 // training points per step
+constexpr int MLP_NP = MLP_NPARAM;  // 1153 parameters
+static_assert(MLP_NP == MLP_H + MLP_H + MLP_H * MLP_H + MLP_H + MLP_H + 1, "parameter count");
+// parameter offsets in the flat vector
+constexpr int P_V1 = 0, P_C1 = 32, P_V2 = 64, P_C2 = 64 + 1024, P_V3 = P_C2 + 32, P_C3 = P_V3 + 32;
+
+struct MlpSmem {
+  float P[MLP_NP];          // raw parameters (V1, c1, V2, c2, V3, c3)
+  float G[MLP_NP];          // this CTA's partial gradient
+  float m1[MLP_NP], m2[MLP_NP];  // Adam moments (CTA 0)
+  float w1[32], W2[1024], w3[32];  // softplus'd weights
+  float x[MLP_NT], t[MLP_NT], dz[MLP_NT], err[MLP_NT];
+  float h1[MLP_NT][33], h2[MLP_NT][33], da1[MLP_NT][33], da2[MLP_NT][33];
+};
+
+__device__ __forceinline__ float tanh_(float v) { return tanhf(v); }
+
+// Forward + backward of this CTA's MLP_NT points; fills S.G with the partial
+// gradient (w.r.t. the raw parameters) and S.err with the squared errors.
+__device__ void mlp_cta_grad(MlpSmem& S, float inv_q) {
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 1024; i += MLP_NT) S.W2[i] = softplusf(S.P[P_V2 + i]);
+  if (tid < 32) {
+    S.w1[tid] = softplusf(S.P[P_V1 + tid]);
+    S.w3[tid] = softplusf(S.P[P_V3 + tid]);
+  }
+  __syncthreads();
+  // per-sample forward and backward to the hidden layers
+  {
+    const float x = S.x[tid];
+    float h1[32], h2[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) h1[j] = tanh_(fmaf(S.w1[j], x, S.P[P_C1 + j]));
+    float z = S.P[P_C3];
+#pragma unroll 4
+    for (int k = 0; k < 32; ++k) {
+      float a = S.P[P_C2 + k];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) a = fmaf(S.W2[k * 32 + j], h1[j], a);
+      h2[k] = tanh_(a);
+      z = fmaf(S.w3[k], h2[k], z);
+    }
+    const float y = sigmoidf_(z);
+    const float e = y - S.t[tid];
+    S.err[tid] = e * e;
+    const float dz = 2.0f * e * inv_q * y * (1.0f - y);
+    S.dz[tid] = dz;
+    float dh1[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) dh1[j] = 0.0f;
+#pragma unroll 4
+    for (int k = 0; k < 32; ++k) {
+      const float da2 = dz * S.w3[k] * (1.0f - h2[k] * h2[k]);
+      S.da2[tid][k] = da2;
+      S.h2[tid][k] = h2[k];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) dh1[j] = fmaf(S.W2[k * 32 + j], da2, dh1[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      S.h1[tid][j] = h1[j];
+      S.da1[tid][j] = dh1[j] * (1.0f - h1[j] * h1[j]);
+    }
+  }
+  __syncthreads();
+  // weight gradients: contractions over the CTA's samples (fixed order)
+  for (int p = tid; p < 1024; p += MLP_NT) {
+    const int k = p >> 5, j = p & 31;
+    float acc = 0.0f;
+    for (int i = 0; i < MLP_NT; ++i) acc = fmaf(S.da2[i][k], S.h1[i][j], acc);
+    S.G[P_V2 + p] = acc * sigmoidf_(S.P[P_V2 + p]);  // d softplus(v) / dv = sigmoid(v)
+  }
+  if (tid < 32) {
+    float gw1 = 0, gc1 = 0, gc2 = 0, gw3 = 0;
+    for (int i = 0; i < MLP_NT; ++i) {
+      gw1 = fmaf(S.da1[i][tid], S.x[i], gw1);
+      gc1 += S.da1[i][tid];
+      gc2 += S.da2[i][tid];
+      gw3 = fmaf(S.dz[i], S.h2[i][tid], gw3);
+    }
+    S.G[P_V1 + tid] = gw1 * sigmoidf_(S.P[P_V1 + tid]);
+    S.G[P_C1 + tid] = gc1;
+    S.G[P_C2 + tid] = gc2;
+    S.G[P_V3 + tid] = gw3 * sigmoidf_(S.P[P_V3 + tid]);
+  } else if (tid == 32) {
+    float gc3 = 0;
+    for (int i = 0; i < MLP_NT; ++i) gc3 += S.dz[i];
+    S.G[P_C3] = gc3;
+  }
+  __syncthreads();
+}
+
+// Training points: Q sample quantiles, x normalized over the knot range of A,
+// target t = (rank + 0.5) / S.
+template <typename K>
+__device__ void mlp_load_points(MlpSmem& S, const K* sorted, uint32_t S_n, const Assigner<K>* A,
+                                const float* px, const float* pt) {
+  const int tid = threadIdx.x;
+  const uint32_t gi = blockIdx.x * MLP_NT + tid;
+  if (px) {  // explicit points (gradient probe)
+    S.x[tid] = px[gi];
+    S.t[tid] = pt[gi];
+    return;
+  }
+  const uint32_t si = (uint32_t)(((uint64_t)(2 * gi + 1) * S_n) / (2 * MLP_Q));
+  const K x0 = A->x[0], xM = A->x[A->M];
+  const float span = key_to_float_rn((K)(xM - x0));
+  S.x[tid] = span > 0.0f ? fminf(__fdiv_rn(key_to_float_rn((K)(sorted[si] - x0)), span), 1.0f) : 0.0f;
+  S.t[tid] = ((float)si + 0.5f) / (float)S_n;
+}
+
+// The cluster training kernel.  steps == 0 with probe != null: one forward /
+// backward at L's parameters, the summed gradient and loss are written to
+// probe[0..MLP_NP) and probe[MLP_NP] (used by the gradient check).
+template <typename K>
+__global__ void __cluster_dims__(MLP_CTAS, 1, 1) __launch_bounds__(MLP_NT)
+mlp_train(const K* __restrict__ sorted, uint32_t S_n, const Assigner<K>* __restrict__ A,
+          LearnState* L, float* Pglob, uint32_t steps, float lr, const float* px, const float* pt,
+          float* probe) {
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  MlpSmem& S = *reinterpret_cast<MlpSmem*>(smem_raw);
+  cg::cluster_group cluster = cg::this_cluster();
+  const unsigned rank = cluster.block_rank();
+  const int tid = threadIdx.x;
+  for (int p = tid; p < MLP_NP; p += MLP_NT) {
+    S.P[p] = Pglob[p];
+    S.m1[p] = 0.0f;
+    S.m2[p] = 0.0f;
+  }
+  mlp_load_points<K>(S, sorted, S_n, A, px, pt);
+  __syncthreads();
+  MlpSmem* S0 = cluster.map_shared_rank(&S, 0);
+  const float inv_q = 1.0f / (float)MLP_Q;
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  float b1t = 1.0f, b2t = 1.0f;
+  const uint32_t iters = steps ? steps : 1u;
+  for (uint32_t it = 0; it < iters; ++it) {
+    mlp_cta_grad(S, inv_q);
+    cluster.sync();  // all partial gradients are in place
+    if (rank == 0) {
+      b1t *= b1;
+      b2t *= b2;
+      for (int p = tid; p < MLP_NP; p += MLP_NT) {
+        float g = 0.0f;
+        for (unsigned r = 0; r < MLP_CTAS; ++r) g += cluster.map_shared_rank(&S, r)->G[p];
+        if (steps == 0) {
+          if (probe) probe[p] = g;
+          continue;
+        }
+        const float m1 = b1 * S.m1[p] + (1.0f - b1) * g;
+        const float m2 = b2 * S.m2[p] + (1.0f - b2) * g * g;
+        S.m1[p] = m1;
+        S.m2[p] = m2;
+        S.P[p] -= lr * (m1 / (1.0f - b1t)) / (sqrtf(m2 / (1.0f - b2t)) + eps);
+      }
+    }
+    cluster.sync();  // CTA 0 has the new parameters
+    if (rank != 0)
+      for (int p = tid; p < MLP_NP; p += MLP_NT) S.P[p] = S0->P[p];
+    __syncthreads();
+  }
+  // final loss at the trained parameters
+  mlp_cta_grad(S, inv_q);
+  if (tid == 0) {
+    float e = 0.0f;
+    for (int i = 0; i < MLP_NT; ++i) e += S.err[i];
+    S.G[0] = e;  // reuse as this CTA's error sum
+  }
+  cluster.sync();
+  if (rank == 0 && tid == 0) {
+    float e = 0.0f;
+    for (unsigned r = 0; r < MLP_CTAS; ++r) e += cluster.map_shared_rank(&S, r)->G[0];
+    const float loss = e * inv_q;
+    if (probe && steps == 0) probe[MLP_NP] = loss;
+    if (L) L->mlp_loss = loss;
+  }
+  if (rank == 0)
+    for (int p = tid; p < MLP_NP; p += MLP_NT) Pglob[p] = S.P[p];
+  cluster.sync();  // keep every CTA's shared memory alive until CTA 0 has read it
+}
+
+// Initial parameters: hidden units of layer 1 step at the sample quantiles.
+template <typename K>
+__global__ void mlp_init(const K* __restrict__ sorted, uint32_t S_n, const Assigner<K>* __restrict__ A,
+                         float* P) {
+  const int tid = threadIdx.x;
+  const K x0 = A->x[0], xM = A->x[A->M];
+  const float span = key_to_float_rn((K)(xM - x0));
+  const float inv_sp1 = 0.5413248546f;  // softplus^-1(1)
+  for (int p = tid; p < MLP_NP; p += blockDim.x) {
+    float v = 0.0f;
+    if (p < P_C1) {                       // V1: w1 = 8
+      v = 7.99966454f;                    // softplus^-1(8)
+    } else if (p < P_V2) {                // c1 = -8 q_j
+      const int j = p - P_C1;
+      const uint32_t si = (uint32_t)(((uint64_t)(2 * j + 1) * S_n) / 64u);
+      const float q = span > 0.0f ? __fdiv_rn(key_to_float_rn((K)(sorted[si] - x0)), span) : 0.0f;
+      v = -8.0f * q;
+    } else if (p < P_C2) {                // V2: W2 ~ 1/32 with a deterministic spread
+      const int i = p - P_V2;
+      const float w = (1.0f / 32.0f) * (0.5f + (float)((i * 2654435761u) >> 22) / 1024.0f);
+      v = logf(expm1f(w));                // softplus^-1(w)
+    } else if (p < P_V3) {                // c2: spread the second layer's centers
+      const int k = p - P_C2;
+      v = 0.8f * ((float)k / 31.0f - 0.5f);
+    } else if (p < P_C3) {                // V3: w3 ~ 0.2
+      v = logf(expm1f(0.2f));
+    } else {
+      v = 0.0f;                           // c3
+    }
+    (void)inv_sp1;
+    P[p] = v;
+  }
+}
+
+// Evaluate the trained MLP at the knots of A and write the normalized CDF.
+template <typename K>
+__global__ void mlp_eval_knots(const float* __restrict__ P, const Assigner<K>* __restrict__ A,
+                               float* cdf) {
+  __shared__ float y[ASG_MAXM + 1];
+  const uint32_t M = A->M;
+  const K x0 = A->x[0];
+  const float span = key_to_float_rn((K)(A->x[M] - x0));
+  for (uint32_t j = threadIdx.x; j <= M; j += blockDim.x) {
+    const float x = span > 0.0f ? fminf(__fdiv_rn(key_to_float_rn((K)(A->x[j] - x0)), span), 1.0f) : 0.0f;
+    float h1[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) h1[i] = tanhf(fmaf(softplusf(P[P_V1 + i]), x, P[P_C1 + i]));
+    float z = P[P_C3];
+    for (int k = 0; k < 32; ++k) {
+      float a = P[P_C2 + k];
+#pragma unroll
+      for (int i = 0; i < 32; ++i) a = fmaf(softplusf(P[P_V2 + k * 32 + i]), h1[i], a);
+      z = fmaf(softplusf(P[P_V3 + k]), tanhf(a), z);
+    }
+    y[j] = sigmoidf_(z);
+  }
+  __syncthreads();
+  const float lo = y[0], hi = y[M];
+  for (uint32_t j = threadIdx.x; j <= M; j += blockDim.x) {
+    float f = (hi > lo) ? (y[j] - lo) / (hi - lo) : (float)j / (float)(M ? M : 1);
+    if (j > 0 && hi > lo) f = fmaxf(f, 0.0f);
+    cdf[j] = f;
+  }
+}
+
 template <typename K>
 static int mlp_fit_and_compile(const K* sorted, uint32_t S, int steps_opt, Assigner<K>* As,
                                LearnState* L, cudaStream_t st, long long* launches) {
-  (void)launches;
-  (void)sorted; (void)S; (void)steps_opt; (void)As; (void)L; (void)st;
-  return GGMS_E_UNSUPPORTED;
+  static bool attr_set = false;
+  if (!attr_set) {
+    if (cudaFuncSetAttribute(mlp_train<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(MlpSmem)) != cudaSuccess)
+      return GGMS_E_CUDA;
+    attr_set = true;
+  }
+  const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 150u;
+  float* P = L->mlp_params;
+  mlp_init<K><<<1, 256, 0, st>>>(sorted, S, &As[1], P);
+  mlp_train<K><<<MLP_CTAS, MLP_NT, sizeof(MlpSmem), st>>>(sorted, S, &As[1], L, P, steps, 0.02f,
+                                                          nullptr, nullptr, nullptr);
+  mlp_eval_knots<K><<<1, 256, 0, st>>>(P, &As[1], L->cdf);
+  pl_compile<K><<<1, 256, 0, st>>>(L->cdf, &As[1], GGMS_ASSIGNER_LEARNED_MLP);
+  *launches += 4;
+  return cudaGetLastError() == cudaSuccess ? GGMS_OK : GGMS_E_CUDA;
 }
 
 }  // namespace ggms

@@ -21,7 +21,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 PKG_ROOT = os.path.dirname(_HERE)
 REPO_ROOT = os.path.dirname(PKG_ROOT)
 LIB_PATH = os.path.join(PKG_ROOT, "lib", "libggms_b200.so")
-HEADER_PATHS = [os.path.join(REPO_ROOT, "include", "ggms.h")]
+HEADER_PATHS = [os.path.join(REPO_ROOT, "include", "ggms.h"),
+                os.path.join(REPO_ROOT, "include", "ggms_diag.h")]
 
 GGMS_OK = 0
 GGMS_E_INVALID_ARG = 1
@@ -119,12 +120,17 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         fn = getattr(lib, f"ggms_multiselect_segmented_{suf}")
         fn.restype = i32
         fn.argtypes = [vp, vp, i64, vp, i64, vp, vp, ctypes.POINTER(Opts), vp]
-    if hasattr(lib, "ggms_diag_pl_gradient"):
-        lib.ggms_diag_pl_gradient.restype = i32
-        lib.ggms_diag_pl_gradient.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp]
-    if hasattr(lib, "ggms_diag_mlp_gradient"):
-        lib.ggms_diag_mlp_gradient.restype = i32
-        lib.ggms_diag_mlp_gradient.argtypes = [vp, vp, i32, vp, vp, vp]
+    lib.ggms_get_default_context.argtypes = [ctypes.POINTER(vp)]
+    lib.ggms_context_profile.argtypes = [vp, i32]
+    lib.ggms_context_pass_times.argtypes = [vp, vp, vp, vp, i32]
+    lib.ggms_context_launches.restype = i64
+    lib.ggms_context_launches.argtypes = [vp]
+    lib.ggms_diag_pl_gradient.restype = i32
+    lib.ggms_diag_pl_gradient.argtypes = [vp, i32, vp, vp, vp, vp, vp]
+    lib.ggms_diag_mlp_gradient.restype = i32
+    lib.ggms_diag_mlp_gradient.argtypes = [vp, vp, vp, vp, vp]
+    lib.ggms_diag_fit.restype = i32
+    lib.ggms_diag_fit.argtypes = [vp, i32, i32, i32, vp, vp, vp, vp]
     _lib = lib
     return lib
 
@@ -242,3 +248,48 @@ def declared_symbols(paths=None):
             txt = f.read()
         names += re.findall(r"GGMS_API\s+[\w\s\*]+?\b(ggms_\w+)\s*\(", txt)
     return sorted(set(names))
+
+
+# ------------------------------------------------------------------ learned-model diagnostics
+def _fp(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def diag_pl_gradient(sorted_keys: np.ndarray, theta: np.ndarray):
+    """GPU loss/gradient of the PL-CDF model; returns (loss, grad[:M], knots[:M+1])."""
+    k = np.ascontiguousarray(sorted_keys, dtype=np.uint32)
+    th = np.zeros(256, np.float32)
+    th[:len(theta)] = theta
+    loss = np.zeros(1, np.float32)
+    grad = np.zeros(256, np.float32)
+    knots = np.zeros(257, np.uint32)
+    m = ctypes.c_int(0)
+    rc = load().ggms_diag_pl_gradient(_fp(k), len(k), _fp(th), _fp(loss), _fp(grad), _fp(knots),
+                                      ctypes.byref(m))
+    if rc:
+        raise GGMSError(rc, "ggms_diag_pl_gradient")
+    return float(loss[0]), grad[:m.value].copy(), knots[:m.value + 1].copy()
+
+
+def diag_mlp_gradient(x: np.ndarray, t: np.ndarray, params: np.ndarray):
+    x = np.ascontiguousarray(x, np.float32)
+    t = np.ascontiguousarray(t, np.float32)
+    p = np.ascontiguousarray(params, np.float32)
+    assert len(x) == 1024 and len(t) == 1024 and len(p) == 1153
+    loss = np.zeros(1, np.float32)
+    grad = np.zeros(1153, np.float32)
+    rc = load().ggms_diag_mlp_gradient(_fp(x), _fp(t), _fp(p), _fp(loss), _fp(grad))
+    if rc:
+        raise GGMSError(rc, "ggms_diag_mlp_gradient")
+    return float(loss[0]), grad
+
+
+def diag_fit(sorted_keys: np.ndarray, kind: int, steps: int = 0):
+    k = np.ascontiguousarray(sorted_keys, dtype=np.uint32)
+    out = np.zeros(4, np.float32)
+    f = [ctypes.c_float() for _ in range(4)]
+    rc = load().ggms_diag_fit(_fp(k), len(k), kind, steps, *[ctypes.byref(v) for v in f])
+    if rc:
+        raise GGMSError(rc, "ggms_diag_fit")
+    return {"loss_before": f[0].value, "loss_after": f[1].value,
+            "imbalance_model": f[2].value, "imbalance_sampled": f[3].value}

@@ -11,6 +11,20 @@ import ggms_oracle as orc
 
 FIXTURES = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
 
+# Inputs on which the reference's bucketMultiselect is itself wrong.  With +-Inf
+# in the data its global min/max pivots are infinite: the first and last
+# segments get slope 0 (bucketMultiselect.cu:675-677 only zeroes infinite
+# slopes) and (x - pivot) is NaN for the infinite elements, so elements land in
+# the wrong buckets and every answer is shifted.  The fixture records that; the
+# oracle is checked there against an independent numpy sort instead.
+REFERENCE_DEFECTS = {"with_inf_f32"}
+
+
+def numpy_select(v, ks):
+    k = orc.keys(v)
+    s = v[np.argsort(k, kind="stable")]
+    return s[len(v) - ks.astype(np.int64)]
+
 
 def test_fixtures_present():
     assert len(FIXTURES) >= 10, "golden fixtures missing (tests/golden/make_golden.py)"
@@ -21,6 +35,11 @@ def test_oracle_matches_reference(path):
     z = np.load(path)
     v, ks, ref = z["values"], z["ks"], z["ref_out"]
     got = orc.select(v, ks)
+    name = os.path.basename(path)[:-4]
+    if name in REFERENCE_DEFECTS:
+        np.testing.assert_array_equal(orc.bits(got), orc.bits(numpy_select(v, ks)))
+        assert not np.array_equal(orc.bits(got), orc.bits(ref)), "reference defect no longer seen"
+        return
     if "signed_zeros" in path:
         # thrust's radix sort orders -0.0 and +0.0 as equal (stable), the oracle
         # orders -0.0 < +0.0: the values agree, the sign bit of a zero may not.
