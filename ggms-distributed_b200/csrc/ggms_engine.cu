@@ -142,7 +142,8 @@ struct Workspace {
   K* samp_raw;
   K* samp_sorted;
   K* samp_tmp;
-  Assigner<K>* asg;       // [0] sampled, [1] learned
+  Assigner<K>* asg;       // [0] sampled, [1] learned (the PL models)
+  Grid<K>* grid;          // [0] sampled, [1] learned (what the passes evaluate)
   LearnState* learn;
   uint32_t* hist0;
   uint32_t* aflag0;
@@ -185,6 +186,7 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
   size_t o_ss = b.take(sizeof(K) * p.S);
   size_t o_st = b.take(sizeof(K) * p.S);
   size_t o_asg = b.take(sizeof(Assigner<K>) * 2);
+  size_t o_grid = b.take(sizeof(Grid<K>) * 2);
   size_t o_learn = b.take(sizeof(LearnState));
   size_t o_h0 = b.take(4ull * p.B);
   size_t o_a0 = b.take(4ull * (p.B / 32));
@@ -212,6 +214,7 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
   w.samp_sorted = (K*)(base + o_ss);
   w.samp_tmp = (K*)(base + o_st);
   w.asg = (Assigner<K>*)(base + o_asg);
+  w.grid = (Grid<K>*)(base + o_grid);
   w.learn = (LearnState*)(base + o_learn);
   w.hist0 = (uint32_t*)(base + o_h0);
   w.aflag0 = (uint32_t*)(base + o_a0);
@@ -269,26 +272,33 @@ constexpr int MAX_LEVELS_32 = 3;
 constexpr int MAX_LEVELS_64 = 6;
 
 template <typename T>
-static size_t l0_smem(uint32_t B) {
-  return (size_t)B * 4u + AsgSmem<typename KeyOf<T>::K>::bytes;
+static size_t l0_count_smem(uint32_t B) { return GRID_SMEM + (size_t)B * 4u; }
+template <typename T>
+static size_t l0_compact_smem(uint32_t B) { return GRID_SMEM + (size_t)(B / 32) * 4u; }
+
+// Launch shapes of the two passes: as many resident CTAs as fit, one wave.
+template <typename T>
+static int l0_grids(Context* c, uint32_t B, int* g_count, int* g_compact) {
+  const size_t s1 = l0_count_smem<T>(B), s2 = l0_compact_smem<T>(B);
+  GGMS_CU(cudaFuncSetAttribute(l0_count<T, L0_NT, L0_UNROLL>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
+  GGMS_CU(cudaFuncSetAttribute(l0_compact<T, L0_NT, L0_UNROLL>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
+  int o1 = 0, o2 = 0;
+  GGMS_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, l0_count<T, L0_NT, L0_UNROLL>, L0_NT, s1));
+  GGMS_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, l0_compact<T, L0_NT, L0_UNROLL>, L0_NT, s2));
+  *g_count = std::max(1, o1) * c->sms;
+  *g_compact = std::max(1, o2) * c->sms;
+  return GGMS_OK;
 }
 
-template <typename T>
-static int l0_grid(Context* c, uint32_t B, int* grid) {
-  static int occ_cache[2][8] = {};
-  const int bi = (B == (1u << 15)) ? 5 : (B == (1u << 14)) ? 4 : (B == (1u << 13)) ? 3
-               : (B == (1u << 12)) ? 2 : (B == (1u << 11)) ? 1 : 0;
-  size_t sm = l0_smem<T>(B);
-  GGMS_CU(cudaFuncSetAttribute(l0_count<T, L0_NT, L0_UNROLL>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  GGMS_CU(cudaFuncSetAttribute(l0_compact<T, L0_NT, L0_UNROLL>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  int occ = 0;
-  GGMS_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, l0_count<T, L0_NT, L0_UNROLL>,
-                                                        L0_NT, sm));
-  (void)occ_cache;
-  (void)bi;
-  *grid = std::max(1, occ) * c->sms;
+template <typename K>
+static int setup_attrs() {
+  static bool done = false;
+  if (done) return GGMS_OK;
+  GGMS_CU(cudaFuncSetAttribute(setup_sampled<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(SetupSmem<K>)));
+  done = true;
   return GGMS_OK;
 }
 
@@ -356,7 +366,13 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   const uint32_t S = p.S;
   ++ctx->launches;
   asg_sample<T><<<cdiv(S, 256), 256, 0, st>>>(d_in, n, S, p.seed, w.samp_raw);
-  if (S <= 4096) {
+  if (S <= 1024) {
+    ++ctx->launches;
+    asg_sort_chunks<K, 1024, 1024><<<1, 1024, 0, st>>>(w.samp_raw, w.samp_sorted, S);
+  } else if (S <= 2048) {
+    ++ctx->launches;
+    asg_sort_chunks<K, 2048, 1024><<<1, 1024, 0, st>>>(w.samp_raw, w.samp_sorted, S);
+  } else if (S <= 4096) {
     ++ctx->launches;
     asg_sort_chunks<K, 4096, 1024><<<1, 1024, 0, st>>>(w.samp_raw, w.samp_sorted, S);
   } else {
@@ -365,24 +381,27 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     ++ctx->launches;
     asg_merge_rank<K><<<cdiv(S, 256), 256, 0, st>>>(w.samp_tmp, w.samp_sorted, S, 4096u);
   }
+  rc = setup_attrs<K>();
+  if (rc) return rc;
   ++ctx->launches;
-  asg_build_sampled<K><<<1, 256, 0, st>>>(w.samp_sorted, S, p.B, &w.asg[0]);
+  setup_sampled<K><<<1, SETUP_NT, sizeof(SetupSmem<K>), st>>>(w.samp_sorted, S, p.B, &w.asg[0],
+                                                               &w.grid[0]);
   if (p.assigner != GGMS_ASSIGNER_SAMPLED) {
     rc = learn_and_choose<K>(p.assigner, w.samp_sorted, S, p.B, p.train_steps, p.bound, w.asg,
-                             w.learn, &w.C->asg_choice, st, &ctx->launches);
+                             w.grid, w.learn, &w.C->asg_choice, st, &ctx->launches);
     if (rc) return rc;
   }
 
   // ---- PASS 1: count
-  int grid = 0;
-  rc = l0_grid<T>(ctx, p.B, &grid);
+  int grid_c = 0, grid_p = 0;
+  rc = l0_grids<T>(ctx, p.B, &grid_c, &grid_p);
   if (rc) return rc;
-  const size_t sm = l0_smem<T>(p.B);
   GGMS_CU(cudaMemsetAsync(w.hist0, 0, 4ull * p.B, st));
   GGMS_CU(cudaMemsetAsync(w.aflag0, 0, 4ull * (p.B / 32), st));
   prof_rec(prof, 1, st);
   ++ctx->launches;
-  l0_count<T, L0_NT, L0_UNROLL><<<grid, L0_NT, sm, st>>>(d_in, n, w.asg, w.C, w.hist0);
+  l0_count<T, L0_NT, L0_UNROLL><<<grid_c, L0_NT, l0_count_smem<T>(p.B), st>>>(d_in, n, w.grid, w.C,
+                                                                               w.hist0);
   prof_rec(prof, 2, st);
   ++ctx->launches;
   l0_scan<<<1, 1024, 0, st>>>(w.hist0, p.B, w.C);
@@ -390,7 +409,7 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   lvl_locate_rows<<<cdiv(nk, 256), 256, 0, st>>>(w.hist0, p.B, nk, w.krank, w.kseg, w.kbin,
                                                    w.aflag0, p.B / 32, w.C);
   ++ctx->launches;
-  l0_children<K><<<cdiv(p.B, 256), 256, 0, st>>>(w.hist0, w.aflag0, p.B, w.asg, w.C, w.cmap0,
+  l0_children<K><<<cdiv(p.B, 256), 256, 0, st>>>(w.hist0, w.aflag0, p.B, w.grid, w.C, w.cmap0,
                                                    w.segs[1], w.cursor[1], w.tiles[1], w.points, caps);
   ++ctx->launches;
   lvl_relabel<K><<<cdiv(nk, 256), 256, 0, st>>>(w.cmap0, p.B, nk, w.kbin, w.kseg, w.kkey,
@@ -398,8 +417,8 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   // ---- PASS 2: compact the buckets that still need refinement
   prof_rec(prof, 3, st);
   ++ctx->launches;
-  l0_compact<T, L0_NT, L0_UNROLL><<<grid, L0_NT, sm, st>>>(d_in, n, w.asg, w.C, w.cmap0,
-                                                           w.segs[1], w.cursor[1], w.cand[0]);
+  l0_compact<T, L0_NT, L0_UNROLL><<<grid_p, L0_NT, l0_compact_smem<T>(p.B), st>>>(
+      d_in, n, w.grid, w.C, w.cmap0, w.segs[1], w.cursor[1], w.cand[0]);
   prof_rec(prof, 4, st);
 
   // ---- refinement levels over candidates
@@ -446,8 +465,8 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   if (host_out) memcpy(out, pin_out, sizeof(T) * nk);
   if (o.stats) {
     ggms_stats* s = o.stats;
-    Assigner<K> a_used;
-    GGMS_CU(cudaMemcpy(&a_used, &w.asg[pin_C->asg_choice], sizeof(Assigner<K>), cudaMemcpyDeviceToHost));
+    Grid<K> a_used;
+    GGMS_CU(cudaMemcpy(&a_used, &w.grid[pin_C->asg_choice], sizeof(Grid<K>), cudaMemcpyDeviceToHost));
     LearnState ls;
     GGMS_CU(cudaMemcpy(&ls, w.learn, sizeof(LearnState), cudaMemcpyDeviceToHost));
     s->assigner_used = (int32_t)a_used.kind;
@@ -632,24 +651,23 @@ struct DevBuf {
 static int pl_gradient(const uint32_t* keys, int S, const float* theta, float* loss, float* grad,
                        uint32_t* knots, int* Mout) {
   if (!keys || S < 2 || !theta || !loss || !grad) return GGMS_E_INVALID_ARG;
-  DevBuf dk, da, dl, dt, dout;
+  DevBuf dk, da, dt, dout;
   GGMS_CU(cudaMalloc(&dk.p, 4ull * S));
   GGMS_CU(cudaMalloc(&da.p, sizeof(Assigner<uint32_t>)));
-  GGMS_CU(cudaMalloc(&dl.p, sizeof(LearnState)));
   GGMS_CU(cudaMalloc(&dt.p, 4ull * PL_M));
   GGMS_CU(cudaMalloc(&dout.p, 4ull * (PL_M + 1)));
   GGMS_CU(cudaMemcpy(dk.p, keys, 4ull * S, cudaMemcpyHostToDevice));
   GGMS_CU(cudaMemcpy(dt.p, theta, 4ull * PL_M, cudaMemcpyHostToDevice));
   auto* A = (Assigner<uint32_t>*)da.p;
-  auto* L = (LearnState*)dl.p;
-  pl_init_knots<uint32_t><<<1, 256>>>((const uint32_t*)dk.p, (uint32_t)S, 1u << 14, A);
-  Assigner<uint32_t> h;
-  GGMS_CU(cudaMemcpy(&h, A, sizeof(h), cudaMemcpyDeviceToHost));
-  pl_stats<uint32_t><<<(PL_M * 32 + 255) / 256, 256>>>((const uint32_t*)dk.p, (uint32_t)S, A, L);
   float* dloss = (float*)dout.p;
   float* dgrad = dloss + 1;
-  pl_grad_probe<<<1, 32>>>(L, (const float*)dt.p, h.M, (uint32_t)S, dloss, dgrad);
+  GGMS_CU(cudaFuncSetAttribute(pl_grad_probe<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(LearnSmem<uint32_t>)));
+  pl_grad_probe<uint32_t><<<1, SETUP_NT, sizeof(LearnSmem<uint32_t>)>>>(
+      (const uint32_t*)dk.p, (uint32_t)S, 1u << 14, (const float*)dt.p, A, dloss, dgrad);
   GGMS_CU(cudaDeviceSynchronize());
+  Assigner<uint32_t> h;
+  GGMS_CU(cudaMemcpy(&h, A, sizeof(h), cudaMemcpyDeviceToHost));
   GGMS_CU(cudaMemcpy(loss, dloss, 4, cudaMemcpyDeviceToHost));
   GGMS_CU(cudaMemcpy(grad, dgrad, 4ull * h.M, cudaMemcpyDeviceToHost));
   if (knots) memcpy(knots, h.x, 4ull * (h.M + 1));
@@ -688,27 +706,31 @@ static int fit(const uint32_t* keys, int S, int kind, int steps, float* l0, floa
                float* imb_s) {
   if (!keys || S < 1024 || (kind != GGMS_ASSIGNER_LEARNED_PL && kind != GGMS_ASSIGNER_LEARNED_MLP))
     return GGMS_E_INVALID_ARG;
-  DevBuf dk, da, dl, dc;
+  DevBuf dk, da, dg, dl, dc;
   GGMS_CU(cudaMalloc(&dk.p, 4ull * S));
   GGMS_CU(cudaMalloc(&da.p, 2 * sizeof(Assigner<uint32_t>)));
+  GGMS_CU(cudaMalloc(&dg.p, 2 * sizeof(Grid<uint32_t>)));
   GGMS_CU(cudaMalloc(&dl.p, sizeof(LearnState)));
   GGMS_CU(cudaMalloc(&dc.p, 4));
   GGMS_CU(cudaMemcpy(dk.p, keys, 4ull * S, cudaMemcpyHostToDevice));
   auto* As = (Assigner<uint32_t>*)da.p;
+  auto* Gs = (Grid<uint32_t>*)dg.p;
   auto* L = (LearnState*)dl.p;
   const uint32_t* k = (const uint32_t*)dk.p;
   const uint32_t B = 1u << 14;
-  asg_build_sampled<uint32_t><<<1, 256>>>(k, (uint32_t)S, B, &As[0]);
+  int rc = setup_attrs<uint32_t>();
+  if (rc) return rc;
+  setup_sampled<uint32_t><<<1, SETUP_NT, sizeof(SetupSmem<uint32_t>)>>>(k, (uint32_t)S, B, &As[0], &Gs[0]);
   long long launches = 0;
-  int rc = learn_and_choose<uint32_t>(kind, k, (uint32_t)S, B, steps, 1e30f, As, L, (uint32_t*)dc.p,
-                                      0, &launches);
+  rc = learn_and_choose<uint32_t>(kind, k, (uint32_t)S, B, steps, 1e30f, As, Gs, L, (uint32_t*)dc.p,
+                                  0, &launches);
   if (rc) return rc;
   GGMS_CU(cudaDeviceSynchronize());
   LearnState hl;
-  Assigner<uint32_t> a0, a1;
+  Grid<uint32_t> a0, a1;
   GGMS_CU(cudaMemcpy(&hl, L, sizeof(hl), cudaMemcpyDeviceToHost));
-  GGMS_CU(cudaMemcpy(&a0, &As[0], sizeof(a0), cudaMemcpyDeviceToHost));
-  GGMS_CU(cudaMemcpy(&a1, &As[1], sizeof(a1), cudaMemcpyDeviceToHost));
+  GGMS_CU(cudaMemcpy(&a0, &Gs[0], sizeof(a0), cudaMemcpyDeviceToHost));
+  GGMS_CU(cudaMemcpy(&a1, &Gs[1], sizeof(a1), cudaMemcpyDeviceToHost));
   if (l0) *l0 = (kind == GGMS_ASSIGNER_LEARNED_PL) ? hl.loss_init : -1.0f;
   if (l1) *l1 = (kind == GGMS_ASSIGNER_LEARNED_PL) ? hl.loss : hl.mlp_loss;
   if (imb_m) *imb_m = a1.quality;

@@ -166,6 +166,60 @@ __device__ __forceinline__ uint32_t asg_eval(const AsgView<K>& a, K key) {
   return b0 + __float2uint_rz(t);
 }
 
+
+// ------------------------------------------------------------------ compiled grid assigner
+// What the two passes evaluate.  Any monotone key -> bucket model (the sampled
+// pivots or a learned CDF, both held as a piecewise-linear Assigner above) is
+// resampled onto a uniform grid of up to 2^11 cells over the sample's key range
+// [lo, lo + span]; the up-to-32 cells holding the most mass are split again into
+// 2^6 sub-cells.  A key costs one shared-memory lookup (two for a split cell),
+// one multiply and one clamp -- no search.  Keys below lo go to bucket 0, keys
+// above lo + span to bucket B-1 (open tails: no min/max pass is needed, unlike
+// the reference's thrust::minmax_element, DistributedSMOS/bucketMultiselect.cu:543-547).
+constexpr int GRID_BITS1 = 11;
+constexpr int GRID_NC1 = 1 << GRID_BITS1;       // level-1 cells
+constexpr int GRID_BITS2 = 6;
+constexpr int GRID_NC2 = 1 << GRID_BITS2;       // sub-cells of a split cell
+constexpr int GRID_NSUB = 32;                   // split cells at most
+constexpr uint32_t GRID_SPLIT = 0x80000000u;    // entry flag: .y is a sub-table index
+
+// entry: .x = base (bits 0-15) | cap (bits 16-30) | GRID_SPLIT; .y = slope (float bits)
+template <typename K>
+struct Grid {
+  K lo;
+  K span;
+  uint32_t sh1, sh2, B, ncell, nsub, kind;
+  float quality;               // max/mean occupancy on the sample (256 bucket groups)
+  float loss;
+  uint32_t pad[2];
+  uint2 t1[GRID_NC1];
+  uint2 t2[GRID_NSUB * GRID_NC2];
+};
+
+template <typename K>
+struct GridView {
+  const uint2* t1;
+  const uint2* t2;
+  K lo, span;
+  uint32_t sh1, sh2, B;
+};
+
+template <typename K>
+__device__ __forceinline__ uint32_t grid_eval(const GridView<K>& g, K key) {
+  if (key < g.lo) return 0u;
+  const K d = (K)(key - g.lo);
+  if (d > g.span) return g.B - 1u;
+  uint2 e = g.t1[(uint32_t)(d >> g.sh1)];
+  uint32_t sh = g.sh1;
+  if (e.x & GRID_SPLIT) {
+    e = g.t2[(e.y << GRID_BITS2) + ((uint32_t)(d >> g.sh2) & (GRID_NC2 - 1))];
+    sh = g.sh2;
+  }
+  const K off = d & (K)(((K)1 << sh) - 1);
+  const float t = __fmul_rn(key_to_float_rn(off), __uint_as_float(e.y));
+  return (e.x & 0xFFFFu) + min(__float2uint_rz(t), (e.x >> 16) & 0x7FFFu);
+}
+
 // ------------------------------------------------------------------ refinement levels
 // A segment of candidates.  Every key of the segment lies in [lo, hi]; its bin
 // is (key - lo) >> shift, shift chosen so that bins < NBIN.

@@ -206,7 +206,10 @@ __device__ void asg_build_from_knots(const K* sorted, const uint32_t* q, const f
                                      uint32_t Mreq, uint32_t B, uint32_t kind, Assigner<K>* A) {
   __shared__ K X[ASG_MAXM + 2];
   __shared__ uint32_t Bs[ASG_MAXM + 2];
+  __shared__ K XK[ASG_MAXM + 1];
   __shared__ uint32_t Ms;
+  for (uint32_t j = threadIdx.x; j <= Mreq; j += blockDim.x) XK[j] = sorted[q[j]];
+  __syncthreads();
   if (threadIdx.x == 0) {
     const float span = (float)(B - 2u);
     uint32_t m = 0;
@@ -215,7 +218,7 @@ __device__ void asg_build_from_knots(const K* sorted, const uint32_t* q, const f
     uint32_t atom_end_b = 0;
     bool atom = false;
     for (uint32_t j = 0; j <= Mreq; ++j) {
-      K xk = sorted[q[j]];
+      K xk = XK[j];
       float f = fminf(fmaxf(cdf[j], 0.0f), 1.0f);
       uint32_t b = 1u + (uint32_t)__float2uint_rn(f * span);
       if (j == 0) b = 1u;
@@ -297,79 +300,28 @@ __device__ __forceinline__ AsgView<K> asg_view_global(const Assigner<K>* A) {
   return v;
 }
 
-// Occupancy of the assigner's buckets on its own (sorted) sample, over 256
-// groups of buckets: max / mean.
-template <typename K>
-__device__ void asg_measure(const K* sorted, uint32_t S, Assigner<K>* A) {
-  __shared__ uint32_t g[256];
-  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) g[i] = 0;
-  __syncthreads();
-  AsgView<K> v = asg_view_global(A);
-  const uint32_t B = A->B;
-  for (uint32_t i = threadIdx.x; i < S; i += blockDim.x) {
-    uint32_t b = asg_eval(v, sorted[i]);
-    atomicAdd(&g[(uint32_t)(((uint64_t)b * 256u) / B)], 1u);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t mx = 0;
-    for (int i = 0; i < 256; ++i) mx = max(mx, g[i]);
-    A->quality = (float)mx / ((float)S / 256.0f);
-  }
-}
-
-// The reference's pivot rule (bucketMultiselect.cu:421-515, sizeOfSample = 1024,
-// numPivots = 17, endOffset = 22, pivotOffset = (1024 - 44) / 14 = 70):
-// pivots {min, s[21], s[21 + 70(i-1)] for i = 2..14, s[1001], max}, every
-// segment gets the same number of buckets.  The global min and max (a full
-// minmax pass in the reference) are replaced by the sample's extremes plus an
-// open tail bucket at each end.  For other sample sizes the offsets scale.
-template <typename K>
-__global__ void asg_build_sampled(const K* __restrict__ sorted, uint32_t S, uint32_t B,
-                                  Assigner<K>* A) {
-  __shared__ uint32_t q[17];
-  __shared__ float cdf[17];
-  if (threadIdx.x == 0) {
-    const uint32_t end_off = max(1u, (22u * S) / 1024u);
-    const uint32_t piv_off = (S - 2u * end_off) / 14u;
-    q[0] = 0;
-    q[1] = end_off - 1u;
-    for (uint32_t i = 2; i <= 14; ++i) q[i] = piv_off * (i - 1u) + end_off - 1u;
-    q[15] = S - end_off - 1u;
-    q[16] = S - 1u;
-    for (int i = 0; i <= 16; ++i) cdf[i] = (float)i / 16.0f;
-  }
-  __syncthreads();
-  asg_build_from_knots<K>(sorted, q, cdf, 16u, B, GGMS_ASSIGNER_SAMPLED, A);
-  __syncthreads();
-  asg_measure<K>(sorted, S, A);
-}
-
 // ------------------------------------------------------------------ level 0 (one vector)
 template <typename K>
-struct AsgSmem {
-  static constexpr size_t bytes =
-      sizeof(K) * (ASG_MAXM + 1) + 4 * (ASG_MAXM + 1) + 4 * ASG_MAXM + 2 * ASG_NCELL;
-};
-
-template <typename K>
-__device__ __forceinline__ AsgView<K> asg_to_smem(const Assigner<K>* __restrict__ A, uint8_t* sm) {
-  K* sx = (K*)sm;
-  uint32_t* sb = (uint32_t*)(sx + ASG_MAXM + 1);
-  float* ss = (float*)(sb + ASG_MAXM + 1);
-  uint16_t* si = (uint16_t*)(ss + ASG_MAXM);
-  const uint32_t M = A->M, nc = A->ncell;
-  for (uint32_t i = threadIdx.x; i <= M; i += blockDim.x) {
-    sx[i] = A->x[i];
-    sb[i] = A->base[i];
-    if (i < M) ss[i] = A->slope[i];
-  }
-  for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) si[i] = A->idx[i];
-  AsgView<K> v;
-  v.x = sx; v.base = sb; v.slope = ss; v.idx = si;
-  v.M = M; v.B = A->B; v.csh = A->csh;
+__device__ __forceinline__ GridView<K> grid_view_global(const Grid<K>* G) {
+  GridView<K> v;
+  v.t1 = G->t1; v.t2 = G->t2; v.lo = G->lo; v.span = G->span;
+  v.sh1 = G->sh1; v.sh2 = G->sh2; v.B = G->B;
   return v;
 }
+
+// Copy the grid into shared memory (t1: GRID_NC1 entries, t2: GRID_NSUB*GRID_NC2).
+template <typename K>
+__device__ __forceinline__ GridView<K> grid_to_smem(const Grid<K>* __restrict__ G, uint2* s1, uint2* s2) {
+  const uint32_t nc = G->ncell, ns = G->nsub * GRID_NC2;
+  for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) s1[i] = G->t1[i];
+  for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x) s2[i] = G->t2[i];
+  GridView<K> v;
+  v.t1 = s1; v.t2 = s2; v.lo = G->lo; v.span = G->span;
+  v.sh1 = G->sh1; v.sh2 = G->sh2; v.B = G->B;
+  return v;
+}
+
+constexpr size_t GRID_SMEM = sizeof(uint2) * (GRID_NC1 + GRID_NSUB * GRID_NC2);
 
 // 16-byte vector view of the input
 template <typename T> struct Vec16 {
@@ -383,84 +335,80 @@ __device__ __forceinline__ void unpack16(const uint4& q, T (&e)[Vec16<T>::N]) {
 }
 
 // PASS 1.  Persistent CTAs; each keeps a shared histogram of the B buckets and
-// flushes its non-zero bins once.  A warp whose 32 x (16-byte vector) all land
-// in one bucket (sorted or clustered data) adds once.
+// flushes its non-zero bins once.  Full rounds (every thread has UNROLL
+// 16-byte vectors) run branch-free; a warp whose 32 vectors all land in one
+// bucket (sorted or clustered data) adds once.
 template <typename T, int NT, int UNROLL>
 __global__ __launch_bounds__(NT) void l0_count(const T* __restrict__ in, uint64_t n,
-                                              const Assigner<typename KeyOf<T>::K>* __restrict__ As,
+                                              const Grid<typename KeyOf<T>::K>* __restrict__ Gs,
                                               const Counters* __restrict__ C,
                                               uint32_t* __restrict__ hist0) {
   using K = typename KeyOf<T>::K;
   constexpr int EPV = Vec16<T>::N;
   extern __shared__ __align__(16) uint8_t smem[];
-  const Assigner<K>* A = As + C->asg_choice;
-  const uint32_t B = A->B;
-  uint32_t* h = (uint32_t*)smem;
-  AsgView<K> av = asg_to_smem<K>(A, smem + (size_t)B * 4u);
+  const Grid<K>* G = Gs + C->asg_choice;
+  uint2* s1 = (uint2*)smem;
+  uint2* s2 = s1 + GRID_NC1;
+  uint32_t* h = (uint32_t*)(smem + GRID_SMEM);
+  const GridView<K> gv = grid_to_smem<K>(G, s1, s2);
+  const uint32_t B = gv.B;
   for (uint32_t i = threadIdx.x; i < B; i += NT) h[i] = 0u;
   __syncthreads();
 
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t gtid = (uint64_t)blockIdx.x * NT + threadIdx.x;
   const uint64_t gstride = (uint64_t)gridDim.x * NT;
-  const uintptr_t addr = (uintptr_t)in;
-  uint64_t head = ((16u - (uint32_t)(addr & 15u)) & 15u) / sizeof(T);
+  uint64_t head = ((16u - (uint32_t)((uintptr_t)in & 15u)) & 15u) / sizeof(T);
   if (head > n) head = n;
   const uint64_t nvec = (n - head) / EPV;
   const T* vbase = in + head;
+  const uint64_t rounds = nvec / (gstride * UNROLL);
 
-  for (uint64_t i0 = gtid; i0 < ((nvec + gstride - 1) / gstride) * gstride; i0 += gstride * UNROLL) {
+  uint64_t i0 = gtid;
+  for (uint64_t r = 0; r < rounds; ++r, i0 += gstride * UNROLL) {
     uint4 q[UNROLL];
 #pragma unroll
-    for (int u = 0; u < UNROLL; ++u) {
-      uint64_t i = i0 + (uint64_t)u * gstride;
-      if (i < nvec) q[u] = ld_stream16(vbase + i * EPV);
-    }
+    for (int u = 0; u < UNROLL; ++u) q[u] = ld_stream16(vbase + (i0 + (uint64_t)u * gstride) * EPV);
 #pragma unroll
     for (int u = 0; u < UNROLL; ++u) {
-      uint64_t i = i0 + (uint64_t)u * gstride;
-      const bool valid = i < nvec;
+      T e[EPV];
+      unpack16<T>(q[u], e);
       uint32_t b[EPV];
       bool same = true;
-      if (valid) {
-        T e[EPV];
-        unpack16<T>(q[u], e);
 #pragma unroll
-        for (int t = 0; t < EPV; ++t) {
-          b[t] = asg_eval<K>(av, KeyOf<T>::to(e[t]));
-          same = same && (b[t] == b[0]);
-        }
-      } else {
-        b[0] = 0u;
+      for (int t = 0; t < EPV; ++t) {
+        b[t] = grid_eval<K>(gv, KeyOf<T>::to(e[t]));
+        same = same && (b[t] == b[0]);
       }
-      const uint32_t vmask = __ballot_sync(FULL, valid);
-      if (vmask == 0u) continue;
-      const uint32_t b0 = __shfl_sync(FULL, b[0], __ffs(vmask) - 1);
-      const bool uni = __all_sync(FULL, !valid || (same && b[0] == b0));
-      if (uni) {
-        if (lane == (uint32_t)(__ffs(vmask) - 1)) atomicAdd(&h[b0], (uint32_t)(EPV * __popc(vmask)));
-      } else if (valid) {
-        if (same) {
-          atomicAdd(&h[b[0]], (uint32_t)EPV);
-        } else {
+      const uint32_t b0 = __shfl_sync(FULL, b[0], 0);
+      if (__all_sync(FULL, same && b[0] == b0)) {
+        if (lane == 0) atomicAdd(&h[b0], (uint32_t)(EPV * 32));
+      } else if (same) {
+        atomicAdd(&h[b[0]], (uint32_t)EPV);
+      } else {
 #pragma unroll
-          for (int t = 0; t < EPV; ++t) atomicAdd(&h[b[t]], 1u);
-        }
+        for (int t = 0; t < EPV; ++t) atomicAdd(&h[b[t]], 1u);
       }
     }
   }
-  // unaligned head and the tail that does not fill a vector
+  // the partial last round, then the unaligned head and the tail that does not fill a vector
+  for (uint64_t i = rounds * gstride * UNROLL + gtid; i < nvec; i += gstride) {
+    T e[EPV];
+    unpack16<T>(ld_stream16(vbase + i * EPV), e);
+#pragma unroll
+    for (int t = 0; t < EPV; ++t) atomicAdd(&h[grid_eval<K>(gv, KeyOf<T>::to(e[t]))], 1u);
+  }
   {
     const uint64_t tail0 = head + nvec * EPV;
     const uint64_t nscalar = head + (n - tail0);
     for (uint64_t j = gtid; j < nscalar; j += gstride) {
-      uint64_t idx = j < head ? j : tail0 + (j - head);
-      atomicAdd(&h[asg_eval<K>(av, KeyOf<T>::to(in[idx]))], 1u);
+      const uint64_t idx = j < head ? j : tail0 + (j - head);
+      atomicAdd(&h[grid_eval<K>(gv, KeyOf<T>::to(in[idx]))], 1u);
     }
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < B; i += NT) {
-    uint32_t v = h[i];
+    const uint32_t v = h[i];
     if (v) atomicAdd(&hist0[i], v);
   }
 }
@@ -499,7 +447,7 @@ __global__ void lvl_locate_rows(const uint32_t* __restrict__ rows, uint32_t row_
 // Active level-0 buckets -> refinement segments (or points).  One thread per bucket.
 template <typename K>
 __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __restrict__ aflag,
-                            uint32_t B, const Assigner<K>* __restrict__ As, Counters* C,
+                            uint32_t B, const Grid<K>* __restrict__ Gs, Counters* C,
                             uint32_t* cmap0, Seg<K>* segs1, uint32_t* cursor1, TileRef* tiles1,
                             K* points, Caps caps) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -508,8 +456,7 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
     cmap0[b] = CM_NONE;
     return;
   }
-  const Assigner<K>* A = As + C->asg_choice;
-  const AsgView<K> av = asg_view_global(A);
+  const GridView<K> gv = grid_view_global<K>(Gs + C->asg_choice);
   const uint32_t start = b ? I[b - 1] : 0u;
   const uint32_t cnt = I[b] - start;
   // key range of bucket b: [L(b), L(b+1) - 1], L(x) = smallest key with eval >= x
@@ -517,7 +464,7 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
     K lo = 0, hi = key_max<K>();
     while (lo < hi) {
       K mid = lo + ((hi - lo) >> 1);
-      if (asg_eval<K>(av, mid) >= target) hi = mid; else lo = mid + 1;
+      if (grid_eval<K>(gv, mid) >= target) hi = mid; else lo = mid + 1;
     }
     return lo;
   };
@@ -574,85 +521,114 @@ __global__ void lvl_relabel(const uint32_t* __restrict__ cmap, uint32_t row_len,
 }
 
 // PASS 2.  Copies the keys of refinement buckets into their segment's region
-// of the candidate buffer.  Slots are reserved per warp and per target segment.
+// of the candidate buffer.  A shared bitmask says which buckets are copied; a
+// warp takes the append path only if one of its lanes hit, and reserves slots
+// once per target segment.
+template <typename K>
+__device__ __forceinline__ void append_warp(bool hit, uint32_t b, K key, const uint32_t* __restrict__ cmap0,
+                                            const Seg<K>* __restrict__ segs1, uint32_t* cursor1, K* dst,
+                                            Counters* C, uint32_t lane) {
+  const uint32_t hm = __ballot_sync(FULL, hit);
+  if (!hit) return;
+  const uint32_t c = cmap0[b];
+  const uint32_t peers = __match_any_sync(hm, c);
+  const int leader = __ffs(peers) - 1;
+  uint32_t basepos = 0;
+  if ((int)lane == leader) basepos = atomicAdd(&cursor1[c], (uint32_t)__popc(peers));
+  basepos = __shfl_sync(peers, basepos, leader);
+  const uint32_t slot = basepos + __popc(peers & lanemask_lt());
+  const Seg<K>& sg = segs1[c];
+  if (slot < sg.cnt) dst[sg.off + slot] = key;
+  else set_status(C, GGMS_E_INTERNAL);
+}
+
+template <typename K>
+__device__ __forceinline__ void append_one(uint32_t b, K key, const uint32_t* __restrict__ cmap0,
+                                           const Seg<K>* __restrict__ segs1, uint32_t* cursor1, K* dst,
+                                           Counters* C) {
+  const uint32_t c = cmap0[b];
+  const uint32_t slot = atomicAdd(&cursor1[c], 1u);
+  const Seg<K>& sg = segs1[c];
+  if (slot < sg.cnt) dst[sg.off + slot] = key;
+  else set_status(C, GGMS_E_INTERNAL);
+}
+
 template <typename T, int NT, int UNROLL>
 __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint64_t n,
-                                                const Assigner<typename KeyOf<T>::K>* __restrict__ As,
-                                                const Counters* __restrict__ C,
-                                                const uint32_t* __restrict__ cmap0,
+                                                const Grid<typename KeyOf<T>::K>* __restrict__ Gs,
+                                                Counters* C, const uint32_t* __restrict__ cmap0,
                                                 const Seg<typename KeyOf<T>::K>* __restrict__ segs1,
                                                 uint32_t* cursor1, typename KeyOf<T>::K* dst) {
   using K = typename KeyOf<T>::K;
   constexpr int EPV = Vec16<T>::N;
   extern __shared__ __align__(16) uint8_t smem[];
-  const Assigner<K>* A = As + C->asg_choice;
-  const uint32_t B = A->B;
-  uint32_t* cm = (uint32_t*)smem;
-  AsgView<K> av = asg_to_smem<K>(A, smem + (size_t)B * 4u);
-  for (uint32_t i = threadIdx.x; i < B; i += NT) cm[i] = cmap0[i];
+  const Grid<K>* G = Gs + C->asg_choice;
+  uint2* s1 = (uint2*)smem;
+  uint2* s2 = s1 + GRID_NC1;
+  uint32_t* amask = (uint32_t*)(smem + GRID_SMEM);
+  const GridView<K> gv = grid_to_smem<K>(G, s1, s2);
+  const uint32_t B = gv.B;
+  const uint32_t lane = threadIdx.x & 31;
+  // bit b of the mask: bucket b is copied (a refinement segment, not a point)
+  for (uint32_t w = threadIdx.x >> 5; w < B / 32; w += NT / 32) {
+    const uint32_t bits = __ballot_sync(FULL, cmap0[w * 32 + lane] < CM_POINT);
+    if (lane == 0) amask[w] = bits;
+  }
   __syncthreads();
 
-  const uint32_t lane = threadIdx.x & 31;
   const uint64_t gtid = (uint64_t)blockIdx.x * NT + threadIdx.x;
   const uint64_t gstride = (uint64_t)gridDim.x * NT;
-  const uintptr_t addr = (uintptr_t)in;
-  uint64_t head = ((16u - (uint32_t)(addr & 15u)) & 15u) / sizeof(T);
+  uint64_t head = ((16u - (uint32_t)((uintptr_t)in & 15u)) & 15u) / sizeof(T);
   if (head > n) head = n;
   const uint64_t nvec = (n - head) / EPV;
   const T* vbase = in + head;
+  const uint64_t rounds = nvec / (gstride * UNROLL);
 
-  auto emit = [&](bool hit, uint32_t e, K key) {
-    const uint32_t hm = __ballot_sync(FULL, hit);
-    if (hm == 0u) return;
-    if (hit) {
-      const uint32_t peers = __match_any_sync(hm, e);
-      const int leader = __ffs(peers) - 1;
-      uint32_t basepos = 0;
-      if ((int)lane == leader) basepos = atomicAdd(&cursor1[e], (uint32_t)__popc(peers));
-      basepos = __shfl_sync(peers, basepos, leader);
-      const uint32_t slot = basepos + __popc(peers & lanemask_lt());
-      const Seg<K>& sg = segs1[e];
-      if (slot < sg.cnt) dst[sg.off + slot] = key;
-      else set_status(const_cast<Counters*>(C), GGMS_E_INTERNAL);
-    }
-  };
-
-  for (uint64_t i0 = gtid; i0 < ((nvec + gstride - 1) / gstride) * gstride; i0 += gstride * UNROLL) {
+  uint64_t i0 = gtid;
+  for (uint64_t r = 0; r < rounds; ++r, i0 += gstride * UNROLL) {
     uint4 q[UNROLL];
 #pragma unroll
-    for (int u = 0; u < UNROLL; ++u) {
-      uint64_t i = i0 + (uint64_t)u * gstride;
-      if (i < nvec) q[u] = ld_stream16(vbase + i * EPV);
-    }
+    for (int u = 0; u < UNROLL; ++u) q[u] = ld_stream16(vbase + (i0 + (uint64_t)u * gstride) * EPV);
 #pragma unroll
     for (int u = 0; u < UNROLL; ++u) {
-      uint64_t i = i0 + (uint64_t)u * gstride;
-      const bool valid = i < nvec;
       T e[EPV];
-      if (valid) unpack16<T>(q[u], e);
+      unpack16<T>(q[u], e);
+      K key[EPV];
+      uint32_t b[EPV];
+      bool any = false;
 #pragma unroll
       for (int t = 0; t < EPV; ++t) {
-        K key = valid ? KeyOf<T>::to(e[t]) : (K)0;
-        uint32_t c = valid ? cm[asg_eval<K>(av, key)] : CM_NONE;
-        emit(valid && c < CM_POINT, c, key);
+        key[t] = KeyOf<T>::to(e[t]);
+        b[t] = grid_eval<K>(gv, key[t]);
+        any |= (amask[b[t] >> 5] >> (b[t] & 31)) & 1u;
       }
+      if (__any_sync(FULL, any)) {
+#pragma unroll
+        for (int t = 0; t < EPV; ++t) {
+          const bool hit = (amask[b[t] >> 5] >> (b[t] & 31)) & 1u;
+          append_warp<K>(hit, b[t], key[t], cmap0, segs1, cursor1, dst, C, lane);
+        }
+      }
+    }
+  }
+  for (uint64_t i = rounds * gstride * UNROLL + gtid; i < nvec; i += gstride) {
+    T e[EPV];
+    unpack16<T>(ld_stream16(vbase + i * EPV), e);
+#pragma unroll
+    for (int t = 0; t < EPV; ++t) {
+      const K key = KeyOf<T>::to(e[t]);
+      const uint32_t b = grid_eval<K>(gv, key);
+      if ((amask[b >> 5] >> (b & 31)) & 1u) append_one<K>(b, key, cmap0, segs1, cursor1, dst, C);
     }
   }
   {
     const uint64_t tail0 = head + nvec * EPV;
     const uint64_t nscalar = head + (n - tail0);
-    const uint64_t rounds = (nscalar + gstride - 1) / gstride;
-    for (uint64_t r = 0; r < rounds; ++r) {
-      uint64_t j = gtid + r * gstride;
-      bool valid = j < nscalar;
-      K key = 0;
-      uint32_t c = CM_NONE;
-      if (valid) {
-        uint64_t idx = j < head ? j : tail0 + (j - head);
-        key = KeyOf<T>::to(in[idx]);
-        c = cm[asg_eval<K>(av, key)];
-      }
-      emit(valid && c < CM_POINT, c, key);
+    for (uint64_t j = gtid; j < nscalar; j += gstride) {
+      const uint64_t idx = j < head ? j : tail0 + (j - head);
+      const K key = KeyOf<T>::to(in[idx]);
+      const uint32_t b = grid_eval<K>(gv, key);
+      if ((amask[b >> 5] >> (b & 31)) & 1u) append_one<K>(b, key, cmap0, segs1, cursor1, dst, C);
     }
   }
 }

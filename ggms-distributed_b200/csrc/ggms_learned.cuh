@@ -20,7 +20,7 @@
 //
 // MLP-CDF model (1-32-32-1, monotone): see ggms_mlp.cuh.
 #pragma once
-#include "ggms_kernels.cuh"
+#include "ggms_setup.cuh"
 
 namespace ggms {
 
@@ -33,11 +33,9 @@ struct PLStats {                 // per segment, in double for a stable sum
 };
 
 struct LearnState {
-  float theta[PL_M];             // PL parameters
-  float m1[PL_M], m2[PL_M];      // Adam moments
-  float grad[PL_M];              // last gradient w.r.t. theta
-  float cdf[PL_M + 1];           // trained CDF at the knots
-  PLStats stats[PL_M];
+  float theta[PL_M];             // trained PL parameters
+  float grad[PL_M];              // gradient at the trained parameters
+  float cdf[PL_M + 1];           // trained CDF at the knots (MLP: its values at the knots)
   float loss_init;               // loss before training
   float loss;                    // loss after training
   float imbalance;               // max/mean of the compiled model on the sample
@@ -55,200 +53,147 @@ __device__ __forceinline__ float softplusf(float x) {
 }
 __device__ __forceinline__ float sigmoidf_(float x) { return 1.0f / (1.0f + expf(-x)); }
 
-// Quantile knots: q_j = round(j * (S - 1) / M), initial CDF j / M.
+// ------------------------------------------------------------------ statistics
+// Per-segment sufficient statistics of the sorted sample; warp w handles
+// segments w, w + nwarps, ... (fixed summation order: deterministic).
 template <typename K>
-__global__ void pl_init_knots(const K* __restrict__ sorted, uint32_t S, uint32_t B,
-                              Assigner<K>* A) {
-  __shared__ uint32_t q[PL_M + 1];
-  __shared__ float cdf[PL_M + 1];
-  for (uint32_t j = threadIdx.x; j <= (uint32_t)PL_M; j += blockDim.x) {
-    q[j] = (uint32_t)(((uint64_t)j * (S - 1u) + PL_M / 2) / PL_M);
-    cdf[j] = (float)j / (float)PL_M;
-  }
-  __syncthreads();
-  asg_build_from_knots<K>(sorted, q, cdf, PL_M, B, GGMS_ASSIGNER_LEARNED_PL, A);
-}
-
-// Per-segment sufficient statistics of the sorted sample (deterministic: one
-// warp per segment, fixed summation order).
-template <typename K>
-__global__ void pl_stats(const K* __restrict__ sorted, uint32_t S, const Assigner<K>* __restrict__ A,
-                         LearnState* L) {
-  const uint32_t M = A->M;
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t lane = threadIdx.x & 31;
-  if (warp >= M) return;
-  // samples of segment j: x_j <= s < x_{j+1} (the last segment also takes s == x_M)
+__device__ void pl_stats_block(const K* __restrict__ sorted, uint32_t S, const K* x, uint32_t M,
+                               PLStats* st) {
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   auto lower = [&](K v) {
     uint32_t lo = 0, hi = S;
     while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (sorted[m] < v) lo = m + 1; else hi = m; }
     return lo;
   };
-  const K xj = A->x[warp], xn = A->x[warp + 1];
-  const uint32_t i0 = lower(xj);
-  const uint32_t i1 = (warp + 1 == M) ? S : lower(xn);
-  const float width = key_to_float_rn((K)(xn - xj));
-  double n = 0, su = 0, su2 = 0, sy = 0, syu = 0, sy2 = 0;
-  for (uint32_t i = i0 + lane; i < i1; i += 32) {
-    float u = fminf(__fdiv_rn(key_to_float_rn((K)(sorted[i] - xj)), width), 1.0f);
-    double y = ((double)i + 0.5) / (double)S;
-    n += 1.0; su += u; su2 += (double)u * u; sy += y; syu += y * u; sy2 += y * y;
-  }
+  for (uint32_t j = warp; j < M; j += nw) {
+    const K xj = x[j], xn = x[j + 1];
+    const uint32_t i0 = lower(xj);
+    const uint32_t i1 = (j + 1 == M) ? S : lower(xn);  // the last segment also takes s == x_M
+    const float width = key_to_float_rn((K)(xn - xj));
+    double n = 0, su = 0, su2 = 0, sy = 0, syu = 0, sy2 = 0;
+    for (uint32_t i = i0 + lane; i < i1; i += 32) {
+      const float u = fminf(__fdiv_rn(key_to_float_rn((K)(sorted[i] - xj)), width), 1.0f);
+      const double y = ((double)i + 0.5) / (double)S;
+      n += 1.0; su += u; su2 += (double)u * u; sy += y; syu += y * u; sy2 += y * y;
+    }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    n += __shfl_xor_sync(FULL, n, o);
-    su += __shfl_xor_sync(FULL, su, o);
-    su2 += __shfl_xor_sync(FULL, su2, o);
-    sy += __shfl_xor_sync(FULL, sy, o);
-    syu += __shfl_xor_sync(FULL, syu, o);
-    sy2 += __shfl_xor_sync(FULL, sy2, o);
+    for (int o = 16; o > 0; o >>= 1) {
+      n += __shfl_xor_sync(FULL, n, o);
+      su += __shfl_xor_sync(FULL, su, o);
+      su2 += __shfl_xor_sync(FULL, su2, o);
+      sy += __shfl_xor_sync(FULL, sy, o);
+      syu += __shfl_xor_sync(FULL, syu, o);
+      sy2 += __shfl_xor_sync(FULL, sy2, o);
+    }
+    if (lane == 0) st[j] = PLStats{n, su, su2, sy, syu, sy2};
   }
-  if (lane == 0) L->stats[warp] = PLStats{n, su, su2, sy, syu, sy2};
 }
 
-// Forward + backward of the PL model on the statistics, one warp, M <= 256,
-// in double (the loss is a small difference of O(n) sums).  Returns the loss;
-// fills g (gradient w.r.t. theta) and, if asked, the CDF at the knots.
-// Lane l owns segments [l*PER, l*PER + PER).
-__device__ float pl_forward_backward(const float* theta, const PLStats* st, uint32_t M, double S,
-                                     float* g, float* cdf_out) {
-  constexpr int PER = PL_M / 32;
-  const uint32_t lane = threadIdx.x & 31;
-  double d[PER], P[PER];
-  double local = 0.0;
+// ------------------------------------------------------------------ forward / backward
+// Run by the first PL_M threads only (8 warps), synchronised with named
+// barrier 1 so the rest of the CTA can wait elsewhere.  Thread j owns segment j.
+constexpr int PL_NT = PL_M;
+__device__ __forceinline__ void bar_pl() { asm volatile("bar.sync 1, %0;" ::"n"(PL_NT) : "memory"); }
+
+struct PLRed {
+  double a[PL_NT / 32], b[PL_NT / 32], c[PL_NT / 32];
+};
+
+// Returns the loss; *g = d loss / d theta_j; cdf_out (if given) gets P_j / D and 1 at M.
+__device__ float pl_fb(float theta, const PLStats* st, uint32_t M, double S, PLRed& red, float* g,
+                       float* cdf_out) {
+  const uint32_t j = threadIdx.x, lane = j & 31, warp = j >> 5;
+  constexpr int NW = PL_NT / 32;
+  const bool act = j < M;
+  const double d = act ? (double)softplusf(theta) : 0.0;
+  // P_j = sum_{t<j} d_t, D = sum d
+  double inc = warp_incl_scan(d, lane);
+  if (lane == 31) red.a[warp] = inc;
+  bar_pl();
+  double P = inc - d, D = 0.0;
 #pragma unroll
-  for (int u = 0; u < PER; ++u) {
-    uint32_t j = lane * PER + u;
-    d[u] = j < M ? (double)softplusf(theta[j]) : 0.0;
-    local += d[u];
+  for (int w = 0; w < NW; ++w) {
+    const double t = red.a[w];
+    if (w < (int)warp) P += t;
+    D += t;
   }
-  double incl = local;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    double t = __shfl_up_sync(FULL, incl, o);
-    if ((int)lane >= o) incl += t;
-  }
-  const double D = __shfl_sync(FULL, incl, 31);
-  double run = incl - local;
-#pragma unroll
-  for (int u = 0; u < PER; ++u) { P[u] = run; run += d[u]; }
-  double R[PER], U[PER];
-  double Q = 0.0, loss = 0.0;
+  bar_pl();
   const double invD = 1.0 / D;
-#pragma unroll
-  for (int u = 0; u < PER; ++u) {
-    uint32_t j = lane * PER + u;
-    R[u] = 0.0; U[u] = 0.0;
-    if (j >= M) continue;
+  double R = 0, U = 0, Qc = 0, Lc = 0;
+  if (act) {
     const PLStats s = st[j];
-    const double p = P[u] * invD, dd = d[u] * invD;
-    // F_i = p + dd * u_i ;  r_i = F_i - y_i
-    R[u] = s.n * p + dd * s.su - s.sy;
-    U[u] = p * s.su + dd * s.su2 - s.syu;
+    const double p = P * invD, dd = d * invD;
+    // F_i = p + dd u_i ;  r_i = F_i - y_i
+    R = s.n * p + dd * s.su - s.sy;
+    U = p * s.su + dd * s.su2 - s.syu;
     const double sF2 = s.n * p * p + 2.0 * p * dd * s.su + dd * dd * s.su2;
     const double sFy = p * s.sy + dd * s.syu;
-    Q += sF2 - sFy;
-    loss += sF2 - 2.0 * sFy + s.sy2;
+    Qc = sF2 - sFy;
+    Lc = sF2 - 2.0 * sFy + s.sy2;
+    if (cdf_out) cdf_out[j] = (float)p;
   }
+  // suffix of R and totals of Qc, Lc
+  double rin = warp_incl_scan(R, lane);
+  double q = Qc, l = Lc;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    Q += __shfl_xor_sync(FULL, Q, o);
-    loss += __shfl_xor_sync(FULL, loss, o);
+    q += __shfl_xor_sync(FULL, q, o);
+    l += __shfl_xor_sync(FULL, l, o);
   }
+  if (lane == 31) red.a[warp] = rin;
+  if (lane == 0) { red.b[warp] = q; red.c[warp] = l; }
+  bar_pl();
+  double before = rin, Rt = 0, Q = 0, L = 0;
+#pragma unroll
+  for (int w = 0; w < NW; ++w) {
+    const double t = red.a[w];
+    if (w < (int)warp) before += t;
+    Rt += t;
+    Q += red.b[w];
+    L += red.c[w];
+  }
+  bar_pl();
   // dF_i/d delta_t = (1{t < j_i} + u_i 1{t = j_i} - F_i) / D
-  double rl = 0.0;
-#pragma unroll
-  for (int u = 0; u < PER; ++u) rl += R[u];
-  double rin = rl;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    double t = __shfl_up_sync(FULL, rin, o);
-    if ((int)lane >= o) rin += t;
-  }
-  const double rtot = __shfl_sync(FULL, rin, 31);
-  double after = rtot - rin;  // sum of R over later lanes
-  const double scale = 2.0 / (S * D);
-#pragma unroll
-  for (int u = PER - 1; u >= 0; --u) {
-    uint32_t j = lane * PER + u;
-    if (j < M) {
-      double gd = scale * (after + U[u] - Q);
-      g[j] = (float)(gd * (double)sigmoidf_(theta[j]));
-      if (cdf_out) cdf_out[j] = (float)(P[u] * invD);
-    }
-    after += R[u];
-  }
-  if (cdf_out && lane == 0) cdf_out[M] = 1.0f;
-  return (float)(loss / S);
+  const double after = Rt - before;
+  if (act) *g = (float)((2.0 / (S * D)) * (after + U - Q) * (double)sigmoidf_(theta));
+  else *g = 0.0f;
+  if (cdf_out && j == 0) cdf_out[M] = 1.0f;
+  return (float)(L / S);
 }
 
-// Adam on theta, one warp.  lr and step count chosen by the host.
-__global__ void pl_train(LearnState* L, const uint32_t* __restrict__ Mp, uint32_t S, uint32_t steps,
-                         float lr) {
-  __shared__ float theta[PL_M], g[PL_M];
-  const uint32_t M = *Mp;
-  const uint32_t lane = threadIdx.x;
-  for (uint32_t j = lane; j < PL_M; j += 32) {
-    theta[j] = 0.5413248546f;  // softplus^-1(1): uniform increments = the quantile init
-    L->m1[j] = 0.0f;
-    L->m2[j] = 0.0f;
-  }
-  __syncwarp();
+// Adam on theta (thread j owns theta_j).  Returns the final loss.
+__device__ float pl_train_block(const PLStats* st, uint32_t M, uint32_t S, uint32_t steps, float lr,
+                                PLRed& red, float* cdf_out, float* loss0_out, float* theta_out,
+                                float* grad_out) {
+  float theta = 0.5413248546f;  // softplus^-1(1): uniform increments = the quantile init
+  float m1 = 0.0f, m2 = 0.0f, g = 0.0f;
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
   float b1t = 1.0f, b2t = 1.0f;
-  float loss0 = pl_forward_backward(theta, L->stats, M, (double)S, g, nullptr);
-  __syncwarp();
-  float loss = loss0;
+  float loss = pl_fb(theta, st, M, (double)S, red, &g, nullptr);
+  if (loss0_out && threadIdx.x == 0) *loss0_out = loss;
   for (uint32_t it = 0; it < steps; ++it) {
     b1t *= b1;
     b2t *= b2;
-    for (uint32_t j = lane; j < M; j += 32) {
-      float m1 = b1 * L->m1[j] + (1.0f - b1) * g[j];
-      float m2 = b2 * L->m2[j] + (1.0f - b2) * g[j] * g[j];
-      L->m1[j] = m1;
-      L->m2[j] = m2;
-      float mh = m1 / (1.0f - b1t), vh = m2 / (1.0f - b2t);
-      theta[j] -= lr * mh / (sqrtf(vh) + eps);
-    }
-    __syncwarp();
-    loss = pl_forward_backward(theta, L->stats, M, (double)S, g, nullptr);
-    __syncwarp();
+    m1 = b1 * m1 + (1.0f - b1) * g;
+    m2 = b2 * m2 + (1.0f - b2) * g * g;
+    theta -= lr * (m1 / (1.0f - b1t)) / (sqrtf(m2 / (1.0f - b2t)) + eps);
+    loss = pl_fb(theta, st, M, (double)S, red, &g, nullptr);
   }
-  pl_forward_backward(theta, L->stats, M, (double)S, g, L->cdf);
-  for (uint32_t j = lane; j < PL_M; j += 32) {
-    L->theta[j] = theta[j];
-    L->grad[j] = g[j];
-  }
-  if (lane == 0) {
-    L->loss_init = loss0;
-    L->loss = loss;
-    L->M = M;
-    L->steps = steps;
-  }
+  loss = pl_fb(theta, st, M, (double)S, red, &g, cdf_out);
+  if (theta_out && threadIdx.x < M) theta_out[threadIdx.x] = theta;
+  if (grad_out && threadIdx.x < M) grad_out[threadIdx.x] = g;
+  return loss;
 }
 
-// Gradient probe used by the tests: forward/backward at the given theta.
-__global__ void pl_grad_probe(LearnState* L, const float* __restrict__ theta_in, uint32_t M,
-                              uint32_t S, float* loss_out, float* grad_out) {
-  __shared__ float theta[PL_M], g[PL_M];
-  for (uint32_t j = threadIdx.x; j < PL_M; j += 32) theta[j] = j < M ? theta_in[j] : 0.0f;
-  __syncwarp();
-  float loss = pl_forward_backward(theta, L->stats, M, (double)S, g, nullptr);
-  __syncwarp();
-  for (uint32_t j = threadIdx.x; j < M; j += 32) grad_out[j] = g[j];
-  if (threadIdx.x == 0) *loss_out = loss;
-}
-
-// Compile trained CDF values at the knots into bases + slopes (same knots, same
-// cell table), with strictly increasing bases.
+// New bases (strictly increasing) and slopes of a PL assigner from CDF values
+// at its knots.  All threads call it.
 template <typename K>
-__global__ void pl_compile(const float* __restrict__ cdf, Assigner<K>* A, uint32_t kind) {
-  __shared__ uint32_t Bs[ASG_MAXM + 1];
+__device__ void pl_set_bases(const float* cdf, Assigner<K>* A, uint32_t* Bs, uint32_t kind) {
   const uint32_t M = A->M, B = A->B;
   if (threadIdx.x == 0) {
     const float span = (float)(B - 2u);
     for (uint32_t t = 0; t <= M; ++t) {
-      float f = fminf(fmaxf(cdf[t], 0.0f), 1.0f);
+      const float f = fminf(fmaxf(cdf[t], 0.0f), 1.0f);
       Bs[t] = 1u + __float2uint_rn(f * span);
     }
     Bs[0] = 1u;
@@ -262,26 +207,104 @@ __global__ void pl_compile(const float* __restrict__ cdf, Assigner<K>* A, uint32
   for (uint32_t t = threadIdx.x; t <= M; t += blockDim.x) {
     A->base[t] = Bs[t];
     if (t < M) {
-      float db = (float)(Bs[t + 1] - Bs[t]);
-      float dx = key_to_float_rn((K)(A->x[t + 1] - A->x[t]));
+      const float db = (float)(Bs[t + 1] - Bs[t]);
+      const float dx = key_to_float_rn((K)(A->x[t + 1] - A->x[t]));
       A->slope[t] = __fdiv_rn(db, dx);
     }
   }
+  __syncthreads();
 }
 
 template <typename K>
-__global__ void asg_measure_kernel(const K* __restrict__ sorted, uint32_t S, Assigner<K>* A) {
-  asg_measure<K>(sorted, S, A);
+struct LearnSmem {
+  SetupSmem<K> su;
+  PLStats st[PL_M];
+  PLRed red;
+  float cdf[PL_M + 1];
+  uint32_t Bs[ASG_MAXM + 1];
+  uint32_t q[PL_M + 1];
+  float qcdf[PL_M + 1];
+};
+
+// Quantile knots: q_j = round(j * (S - 1) / M), initial CDF j / M.
+template <typename K>
+__device__ void pl_knots(const K* sorted, uint32_t S, uint32_t B, uint32_t kind, Assigner<K>* A,
+                         LearnSmem<K>& sm) {
+  for (uint32_t j = threadIdx.x; j <= (uint32_t)PL_M; j += blockDim.x) {
+    sm.q[j] = (uint32_t)(((uint64_t)j * (S - 1u) + PL_M / 2) / PL_M);
+    sm.qcdf[j] = (float)j / (float)PL_M;
+  }
+  __syncthreads();
+  asg_build_from_knots<K>(sorted, sm.q, sm.qcdf, PL_M, B, kind, A);
+  __syncthreads();
 }
 
-// learned accepted if its imbalance is within the bound
+// Final stage shared by both learned models: compile the PL assigner A into
+// the grid G, measure it on the sample and decide learned vs sampled.
 template <typename K>
-__global__ void asg_choose(Assigner<K>* As, LearnState* L, float bound, uint32_t* choice) {
-  const float q = As[1].quality;
-  const uint32_t c = (q <= bound) ? 1u : 0u;
-  *choice = c;
-  L->choice = c;
-  L->imbalance = q;
+__device__ void learned_finish(const K* sorted, uint32_t S, uint32_t B, uint32_t kind, float bound,
+                               Assigner<K>* A, Grid<K>* G, LearnState* L, uint32_t* choice,
+                               LearnSmem<K>& sm) {
+  const AsgView<K> av = asg_copy<K>(A, sm.su.asg);
+  const GridView<K> gv = grid_compile<K>(av, B, kind, G, sm.su.s1, sm.su.s2, sm.su.cs);
+  const float qv = grid_measure<K>(gv, sorted, S, sm.su.hist256);
+  if (threadIdx.x == 0) {
+    G->quality = qv;
+    const uint32_t c = (qv <= bound) ? 1u : 0u;
+    *choice = c;
+    L->choice = c;
+    L->imbalance = qv;
+  }
+}
+
+// The whole learned-PL setup in one CTA: knots -> statistics -> training ->
+// bases -> grid -> occupancy -> choice (grid 1 if within the bound, else the
+// sampled grid 0 stays in use).
+template <typename K>
+__global__ __launch_bounds__(SETUP_NT) void setup_learned_pl(const K* __restrict__ sorted, uint32_t S,
+                                                            uint32_t B, uint32_t steps, float lr,
+                                                            float bound, Assigner<K>* A, Grid<K>* G,
+                                                            LearnState* L, uint32_t* choice) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
+  pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, A, sm);
+  const uint32_t M = A->M;
+  pl_stats_block<K>(sorted, S, A->x, M, sm.st);
+  __syncthreads();
+  if (threadIdx.x < PL_NT) {
+    const float loss = pl_train_block(sm.st, M, S, steps, lr, sm.red, sm.cdf, &L->loss_init,
+                                      L->theta, L->grad);
+    if (threadIdx.x == 0) {
+      L->loss = loss;
+      L->M = M;
+      L->steps = steps;
+    }
+  }
+  __syncthreads();
+  pl_set_bases<K>(sm.cdf, A, sm.Bs, GGMS_ASSIGNER_LEARNED_PL);
+  learned_finish<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, bound, A, G, L, choice, sm);
+}
+
+// Gradient probe (diagnostics): knots and statistics as above, then one
+// forward/backward at the given theta.
+template <typename K>
+__global__ __launch_bounds__(SETUP_NT) void pl_grad_probe(const K* __restrict__ sorted, uint32_t S,
+                                                         uint32_t B, const float* __restrict__ theta_in,
+                                                         Assigner<K>* A, float* loss_out,
+                                                         float* grad_out) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
+  pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, A, sm);
+  const uint32_t M = A->M;
+  pl_stats_block<K>(sorted, S, A->x, M, sm.st);
+  __syncthreads();
+  if (threadIdx.x < PL_NT) {
+    float g = 0.0f;
+    const float th = threadIdx.x < M ? theta_in[threadIdx.x] : 0.0f;
+    const float loss = pl_fb(th, sm.st, M, (double)S, sm.red, &g, nullptr);
+    if (threadIdx.x < M) grad_out[threadIdx.x] = g;
+    if (threadIdx.x == 0) *loss_out = loss;
+  }
 }
 
 }  // namespace ggms
@@ -292,23 +315,24 @@ namespace ggms {
 
 template <typename K>
 static int learn_and_choose(int kind, const K* sorted, uint32_t S, uint32_t B, int steps_opt,
-                            float bound, Assigner<K>* As, LearnState* L, uint32_t* choice,
-                            cudaStream_t st, long long* launches) {
-  pl_init_knots<K><<<1, 256, 0, st>>>(sorted, S, B, &As[1]);
-  *launches += 1;
+                            float bound, Assigner<K>* As, Grid<K>* Gs, LearnState* L,
+                            uint32_t* choice, cudaStream_t st, long long* launches) {
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(setup_learned_pl<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(LearnSmem<K>)) != cudaSuccess)
+      return GGMS_E_CUDA;
+    attr = true;
+  }
   if (kind == GGMS_ASSIGNER_LEARNED_MLP) {
-    int rc = mlp_fit_and_compile<K>(sorted, S, steps_opt, As, L, st, launches);
+    int rc = mlp_fit_and_compile<K>(sorted, S, B, steps_opt, bound, As, Gs, L, choice, st, launches);
     if (rc) return rc;
   } else {
     const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 64u;
-    pl_stats<K><<<(PL_M * 32 + 255) / 256, 256, 0, st>>>(sorted, S, &As[1], L);
-    pl_train<<<1, 32, 0, st>>>(L, &As[1].M, S, steps, 0.05f);
-    pl_compile<K><<<1, 256, 0, st>>>(L->cdf, &As[1], GGMS_ASSIGNER_LEARNED_PL);
-    *launches += 3;
+    setup_learned_pl<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, steps, 0.05f, bound,
+                                                                    &As[1], &Gs[1], L, choice);
+    *launches += 1;
   }
-  asg_measure_kernel<K><<<1, 1024, 0, st>>>(sorted, S, &As[1]);
-  asg_choose<K><<<1, 1, 0, st>>>(As, L, bound, choice);
-  *launches += 2;
   return cudaGetLastError() == cudaSuccess ? GGMS_OK : GGMS_E_CUDA;
 }
 

@@ -18,7 +18,6 @@
 #pragma once
 #include <cooperative_groups.h>
 
-#include "ggms_learned.cuh"
 
 namespace ggms {
 
@@ -209,7 +208,7 @@ mlp_train(const K* __restrict__ sorted, uint32_t S_n, const Assigner<K>* __restr
 
 // Initial parameters: hidden units of layer 1 step at the sample quantiles.
 template <typename K>
-__global__ void mlp_init(const K* __restrict__ sorted, uint32_t S_n, const Assigner<K>* __restrict__ A,
+__device__ void mlp_init(const K* __restrict__ sorted, uint32_t S_n, const Assigner<K>* __restrict__ A,
                          float* P) {
   const int tid = threadIdx.x;
   const K x0 = A->x[0], xM = A->x[A->M];
@@ -243,9 +242,8 @@ __global__ void mlp_init(const K* __restrict__ sorted, uint32_t S_n, const Assig
 
 // Evaluate the trained MLP at the knots of A and write the normalized CDF.
 template <typename K>
-__global__ void mlp_eval_knots(const float* __restrict__ P, const Assigner<K>* __restrict__ A,
-                               float* cdf) {
-  __shared__ float y[ASG_MAXM + 1];
+__device__ void mlp_eval_knots(const float* __restrict__ P, const Assigner<K>* __restrict__ A,
+                               float* y, float* cdf) {
   const uint32_t M = A->M;
   const K x0 = A->x[0];
   const float span = key_to_float_rn((K)(A->x[M] - x0));
@@ -265,31 +263,56 @@ __global__ void mlp_eval_knots(const float* __restrict__ P, const Assigner<K>* _
   }
   __syncthreads();
   const float lo = y[0], hi = y[M];
-  for (uint32_t j = threadIdx.x; j <= M; j += blockDim.x) {
-    float f = (hi > lo) ? (y[j] - lo) / (hi - lo) : (float)j / (float)(M ? M : 1);
-    if (j > 0 && hi > lo) f = fmaxf(f, 0.0f);
-    cdf[j] = f;
-  }
+  for (uint32_t j = threadIdx.x; j <= M; j += blockDim.x)
+    cdf[j] = (hi > lo) ? fmaxf((y[j] - lo) / (hi - lo), 0.0f) : (float)j / (float)(M ? M : 1);
+  __syncthreads();
 }
 
 template <typename K>
-static int mlp_fit_and_compile(const K* sorted, uint32_t S, int steps_opt, Assigner<K>* As,
-                               LearnState* L, cudaStream_t st, long long* launches) {
+__global__ __launch_bounds__(SETUP_NT) void setup_mlp_begin(const K* __restrict__ sorted, uint32_t S,
+                                                           uint32_t B, Assigner<K>* A, float* P) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
+  pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_MLP, A, sm);
+  mlp_init<K>(sorted, S, A, P);
+}
+
+template <typename K>
+__global__ __launch_bounds__(SETUP_NT) void setup_mlp_finish(const K* __restrict__ sorted, uint32_t S,
+                                                            uint32_t B, float bound, const float* P,
+                                                            Assigner<K>* A, Grid<K>* G, LearnState* L,
+                                                            uint32_t* choice) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
+  mlp_eval_knots<K>(P, A, (float*)sm.Bs, sm.cdf);
+  for (uint32_t j = threadIdx.x; j <= A->M; j += blockDim.x) L->cdf[j] = sm.cdf[j];
+  pl_set_bases<K>(sm.cdf, A, sm.Bs, GGMS_ASSIGNER_LEARNED_MLP);
+  learned_finish<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_MLP, bound, A, G, L, choice, sm);
+}
+
+template <typename K>
+static int mlp_fit_and_compile(const K* sorted, uint32_t S, uint32_t B, int steps_opt, float bound,
+                               Assigner<K>* As, Grid<K>* Gs, LearnState* L, uint32_t* choice,
+                               cudaStream_t st, long long* launches) {
   static bool attr_set = false;
   if (!attr_set) {
     if (cudaFuncSetAttribute(mlp_train<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(MlpSmem)) != cudaSuccess)
+                             (int)sizeof(MlpSmem)) != cudaSuccess ||
+        cudaFuncSetAttribute(setup_mlp_begin<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(LearnSmem<K>)) != cudaSuccess ||
+        cudaFuncSetAttribute(setup_mlp_finish<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(LearnSmem<K>)) != cudaSuccess)
       return GGMS_E_CUDA;
     attr_set = true;
   }
   const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 150u;
   float* P = L->mlp_params;
-  mlp_init<K><<<1, 256, 0, st>>>(sorted, S, &As[1], P);
+  setup_mlp_begin<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, &As[1], P);
   mlp_train<K><<<MLP_CTAS, MLP_NT, sizeof(MlpSmem), st>>>(sorted, S, &As[1], L, P, steps, 0.02f,
                                                           nullptr, nullptr, nullptr);
-  mlp_eval_knots<K><<<1, 256, 0, st>>>(P, &As[1], L->cdf);
-  pl_compile<K><<<1, 256, 0, st>>>(L->cdf, &As[1], GGMS_ASSIGNER_LEARNED_MLP);
-  *launches += 4;
+  setup_mlp_finish<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, bound, P, &As[1],
+                                                                  &Gs[1], L, choice);
+  *launches += 3;
   return cudaGetLastError() == cudaSuccess ? GGMS_OK : GGMS_E_CUDA;
 }
 

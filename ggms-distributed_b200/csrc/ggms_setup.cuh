@@ -1,0 +1,270 @@
+// ggms_setup.cuh -- building the level-0 bucket assigner on the device.
+//
+// Sample -> sort -> a piecewise-linear model (Assigner, knots at sample
+// quantiles) -> compiled into the Grid the two passes evaluate.  Everything
+// after the sort runs in ONE kernel of one CTA (1024 threads); nothing goes
+// back to the host.  The reference does the same job with a thrust sort of
+// 1024 samples and 17 single-element cudaMemcpy calls to the host
+// (DistributedSMOS/bucketMultiselect.cu:421-515).
+#pragma once
+#include "ggms_kernels.cuh"
+
+namespace ggms {
+
+constexpr int SETUP_NT = 1024;
+
+// ------------------------------------------------------------------ block helpers (1024 threads)
+template <typename V>
+__device__ __forceinline__ V warp_incl_scan(V v, uint32_t lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    V t = __shfl_up_sync(FULL, v, o);
+    if ((int)lane >= o) v += t;
+  }
+  return v;
+}
+
+// Exclusive scan over the block (each thread one value); returns the exclusive
+// prefix and writes the block total to *total.  `red` holds 33 V.
+template <typename V>
+__device__ V block_excl_scan(V v, V* red, V* total) {
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const V inc = warp_incl_scan(v, lane);
+  if (lane == 31) red[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    V w = lane < (blockDim.x >> 5) ? red[lane] : (V)0;
+    w = warp_incl_scan(w, lane);
+    red[lane] = w;  // inclusive warp totals
+  }
+  __syncthreads();
+  const V out = inc - v + (warp ? red[warp - 1] : (V)0);
+  const V tot = red[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  *total = tot;
+  return out;
+}
+
+template <typename V>
+__device__ V block_sum(V v, V* red) {
+  V tot;
+  block_excl_scan<V>(v, red, &tot);
+  return tot;
+}
+
+// ------------------------------------------------------------------ grid compilation
+// Resamples a monotone model (the PL assigner `a`) onto the grid.  Cells whose
+// bucket span is at least T (the smallest power of two >= 4x the mean span that
+// leaves at most GRID_NSUB such cells) are split into sub-cells.  Writes the
+// grid to `G` (global) and to the shared copies s1/s2.  All threads call it.
+template <typename K>
+struct CompileSmem {
+  uint32_t bnd[GRID_NC1 + 1];   // bucket at each cell boundary
+  uint32_t sub_of[GRID_NC1];    // sub-table index of a split cell
+  uint32_t cell_of[GRID_NSUB];  // cell of each sub-table
+  uint32_t hist[33];
+  uint32_t red[33];
+  uint32_t thresh;
+};
+
+template <typename K>
+__device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t kind, Grid<K>* G,
+                                    uint2* s1, uint2* s2, CompileSmem<K>& cs) {
+  const uint32_t tid = threadIdx.x, NT = blockDim.x;
+  const K lo = a.x[0];
+  const K hi = a.x[a.M];
+  const K span = (K)(hi - lo);
+  const int sh1 = max(0, bitlen(span) - GRID_BITS1);
+  const uint32_t nc = (uint32_t)(span >> sh1) + 1u;
+  const int sh2 = sh1 >= GRID_BITS2 ? sh1 - GRID_BITS2 : 0;
+  const bool splittable = sh1 >= GRID_BITS2;
+  for (uint32_t c = tid; c <= nc; c += NT) {
+    uint32_t b;
+    if (c < nc) b = asg_eval<K>(a, (K)(lo + ((K)c << sh1)));
+    else b = min(asg_eval<K>(a, hi) + 1u, B - 1u);
+    cs.bnd[c] = b;
+  }
+  if (tid < 33) cs.hist[tid] = 0;
+  __syncthreads();
+  // split threshold from a histogram of log2(span)
+  const uint32_t mean = max(1u, (B - 2u) / nc);
+  for (uint32_t c = tid; c < nc; c += NT) {
+    const uint32_t sp = cs.bnd[c + 1] - cs.bnd[c];
+    if (sp >= 4u * mean && splittable) atomicAdd(&cs.hist[bitlen(sp)], 1u);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t cum = 0, t = 33;
+    for (int k = 32; k >= 1; --k) {
+      if (cum + cs.hist[k] > (uint32_t)GRID_NSUB) break;
+      cum += cs.hist[k];
+      t = (uint32_t)k;
+    }
+    // cells with bitlen(span) >= t are split (t == 33: none)
+    cs.thresh = t;
+  }
+  __syncthreads();
+  const uint32_t thr = cs.thresh;
+  // deterministic sub-table indices: prefix over split flags in cell order (2 cells per thread)
+  uint32_t flags = 0;
+  for (uint32_t k = 0; k < 2; ++k) {
+    const uint32_t c = tid * 2 + k;
+    if (c < nc) {
+      const uint32_t sp = cs.bnd[c + 1] - cs.bnd[c];
+      if (splittable && sp >= 4u * mean && (uint32_t)bitlen(sp) >= thr) flags |= 1u << k;
+    }
+  }
+  uint32_t total = 0;
+  const uint32_t pre = block_excl_scan<uint32_t>(__popc(flags), cs.red, &total);
+  {
+    uint32_t idx = pre;
+    for (uint32_t k = 0; k < 2; ++k) {
+      const uint32_t c = tid * 2 + k;
+      if (c < nc) cs.sub_of[c] = ((flags >> k) & 1u) ? idx++ : 0xFFFFFFFFu;
+    }
+  }
+  __syncthreads();
+  const uint32_t nsub = min(total, (uint32_t)GRID_NSUB);
+  for (uint32_t c = tid; c < nc; c += NT)
+    if (cs.sub_of[c] < nsub) cs.cell_of[cs.sub_of[c]] = c;
+  __syncthreads();
+  const float inv_w1 = __uint_as_float((uint32_t)(127 - sh1) << 23);  // 2^-sh1, exact
+  const float inv_w2 = __uint_as_float((uint32_t)(127 - sh2) << 23);
+  for (uint32_t c = tid; c < nc; c += NT) {
+    const uint32_t b0 = cs.bnd[c], b1 = cs.bnd[c + 1];
+    const uint32_t sp = b1 - b0;
+    uint2 e;
+    const uint32_t si = cs.sub_of[c];
+    if (si < nsub) {
+      e.x = GRID_SPLIT | b0;
+      e.y = si;
+    } else {
+      e.x = b0 | ((sp ? sp - 1u : 0u) << 16);
+      e.y = __float_as_uint(__fmul_rn((float)sp, inv_w1));
+    }
+    s1[c] = e;
+    G->t1[c] = e;
+  }
+  // sub-cells of split cells
+  for (uint32_t i = tid; i < nsub * GRID_NC2; i += NT) {
+    const uint32_t si = i >> GRID_BITS2, s = i & (GRID_NC2 - 1);
+    const uint32_t c = cs.cell_of[si];
+    const K cell_lo = (K)(lo + ((K)c << sh1));
+    const K room = (K)(hi - cell_lo);  // sub-boundaries past hi (last cell only) take the cell's end
+    auto bnd_at = [&](uint32_t sb) -> uint32_t {
+      if (sb == (uint32_t)GRID_NC2) return cs.bnd[c + 1];
+      const K off = (K)sb << sh2;
+      return off > room ? cs.bnd[c + 1] : asg_eval<K>(a, (K)(cell_lo + off));
+    };
+    const uint32_t b0 = bnd_at(s);
+    const uint32_t b1 = bnd_at(s + 1);
+    const uint32_t sp = b1 - b0;
+    uint2 e;
+    e.x = b0 | ((sp ? sp - 1u : 0u) << 16);
+    e.y = __float_as_uint(__fmul_rn((float)sp, inv_w2));
+    s2[i] = e;
+    G->t2[i] = e;
+  }
+  if (tid == 0) {
+    G->lo = lo;
+    G->span = span;
+    G->sh1 = (uint32_t)sh1;
+    G->sh2 = (uint32_t)sh2;
+    G->B = B;
+    G->ncell = nc;
+    G->nsub = nsub;
+    G->kind = kind;
+    G->loss = 0.0f;
+  }
+  __syncthreads();
+  GridView<K> v;
+  v.t1 = s1; v.t2 = s2; v.lo = lo; v.span = span;
+  v.sh1 = (uint32_t)sh1; v.sh2 = (uint32_t)sh2; v.B = B;
+  return v;
+}
+
+// Occupancy of the grid's buckets on the (sorted) sample, over 256 groups of
+// buckets: max / mean.
+template <typename K>
+__device__ float grid_measure(const GridView<K>& g, const K* sorted, uint32_t S, uint32_t* hist256) {
+  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) hist256[i] = 0;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < S; i += blockDim.x) {
+    const uint32_t b = grid_eval<K>(g, sorted[i]);
+    atomicAdd(&hist256[(uint32_t)(((uint64_t)b * 256u) / g.B)], 1u);
+  }
+  __syncthreads();
+  uint32_t mx = 0;
+  for (uint32_t i = 0; i < 256; ++i) mx = max(mx, hist256[i]);
+  __syncthreads();
+  return (float)mx / ((float)S / 256.0f);
+}
+
+// Copy a PL assigner (global) into shared memory.
+template <typename K>
+struct AsgCopy {
+  K x[ASG_MAXM + 1];
+  uint32_t base[ASG_MAXM + 1];
+  float slope[ASG_MAXM];
+  uint16_t idx[ASG_NCELL];
+};
+
+template <typename K>
+__device__ AsgView<K> asg_copy(const Assigner<K>* A, AsgCopy<K>& c) {
+  const uint32_t M = A->M;
+  for (uint32_t i = threadIdx.x; i <= M; i += blockDim.x) {
+    c.x[i] = A->x[i];
+    c.base[i] = A->base[i];
+    if (i < M) c.slope[i] = A->slope[i];
+  }
+  for (uint32_t i = threadIdx.x; i < A->ncell; i += blockDim.x) c.idx[i] = A->idx[i];
+  __syncthreads();
+  AsgView<K> v;
+  v.x = c.x; v.base = c.base; v.slope = c.slope; v.idx = c.idx;
+  v.M = M; v.B = A->B; v.csh = A->csh;
+  return v;
+}
+
+template <typename K>
+struct SetupSmem {
+  AsgCopy<K> asg;
+  CompileSmem<K> cs;
+  uint2 s1[GRID_NC1];
+  uint2 s2[GRID_NSUB * GRID_NC2];
+  uint32_t hist256[256];
+};
+
+// The reference's pivot rule (bucketMultiselect.cu:421-515, sizeOfSample = 1024,
+// numPivots = 17, endOffset = 22, pivotOffset = (1024 - 44) / 14 = 70):
+// pivots {min, s[21], s[21 + 70(i-1)] for i = 2..14, s[1001], max}, every
+// segment gets the same number of buckets.  The global min and max (a full
+// minmax pass in the reference) are replaced by the sample's extremes plus an
+// open tail bucket at each end.  For other sample sizes the offsets scale.
+// One CTA: pivots -> PL assigner A -> grid G -> occupancy on the sample.
+template <typename K>
+__global__ __launch_bounds__(SETUP_NT) void setup_sampled(const K* __restrict__ sorted, uint32_t S,
+                                                         uint32_t B, Assigner<K>* A, Grid<K>* G) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  SetupSmem<K>& sm = *reinterpret_cast<SetupSmem<K>*>(smem);
+  __shared__ uint32_t q[17];
+  __shared__ float cdf[17];
+  if (threadIdx.x == 0) {
+    const uint32_t end_off = max(1u, (22u * S) / 1024u);
+    const uint32_t piv_off = (S - 2u * end_off) / 14u;
+    q[0] = 0;
+    q[1] = end_off - 1u;
+    for (uint32_t i = 2; i <= 14; ++i) q[i] = piv_off * (i - 1u) + end_off - 1u;
+    q[15] = S - end_off - 1u;
+    q[16] = S - 1u;
+    for (int i = 0; i <= 16; ++i) cdf[i] = (float)i / 16.0f;
+  }
+  __syncthreads();
+  asg_build_from_knots<K>(sorted, q, cdf, 16u, B, GGMS_ASSIGNER_SAMPLED, A);
+  __syncthreads();
+  const AsgView<K> av = asg_copy<K>(A, sm.asg);
+  const GridView<K> gv = grid_compile<K>(av, B, GGMS_ASSIGNER_SAMPLED, G, sm.s1, sm.s2, sm.cs);
+  const float qv = grid_measure<K>(gv, sorted, S, sm.hist256);
+  if (threadIdx.x == 0) G->quality = qv;
+}
+
+}  // namespace ggms
