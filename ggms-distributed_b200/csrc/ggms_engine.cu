@@ -148,11 +148,15 @@ struct Workspace {
   uint32_t* hist0;
   uint32_t* aflag0;
   uint32_t* cmap0;
+  uint32_t* crow;         // per-CTA bucket counts of PASS 1 -> per-CTA cursors of PASS 2
   Seg<K>* segs[2];
   uint32_t* cursor[2];
   TileRef* tiles[2];
   uint32_t* rows[2];
   uint32_t* aflag[2];
+  uint32_t* khead[2];     // per segment: head of its k list (small segments)
+  uint32_t* knext;        // per k: next k in its segment's list
+  uint32_t* smalls;       // ids of the small segments the current level created
   K* points;
   K* cand[2];
   void* out_dev;
@@ -166,6 +170,7 @@ struct Plan {
   uint32_t S;        // sample size
   uint32_t cap_seg;
   uint32_t cap_tiles;
+  uint32_t ncta;     // CTAs of the two passes (identical grids)
   int assigner;
   int train_steps;
   float bound;
@@ -191,8 +196,12 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
   size_t o_h0 = b.take(4ull * p.B);
   size_t o_a0 = b.take(4ull * (p.B / 32));
   size_t o_c0 = b.take(4ull * p.B);
-  size_t o_segs[2], o_cur[2], o_tiles[2], o_rows[2], o_af[2], o_cand[2];
+  size_t o_crow = b.take(4ull * p.B * (p.ncta ? p.ncta : 1));
+  size_t o_segs[2], o_cur[2], o_tiles[2], o_rows[2], o_af[2], o_cand[2], o_kh[2];
+  size_t o_knext = b.take(4ull * p.nk);
+  size_t o_smalls = b.take(4ull * p.cap_seg);
   for (int i = 0; i < 2; ++i) {
+    o_kh[i] = b.take(4ull * p.cap_seg);
     o_segs[i] = b.take(sizeof(Seg<K>) * p.cap_seg);
     o_cur[i] = b.take(4ull * p.cap_seg);
     o_tiles[i] = b.take(sizeof(TileRef) * p.cap_tiles);
@@ -219,6 +228,7 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
   w.hist0 = (uint32_t*)(base + o_h0);
   w.aflag0 = (uint32_t*)(base + o_a0);
   w.cmap0 = (uint32_t*)(base + o_c0);
+  w.crow = (uint32_t*)(base + o_crow);
   for (int i = 0; i < 2; ++i) {
     w.segs[i] = (Seg<K>*)(base + o_segs[i]);
     w.cursor[i] = (uint32_t*)(base + o_cur[i]);
@@ -226,7 +236,10 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
     w.rows[i] = (uint32_t*)(base + o_rows[i]);
     w.aflag[i] = (uint32_t*)(base + o_af[i]);
     w.cand[i] = (K*)(base + o_cand[i]);
+    w.khead[i] = (uint32_t*)(base + o_kh[i]);
   }
+  w.knext = (uint32_t*)(base + o_knext);
+  w.smalls = (uint32_t*)(base + o_smalls);
   w.points = (K*)(base + o_pts);
   w.out_dev = (void*)(base + o_out);
   return w;
@@ -256,6 +269,7 @@ static int make_plan(Plan* p, uint64_t n, uint32_t nk, const ggms_opts& o) {
   if (S == 0) S = (asg == GGMS_ASSIGNER_SAMPLED) ? 1024u : (1u << 16);
   if (S < 1024u || S > 65536u || (S & (S - 1))) return GGMS_E_INVALID_ARG;
   p->S = S;
+  p->ncta = 0;
   p->cap_seg = nk + 1;
   p->cap_tiles = (uint32_t)((n + TILE - 1) / TILE) + p->cap_seg;
   p->train_steps = o.train_steps > 0 ? o.train_steps : 0;
@@ -274,11 +288,13 @@ constexpr int MAX_LEVELS_64 = 6;
 template <typename T>
 static size_t l0_count_smem(uint32_t B) { return GRID_SMEM + (size_t)B * 4u; }
 template <typename T>
-static size_t l0_compact_smem(uint32_t B) { return GRID_SMEM + (size_t)(B / 32) * 4u; }
+static size_t l0_compact_smem(uint32_t B) { return GRID_SMEM + (MAX_B0 / 32) * 4u + (size_t)B * 4u; }
 
-// Launch shapes of the two passes: as many resident CTAs as fit, one wave.
+// The two passes must split the input among CTAs identically (PASS 2 writes
+// into per-CTA ranges sized by PASS 1), so both get the same grid: as many
+// CTAs as fit on every SM at once for the larger of the two.
 template <typename T>
-static int l0_grids(Context* c, uint32_t B, int* g_count, int* g_compact) {
+static int l0_ncta(Context* c, uint32_t B, uint32_t* ncta) {
   const size_t s1 = l0_count_smem<T>(B), s2 = l0_compact_smem<T>(B);
   GGMS_CU(cudaFuncSetAttribute(l0_count<T, L0_NT, L0_UNROLL>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
@@ -287,8 +303,7 @@ static int l0_grids(Context* c, uint32_t B, int* g_count, int* g_compact) {
   int o1 = 0, o2 = 0;
   GGMS_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, l0_count<T, L0_NT, L0_UNROLL>, L0_NT, s1));
   GGMS_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, l0_compact<T, L0_NT, L0_UNROLL>, L0_NT, s2));
-  *g_count = std::max(1, o1) * c->sms;
-  *g_compact = std::max(1, o2) * c->sms;
+  *ncta = (uint32_t)(std::max(1, std::min(o1, o2)) * c->sms);
   return GGMS_OK;
 }
 
@@ -299,6 +314,24 @@ static int setup_attrs() {
   GGMS_CU(cudaFuncSetAttribute(setup_sampled<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(SetupSmem<K>)));
   done = true;
+  return GGMS_OK;
+}
+
+constexpr int SS_NT = 512;
+
+template <typename K>
+static int launch_small_select(Context* ctx, const K* src, const Seg<K>* segs_q, const uint32_t* khead_q,
+                               const Workspace<K>& w, const Caps& caps, cudaStream_t st) {
+  static bool attr = false;
+  const size_t sm = SMALL_SMEM + (size_t)SS_GROUP * 256 * 4;
+  if (!attr) {
+    GGMS_CU(cudaFuncSetAttribute(small_select<K, SS_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sm));
+    attr = true;
+  }
+  ++ctx->launches;
+  small_select<K, SS_NT><<<ctx->sms * 2, SS_NT, sm, st>>>(src, segs_q, w.smalls, w.C, khead_q, w.knext,
+                                                          w.krank, w.kseg, w.kkey, caps.small_keys, caps);
   return GGMS_OK;
 }
 
@@ -321,11 +354,14 @@ static inline unsigned cdiv(uint64_t a, uint64_t b) { return (unsigned)((a + b -
 // ------------------------------------------------------------------ the single-vector path
 template <typename T>
 static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* ks, uint64_t nk64,
-                      T* out, const ggms_opts& o, cudaStream_t st) {
+                      T* out, const ggms_opts& o_in, cudaStream_t st, bool topk = false) {
   using K = typename KeyOf<T>::K;
   if (!d_in || n == 0 || n > 0xFFFFFFFFull || nk64 > 0x7FFFFFFFull) return GGMS_E_INVALID_ARG;
   if (nk64 == 0) return GGMS_OK;
-  if (!ks || !out) return GGMS_E_INVALID_ARG;
+  if ((!ks && !topk) || !out) return GGMS_E_INVALID_ARG;
+  if (topk && nk64 > n) return GGMS_E_INVALID_ARG;
+  ggms_opts o = o_in;
+  if (topk) o.ks_on_device = 1;  // no k array to upload
   if ((uintptr_t)d_in % sizeof(T) != 0) return GGMS_E_INVALID_ARG;
   const uint32_t nk = (uint32_t)nk64;
   if (!o.ks_on_device) {
@@ -336,11 +372,13 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   int rc = make_plan(&p, n, nk, o);
   if (rc) return rc;
   GGMS_CU(cudaSetDevice(ctx->device));
+  rc = l0_ncta<T>(ctx, p.B, &p.ncta);
+  if (rc) return rc;
   Workspace<K> w0 = layout<K>(p, sizeof(T), nullptr);
   rc = ensure_arena(ctx, w0.bytes);
   if (rc) return rc;
   Workspace<K> w = layout<K>(p, sizeof(T), ctx->arena);
-  const bool host_k = !o.ks_on_device, host_out = !o.out_on_device;
+  const bool host_k = !o.ks_on_device && !topk, host_out = !o.out_on_device;
   const size_t pin_bytes = (host_k ? 4ull * nk : 0) + (host_out ? sizeof(T) * nk : 0) + sizeof(Counters) + 64;
   rc = ensure_pinned(ctx, pin_bytes);
   if (rc) return rc;
@@ -349,18 +387,21 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   uint8_t* pin_k = pin + ((sizeof(Counters) + 63) & ~(size_t)63);
   uint8_t* pin_out = pin_k + (host_k ? ((4ull * nk + 63) & ~(size_t)63) : 0);
 
-  const Caps caps{p.cap_seg, p.cap_tiles, p.nk};
+  const Caps caps{p.cap_seg, p.cap_tiles, p.nk, (uint32_t)(SMALL_SMEM / sizeof(K))};
   cudaEvent_t* prof = prof_slot(ctx);
   prof_rec(prof, 0, st);
   GGMS_CU(cudaMemsetAsync(w.C, 0, sizeof(Counters), st));
   const uint32_t* d_k = ks;
-  if (host_k) {
+  if (host_k && !topk) {
     memcpy(pin_k, ks, 4ull * nk);
     GGMS_CU(cudaMemcpyAsync(w.kin, pin_k, 4ull * nk, cudaMemcpyHostToDevice, st));
     d_k = w.kin;
   }
   ++ctx->launches;
-  k_init_single<<<cdiv(nk, 256), 256, 0, st>>>(d_k, nk, n, w.krank, w.kseg, w.C);
+  if (topk)
+    k_init_topk<<<cdiv(nk, 256), 256, 0, st>>>(nk, n, w.krank, w.kseg);
+  else
+    k_init_single<<<cdiv(nk, 256), 256, 0, st>>>(d_k, nk, n, w.krank, w.kseg, w.C);
 
   // ---- level-0 assigner
   const uint32_t S = p.S;
@@ -393,15 +434,13 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   }
 
   // ---- PASS 1: count
-  int grid_c = 0, grid_p = 0;
-  rc = l0_grids<T>(ctx, p.B, &grid_c, &grid_p);
-  if (rc) return rc;
+  const int grid_c = (int)p.ncta;
   GGMS_CU(cudaMemsetAsync(w.hist0, 0, 4ull * p.B, st));
   GGMS_CU(cudaMemsetAsync(w.aflag0, 0, 4ull * (p.B / 32), st));
   prof_rec(prof, 1, st);
   ++ctx->launches;
   l0_count<T, L0_NT, L0_UNROLL><<<grid_c, L0_NT, l0_count_smem<T>(p.B), st>>>(d_in, n, w.grid, w.C,
-                                                                               w.hist0);
+                                                                               w.hist0, w.crow);
   prof_rec(prof, 2, st);
   ++ctx->launches;
   l0_scan<<<1, 1024, 0, st>>>(w.hist0, p.B, w.C);
@@ -410,16 +449,21 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
                                                    w.aflag0, p.B / 32, w.C);
   ++ctx->launches;
   l0_children<K><<<cdiv(p.B, 256), 256, 0, st>>>(w.hist0, w.aflag0, p.B, w.grid, w.C, w.cmap0,
-                                                   w.segs[1], w.cursor[1], w.tiles[1], w.points, caps);
+                                                   w.segs[1], w.cursor[1], w.tiles[1], w.points,
+                                                   w.khead[1], w.smalls, caps);
   ++ctx->launches;
   lvl_relabel<K><<<cdiv(nk, 256), 256, 0, st>>>(w.cmap0, p.B, nk, w.kbin, w.kseg, w.kkey,
-                                                  w.points, w.C);
+                                                  w.points, w.C, w.segs[1], w.khead[1], w.knext);
+  ++ctx->launches;
+  l0_bases<K><<<ctx->sms * 4, 256, 0, st>>>(w.crow, p.B, p.ncta, w.segs[1], w.C, caps);
   // ---- PASS 2: compact the buckets that still need refinement
   prof_rec(prof, 3, st);
   ++ctx->launches;
-  l0_compact<T, L0_NT, L0_UNROLL><<<grid_p, L0_NT, l0_compact_smem<T>(p.B), st>>>(
-      d_in, n, w.grid, w.C, w.cmap0, w.segs[1], w.cursor[1], w.cand[0]);
+  l0_compact<T, L0_NT, L0_UNROLL><<<grid_c, L0_NT, l0_compact_smem<T>(p.B), st>>>(
+      d_in, n, w.grid, w.C, w.cmap0, w.crow, w.cand[0], (uint64_t)n);
   prof_rec(prof, 4, st);
+  rc = launch_small_select<K>(ctx, w.cand[0], w.segs[1], w.khead[1], w, caps, st);
+  if (rc) return rc;
 
   // ---- refinement levels over candidates
   const int maxlev = (sizeof(K) == 4) ? MAX_LEVELS_32 : MAX_LEVELS_64;
@@ -440,14 +484,17 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
                                                      w.aflag[pp], NBIN_WORDS, w.C);
     ++ctx->launches;
     lvl_children<K, 1024><<<seg_grid, 1024, 0, st>>>(w.rows[pp], w.aflag[pp], w.segs[pp], w.C, pp,
-                                                     w.segs[q], w.cursor[q], w.tiles[q], w.points, caps);
+                                                     w.segs[q], w.cursor[q], w.tiles[q], w.points,
+                                                     w.khead[q], w.smalls, caps);
     ++ctx->launches;
     lvl_relabel<K><<<cdiv(nk, 256), 256, 0, st>>>(w.rows[pp], NBIN, nk, w.kbin, w.kseg, w.kkey,
-                                                    w.points, w.C);
+                                                    w.points, w.C, w.segs[q], w.khead[q], w.knext);
     if (l < maxlev) {
       ++ctx->launches;
       lvl_compact<K, LV_NT><<<lv_grid, LV_NT, 0, st>>>(src, w.segs[pp], w.tiles[pp], w.C, pp,
                                                        w.rows[pp], w.segs[q], w.cursor[q], dst, caps);
+      rc = launch_small_select<K>(ctx, dst, w.segs[q], w.khead[q], w, caps, st);
+      if (rc) return rc;
     }
   }
 
@@ -497,6 +544,25 @@ static int dropin(const T* d_vector, int length, const uint32_t* kVals, int numK
   ggms_opts o;
   ggms_default_opts(&o);
   return run_single<T>(c, d_vector, (uint64_t)length, kVals, (uint64_t)numKs, outputs, o, 0);
+}
+
+template <typename T>
+static int topk_call(ggms_context* cx, const T* d_in, int64_t n, int64_t K, T* out,
+                     const ggms_opts* opts, void* stream) {
+  if (n <= 0 || K <= 0) return GGMS_E_INVALID_ARG;
+  ggms_opts o;
+  ggms_default_opts(&o);
+  if (opts) {
+    if (opts->struct_size != (int32_t)sizeof(ggms_opts)) return GGMS_E_INVALID_ARG;
+    o = *opts;
+  }
+  Context* c = (Context*)cx;
+  if (!c) {
+    int rc = default_context(&c);
+    if (rc) return rc;
+  }
+  std::lock_guard<std::mutex> lk(c->mu);
+  return run_single<T>(c, d_in, (uint64_t)n, nullptr, (uint64_t)K, out, o, (cudaStream_t)stream, true);
 }
 
 template <typename T>
@@ -556,7 +622,7 @@ static int run_segmented(Context* ctx, const T* d_in, const int64_t* seg_off, in
   rc = ensure_arena(ctx, w0.bytes);
   if (rc) return rc;
   Workspace<K> w = layout<K>(p, sizeof(T), ctx->arena);
-  const Caps caps{p.cap_seg, p.cap_tiles, p.nk};
+  const Caps caps{p.cap_seg, p.cap_tiles, p.nk, (uint32_t)(SMALL_SMEM / sizeof(K))};
   GGMS_CU(cudaMemsetAsync(w.C, 0, sizeof(Counters), st));
   ++ctx->launches;
   k_init_seg<<<cdiv(nk, 256), 256, 0, st>>>(ks, nk, seg_off, k_off, nseg, w.krank, w.kseg, w.C);
@@ -587,21 +653,22 @@ static int run_segmented(Context* ctx, const T* d_in, const int64_t* seg_off, in
                                                      w.aflag[pp], NBIN_WORDS, w.C);
     ++ctx->launches;
     lvl_children<K, 1024><<<seg_grid, 1024, 0, st>>>(w.rows[pp], w.aflag[pp], w.segs[pp], w.C, pp,
-                                                     w.segs[q], w.cursor[q], w.tiles[q], w.points, caps);
+                                                     w.segs[q], w.cursor[q], w.tiles[q], w.points,
+                                                     w.khead[q], w.smalls, caps);
     ++ctx->launches;
     lvl_relabel<K><<<cdiv(nk, 256), 256, 0, st>>>(w.rows[pp], NBIN, nk, w.kbin, w.kseg, w.kkey,
-                                                    w.points, w.C);
+                                                    w.points, w.C, w.segs[q], w.khead[q], w.knext);
     if (l + 1 < maxlev) {
-      if (l == 0) {
-          ++ctx->launches;
-          lvl_compact<T, LV_NT><<<lv_grid, LV_NT, 0, st>>>(d_in, w.segs[pp], w.tiles[pp], w.C, pp,
-                                                           w.rows[pp], w.segs[q], w.cursor[q], dst, caps);
-        } else {
-          ++ctx->launches;
-          lvl_compact<K, LV_NT><<<lv_grid, LV_NT, 0, st>>>(w.cand[(l - 1) & 1], w.segs[pp], w.tiles[pp],
-                                                           w.C, pp, w.rows[pp], w.segs[q], w.cursor[q],
-                                                           dst, caps);
-        }
+      ++ctx->launches;
+      if (l == 0)
+        lvl_compact<T, LV_NT><<<lv_grid, LV_NT, 0, st>>>(d_in, w.segs[pp], w.tiles[pp], w.C, pp,
+                                                         w.rows[pp], w.segs[q], w.cursor[q], dst, caps);
+      else
+        lvl_compact<K, LV_NT><<<lv_grid, LV_NT, 0, st>>>(w.cand[(l - 1) & 1], w.segs[pp], w.tiles[pp],
+                                                         w.C, pp, w.rows[pp], w.segs[q], w.cursor[q],
+                                                         dst, caps);
+      rc = launch_small_select<K>(ctx, dst, w.segs[q], w.khead[q], w, caps, st);
+      if (rc) return rc;
     }
   }
   ++ctx->launches;
@@ -857,6 +924,17 @@ GGMS_EX(ggms_multiselect_f32_ex, float)
 GGMS_EX(ggms_multiselect_f64_ex, double)
 GGMS_EX(ggms_multiselect_u32_ex, uint32_t)
 GGMS_EX(ggms_multiselect_i32_ex, int32_t)
+
+#define GGMS_TOPK(NAME, T)                                                                   \
+  int NAME(ggms_context* ctx, const T* d_in, int64_t n, int64_t K, T* out,                  \
+           const ggms_opts* opts, void* stream) {                                            \
+    return topk_call<T>(ctx, d_in, n, K, out, opts, stream);                                 \
+  }
+
+GGMS_TOPK(ggms_topk_f32, float)
+GGMS_TOPK(ggms_topk_f64, double)
+GGMS_TOPK(ggms_topk_u32, uint32_t)
+GGMS_TOPK(ggms_topk_i32, int32_t)
 
 int ggms_multiselect_segmented_f32(ggms_context* ctx, const float* d_in, const int64_t* seg_off,
                                    int64_t nseg, const uint32_t* ks, const int64_t* k_off,

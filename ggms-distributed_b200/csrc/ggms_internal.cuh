@@ -170,29 +170,33 @@ __device__ __forceinline__ uint32_t asg_eval(const AsgView<K>& a, K key) {
 // ------------------------------------------------------------------ compiled grid assigner
 // What the two passes evaluate.  Any monotone key -> bucket model (the sampled
 // pivots or a learned CDF, both held as a piecewise-linear Assigner above) is
-// resampled onto a uniform grid of up to 2^11 cells over the sample's key range
-// [lo, lo + span]; the up-to-32 cells holding the most mass are split again into
-// 2^6 sub-cells.  A key costs one shared-memory lookup (two for a split cell),
-// one multiply and one clamp -- no search.  Keys below lo go to bucket 0, keys
-// above lo + span to bucket B-1 (open tails: no min/max pass is needed, unlike
-// the reference's thrust::minmax_element, DistributedSMOS/bucketMultiselect.cu:543-547).
+// resampled onto a uniform grid of up to 2^11 cells over the sample's key range,
+// with one extra cell below and above for the open tails (buckets 0 and B-1:
+// no min/max pass is needed, unlike the reference's thrust::minmax_element,
+// DistributedSMOS/bucketMultiselect.cu:543-547).  Keys are clamped into the
+// grid, so a key costs: two min/max, one shared-memory lookup (two in one of the
+// up-to-32 heaviest cells, which are split into 2^6 sub-cells), and an integer
+// interpolation b_c + (offset * (b_{c+1} - b_c)) >> shift -- exact, monotone by
+// construction, no search and no floating point.
 constexpr int GRID_BITS1 = 11;
-constexpr int GRID_NC1 = 1 << GRID_BITS1;       // level-1 cells
+constexpr int GRID_NC1 = 1 << GRID_BITS1;       // interior level-1 cells
+constexpr int GRID_T1 = GRID_NC1 + 2;           // + the two tail cells
 constexpr int GRID_BITS2 = 6;
 constexpr int GRID_NC2 = 1 << GRID_BITS2;       // sub-cells of a split cell
 constexpr int GRID_NSUB = 32;                   // split cells at most
 constexpr uint32_t GRID_SPLIT = 0x80000000u;    // entry flag: .y is a sub-table index
 
-// entry: .x = base (bits 0-15) | cap (bits 16-30) | GRID_SPLIT; .y = slope (float bits)
+// entry: .x = bucket at the cell's first key, .y = bucket at the next cell's
+// first key; or .x = GRID_SPLIT | ..., .y = sub-table index.
 template <typename K>
 struct Grid {
-  K lo;
-  K span;
+  K origin;                    // first key of cell 0
+  K gmax;                      // last key of the last cell (keys are clamped to [origin, gmax])
   uint32_t sh1, sh2, B, ncell, nsub, kind;
   float quality;               // max/mean occupancy on the sample (256 bucket groups)
   float loss;
   uint32_t pad[2];
-  uint2 t1[GRID_NC1];
+  uint2 t1[GRID_T1];
   uint2 t2[GRID_NSUB * GRID_NC2];
 };
 
@@ -200,15 +204,23 @@ template <typename K>
 struct GridView {
   const uint2* t1;
   const uint2* t2;
-  K lo, span;
+  K origin, gmax;
   uint32_t sh1, sh2, B;
 };
 
+// floor(off * span / 2^sh) for off < 2^sh, span < 2^16: monotone in off, < span.
+__device__ __forceinline__ uint32_t grid_lin(uint32_t off, uint32_t span, uint32_t sh) {
+  return (uint32_t)(((uint64_t)off * span) >> sh);
+}
+__device__ __forceinline__ uint32_t grid_lin(uint64_t off, uint32_t span, uint32_t sh) {
+  const uint32_t s = min(sh, 32u);  // keep the top 32 bits of the offset
+  return (uint32_t)((((uint64_t)(uint32_t)(off >> (sh - s))) * span) >> s);
+}
+
 template <typename K>
 __device__ __forceinline__ uint32_t grid_eval(const GridView<K>& g, K key) {
-  if (key < g.lo) return 0u;
-  const K d = (K)(key - g.lo);
-  if (d > g.span) return g.B - 1u;
+  const K kc = min(max(key, g.origin), g.gmax);
+  const K d = (K)(kc - g.origin);
   uint2 e = g.t1[(uint32_t)(d >> g.sh1)];
   uint32_t sh = g.sh1;
   if (e.x & GRID_SPLIT) {
@@ -216,8 +228,7 @@ __device__ __forceinline__ uint32_t grid_eval(const GridView<K>& g, K key) {
     sh = g.sh2;
   }
   const K off = d & (K)(((K)1 << sh) - 1);
-  const float t = __fmul_rn(key_to_float_rn(off), __uint_as_float(e.y));
-  return (e.x & 0xFFFFu) + min(__float2uint_rz(t), (e.x >> 16) & 0x7FFFu);
+  return e.x + grid_lin(off, e.y - e.x, sh);
 }
 
 // ------------------------------------------------------------------ refinement levels
@@ -230,7 +241,12 @@ struct Seg {
   uint32_t shift;
   K lo;
   K hi;
+  uint32_t small; // finished by small_select (in shared memory), not by another level
+  uint32_t pad;
 };
+
+constexpr uint32_t K_NIL = 0xFFFFFFFFu;        // end of a per-segment k list
+constexpr size_t SMALL_SMEM = 64 * 1024;         // keys of one small segment in shared memory (a power of two)
 
 struct TileRef {
   uint32_t seg;   // segment id in the level's list
@@ -247,8 +263,8 @@ struct Counters {
   uint32_t point0;            // of which single-key
   uint32_t levels_run;        // refinement levels that had work
   uint32_t max_bucket0;       // largest level-0 bucket
-  uint32_t small_segs;
-  uint32_t pad0;
+  uint32_t small_segs;        // segments finished in shared memory (all levels)
+  uint32_t nsmall;            // small segments created by the current level
   unsigned long long cand0;   // elements copied by the level-0 compaction
   unsigned long long refine_elems;
   uint32_t asg_choice;        // index of the assigner in use (0 sampled, 1 learned)
@@ -261,6 +277,7 @@ struct Caps {
   uint32_t segs;
   uint32_t tiles;
   uint32_t points;
+  uint32_t small_keys;        // a child with at most this many keys is finished by small_select
 };
 
 }  // namespace ggms

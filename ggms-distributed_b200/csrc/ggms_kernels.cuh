@@ -132,6 +132,14 @@ __global__ void k_init_single(const uint32_t* __restrict__ ks, uint32_t nk, uint
   k_seg[i] = 0;
 }
 
+// top-k: k_i = i + 1 (the (i+1)-th largest), i.e. ascending rank n - 1 - i
+__global__ void k_init_topk(uint32_t nk, uint64_t n, uint32_t* k_rank, uint32_t* k_seg) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nk) return;
+  k_rank[i] = (uint32_t)(n - 1u - i);
+  k_seg[i] = 0;
+}
+
 // ------------------------------------------------------------------ sampling
 template <typename T>
 __global__ void asg_sample(const T* __restrict__ in, uint64_t n, uint32_t S, uint64_t seed,
@@ -304,24 +312,24 @@ __device__ __forceinline__ AsgView<K> asg_view_global(const Assigner<K>* A) {
 template <typename K>
 __device__ __forceinline__ GridView<K> grid_view_global(const Grid<K>* G) {
   GridView<K> v;
-  v.t1 = G->t1; v.t2 = G->t2; v.lo = G->lo; v.span = G->span;
+  v.t1 = G->t1; v.t2 = G->t2; v.origin = G->origin; v.gmax = G->gmax;
   v.sh1 = G->sh1; v.sh2 = G->sh2; v.B = G->B;
   return v;
 }
 
-// Copy the grid into shared memory (t1: GRID_NC1 entries, t2: GRID_NSUB*GRID_NC2).
+// Copy the grid into shared memory (t1: GRID_T1 entries, t2: GRID_NSUB*GRID_NC2).
 template <typename K>
 __device__ __forceinline__ GridView<K> grid_to_smem(const Grid<K>* __restrict__ G, uint2* s1, uint2* s2) {
   const uint32_t nc = G->ncell, ns = G->nsub * GRID_NC2;
   for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) s1[i] = G->t1[i];
   for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x) s2[i] = G->t2[i];
   GridView<K> v;
-  v.t1 = s1; v.t2 = s2; v.lo = G->lo; v.span = G->span;
+  v.t1 = s1; v.t2 = s2; v.origin = G->origin; v.gmax = G->gmax;
   v.sh1 = G->sh1; v.sh2 = G->sh2; v.B = G->B;
   return v;
 }
 
-constexpr size_t GRID_SMEM = sizeof(uint2) * (GRID_NC1 + GRID_NSUB * GRID_NC2);
+constexpr size_t GRID_SMEM = sizeof(uint2) * (GRID_T1 + GRID_NSUB * GRID_NC2);
 
 // 16-byte vector view of the input
 template <typename T> struct Vec16 {
@@ -334,56 +342,53 @@ __device__ __forceinline__ void unpack16(const uint4& q, T (&e)[Vec16<T>::N]) {
   __builtin_memcpy(e, &q, 16);
 }
 
-// PASS 1.  Persistent CTAs; each keeps a shared histogram of the B buckets and
-// flushes its non-zero bins once.  Full rounds (every thread has UNROLL
-// 16-byte vectors) run branch-free; a warp whose 32 vectors all land in one
-// bucket (sorted or clustered data) adds once.
+// PASS 1.  Persistent CTAs; each keeps a shared histogram of the B buckets.
+// At the end a CTA adds its non-zero bins to the global histogram and writes
+// its whole row to crow[blockIdx][*] -- PASS 2 turns those rows into private
+// per-CTA write cursors, so it needs no global atomics.  Element -> CTA
+// assignment is a pure function of (n, grid, NT, UNROLL, input alignment), the
+// same in both passes.  A thread whose vector's elements share a bucket adds
+// once (sorted or clustered data).
 template <typename T, int NT, int UNROLL>
 __global__ __launch_bounds__(NT) void l0_count(const T* __restrict__ in, uint64_t n,
                                               const Grid<typename KeyOf<T>::K>* __restrict__ Gs,
                                               const Counters* __restrict__ C,
-                                              uint32_t* __restrict__ hist0) {
+                                              uint32_t* __restrict__ hist0, uint32_t* __restrict__ crow) {
   using K = typename KeyOf<T>::K;
   constexpr int EPV = Vec16<T>::N;
   extern __shared__ __align__(16) uint8_t smem[];
   const Grid<K>* G = Gs + C->asg_choice;
   uint2* s1 = (uint2*)smem;
-  uint2* s2 = s1 + GRID_NC1;
+  uint2* s2 = s1 + GRID_T1;
   uint32_t* h = (uint32_t*)(smem + GRID_SMEM);
   const GridView<K> gv = grid_to_smem<K>(G, s1, s2);
   const uint32_t B = gv.B;
   for (uint32_t i = threadIdx.x; i < B; i += NT) h[i] = 0u;
   __syncthreads();
 
-  const uint32_t lane = threadIdx.x & 31;
   const uint64_t gtid = (uint64_t)blockIdx.x * NT + threadIdx.x;
   const uint64_t gstride = (uint64_t)gridDim.x * NT;
   uint64_t head = ((16u - (uint32_t)((uintptr_t)in & 15u)) & 15u) / sizeof(T);
   if (head > n) head = n;
   const uint64_t nvec = (n - head) / EPV;
-  const T* vbase = in + head;
+  const uint4* vp = reinterpret_cast<const uint4*>(in + head) + gtid;
   const uint64_t rounds = nvec / (gstride * UNROLL);
 
-  uint64_t i0 = gtid;
-  for (uint64_t r = 0; r < rounds; ++r, i0 += gstride * UNROLL) {
+  for (uint64_t r = 0; r < rounds; ++r, vp += gstride * UNROLL) {
     uint4 q[UNROLL];
 #pragma unroll
-    for (int u = 0; u < UNROLL; ++u) q[u] = ld_stream16(vbase + (i0 + (uint64_t)u * gstride) * EPV);
+    for (int u = 0; u < UNROLL; ++u) q[u] = ld_stream16(vp + u * gstride);
 #pragma unroll
     for (int u = 0; u < UNROLL; ++u) {
       T e[EPV];
       unpack16<T>(q[u], e);
       uint32_t b[EPV];
+#pragma unroll
+      for (int t = 0; t < EPV; ++t) b[t] = grid_eval<K>(gv, KeyOf<T>::to(e[t]));
       bool same = true;
 #pragma unroll
-      for (int t = 0; t < EPV; ++t) {
-        b[t] = grid_eval<K>(gv, KeyOf<T>::to(e[t]));
-        same = same && (b[t] == b[0]);
-      }
-      const uint32_t b0 = __shfl_sync(FULL, b[0], 0);
-      if (__all_sync(FULL, same && b[0] == b0)) {
-        if (lane == 0) atomicAdd(&h[b0], (uint32_t)(EPV * 32));
-      } else if (same) {
+      for (int t = 1; t < EPV; ++t) same = same && (b[t] == b[0]);
+      if (same) {
         atomicAdd(&h[b[0]], (uint32_t)EPV);
       } else {
 #pragma unroll
@@ -392,6 +397,7 @@ __global__ __launch_bounds__(NT) void l0_count(const T* __restrict__ in, uint64_
     }
   }
   // the partial last round, then the unaligned head and the tail that does not fill a vector
+  const T* vbase = in + head;
   for (uint64_t i = rounds * gstride * UNROLL + gtid; i < nvec; i += gstride) {
     T e[EPV];
     unpack16<T>(ld_stream16(vbase + i * EPV), e);
@@ -407,8 +413,10 @@ __global__ __launch_bounds__(NT) void l0_count(const T* __restrict__ in, uint64_
     }
   }
   __syncthreads();
+  uint32_t* row = crow + (size_t)blockIdx.x * B;
   for (uint32_t i = threadIdx.x; i < B; i += NT) {
     const uint32_t v = h[i];
+    row[i] = v;
     if (v) atomicAdd(&hist0[i], v);
   }
 }
@@ -449,7 +457,7 @@ template <typename K>
 __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __restrict__ aflag,
                             uint32_t B, const Grid<K>* __restrict__ Gs, Counters* C,
                             uint32_t* cmap0, Seg<K>* segs1, uint32_t* cursor1, TileRef* tiles1,
-                            K* points, Caps caps) {
+                            K* points, uint32_t* khead1, uint32_t* smalls, Caps caps) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= B) return;
   if (!((aflag[b >> 5] >> (b & 31)) & 1u)) {
@@ -487,21 +495,30 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
   s.lo = lo;
   s.hi = hi;
   s.shift = (uint32_t)max(0, bitlen((K)(hi - lo)) - RADIX_BITS);
+  s.small = cnt <= caps.small_keys ? 1u : 0u;
+  s.pad = b;  // the level-0 bucket (l0_bases needs it)
   segs1[id] = s;
   cursor1[id] = 0u;
-  const uint32_t nt = (cnt + TILE - 1) / TILE;
-  const uint32_t t0 = atomicAdd(&C->ntiles[1], nt);
-  if (t0 + nt > caps.tiles || t0 + nt < t0) { set_status(C, GGMS_E_INTERNAL); cmap0[b] = CM_NONE; return; }
-  for (uint32_t t = 0; t < nt; ++t) tiles1[t0 + t] = TileRef{id, t};
+  khead1[id] = K_NIL;
   cmap0[b] = id;
   atomicAdd(&C->cand0, (unsigned long long)cnt);
+  if (s.small) {
+    const uint32_t si = atomicAdd(&C->nsmall, 1u);
+    if (si < caps.segs) smalls[si] = id; else set_status(C, GGMS_E_INTERNAL);
+    return;
+  }
+  const uint32_t nt = (cnt + TILE - 1) / TILE;
+  const uint32_t t0 = atomicAdd(&C->ntiles[1], nt);
+  if (t0 + nt > caps.tiles || t0 + nt < t0) { set_status(C, GGMS_E_INTERNAL); return; }
+  for (uint32_t t = 0; t < nt; ++t) tiles1[t0 + t] = TileRef{id, t};
 }
 
 // ks follow their bin: resolved (single key) or the id of the next segment.
 template <typename K>
 __global__ void lvl_relabel(const uint32_t* __restrict__ cmap, uint32_t row_len, uint32_t nk,
                             const uint32_t* __restrict__ k_bin, uint32_t* k_seg, K* k_key,
-                            const K* __restrict__ points, Counters* C) {
+                            const K* __restrict__ points, Counters* C,
+                            const Seg<K>* __restrict__ segs_q, uint32_t* khead_q, uint32_t* knext) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nk) return;
   const uint32_t s = k_seg[i];
@@ -517,61 +534,67 @@ __global__ void lvl_relabel(const uint32_t* __restrict__ cmap, uint32_t row_len,
     k_seg[i] = K_DONE;
   } else {
     k_seg[i] = e;
+    if (segs_q[e].small) knext[i] = atomicExch(&khead_q[e], i);  // lock-free push
   }
 }
 
-// PASS 2.  Copies the keys of refinement buckets into their segment's region
-// of the candidate buffer.  A shared bitmask says which buckets are copied; a
-// warp takes the append path only if one of its lanes hit, and reserves slots
-// once per target segment.
+// Per-CTA write cursors for PASS 2: for every level-0 child (a copied bucket
+// b), one warp turns column b of the per-CTA count rows into exclusive
+// prefixes plus the child's offset, in place.  CTA g of PASS 2 then owns the
+// slots [crow[g][b], crow[g][b] + its count) of bucket b.
 template <typename K>
-__device__ __forceinline__ void append_warp(bool hit, uint32_t b, K key, const uint32_t* __restrict__ cmap0,
-                                            const Seg<K>* __restrict__ segs1, uint32_t* cursor1, K* dst,
-                                            Counters* C, uint32_t lane) {
-  const uint32_t hm = __ballot_sync(FULL, hit);
-  if (!hit) return;
-  const uint32_t c = cmap0[b];
-  const uint32_t peers = __match_any_sync(hm, c);
-  const int leader = __ffs(peers) - 1;
-  uint32_t basepos = 0;
-  if ((int)lane == leader) basepos = atomicAdd(&cursor1[c], (uint32_t)__popc(peers));
-  basepos = __shfl_sync(peers, basepos, leader);
-  const uint32_t slot = basepos + __popc(peers & lanemask_lt());
-  const Seg<K>& sg = segs1[c];
-  if (slot < sg.cnt) dst[sg.off + slot] = key;
-  else set_status(C, GGMS_E_INTERNAL);
+__global__ void l0_bases(uint32_t* crow, uint32_t B, uint32_t ncta, const Seg<K>* __restrict__ segs1,
+                         const Counters* __restrict__ C, Caps caps) {
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const uint32_t ns = min(C->nsegs[1], caps.segs);
+  for (uint32_t id = warp; id < ns; id += (gridDim.x * blockDim.x) >> 5) {
+    const Seg<K> s = segs1[id];
+    const uint32_t b = s.pad;  // the level-0 bucket this child came from
+    uint64_t run = s.off;
+    for (uint32_t g0 = 0; g0 < ncta; g0 += 32) {
+      const uint32_t g = g0 + lane;
+      const uint32_t v = g < ncta ? crow[(size_t)g * B + b] : 0u;
+      uint32_t inc = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(FULL, inc, o);
+        if ((int)lane >= o) inc += t;
+      }
+      if (g < ncta) crow[(size_t)g * B + b] = (uint32_t)(run + inc - v);
+      run += __shfl_sync(FULL, inc, 31);
+    }
+  }
 }
 
-template <typename K>
-__device__ __forceinline__ void append_one(uint32_t b, K key, const uint32_t* __restrict__ cmap0,
-                                           const Seg<K>* __restrict__ segs1, uint32_t* cursor1, K* dst,
-                                           Counters* C) {
-  const uint32_t c = cmap0[b];
-  const uint32_t slot = atomicAdd(&cursor1[c], 1u);
-  const Seg<K>& sg = segs1[c];
-  if (slot < sg.cnt) dst[sg.off + slot] = key;
-  else set_status(C, GGMS_E_INTERNAL);
-}
+// PASS 2.  Re-reads the input with the same element -> CTA assignment as
+// PASS 1; a key whose bucket is copied goes to slot atomicAdd(&cur[b], 1) of
+// this CTA's private range (a shared-memory atomic: no global round trip).
+// A shared bitmask says which buckets are copied (not points, not inactive).
+constexpr uint32_t MAX_B0 = 1u << 15;
 
 template <typename T, int NT, int UNROLL>
 __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint64_t n,
                                                 const Grid<typename KeyOf<T>::K>* __restrict__ Gs,
                                                 Counters* C, const uint32_t* __restrict__ cmap0,
-                                                const Seg<typename KeyOf<T>::K>* __restrict__ segs1,
-                                                uint32_t* cursor1, typename KeyOf<T>::K* dst) {
+                                                const uint32_t* __restrict__ crow,
+                                                typename KeyOf<T>::K* dst, uint64_t dst_cap) {
   using K = typename KeyOf<T>::K;
   constexpr int EPV = Vec16<T>::N;
   extern __shared__ __align__(16) uint8_t smem[];
   const Grid<K>* G = Gs + C->asg_choice;
   uint2* s1 = (uint2*)smem;
-  uint2* s2 = s1 + GRID_NC1;
-  uint32_t* amask = (uint32_t*)(smem + GRID_SMEM);
+  uint2* s2 = s1 + GRID_T1;
+  uint32_t* amask = (uint32_t*)(smem + GRID_SMEM);  // [MAX_B0 / 32]
+  uint32_t* cur = amask + MAX_B0 / 32;               // [B]
   const GridView<K> gv = grid_to_smem<K>(G, s1, s2);
   const uint32_t B = gv.B;
   const uint32_t lane = threadIdx.x & 31;
-  // bit b of the mask: bucket b is copied (a refinement segment, not a point)
+  const uint32_t* myrow = crow + (size_t)blockIdx.x * B;
   for (uint32_t w = threadIdx.x >> 5; w < B / 32; w += NT / 32) {
-    const uint32_t bits = __ballot_sync(FULL, cmap0[w * 32 + lane] < CM_POINT);
+    const uint32_t b = w * 32 + lane;
+    const bool copied = cmap0[b] < CM_POINT;
+    if (copied) cur[b] = myrow[b];
+    const uint32_t bits = __ballot_sync(FULL, copied);
     if (lane == 0) amask[w] = bits;
   }
   __syncthreads();
@@ -581,36 +604,31 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
   uint64_t head = ((16u - (uint32_t)((uintptr_t)in & 15u)) & 15u) / sizeof(T);
   if (head > n) head = n;
   const uint64_t nvec = (n - head) / EPV;
-  const T* vbase = in + head;
+  const uint4* vp = reinterpret_cast<const uint4*>(in + head) + gtid;
   const uint64_t rounds = nvec / (gstride * UNROLL);
+  bool overflow = false;
+  auto put = [&](uint32_t b, K key) {
+    const uint32_t slot = atomicAdd(&cur[b], 1u);
+    if (slot < dst_cap) dst[slot] = key; else overflow = true;
+  };
 
-  uint64_t i0 = gtid;
-  for (uint64_t r = 0; r < rounds; ++r, i0 += gstride * UNROLL) {
+  for (uint64_t r = 0; r < rounds; ++r, vp += gstride * UNROLL) {
     uint4 q[UNROLL];
 #pragma unroll
-    for (int u = 0; u < UNROLL; ++u) q[u] = ld_stream16(vbase + (i0 + (uint64_t)u * gstride) * EPV);
+    for (int u = 0; u < UNROLL; ++u) q[u] = ld_stream16(vp + u * gstride);
 #pragma unroll
     for (int u = 0; u < UNROLL; ++u) {
       T e[EPV];
       unpack16<T>(q[u], e);
-      K key[EPV];
-      uint32_t b[EPV];
-      bool any = false;
 #pragma unroll
       for (int t = 0; t < EPV; ++t) {
-        key[t] = KeyOf<T>::to(e[t]);
-        b[t] = grid_eval<K>(gv, key[t]);
-        any |= (amask[b[t] >> 5] >> (b[t] & 31)) & 1u;
-      }
-      if (__any_sync(FULL, any)) {
-#pragma unroll
-        for (int t = 0; t < EPV; ++t) {
-          const bool hit = (amask[b[t] >> 5] >> (b[t] & 31)) & 1u;
-          append_warp<K>(hit, b[t], key[t], cmap0, segs1, cursor1, dst, C, lane);
-        }
+        const K key = KeyOf<T>::to(e[t]);
+        const uint32_t b = grid_eval<K>(gv, key);
+        if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
       }
     }
   }
+  const T* vbase = in + head;
   for (uint64_t i = rounds * gstride * UNROLL + gtid; i < nvec; i += gstride) {
     T e[EPV];
     unpack16<T>(ld_stream16(vbase + i * EPV), e);
@@ -618,7 +636,7 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
     for (int t = 0; t < EPV; ++t) {
       const K key = KeyOf<T>::to(e[t]);
       const uint32_t b = grid_eval<K>(gv, key);
-      if ((amask[b >> 5] >> (b & 31)) & 1u) append_one<K>(b, key, cmap0, segs1, cursor1, dst, C);
+      if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
     }
   }
   {
@@ -628,9 +646,10 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
       const uint64_t idx = j < head ? j : tail0 + (j - head);
       const K key = KeyOf<T>::to(in[idx]);
       const uint32_t b = grid_eval<K>(gv, key);
-      if ((amask[b >> 5] >> (b & 31)) & 1u) append_one<K>(b, key, cmap0, segs1, cursor1, dst, C);
+      if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
     }
   }
+  if (overflow) set_status(C, GGMS_E_INTERNAL);
 }
 
 // ------------------------------------------------------------------ refinement levels
@@ -649,6 +668,7 @@ __global__ void lvl_prep(uint32_t* rows, uint32_t* aflag, Counters* C, int p, Ca
   if (gt == 0) {
     C->nsegs[p ^ 1] = 0u;
     C->ntiles[p ^ 1] = 0u;
+    C->nsmall = 0u;
     if (ns) C->levels_run += 1u;
   }
 }
@@ -702,11 +722,13 @@ template <typename K, int NT>
 __global__ __launch_bounds__(NT) void lvl_children(uint32_t* rows, const uint32_t* __restrict__ aflag,
                                                   const Seg<K>* __restrict__ segs, Counters* C, int p,
                                                   Seg<K>* segs_q, uint32_t* cursor_q, TileRef* tiles_q,
-                                                  K* points, Caps caps) {
+                                                  K* points, uint32_t* khead_q, uint32_t* smalls,
+                                                  Caps caps) {
   constexpr int PER = NBIN / NT;
   const uint32_t ns = min(C->nsegs[p], caps.segs);
   for (uint32_t sid = blockIdx.x; sid < ns; sid += gridDim.x) {
     const Seg<K> s = segs[sid];
+    if (s.small) continue;  // finished by small_select
     uint32_t* I = rows + (size_t)sid * NBIN;
     const uint32_t* F = aflag + (size_t)sid * NBIN_WORDS;
     uint32_t out[PER];
@@ -736,13 +758,21 @@ __global__ __launch_bounds__(NT) void lvl_children(uint32_t* rows, const uint32_
       c.lo = blo;
       c.hi = bhi;
       c.shift = (uint32_t)max(0, bitlen((K)(bhi - blo)) - RADIX_BITS);
+      c.small = cnt <= caps.small_keys ? 1u : 0u;
+      c.pad = 0u;
       segs_q[id] = c;
       cursor_q[id] = 0u;
+      khead_q[id] = K_NIL;
+      out[u] = id;
+      if (c.small) {
+        const uint32_t si = atomicAdd(&C->nsmall, 1u);
+        if (si < caps.segs) smalls[si] = id; else set_status(C, GGMS_E_INTERNAL);
+        continue;
+      }
       const uint32_t nt = (cnt + TILE - 1) / TILE;
       const uint32_t t0 = atomicAdd(&C->ntiles[p ^ 1], nt);
       if (t0 + nt > caps.tiles || t0 + nt < t0) { set_status(C, GGMS_E_INTERNAL); continue; }
       for (uint32_t t = 0; t < nt; ++t) tiles_q[t0 + t] = TileRef{id, t};
-      out[u] = id;
     }
     __syncthreads();
 #pragma unroll
@@ -805,6 +835,147 @@ __global__ __launch_bounds__(NT) void lvl_compact(const InT* __restrict__ src,
 }
 
 
+
+// ------------------------------------------------------------------ small segments
+// One CTA finishes a whole small segment in shared memory: its keys (as
+// offsets from the segment's lo) are loaded once, then a radix select with
+// 8-bit digits runs for up to SS_GROUP ks at a time (one 256-bin histogram per
+// k, built from the keys that still match the k's prefix); a segment with more
+// than SS_SORT_ABOVE ks is bitonic-sorted in place once instead.  The ks of the
+// segment come from the lock-free list the relabel step built.
+constexpr int SS_GROUP = 16;
+constexpr int SS_MAXK = 256;
+constexpr int SS_SORT_ABOVE = 64;   // more ks than this in one segment: bitonic sort instead
+
+template <typename K, int NT>
+__global__ __launch_bounds__(NT) void small_select(const K* __restrict__ src,
+                                                  const Seg<K>* __restrict__ segs_q,
+                                                  const uint32_t* __restrict__ smalls,
+                                                  const Counters* __restrict__ C_,
+                                                  const uint32_t* __restrict__ khead_q,
+                                                  const uint32_t* __restrict__ knext,
+                                                  const uint32_t* __restrict__ k_rank, uint32_t* k_seg,
+                                                  K* k_key, uint32_t small_keys, Caps caps) {
+  Counters* C = const_cast<Counters*>(C_);
+  extern __shared__ __align__(16) uint8_t smem[];
+  K* vals = (K*)smem;
+  uint32_t* hist = (uint32_t*)(smem + SMALL_SMEM);           // [SS_GROUP][256]
+  __shared__ uint32_t kid[SS_MAXK];
+  __shared__ uint32_t nk_s, next_s;
+  __shared__ uint32_t rk[SS_GROUP];
+  __shared__ K pk[SS_GROUP];
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t ns = min(C->nsmall, caps.segs);
+  for (uint32_t t = blockIdx.x; t < ns; t += gridDim.x) {
+    const uint32_t id = smalls[t];
+    const Seg<K> s = segs_q[id];
+    const uint32_t cnt = min(s.cnt, small_keys);
+    if (s.cnt > small_keys) set_status(C, GGMS_E_INTERNAL);
+    for (uint32_t i = tid; i < cnt; i += NT) vals[i] = (K)(src[s.off + i] - s.lo);
+    const int bits = bitlen((K)(s.hi - s.lo));
+    const int rounds = (bits + 7) / 8;
+    bool sorted_seg = false;
+    if (tid == 0) next_s = khead_q[id];
+    __syncthreads();
+    while (next_s != K_NIL) {
+      __syncthreads();
+      if (tid == 0) {  // collect up to SS_MAXK ks from the list
+        uint32_t k = next_s, m = 0;
+        while (k != K_NIL && m < (uint32_t)SS_MAXK) { kid[m++] = k; k = knext[k]; }
+        nk_s = m;
+        next_s = k;
+      }
+      __syncthreads();
+      const uint32_t m = nk_s;
+      if (m > (uint32_t)SS_SORT_ABOVE) {
+        // many ks in one segment (e.g. a top-k): sort the segment once instead
+        if (!sorted_seg) {
+          uint32_t N = 1;
+          while (N < cnt) N <<= 1;
+          for (uint32_t i = cnt + tid; i < N; i += NT) vals[i] = key_max<K>();
+          __syncthreads();
+          for (uint32_t kk = 2; kk <= N; kk <<= 1) {
+            for (uint32_t jj = kk >> 1; jj > 0; jj >>= 1) {
+              for (uint32_t i = tid; i < N; i += NT) {
+                const uint32_t ixj = i ^ jj;
+                if (ixj > i) {
+                  const K a = vals[i], b = vals[ixj];
+                  if ((a > b) == ((i & kk) == 0)) { vals[i] = b; vals[ixj] = a; }
+                }
+              }
+              __syncthreads();
+            }
+          }
+          sorted_seg = true;
+        }
+        for (uint32_t j = tid; j < m; j += NT) {
+          const uint32_t k = kid[j];
+          const uint32_t r = k_rank[k];
+          if (r < cnt) k_key[k] = (K)(s.lo + vals[r]);
+          else set_status(C, GGMS_E_INTERNAL);
+          k_seg[k] = K_DONE;
+        }
+        __syncthreads();
+        continue;
+      }
+      for (uint32_t g0 = 0; g0 < m; g0 += SS_GROUP) {
+        const uint32_t g = min((uint32_t)SS_GROUP, m - g0);
+        if (tid < g) {
+          rk[tid] = k_rank[kid[g0 + tid]];
+          pk[tid] = 0;
+        }
+        for (int rd = rounds - 1; rd >= 0; --rd) {
+          const int sh = rd * 8;
+          for (uint32_t i = tid; i < g * 256; i += NT) hist[i] = 0u;
+          __syncthreads();
+          for (uint32_t i = tid; i < cnt; i += NT) {
+            const K v = vals[i];
+            for (uint32_t j = 0; j < g; ++j)
+              if ((((v ^ pk[j]) >> sh) >> 8) == 0) atomicAdd(&hist[j * 256 + (uint32_t)((v >> sh) & 255)], 1u);
+          }
+          __syncthreads();
+          if (warp < g) {  // warp j picks the digit holding rank rk[j]
+            const uint32_t j = warp;
+            uint32_t c8[8], sum = 0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) { c8[q] = hist[j * 256 + lane * 8 + q]; sum += c8[q]; }
+            uint32_t inc = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+              const uint32_t tt = __shfl_up_sync(FULL, inc, o);
+              if ((int)lane >= o) inc += tt;
+            }
+            const uint32_t r = rk[j];
+            const uint32_t before = inc - sum;
+            const bool mine = before <= r && r < inc;
+            const uint32_t who = __ballot_sync(FULL, mine);
+            if (mine) {
+              uint32_t cum = before, d = lane * 8;
+#pragma unroll
+              for (int q = 0; q < 8; ++q) {
+                if (r < cum + c8[q]) { d = lane * 8 + q; break; }
+                cum += c8[q];
+              }
+              rk[j] = r - cum;
+              pk[j] = pk[j] | ((K)d << sh);
+            }
+            if (who == 0 && lane == 0) set_status(C, GGMS_E_INTERNAL);  // rank beyond the segment
+          }
+          __syncthreads();
+        }
+        if (tid < g) {
+          const uint32_t k = kid[g0 + tid];
+          k_key[k] = (K)(s.lo + pk[tid]);
+          k_seg[k] = K_DONE;
+        }
+        __syncthreads();
+      }
+    }
+    if (tid == 0) atomicAdd(&C->small_segs, 1u);
+    __syncthreads();
+  }
+}
+
 // ------------------------------------------------------------------ batched segments
 // Level 0 of the batched mode: every caller segment that holds a k becomes a
 // radix segment over the whole key space (top 11 key bits first).
@@ -821,6 +992,8 @@ __global__ void seg_init(const int64_t* __restrict__ seg_off, uint32_t nseg,
   d.lo = 0;
   d.hi = key_max<K>();
   d.shift = (uint32_t)(KeyBits<K>::value - RADIX_BITS);
+  d.small = 0u;
+  d.pad = 0u;
   segs0[s] = d;
   if (b < a) set_status(C, GGMS_E_INVALID_ARG);
   if (k_off[s + 1] == k_off[s] || d.cnt == 0) return;  // nothing to select here

@@ -171,6 +171,9 @@ __device__ float pl_train_block(const PLStats* st, uint32_t M, uint32_t S, uint3
   float b1t = 1.0f, b2t = 1.0f;
   float loss = pl_fb(theta, st, M, (double)S, red, &g, nullptr);
   if (loss0_out && threadIdx.x == 0) *loss0_out = loss;
+  // keep the best parameters seen: the quantile init is already close to the
+  // optimum, so a step can overshoot; the result never loses to the init
+  float best = loss, best_theta = theta;
   for (uint32_t it = 0; it < steps; ++it) {
     b1t *= b1;
     b2t *= b2;
@@ -178,7 +181,12 @@ __device__ float pl_train_block(const PLStats* st, uint32_t M, uint32_t S, uint3
     m2 = b2 * m2 + (1.0f - b2) * g * g;
     theta -= lr * (m1 / (1.0f - b1t)) / (sqrtf(m2 / (1.0f - b2t)) + eps);
     loss = pl_fb(theta, st, M, (double)S, red, &g, nullptr);
+    if (loss < best) {  // the loss is block-uniform: every thread takes the same branch
+      best = loss;
+      best_theta = theta;
+    }
   }
+  theta = best_theta;
   loss = pl_fb(theta, st, M, (double)S, red, &g, cdf_out);
   if (theta_out && threadIdx.x < M) theta_out[threadIdx.x] = theta;
   if (grad_out && threadIdx.x < M) grad_out[threadIdx.x] = g;
@@ -329,7 +337,7 @@ static int learn_and_choose(int kind, const K* sorted, uint32_t S, uint32_t B, i
     if (rc) return rc;
   } else {
     const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 64u;
-    setup_learned_pl<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, steps, 0.05f, bound,
+    setup_learned_pl<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, steps, 0.01f, bound,
                                                                     &As[1], &Gs[1], L, choice);
     *launches += 1;
   }

@@ -71,11 +71,23 @@ template <typename K>
 __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t kind, Grid<K>* G,
                                     uint2* s1, uint2* s2, CompileSmem<K>& cs) {
   const uint32_t tid = threadIdx.x, NT = blockDim.x;
+  const K KMAX = key_max<K>();
   const K lo = a.x[0];
   const K hi = a.x[a.M];
   const K span = (K)(hi - lo);
   const int sh1 = max(0, bitlen(span) - GRID_BITS1);
-  const uint32_t nc = (uint32_t)(span >> sh1) + 1u;
+  const K w = (K)1 << sh1;
+  const uint32_t nc = (uint32_t)(span >> sh1) + 1u;        // interior cells
+  const bool has_lo = lo >= w;                              // room for a low tail cell
+  const bool has_hi = (K)(KMAX - lo) >= (K)((K)nc << sh1);  // room for a high tail cell
+  const uint32_t first = has_lo ? 1u : 0u;
+  const K origin = has_lo ? (K)(lo - w) : lo;
+  K gmax = KMAX;
+  if (has_hi) {
+    const K top = (K)(lo + ((K)nc << sh1));                 // first key of the high tail cell
+    gmax = ((K)(KMAX - top) >= (K)(w - 1)) ? (K)(top + (w - 1)) : KMAX;
+  }
+  const uint32_t ntot = first + nc + (has_hi ? 1u : 0u);
   const int sh2 = sh1 >= GRID_BITS2 ? sh1 - GRID_BITS2 : 0;
   const bool splittable = sh1 >= GRID_BITS2;
   for (uint32_t c = tid; c <= nc; c += NT) {
@@ -100,8 +112,7 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
       cum += cs.hist[k];
       t = (uint32_t)k;
     }
-    // cells with bitlen(span) >= t are split (t == 33: none)
-    cs.thresh = t;
+    cs.thresh = t;  // cells with bitlen(span) >= t are split (t == 33: none)
   }
   __syncthreads();
   const uint32_t thr = cs.thresh;
@@ -128,19 +139,17 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
   for (uint32_t c = tid; c < nc; c += NT)
     if (cs.sub_of[c] < nsub) cs.cell_of[cs.sub_of[c]] = c;
   __syncthreads();
-  const float inv_w1 = __uint_as_float((uint32_t)(127 - sh1) << 23);  // 2^-sh1, exact
-  const float inv_w2 = __uint_as_float((uint32_t)(127 - sh2) << 23);
-  for (uint32_t c = tid; c < nc; c += NT) {
-    const uint32_t b0 = cs.bnd[c], b1 = cs.bnd[c + 1];
-    const uint32_t sp = b1 - b0;
+  for (uint32_t c = tid; c < ntot; c += NT) {
     uint2 e;
-    const uint32_t si = cs.sub_of[c];
-    if (si < nsub) {
-      e.x = GRID_SPLIT | b0;
-      e.y = si;
+    if (c < first) {
+      e = make_uint2(0u, 0u);                                 // low tail: bucket 0
+    } else if (c >= first + nc) {
+      e = make_uint2(B - 1u, B - 1u);                         // high tail: bucket B-1
     } else {
-      e.x = b0 | ((sp ? sp - 1u : 0u) << 16);
-      e.y = __float_as_uint(__fmul_rn((float)sp, inv_w1));
+      const uint32_t i = c - first;
+      const uint32_t si = cs.sub_of[i];
+      if (si < nsub) e = make_uint2(GRID_SPLIT | cs.bnd[i], si);
+      else e = make_uint2(cs.bnd[i], cs.bnd[i + 1]);
     }
     s1[c] = e;
     G->t1[c] = e;
@@ -156,29 +165,24 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
       const K off = (K)sb << sh2;
       return off > room ? cs.bnd[c + 1] : asg_eval<K>(a, (K)(cell_lo + off));
     };
-    const uint32_t b0 = bnd_at(s);
-    const uint32_t b1 = bnd_at(s + 1);
-    const uint32_t sp = b1 - b0;
-    uint2 e;
-    e.x = b0 | ((sp ? sp - 1u : 0u) << 16);
-    e.y = __float_as_uint(__fmul_rn((float)sp, inv_w2));
+    const uint2 e = make_uint2(bnd_at(s), bnd_at(s + 1));
     s2[i] = e;
     G->t2[i] = e;
   }
   if (tid == 0) {
-    G->lo = lo;
-    G->span = span;
+    G->origin = origin;
+    G->gmax = gmax;
     G->sh1 = (uint32_t)sh1;
     G->sh2 = (uint32_t)sh2;
     G->B = B;
-    G->ncell = nc;
+    G->ncell = ntot;
     G->nsub = nsub;
     G->kind = kind;
     G->loss = 0.0f;
   }
   __syncthreads();
   GridView<K> v;
-  v.t1 = s1; v.t2 = s2; v.lo = lo; v.span = span;
+  v.t1 = s1; v.t2 = s2; v.origin = origin; v.gmax = gmax;
   v.sh1 = (uint32_t)sh1; v.sh2 = (uint32_t)sh2; v.B = B;
   return v;
 }
@@ -229,7 +233,7 @@ template <typename K>
 struct SetupSmem {
   AsgCopy<K> asg;
   CompileSmem<K> cs;
-  uint2 s1[GRID_NC1];
+  uint2 s1[GRID_T1];
   uint2 s2[GRID_NSUB * GRID_NC2];
   uint32_t hist256[256];
 };

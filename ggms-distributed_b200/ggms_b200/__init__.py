@@ -116,6 +116,10 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         fn = getattr(lib, f"ggms_multiselect_{suf}_ex")
         fn.restype = i32
         fn.argtypes = [vp, vp, i64, u32p, i64, vp, ctypes.POINTER(Opts), vp]
+    for suf in ("f32", "f64", "u32", "i32"):
+        fn = getattr(lib, f"ggms_topk_{suf}")
+        fn.restype = i32
+        fn.argtypes = [vp, vp, i64, i64, vp, ctypes.POINTER(Opts), vp]
     for suf in ("f32", "u32"):
         fn = getattr(lib, f"ggms_multiselect_segmented_{suf}")
         fn.restype = i32
@@ -225,6 +229,18 @@ def select(ctx: Optional[Context], d_ptr: int, n: int, ks: np.ndarray, dtype, as
     if rc:
         raise GGMSError(rc, "ggms_multiselect_ex")
     return (out, st.as_dict()) if stats else out
+
+
+def topk(ctx: Optional[Context], d_ptr: int, n: int, K: int, dtype, **kw) -> np.ndarray:
+    """The K largest values, largest first (host result)."""
+    out = np.empty(K, dtype=dtype)
+    o = default_opts(**kw)
+    rc = getattr(load(), f"ggms_topk_{_suffix(dtype)}")(
+        ctx.ptr if ctx else None, ctypes.c_void_p(d_ptr), int(n), int(K),
+        out.ctypes.data_as(ctypes.c_void_p), ctypes.byref(o), None)
+    if rc:
+        raise GGMSError(rc, "ggms_topk")
+    return out
 
 
 def segmented(ctx: Optional[Context], d_ptr: int, seg_off_ptr: int, nseg: int, ks_ptr: int,

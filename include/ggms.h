@@ -159,6 +159,20 @@ GGMS_API int ggms_multiselect_i32_ex(ggms_context* ctx, const int32_t* d_in, int
                             const uint32_t* ks, int64_t nk, int32_t* out,
                             const ggms_opts* opts, void* stream);
 
+/* ---- top-k: the K largest values, largest first ----
+ * The reference's timeBucketTopkselect (DistributedSMOS/iterativeSMOSTimingFunctions.cu:307-333)
+ * runs bucketMultiselect with ks = 1..K; this does the same on the device (no
+ * k array is uploaded): out[i] = the (i+1)-th largest, exact.  `out` is host
+ * memory unless opts->out_on_device.  1 <= K <= n. */
+GGMS_API int ggms_topk_f32(ggms_context* ctx, const float* d_in, int64_t n, int64_t K, float* out,
+                           const ggms_opts* opts, void* stream);
+GGMS_API int ggms_topk_f64(ggms_context* ctx, const double* d_in, int64_t n, int64_t K, double* out,
+                           const ggms_opts* opts, void* stream);
+GGMS_API int ggms_topk_u32(ggms_context* ctx, const uint32_t* d_in, int64_t n, int64_t K, uint32_t* out,
+                           const ggms_opts* opts, void* stream);
+GGMS_API int ggms_topk_i32(ggms_context* ctx, const int32_t* d_in, int64_t n, int64_t K, int32_t* out,
+                           const ggms_opts* opts, void* stream);
+
 /* ---- batched segmented selection (no reference counterpart: the reference has
  *      no batched API; its callers loop over per-vector wrapper calls) ----
  * Segment s is d_in[seg_off[s] .. seg_off[s+1]); its ks are

@@ -1,0 +1,72 @@
+"""Batched segmented selection and top-k through the C ABI, bit-exact against
+the oracle (per segment)."""
+import numpy as np
+import pytest
+
+import ggms_b200 as G
+import ggms_oracle as orc
+from ggms_b200 import datagen as D
+from conftest import to_device
+
+pytestmark = pytest.mark.gpu
+
+
+def run_segmented(ctx, vals, seg_off, ks, k_off):
+    import torch
+    dv = to_device(vals)
+    dso = torch.from_numpy(seg_off).cuda()
+    dk = to_device(ks)
+    dko = torch.from_numpy(k_off).cuda()
+    tdt = {np.dtype(np.float32): torch.float32, np.dtype(np.uint32): torch.int32}[vals.dtype]
+    dout = torch.empty(len(ks), dtype=tdt, device="cuda")
+    rc = G.segmented(ctx, dv.data_ptr(), dso.data_ptr(), len(seg_off) - 1, dk.data_ptr(),
+                     dko.data_ptr(), dout.data_ptr(), vals.dtype)
+    assert rc == 0, G.status_string(rc)
+    torch.cuda.synchronize()
+    out = dout.cpu().numpy()
+    return out.view(np.uint32) if vals.dtype == np.uint32 else out
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.uint32])
+@pytest.mark.parametrize("nseg,lo,hi", [(1, 10, 10), (7, 0, 6), (64, 4, 14), (300, 10, 16)])
+def test_segmented_small(ctx, dtype, nseg, lo, hi):
+    vals, seg_off, ks, k_off = D.segmented_batch(nseg, nseg + lo, lo, hi, kmax=40, dtype=dtype)
+    got = run_segmented(ctx, vals, seg_off, ks, k_off)
+    exp = orc.select_segmented(vals, seg_off, ks, k_off)
+    np.testing.assert_array_equal(orc.bits(got), orc.bits(exp))
+
+
+def test_segmented_with_empty_k_segments_and_duplicates(ctx):
+    g = np.random.default_rng(5)
+    lens = np.array([5, 0, 1000, 3, 70000, 1], dtype=np.int64)
+    seg_off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    vals = g.integers(0, 50, size=seg_off[-1]).astype(np.float32)  # heavy duplicates
+    nks = np.array([2, 0, 0, 3, 100, 1])
+    k_off = np.concatenate([[0], np.cumsum(nks)]).astype(np.int64)
+    ks = np.concatenate([g.integers(1, max(l, 1) + 1, size=c) for l, c in zip(lens, nks)]).astype(np.uint32)
+    got = run_segmented(ctx, vals, seg_off, ks, k_off)
+    np.testing.assert_array_equal(orc.bits(got), orc.bits(orc.select_segmented(vals, seg_off, ks, k_off)))
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.uint32])
+def test_segmented_config5_shape(ctx, dtype):
+    # the benchmark's batched shape, scaled to 2^26 elements in total for test time
+    vals, seg_off, ks, k_off = D.segmented_batch(1024, 41, 10, 22, kmax=512, dtype=dtype,
+                                                 total_cap=1 << 26)
+    got = run_segmented(ctx, vals, seg_off, ks, k_off)
+    exp = orc.select_segmented(vals, seg_off, ks, k_off)
+    np.testing.assert_array_equal(orc.bits(got), orc.bits(exp))
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64, np.uint32, np.int32])
+@pytest.mark.parametrize("n,K", [(1, 1), (1000, 1000), (100_000, 17), (1 << 20, 4096), (1 << 22, 100)])
+def test_topk(ctx, dtype, n, K):
+    g = np.random.default_rng(n + K)
+    if np.dtype(dtype).kind == "f":
+        v = g.standard_normal(n).astype(dtype)
+    else:
+        v = g.integers(np.iinfo(dtype).min, np.iinfo(dtype).max, size=n, dtype=dtype, endpoint=True)
+    d = to_device(v)
+    got = G.topk(ctx, d.data_ptr(), n, K, dtype)
+    exp = orc.select(v, np.arange(1, K + 1, dtype=np.uint32))
+    np.testing.assert_array_equal(orc.bits(got), orc.bits(exp))
