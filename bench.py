@@ -155,14 +155,22 @@ def dist_setup(args):
     return world, rank, local
 
 
-def max_over_ranks(x: float, world: int, device) -> float:
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """Max of a per-rank device time over all ranks (every rank gets it).
+    device None: a CPU tensor (gloo)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device=device)
+    t = torch.tensor([x], dtype=torch.float64, device=device if device is not None else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_rate(elems_per_rank: int, world: int, ms_total_max: float, steps: int) -> float:
+    """elements/s of the whole job: every rank processed elems_per_rank per step;
+    the slowest rank's time bounds the job (weak scaling, replicas)."""
+    return world * elems_per_rank / (ms_total_max / steps / 1e3)
 
 
 def barrier(world: int, device=None):
@@ -262,7 +270,7 @@ def run_ours(args):
     p1 = list(p1)[args.warmup:got]
     p2 = list(p2)[args.warmup:got]
     ms_step = ms / args.steps
-    value = world * N_ELEMS / (ms_step / 1e3)
+    value = whole_job_rate(N_ELEMS, world, ms, args.steps)
 
     # stats of one call (passes, candidates, occupancy)
     _, st_auto = G.select(ctx, d_v.data_ptr(), N_ELEMS, ks, np.float32, assigner=G.ASSIGNER_AUTO,

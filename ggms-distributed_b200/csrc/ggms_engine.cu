@@ -311,6 +311,8 @@ template <typename K>
 static int setup_attrs() {
   static bool done = false;
   if (done) return GGMS_OK;
+  GGMS_CU(cudaFuncSetAttribute(l0_scan, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(4u * MAX_B0)));
   GGMS_CU(cudaFuncSetAttribute(setup_sampled<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(SetupSmem<K>)));
   done = true;
@@ -443,7 +445,7 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
                                                                                w.hist0, w.crow);
   prof_rec(prof, 2, st);
   ++ctx->launches;
-  l0_scan<<<1, 1024, 0, st>>>(w.hist0, p.B, w.C);
+  l0_scan<<<1, 1024, 4u * p.B, st>>>(w.hist0, p.B, w.C);
   ++ctx->launches;
   lvl_locate_rows<<<cdiv(nk, 256), 256, 0, st>>>(w.hist0, p.B, nk, w.krank, w.kseg, w.kbin,
                                                    w.aflag0, p.B / 32, w.C);

@@ -181,23 +181,23 @@ __device__ __forceinline__ uint32_t asg_eval(const AsgView<K>& a, K key) {
 constexpr int GRID_BITS1 = 11;
 constexpr int GRID_NC1 = 1 << GRID_BITS1;       // interior level-1 cells
 constexpr int GRID_T1 = GRID_NC1 + 2;           // + the two tail cells
-constexpr int GRID_BITS2 = 6;
-constexpr int GRID_NC2 = 1 << GRID_BITS2;       // sub-cells of a split cell
-constexpr int GRID_NSUB = 32;                   // split cells at most
-constexpr uint32_t GRID_SPLIT = 0x80000000u;    // entry flag: .y is a sub-table index
+constexpr int GRID_SUBCAP = 2048;               // sub-cell entries shared by all split cells
+constexpr int GRID_MAXSB = 10;                  // a split cell has 2^1 .. 2^10 sub-cells
+constexpr uint32_t GRID_SPLIT = 0x80000000u;    // entry flag
 
 // entry: .x = bucket at the cell's first key, .y = bucket at the next cell's
-// first key; or .x = GRID_SPLIT | ..., .y = sub-table index.
+// first key; or, for a split cell, .x = GRID_SPLIT | (sub_bits << 16),
+// .y = index of its first sub-cell entry (sub-cells are plain entries).
 template <typename K>
 struct Grid {
   K origin;                    // first key of cell 0
   K gmax;                      // last key of the last cell (keys are clamped to [origin, gmax])
-  uint32_t sh1, sh2, B, ncell, nsub, kind;
+  uint32_t sh1, nsubent, B, ncell, nsplit, kind;
   float quality;               // max/mean occupancy on the sample (256 bucket groups)
   float loss;
   uint32_t pad[2];
   uint2 t1[GRID_T1];
-  uint2 t2[GRID_NSUB * GRID_NC2];
+  uint2 t2[GRID_SUBCAP];
 };
 
 template <typename K>
@@ -205,7 +205,7 @@ struct GridView {
   const uint2* t1;
   const uint2* t2;
   K origin, gmax;
-  uint32_t sh1, sh2, B;
+  uint32_t sh1, B;
 };
 
 // floor(off * span / 2^sh) for off < 2^sh, span < 2^16: monotone in off, < span.
@@ -224,8 +224,9 @@ __device__ __forceinline__ uint32_t grid_eval(const GridView<K>& g, K key) {
   uint2 e = g.t1[(uint32_t)(d >> g.sh1)];
   uint32_t sh = g.sh1;
   if (e.x & GRID_SPLIT) {
-    e = g.t2[(e.y << GRID_BITS2) + ((uint32_t)(d >> g.sh2) & (GRID_NC2 - 1))];
-    sh = g.sh2;
+    const uint32_t sb = (e.x >> 16) & 31u;
+    sh = g.sh1 - sb;
+    e = g.t2[e.y + ((uint32_t)(d >> sh) & ((1u << sb) - 1u))];
   }
   const K off = d & (K)(((K)1 << sh) - 1);
   return e.x + grid_lin(off, e.y - e.x, sh);

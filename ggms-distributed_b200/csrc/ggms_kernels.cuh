@@ -313,23 +313,23 @@ template <typename K>
 __device__ __forceinline__ GridView<K> grid_view_global(const Grid<K>* G) {
   GridView<K> v;
   v.t1 = G->t1; v.t2 = G->t2; v.origin = G->origin; v.gmax = G->gmax;
-  v.sh1 = G->sh1; v.sh2 = G->sh2; v.B = G->B;
+  v.sh1 = G->sh1; v.B = G->B;
   return v;
 }
 
-// Copy the grid into shared memory (t1: GRID_T1 entries, t2: GRID_NSUB*GRID_NC2).
+// Copy the grid into shared memory (t1: GRID_T1 entries, t2: GRID_SUBCAP).
 template <typename K>
 __device__ __forceinline__ GridView<K> grid_to_smem(const Grid<K>* __restrict__ G, uint2* s1, uint2* s2) {
-  const uint32_t nc = G->ncell, ns = G->nsub * GRID_NC2;
+  const uint32_t nc = G->ncell, ns = G->nsubent;
   for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) s1[i] = G->t1[i];
   for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x) s2[i] = G->t2[i];
   GridView<K> v;
   v.t1 = s1; v.t2 = s2; v.origin = G->origin; v.gmax = G->gmax;
-  v.sh1 = G->sh1; v.sh2 = G->sh2; v.B = G->B;
+  v.sh1 = G->sh1; v.B = G->B;
   return v;
 }
 
-constexpr size_t GRID_SMEM = sizeof(uint2) * (GRID_T1 + GRID_NSUB * GRID_NC2);
+constexpr size_t GRID_SMEM = sizeof(uint2) * (GRID_T1 + GRID_SUBCAP);
 
 // 16-byte vector view of the input
 template <typename T> struct Vec16 {
@@ -421,10 +421,15 @@ __global__ __launch_bounds__(NT) void l0_count(const T* __restrict__ in, uint64_
   }
 }
 
-// Inclusive scan of the level-0 counts (one CTA) + the largest bucket.
+// Inclusive scan of the level-0 counts (one CTA) + the largest bucket.  The
+// counts are staged through shared memory with coalesced loads/stores.
 __global__ __launch_bounds__(1024) void l0_scan(uint32_t* hist0, uint32_t B, Counters* C) {
+  extern __shared__ uint32_t sh_counts[];
   __shared__ uint32_t w[72];
-  block_inclusive_scan_global<1024>(hist0, B, w, &C->max_bucket0);
+  for (uint32_t i = threadIdx.x; i < B; i += 1024) sh_counts[i] = hist0[i];
+  __syncthreads();
+  block_inclusive_scan_global<1024>(sh_counts, B, w, &C->max_bucket0);
+  for (uint32_t i = threadIdx.x; i < B; i += 1024) hist0[i] = sh_counts[i];
 }
 
 // Each k finds the bucket holding its rank: the smallest b with I[b] > r.
@@ -864,6 +869,9 @@ __global__ __launch_bounds__(NT) void small_select(const K* __restrict__ src,
   __shared__ uint32_t nk_s, next_s;
   __shared__ uint32_t rk[SS_GROUP];
   __shared__ K pk[SS_GROUP];
+  __shared__ K upk[SS_GROUP];       // distinct prefixes of the current round
+  __shared__ uint32_t hmap[SS_GROUP];  // k -> its prefix's histogram
+  __shared__ uint32_t nuniq;
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t ns = min(C->nsmall, caps.segs);
   for (uint32_t t = blockIdx.x; t < ns; t += gridDim.x) {
@@ -873,7 +881,6 @@ __global__ __launch_bounds__(NT) void small_select(const K* __restrict__ src,
     if (s.cnt > small_keys) set_status(C, GGMS_E_INTERNAL);
     for (uint32_t i = tid; i < cnt; i += NT) vals[i] = (K)(src[s.off + i] - s.lo);
     const int bits = bitlen((K)(s.hi - s.lo));
-    const int rounds = (bits + 7) / 8;
     bool sorted_seg = false;
     if (tid == 0) next_s = khead_q[id];
     __syncthreads();
@@ -924,21 +931,42 @@ __global__ __launch_bounds__(NT) void small_select(const K* __restrict__ src,
           rk[tid] = k_rank[kid[g0 + tid]];
           pk[tid] = 0;
         }
-        for (int rd = rounds - 1; rd >= 0; --rd) {
-          const int sh = rd * 8;
-          for (uint32_t i = tid; i < g * 256; i += NT) hist[i] = 0u;
+        // digits of 8 bits from the top of the segment's range: v < 2^bits
+        for (int top = bits; top > 0;) {
+          const int width = min(8, top);
+          const int sh = top - width;
+          const uint32_t dmask = (1u << width) - 1u;
+          __syncthreads();
+          if (tid == 0) {  // ks with the same prefix share one histogram
+            uint32_t h = 0;
+            for (uint32_t j = 0; j < g; ++j) {
+              uint32_t u = 0;
+              while (u < h && upk[u] != pk[j]) ++u;
+              if (u == h) upk[h++] = pk[j];
+              hmap[j] = u;
+            }
+            nuniq = h;
+          }
+          __syncthreads();
+          const uint32_t h = nuniq;
+          for (uint32_t i = tid; i < h * 256; i += NT) hist[i] = 0u;
           __syncthreads();
           for (uint32_t i = tid; i < cnt; i += NT) {
             const K v = vals[i];
-            for (uint32_t j = 0; j < g; ++j)
-              if ((((v ^ pk[j]) >> sh) >> 8) == 0) atomicAdd(&hist[j * 256 + (uint32_t)((v >> sh) & 255)], 1u);
+            for (uint32_t u = 0; u < h; ++u) {
+              if ((((v ^ upk[u]) >> sh) >> width) == 0) {  // same bits above this digit
+                atomicAdd(&hist[u * 256 + (uint32_t)((v >> sh) & dmask)], 1u);
+                break;  // prefixes of one length are disjoint
+              }
+            }
           }
           __syncthreads();
           if (warp < g) {  // warp j picks the digit holding rank rk[j]
             const uint32_t j = warp;
+            const uint32_t* hj = hist + hmap[j] * 256;
             uint32_t c8[8], sum = 0;
 #pragma unroll
-            for (int q = 0; q < 8; ++q) { c8[q] = hist[j * 256 + lane * 8 + q]; sum += c8[q]; }
+            for (int q = 0; q < 8; ++q) { c8[q] = hj[lane * 8 + q]; sum += c8[q]; }
             uint32_t inc = sum;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -961,8 +989,9 @@ __global__ __launch_bounds__(NT) void small_select(const K* __restrict__ src,
             }
             if (who == 0 && lane == 0) set_status(C, GGMS_E_INTERNAL);  // rank beyond the segment
           }
-          __syncthreads();
+          top = sh;
         }
+        __syncthreads();
         if (tid < g) {
           const uint32_t k = kid[g0 + tid];
           k_key[k] = (K)(s.lo + pk[tid]);

@@ -58,17 +58,23 @@ __device__ __forceinline__ float sigmoidf_(float x) { return 1.0f / (1.0f + expf
 // segments w, w + nwarps, ... (fixed summation order: deterministic).
 template <typename K>
 __device__ void pl_stats_block(const K* __restrict__ sorted, uint32_t S, const K* x, uint32_t M,
-                               PLStats* st) {
+                               PLStats* st, uint32_t* seg_start) {
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  auto lower = [&](K v) {
+  // first sample of every segment: one binary search per knot, all in parallel
+  for (uint32_t j = threadIdx.x; j <= M; j += blockDim.x) {
     uint32_t lo = 0, hi = S;
-    while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (sorted[m] < v) lo = m + 1; else hi = m; }
-    return lo;
-  };
+    if (j == M) {
+      lo = S;  // the last segment also takes s == x_M
+    } else {
+      const K v = x[j];
+      while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (sorted[m] < v) lo = m + 1; else hi = m; }
+    }
+    seg_start[j] = lo;
+  }
+  __syncthreads();
   for (uint32_t j = warp; j < M; j += nw) {
     const K xj = x[j], xn = x[j + 1];
-    const uint32_t i0 = lower(xj);
-    const uint32_t i1 = (j + 1 == M) ? S : lower(xn);  // the last segment also takes s == x_M
+    const uint32_t i0 = seg_start[j], i1 = seg_start[j + 1];
     const float width = key_to_float_rn((K)(xn - xj));
     double n = 0, su = 0, su2 = 0, sy = 0, syu = 0, sy2 = 0;
     for (uint32_t i = i0 + lane; i < i1; i += 32) {
@@ -232,6 +238,7 @@ struct LearnSmem {
   uint32_t Bs[ASG_MAXM + 1];
   uint32_t q[PL_M + 1];
   float qcdf[PL_M + 1];
+  uint32_t seg_start[PL_M + 1];
 };
 
 // Quantile knots: q_j = round(j * (S - 1) / M), initial CDF j / M.
@@ -277,7 +284,7 @@ __global__ __launch_bounds__(SETUP_NT) void setup_learned_pl(const K* __restrict
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
   pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, A, sm);
   const uint32_t M = A->M;
-  pl_stats_block<K>(sorted, S, A->x, M, sm.st);
+  pl_stats_block<K>(sorted, S, A->x, M, sm.st, sm.seg_start);
   __syncthreads();
   if (threadIdx.x < PL_NT) {
     const float loss = pl_train_block(sm.st, M, S, steps, lr, sm.red, sm.cdf, &L->loss_init,
@@ -304,7 +311,7 @@ __global__ __launch_bounds__(SETUP_NT) void pl_grad_probe(const K* __restrict__ 
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
   pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, A, sm);
   const uint32_t M = A->M;
-  pl_stats_block<K>(sorted, S, A->x, M, sm.st);
+  pl_stats_block<K>(sorted, S, A->x, M, sm.st, sm.seg_start);
   __syncthreads();
   if (threadIdx.x < PL_NT) {
     float g = 0.0f;

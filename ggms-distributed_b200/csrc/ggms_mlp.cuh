@@ -33,7 +33,9 @@ constexpr int P_V1 = 0, P_C1 = 32, P_V2 = 64, P_C2 = 64 + 1024, P_V3 = P_C2 + 32
 
 struct MlpSmem {
   float P[MLP_NP];          // raw parameters (V1, c1, V2, c2, V3, c3)
-  float G[MLP_NP];          // this CTA's partial gradient
+  float Pbest[MLP_NP];      // best parameters seen (CTA 0)
+  float G[MLP_NP + 1];      // this CTA's partial gradient, then its squared-error sum
+  float best, cur_loss;
   float m1[MLP_NP], m2[MLP_NP];  // Adam moments (CTA 0)
   float w1[32], W2[1024], w3[32];  // softplus'd weights
   float x[MLP_NT], t[MLP_NT], dz[MLP_NT], err[MLP_NT];
@@ -113,6 +115,10 @@ __device__ void mlp_cta_grad(MlpSmem& S, float inv_q) {
     float gc3 = 0;
     for (int i = 0; i < MLP_NT; ++i) gc3 += S.dz[i];
     S.G[P_C3] = gc3;
+  } else if (tid == 64) {
+    float e = 0;
+    for (int i = 0; i < MLP_NT; ++i) e += S.err[i];
+    S.G[MLP_NP] = e;
   }
   __syncthreads();
 }
@@ -161,10 +167,20 @@ mlp_train(const K* __restrict__ sorted, uint32_t S_n, const Assigner<K>* __restr
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
   float b1t = 1.0f, b2t = 1.0f;
   const uint32_t iters = steps ? steps : 1u;
+  if (tid == 0) S.best = 3.0e38f;
   for (uint32_t it = 0; it < iters; ++it) {
     mlp_cta_grad(S, inv_q);
     cluster.sync();  // all partial gradients are in place
     if (rank == 0) {
+      if (tid == 0) {
+        float e = 0.0f;
+        for (unsigned r = 0; r < MLP_CTAS; ++r) e += cluster.map_shared_rank(&S, r)->G[MLP_NP];
+        S.cur_loss = e * inv_q;
+      }
+      __syncthreads();
+      const bool better = S.cur_loss < S.best;  // loss at the parameters before this step
+      if (better)
+        for (int p = tid; p < MLP_NP; p += MLP_NT) S.Pbest[p] = S.P[p];
       b1t *= b1;
       b2t *= b2;
       for (int p = tid; p < MLP_NP; p += MLP_NT) {
@@ -180,62 +196,69 @@ mlp_train(const K* __restrict__ sorted, uint32_t S_n, const Assigner<K>* __restr
         S.m2[p] = m2;
         S.P[p] -= lr * (m1 / (1.0f - b1t)) / (sqrtf(m2 / (1.0f - b2t)) + eps);
       }
+      __syncthreads();
+      if (tid == 0 && better) S.best = S.cur_loss;
     }
     cluster.sync();  // CTA 0 has the new parameters
     if (rank != 0)
       for (int p = tid; p < MLP_NP; p += MLP_NT) S.P[p] = S0->P[p];
     __syncthreads();
   }
-  // final loss at the trained parameters
+  // loss at the final parameters; keep them only if they beat the best seen
   mlp_cta_grad(S, inv_q);
-  if (tid == 0) {
-    float e = 0.0f;
-    for (int i = 0; i < MLP_NT; ++i) e += S.err[i];
-    S.G[0] = e;  // reuse as this CTA's error sum
-  }
   cluster.sync();
-  if (rank == 0 && tid == 0) {
-    float e = 0.0f;
-    for (unsigned r = 0; r < MLP_CTAS; ++r) e += cluster.map_shared_rank(&S, r)->G[0];
-    const float loss = e * inv_q;
-    if (probe && steps == 0) probe[MLP_NP] = loss;
-    if (L) L->mlp_loss = loss;
+  if (rank == 0) {
+    if (tid == 0) {
+      float e = 0.0f;
+      for (unsigned r = 0; r < MLP_CTAS; ++r) e += cluster.map_shared_rank(&S, r)->G[MLP_NP];
+      S.cur_loss = e * inv_q;
+      if (probe && steps == 0) probe[MLP_NP] = S.cur_loss;
+    }
+    __syncthreads();
+    const bool use_best = steps > 0 && S.best < S.cur_loss;
+    for (int p = tid; p < MLP_NP; p += MLP_NT) Pglob[p] = use_best ? S.Pbest[p] : S.P[p];
+    if (tid == 0 && L) L->mlp_loss = use_best ? S.best : S.cur_loss;
   }
-  if (rank == 0)
-    for (int p = tid; p < MLP_NP; p += MLP_NT) Pglob[p] = S.P[p];
   cluster.sync();  // keep every CTA's shared memory alive until CTA 0 has read it
 }
 
-// Initial parameters: hidden units of layer 1 step at the sample quantiles.
+// Initial parameters.  Layer 1: unit j is a step at the sample quantile
+// q_j = (2j+1)/64 whose width is the local quantile spacing (steep where the
+// data is dense), so mean_j (h1_j + 1)/2 already approximates the CDF.  Layer 2:
+// unit k steps where that approximation crosses (k + 0.5)/32.  Layer 3: the
+// mean of the layer-2 steps through the near-linear part of the sigmoid.
 template <typename K>
 __device__ void mlp_init(const K* __restrict__ sorted, uint32_t S_n, const Assigner<K>* __restrict__ A,
                          float* P) {
   const int tid = threadIdx.x;
   const K x0 = A->x[0], xM = A->x[A->M];
   const float span = key_to_float_rn((K)(xM - x0));
-  const float inv_sp1 = 0.5413248546f;  // softplus^-1(1)
+  auto qx = [&](int j) -> float {  // normalized key of quantile (2j+1)/64; -1 -> 0, 32 -> 1
+    if (j < 0) return 0.0f;
+    if (j > 31) return 1.0f;
+    const uint32_t si = (uint32_t)(((uint64_t)(2 * j + 1) * S_n) / 64u);
+    return span > 0.0f ? __fdiv_rn(key_to_float_rn((K)(sorted[si] - x0)), span) : 0.0f;
+  };
   for (int p = tid; p < MLP_NP; p += blockDim.x) {
     float v = 0.0f;
-    if (p < P_C1) {                       // V1: w1 = 8
-      v = 7.99966454f;                    // softplus^-1(8)
-    } else if (p < P_V2) {                // c1 = -8 q_j
+    if (p < P_C1) {                       // V1: w1 = 2 / local spacing
+      const int j = p - P_V1;
+      const float w1 = fminf(2.0f / fmaxf(qx(j + 1) - qx(j - 1), 1e-7f), 1e6f);
+      v = w1 + log1pf(-expf(-w1));        // softplus^-1(w1)
+    } else if (p < P_V2) {                // c1 = -w1 q_j
       const int j = p - P_C1;
-      const uint32_t si = (uint32_t)(((uint64_t)(2 * j + 1) * S_n) / 64u);
-      const float q = span > 0.0f ? __fdiv_rn(key_to_float_rn((K)(sorted[si] - x0)), span) : 0.0f;
-      v = -8.0f * q;
-    } else if (p < P_C2) {                // V2: W2 ~ 1/32 with a deterministic spread
-      const int i = p - P_V2;
-      const float w = (1.0f / 32.0f) * (0.5f + (float)((i * 2654435761u) >> 22) / 1024.0f);
-      v = logf(expm1f(w));                // softplus^-1(w)
-    } else if (p < P_V3) {                // c2: spread the second layer's centers
+      const float w1 = fminf(2.0f / fmaxf(qx(j + 1) - qx(j - 1), 1e-7f), 1e6f);
+      v = -w1 * qx(j);
+    } else if (p < P_C2) {                // V2: W2 = 1/32
+      v = logf(expm1f(1.0f / 32.0f));
+    } else if (p < P_V3) {                // c2: steps at (k + 0.5) / 32
       const int k = p - P_C2;
-      v = 0.8f * ((float)k / 31.0f - 0.5f);
-    } else if (p < P_C3) {                // V3: w3 ~ 0.2
-      v = logf(expm1f(0.2f));
+      v = (1.0f / 32.0f) * (32.0f - 64.0f * ((float)k + 0.5f) / 32.0f);
+    } else if (p < P_C3) {                // V3: w3 = 1/16
+      v = logf(expm1f(1.0f / 16.0f));
     } else {
       v = 0.0f;                           // c3
     }
-    (void)inv_sp1;
     P[p] = v;
   }
 }
@@ -308,7 +331,7 @@ static int mlp_fit_and_compile(const K* sorted, uint32_t S, uint32_t B, int step
   const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 150u;
   float* P = L->mlp_params;
   setup_mlp_begin<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, &As[1], P);
-  mlp_train<K><<<MLP_CTAS, MLP_NT, sizeof(MlpSmem), st>>>(sorted, S, &As[1], L, P, steps, 0.02f,
+  mlp_train<K><<<MLP_CTAS, MLP_NT, sizeof(MlpSmem), st>>>(sorted, S, &As[1], L, P, steps, 0.05f,
                                                           nullptr, nullptr, nullptr);
   setup_mlp_finish<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, bound, P, &As[1],
                                                                   &Gs[1], L, choice);

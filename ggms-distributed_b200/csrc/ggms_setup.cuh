@@ -53,19 +53,25 @@ __device__ V block_sum(V v, V* red) {
 }
 
 // ------------------------------------------------------------------ grid compilation
-// Resamples a monotone model (the PL assigner `a`) onto the grid.  Cells whose
+// Resamples a monotone model (the PL assigner `a`) onto the grid; the heaviest
 // bucket span is at least T (the smallest power of two >= 4x the mean span that
 // leaves at most GRID_NSUB such cells) are split into sub-cells.  Writes the
 // grid to `G` (global) and to the shared copies s1/s2.  All threads call it.
 template <typename K>
 struct CompileSmem {
-  uint32_t bnd[GRID_NC1 + 1];   // bucket at each cell boundary
-  uint32_t sub_of[GRID_NC1];    // sub-table index of a split cell
-  uint32_t cell_of[GRID_NSUB];  // cell of each sub-table
+  uint32_t bnd[GRID_NC1 + 1];   // bucket at each interior cell boundary
+  uint32_t sub_base[GRID_NC1];  // first sub-cell entry of a split cell (0xFFFFFFFF: not split)
+  uint32_t split_cell[GRID_SUBCAP / 2];  // split cells in order (each has >= 2 sub-cells)
+  uint32_t split_base[GRID_SUBCAP / 2];
   uint32_t hist[33];
   uint32_t red[33];
   uint32_t thresh;
 };
+
+// sub-cell bits of an interior cell with bucket span sp
+__device__ __forceinline__ uint32_t grid_sub_bits(uint32_t sp, int sh1) {
+  return (uint32_t)min(min(bitlen(sp), GRID_MAXSB), sh1);
+}
 
 template <typename K>
 __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t kind, Grid<K>* G,
@@ -88,8 +94,6 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
     gmax = ((K)(KMAX - top) >= (K)(w - 1)) ? (K)(top + (w - 1)) : KMAX;
   }
   const uint32_t ntot = first + nc + (has_hi ? 1u : 0u);
-  const int sh2 = sh1 >= GRID_BITS2 ? sh1 - GRID_BITS2 : 0;
-  const bool splittable = sh1 >= GRID_BITS2;
   for (uint32_t c = tid; c <= nc; c += NT) {
     uint32_t b;
     if (c < nc) b = asg_eval<K>(a, (K)(lo + ((K)c << sh1)));
@@ -98,46 +102,57 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
   }
   if (tid < 33) cs.hist[tid] = 0;
   __syncthreads();
-  // split threshold from a histogram of log2(span)
-  const uint32_t mean = max(1u, (B - 2u) / nc);
+  // Split the heaviest cells so that a sub-cell spans about one bucket.  Cells
+  // with bitlen(span) >= t are split (2^sub_bits sub-cells each); t is the
+  // smallest value >= 3 whose total fits the GRID_SUBCAP entries.
   for (uint32_t c = tid; c < nc; c += NT) {
     const uint32_t sp = cs.bnd[c + 1] - cs.bnd[c];
-    if (sp >= 4u * mean && splittable) atomicAdd(&cs.hist[bitlen(sp)], 1u);
+    if (sp >= 4u && sh1 >= 1) atomicAdd(&cs.hist[bitlen(sp)], 1u);
   }
   __syncthreads();
   if (tid == 0) {
-    uint32_t cum = 0, t = 33;
-    for (int k = 32; k >= 1; --k) {
-      if (cum + cs.hist[k] > (uint32_t)GRID_NSUB) break;
-      cum += cs.hist[k];
+    uint32_t cost = 0, t = 33;
+    for (int k = 32; k >= 3; --k) {
+      const uint32_t per = 1u << (uint32_t)min(min(k, GRID_MAXSB), sh1);
+      const uint32_t add = cs.hist[k] * per;
+      if (cost + add > (uint32_t)GRID_SUBCAP) break;
+      cost += add;
       t = (uint32_t)k;
     }
-    cs.thresh = t;  // cells with bitlen(span) >= t are split (t == 33: none)
+    cs.thresh = t;
   }
   __syncthreads();
   const uint32_t thr = cs.thresh;
-  // deterministic sub-table indices: prefix over split flags in cell order (2 cells per thread)
-  uint32_t flags = 0;
+  // sub-table bases: prefix over the split cells' sizes in cell order (2 cells per thread)
+  uint32_t sz[2] = {0, 0};
   for (uint32_t k = 0; k < 2; ++k) {
     const uint32_t c = tid * 2 + k;
     if (c < nc) {
       const uint32_t sp = cs.bnd[c + 1] - cs.bnd[c];
-      if (splittable && sp >= 4u * mean && (uint32_t)bitlen(sp) >= thr) flags |= 1u << k;
+      if (sp >= 4u && sh1 >= 1 && (uint32_t)bitlen(sp) >= thr) sz[k] = 1u << grid_sub_bits(sp, sh1);
     }
   }
   uint32_t total = 0;
-  const uint32_t pre = block_excl_scan<uint32_t>(__popc(flags), cs.red, &total);
+  const uint32_t pre = block_excl_scan<uint32_t>(sz[0] + sz[1], cs.red, &total);
+  uint32_t nsplit_tot = 0;
+  const uint32_t spre = block_excl_scan<uint32_t>((sz[0] ? 1u : 0u) + (sz[1] ? 1u : 0u), cs.red, &nsplit_tot);
   {
-    uint32_t idx = pre;
+    uint32_t base = pre, si = spre;
     for (uint32_t k = 0; k < 2; ++k) {
       const uint32_t c = tid * 2 + k;
-      if (c < nc) cs.sub_of[c] = ((flags >> k) & 1u) ? idx++ : 0xFFFFFFFFu;
+      if (c < nc) {
+        if (sz[k]) {
+          cs.sub_base[c] = base;
+          cs.split_cell[si] = c;
+          cs.split_base[si] = base;
+          ++si;
+          base += sz[k];
+        } else {
+          cs.sub_base[c] = 0xFFFFFFFFu;
+        }
+      }
     }
   }
-  __syncthreads();
-  const uint32_t nsub = min(total, (uint32_t)GRID_NSUB);
-  for (uint32_t c = tid; c < nc; c += NT)
-    if (cs.sub_of[c] < nsub) cs.cell_of[cs.sub_of[c]] = c;
   __syncthreads();
   for (uint32_t c = tid; c < ntot; c += NT) {
     uint2 e;
@@ -147,22 +162,33 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
       e = make_uint2(B - 1u, B - 1u);                         // high tail: bucket B-1
     } else {
       const uint32_t i = c - first;
-      const uint32_t si = cs.sub_of[i];
-      if (si < nsub) e = make_uint2(GRID_SPLIT | cs.bnd[i], si);
-      else e = make_uint2(cs.bnd[i], cs.bnd[i + 1]);
+      const uint32_t sb0 = cs.sub_base[i];
+      if (sb0 != 0xFFFFFFFFu) {
+        const uint32_t sp = cs.bnd[i + 1] - cs.bnd[i];
+        e = make_uint2(GRID_SPLIT | (grid_sub_bits(sp, sh1) << 16), sb0);
+      } else {
+        e = make_uint2(cs.bnd[i], cs.bnd[i + 1]);
+      }
     }
     s1[c] = e;
     G->t1[c] = e;
   }
-  // sub-cells of split cells
-  for (uint32_t i = tid; i < nsub * GRID_NC2; i += NT) {
-    const uint32_t si = i >> GRID_BITS2, s = i & (GRID_NC2 - 1);
-    const uint32_t c = cs.cell_of[si];
+  // sub-cell entries
+  for (uint32_t i = tid; i < total; i += NT) {
+    uint32_t lo_i = 0, hi_i = nsplit_tot - 1;  // last split cell whose base <= i
+    while (lo_i < hi_i) {
+      const uint32_t m = (lo_i + hi_i + 1) >> 1;
+      if (cs.split_base[m] <= i) lo_i = m; else hi_i = m - 1;
+    }
+    const uint32_t c = cs.split_cell[lo_i];
+    const uint32_t s = i - cs.split_base[lo_i];
+    const uint32_t sb = grid_sub_bits(cs.bnd[c + 1] - cs.bnd[c], sh1);
+    const int shs = sh1 - (int)sb;
     const K cell_lo = (K)(lo + ((K)c << sh1));
     const K room = (K)(hi - cell_lo);  // sub-boundaries past hi (last cell only) take the cell's end
-    auto bnd_at = [&](uint32_t sb) -> uint32_t {
-      if (sb == (uint32_t)GRID_NC2) return cs.bnd[c + 1];
-      const K off = (K)sb << sh2;
+    auto bnd_at = [&](uint32_t q) -> uint32_t {
+      if (q == (1u << sb)) return cs.bnd[c + 1];
+      const K off = (K)q << shs;
       return off > room ? cs.bnd[c + 1] : asg_eval<K>(a, (K)(cell_lo + off));
     };
     const uint2 e = make_uint2(bnd_at(s), bnd_at(s + 1));
@@ -173,17 +199,17 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
     G->origin = origin;
     G->gmax = gmax;
     G->sh1 = (uint32_t)sh1;
-    G->sh2 = (uint32_t)sh2;
+    G->nsubent = total;
     G->B = B;
     G->ncell = ntot;
-    G->nsub = nsub;
+    G->nsplit = nsplit_tot;
     G->kind = kind;
     G->loss = 0.0f;
   }
   __syncthreads();
   GridView<K> v;
   v.t1 = s1; v.t2 = s2; v.origin = origin; v.gmax = gmax;
-  v.sh1 = (uint32_t)sh1; v.sh2 = (uint32_t)sh2; v.B = B;
+  v.sh1 = (uint32_t)sh1; v.B = B;
   return v;
 }
 
@@ -193,10 +219,21 @@ template <typename K>
 __device__ float grid_measure(const GridView<K>& g, const K* sorted, uint32_t S, uint32_t* hist256) {
   for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) hist256[i] = 0;
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < S; i += blockDim.x) {
-    const uint32_t b = grid_eval<K>(g, sorted[i]);
-    atomicAdd(&hist256[(uint32_t)(((uint64_t)b * 256u) / g.B)], 1u);
+  // each thread takes a contiguous run of the sorted sample: its groups are
+  // non-decreasing, so it adds one count per run instead of one per sample
+  const uint32_t per = (S + blockDim.x - 1) / blockDim.x;
+  const uint32_t i0 = threadIdx.x * per, i1 = min(S, i0 + per);
+  uint32_t cur = 0xFFFFFFFFu, run = 0;
+  for (uint32_t i = i0; i < i1; ++i) {
+    const uint32_t grp = (uint32_t)(((uint64_t)grid_eval<K>(g, sorted[i]) * 256u) / g.B);
+    if (grp != cur) {
+      if (run) atomicAdd(&hist256[cur], run);
+      cur = grp;
+      run = 0;
+    }
+    ++run;
   }
+  if (run) atomicAdd(&hist256[cur], run);
   __syncthreads();
   uint32_t mx = 0;
   for (uint32_t i = 0; i < 256; ++i) mx = max(mx, hist256[i]);
@@ -234,7 +271,7 @@ struct SetupSmem {
   AsgCopy<K> asg;
   CompileSmem<K> cs;
   uint2 s1[GRID_T1];
-  uint2 s2[GRID_NSUB * GRID_NC2];
+  uint2 s2[GRID_SUBCAP];
   uint32_t hist256[256];
 };
 

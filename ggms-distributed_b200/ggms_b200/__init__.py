@@ -123,7 +123,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     for suf in ("f32", "u32"):
         fn = getattr(lib, f"ggms_multiselect_segmented_{suf}")
         fn.restype = i32
-        fn.argtypes = [vp, vp, i64, vp, i64, vp, vp, ctypes.POINTER(Opts), vp]
+        fn.argtypes = [vp, vp, vp, i64, vp, vp, vp, ctypes.POINTER(Opts), vp]
     lib.ggms_get_default_context.argtypes = [ctypes.POINTER(vp)]
     lib.ggms_context_profile.argtypes = [vp, i32]
     lib.ggms_context_pass_times.argtypes = [vp, vp, vp, vp, i32]
