@@ -77,10 +77,19 @@ __device__ void pl_stats_block(const K* __restrict__ sorted, uint32_t S, const K
     const uint32_t i0 = seg_start[j], i1 = seg_start[j + 1];
     const float width = key_to_float_rn((K)(xn - xj));
     double n = 0, su = 0, su2 = 0, sy = 0, syu = 0, sy2 = 0;
-    for (uint32_t i = i0 + lane; i < i1; i += 32) {
-      const float u = fminf(__fdiv_rn(key_to_float_rn((K)(sorted[i] - xj)), width), 1.0f);
-      const double y = ((double)i + 0.5) / (double)S;
-      n += 1.0; su += u; su2 += (double)u * u; sy += y; syu += y * u; sy2 += y * y;
+    for (uint32_t i = i0 + lane; i < i1; i += 128) {  // four independent loads in flight
+      K v[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v[q] = (i + 32 * q < i1) ? sorted[i + 32 * q] : xj;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t ii = i + 32 * q;
+        if (ii < i1) {
+          const float u = fminf(__fdiv_rn(key_to_float_rn((K)(v[q] - xj)), width), 1.0f);
+          const double y = ((double)ii + 0.5) / (double)S;
+          n += 1.0; su += u; su2 += (double)u * u; sy += y; syu += y * u; sy2 += y * y;
+        }
+      }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {

@@ -219,21 +219,31 @@ template <typename K>
 __device__ float grid_measure(const GridView<K>& g, const K* sorted, uint32_t S, uint32_t* hist256) {
   for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) hist256[i] = 0;
   __syncthreads();
-  // each thread takes a contiguous run of the sorted sample: its groups are
-  // non-decreasing, so it adds one count per run instead of one per sample
-  const uint32_t per = (S + blockDim.x - 1) / blockDim.x;
-  const uint32_t i0 = threadIdx.x * per, i1 = min(S, i0 + per);
-  uint32_t cur = 0xFFFFFFFFu, run = 0;
-  for (uint32_t i = i0; i < i1; ++i) {
-    const uint32_t grp = (uint32_t)(((uint64_t)grid_eval<K>(g, sorted[i]) * 256u) / g.B);
-    if (grp != cur) {
-      if (run) atomicAdd(&hist256[cur], run);
-      cur = grp;
-      run = 0;
+  // coalesced loads, four in flight per thread; the sample is sorted, so the
+  // 32 lanes of a warp usually share a group: one add per warp then
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t NTh = blockDim.x;
+  for (uint32_t base = 0; base < S; base += 4 * NTh) {
+    K v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t i = base + u * NTh + threadIdx.x;
+      v[u] = i < S ? sorted[i] : (K)0;
     }
-    ++run;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t i = base + u * NTh + threadIdx.x;
+      const bool ok = i < S;
+      const uint32_t grp = ok ? (uint32_t)(((uint64_t)grid_eval<K>(g, v[u]) * 256u) / g.B) : 0xFFFFFFFFu;
+      const uint32_t g0 = __shfl_sync(FULL, grp, 0);
+      const uint32_t okm = __ballot_sync(FULL, ok);
+      if (__all_sync(FULL, !ok || grp == g0)) {
+        if (lane == 0 && okm) atomicAdd(&hist256[g0], (uint32_t)__popc(okm));
+      } else if (ok) {
+        atomicAdd(&hist256[grp], 1u);
+      }
+    }
   }
-  if (run) atomicAdd(&hist256[cur], run);
   __syncthreads();
   uint32_t mx = 0;
   for (uint32_t i = 0; i < 256; ++i) mx = max(mx, hist256[i]);
