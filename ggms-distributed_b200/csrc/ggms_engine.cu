@@ -279,7 +279,7 @@ static int make_plan(Plan* p, uint64_t n, uint32_t nk, const ggms_opts& o) {
 }
 
 // ------------------------------------------------------------------ kernel configs
-constexpr int L0_NT = 512;
+constexpr int L0_NT = 1024;
 constexpr int L0_UNROLL = 4;
 constexpr int LV_NT = 256;
 constexpr int MAX_LEVELS_32 = 3;

@@ -879,7 +879,19 @@ __global__ __launch_bounds__(NT) void small_select(const K* __restrict__ src,
     const Seg<K> s = segs_q[id];
     const uint32_t cnt = min(s.cnt, small_keys);
     if (s.cnt > small_keys) set_status(C, GGMS_E_INTERNAL);
-    for (uint32_t i = tid; i < cnt; i += NT) vals[i] = (K)(src[s.off + i] - s.lo);
+    for (uint32_t i0 = tid; i0 < cnt; i0 += 8 * NT) {  // eight independent loads in flight
+      K v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const uint32_t i = i0 + q * NT;
+        v[q] = i < cnt ? src[s.off + i] : s.lo;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const uint32_t i = i0 + q * NT;
+        if (i < cnt) vals[i] = (K)(v[q] - s.lo);
+      }
+    }
     const int bits = bitlen((K)(s.hi - s.lo));
     bool sorted_seg = false;
     if (tid == 0) next_s = khead_q[id];

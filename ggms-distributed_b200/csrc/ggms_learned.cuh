@@ -352,8 +352,8 @@ static int learn_and_choose(int kind, const K* sorted, uint32_t S, uint32_t B, i
     int rc = mlp_fit_and_compile<K>(sorted, S, B, steps_opt, bound, As, Gs, L, choice, st, launches);
     if (rc) return rc;
   } else {
-    const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 64u;
-    setup_learned_pl<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, steps, 0.01f, bound,
+    const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 16u;
+    setup_learned_pl<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, steps, 0.02f, bound,
                                                                     &As[1], &Gs[1], L, choice);
     *launches += 1;
   }

@@ -66,11 +66,12 @@ struct CompileSmem {
   uint32_t hist[33];
   uint32_t red[33];
   uint32_t thresh;
+  uint32_t cap;
 };
 
-// sub-cell bits of an interior cell with bucket span sp
-__device__ __forceinline__ uint32_t grid_sub_bits(uint32_t sp, int sh1) {
-  return (uint32_t)min(min(bitlen(sp), GRID_MAXSB), sh1);
+// sub-cell bits of a split cell with bucket span sp under depth cap (cap <= sh1)
+__device__ __forceinline__ uint32_t grid_sub_bits(uint32_t sp, int cap) {
+  return (uint32_t)min(min(bitlen(sp), GRID_MAXSB), cap);
 }
 
 template <typename K>
@@ -102,34 +103,45 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
   }
   if (tid < 33) cs.hist[tid] = 0;
   __syncthreads();
-  // Split the heaviest cells so that a sub-cell spans about one bucket.  Cells
-  // with bitlen(span) >= t are split (2^sub_bits sub-cells each); t is the
-  // smallest value >= 3 whose total fits the GRID_SUBCAP entries.
+  // Split heavy cells so that a sub-cell spans about one bucket: a cell of
+  // bucket span sp gets 2^min(bitlen(sp), cap) sub-cells.  cap is the largest
+  // depth (<= GRID_MAXSB) whose total fits GRID_SUBCAP entries over all cells
+  // with sp >= 4; if even depth 1 does not fit, only the cells with
+  // bitlen(sp) >= t are split (at depth 1), t the smallest value that fits.
   for (uint32_t c = tid; c < nc; c += NT) {
     const uint32_t sp = cs.bnd[c + 1] - cs.bnd[c];
     if (sp >= 4u && sh1 >= 1) atomicAdd(&cs.hist[bitlen(sp)], 1u);
   }
   __syncthreads();
   if (tid == 0) {
-    uint32_t cost = 0, t = 33;
-    for (int k = 32; k >= 3; --k) {
-      const uint32_t per = 1u << (uint32_t)min(min(k, GRID_MAXSB), sh1);
-      const uint32_t add = cs.hist[k] * per;
-      if (cost + add > (uint32_t)GRID_SUBCAP) break;
-      cost += add;
-      t = (uint32_t)k;
+    uint32_t cap = 0, t = 3;
+    for (int d = min(GRID_MAXSB, sh1); d >= 1 && cap == 0; --d) {
+      uint32_t cost = 0;
+      for (int k = 3; k <= 32; ++k) cost += cs.hist[k] << (uint32_t)min(k, d);
+      if (cost <= (uint32_t)GRID_SUBCAP) cap = (uint32_t)d;
+    }
+    if (cap == 0 && sh1 >= 1) {  // too many heavy cells: depth 1 for the heaviest only
+      uint32_t cost = 0;
+      t = 33;
+      for (int k = 32; k >= 3; --k) {
+        if (cost + (cs.hist[k] << 1) > (uint32_t)GRID_SUBCAP) break;
+        cost += cs.hist[k] << 1;
+        t = (uint32_t)k;
+      }
+      cap = 1;
     }
     cs.thresh = t;
+    cs.cap = cap;
   }
   __syncthreads();
-  const uint32_t thr = cs.thresh;
+  const uint32_t thr = cs.thresh, cap = cs.cap;
   // sub-table bases: prefix over the split cells' sizes in cell order (2 cells per thread)
   uint32_t sz[2] = {0, 0};
   for (uint32_t k = 0; k < 2; ++k) {
     const uint32_t c = tid * 2 + k;
     if (c < nc) {
       const uint32_t sp = cs.bnd[c + 1] - cs.bnd[c];
-      if (sp >= 4u && sh1 >= 1 && (uint32_t)bitlen(sp) >= thr) sz[k] = 1u << grid_sub_bits(sp, sh1);
+      if (cap && sp >= 4u && (uint32_t)bitlen(sp) >= thr) sz[k] = 1u << grid_sub_bits(sp, cap);
     }
   }
   uint32_t total = 0;
@@ -165,7 +177,7 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
       const uint32_t sb0 = cs.sub_base[i];
       if (sb0 != 0xFFFFFFFFu) {
         const uint32_t sp = cs.bnd[i + 1] - cs.bnd[i];
-        e = make_uint2(GRID_SPLIT | (grid_sub_bits(sp, sh1) << 16), sb0);
+        e = make_uint2(GRID_SPLIT | (grid_sub_bits(sp, (int)cap) << 16), sb0);
       } else {
         e = make_uint2(cs.bnd[i], cs.bnd[i + 1]);
       }
@@ -182,7 +194,7 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
     }
     const uint32_t c = cs.split_cell[lo_i];
     const uint32_t s = i - cs.split_base[lo_i];
-    const uint32_t sb = grid_sub_bits(cs.bnd[c + 1] - cs.bnd[c], sh1);
+    const uint32_t sb = grid_sub_bits(cs.bnd[c + 1] - cs.bnd[c], (int)cap);
     const int shs = sh1 - (int)sb;
     const K cell_lo = (K)(lo + ((K)c << sh1));
     const K room = (K)(hi - cell_lo);  // sub-boundaries past hi (last cell only) take the cell's end
@@ -215,8 +227,14 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
 
 // Occupancy of the grid's buckets on the (sorted) sample, over 256 groups of
 // buckets: max / mean.
+// At most GRID_MEASURE_N samples are used (a strided subsample of the sorted
+// sample, still sorted): 64 per group on average, enough to see imbalance.
+constexpr uint32_t GRID_MEASURE_N = 16384;
+
 template <typename K>
-__device__ float grid_measure(const GridView<K>& g, const K* sorted, uint32_t S, uint32_t* hist256) {
+__device__ float grid_measure(const GridView<K>& g, const K* sorted_all, uint32_t S_all, uint32_t* hist256) {
+  const uint32_t stride = S_all > GRID_MEASURE_N ? S_all / GRID_MEASURE_N : 1u;
+  const uint32_t S = S_all / stride;
   for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) hist256[i] = 0;
   __syncthreads();
   // coalesced loads, four in flight per thread; the sample is sorted, so the
@@ -228,7 +246,7 @@ __device__ float grid_measure(const GridView<K>& g, const K* sorted, uint32_t S,
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const uint32_t i = base + u * NTh + threadIdx.x;
-      v[u] = i < S ? sorted[i] : (K)0;
+      v[u] = i < S ? sorted_all[(size_t)i * stride] : (K)0;
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
