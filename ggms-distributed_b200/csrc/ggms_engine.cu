@@ -279,8 +279,6 @@ static int make_plan(Plan* p, uint64_t n, uint32_t nk, const ggms_opts& o) {
 }
 
 // ------------------------------------------------------------------ kernel configs
-constexpr int L0_NT = 1024;
-constexpr int L0_UNROLL = 4;
 constexpr int LV_NT = 256;
 constexpr int MAX_LEVELS_32 = 3;
 constexpr int MAX_LEVELS_64 = 6;
@@ -290,19 +288,47 @@ static size_t l0_count_smem(uint32_t B) { return GRID_SMEM + (size_t)B * 4u; }
 template <typename T>
 static size_t l0_compact_smem(uint32_t B) { return GRID_SMEM + (MAX_B0 / 32) * 4u + (size_t)B * 4u; }
 
+// Launch shapes of the two passes (CTA size x 16-byte loads in flight per
+// thread); the default and the autotuner pick among these instantiations.
+template <typename T>
+struct PassVariant {
+  using K = typename KeyOf<T>::K;
+  int nt, unroll;
+  void (*count)(const T*, uint64_t, const Grid<K>*, const Counters*, uint32_t*, uint32_t*);
+  void (*compact)(const T*, uint64_t, const Grid<K>*, Counters*, const uint32_t*, const uint32_t*, K*,
+                  uint64_t);
+};
+
+template <typename T>
+static const PassVariant<T>* pass_variant(int nt, int unroll) {
+  static const PassVariant<T> v[] = {
+      {256, 4, l0_count<T, 256, 4>, l0_compact<T, 256, 4>},
+      {256, 8, l0_count<T, 256, 8>, l0_compact<T, 256, 8>},
+      {512, 2, l0_count<T, 512, 2>, l0_compact<T, 512, 2>},
+      {512, 4, l0_count<T, 512, 4>, l0_compact<T, 512, 4>},
+      {512, 8, l0_count<T, 512, 8>, l0_compact<T, 512, 8>},
+      {1024, 2, l0_count<T, 1024, 2>, l0_compact<T, 1024, 2>},
+      {1024, 4, l0_count<T, 1024, 4>, l0_compact<T, 1024, 4>},
+  };
+  for (const auto& x : v)
+    if (x.nt == nt && x.unroll == unroll) return &x;
+  return nullptr;
+}
+
+constexpr int DEFAULT_PASS_NT = 512;
+constexpr int DEFAULT_PASS_UNROLL = 4;
+
 // The two passes must split the input among CTAs identically (PASS 2 writes
 // into per-CTA ranges sized by PASS 1), so both get the same grid: as many
 // CTAs as fit on every SM at once for the larger of the two.
 template <typename T>
-static int l0_ncta(Context* c, uint32_t B, uint32_t* ncta) {
+static int l0_ncta(Context* c, const PassVariant<T>* pv, uint32_t B, uint32_t* ncta) {
   const size_t s1 = l0_count_smem<T>(B), s2 = l0_compact_smem<T>(B);
-  GGMS_CU(cudaFuncSetAttribute(l0_count<T, L0_NT, L0_UNROLL>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
-  GGMS_CU(cudaFuncSetAttribute(l0_compact<T, L0_NT, L0_UNROLL>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
+  GGMS_CU(cudaFuncSetAttribute((const void*)pv->count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
+  GGMS_CU(cudaFuncSetAttribute((const void*)pv->compact, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
   int o1 = 0, o2 = 0;
-  GGMS_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, l0_count<T, L0_NT, L0_UNROLL>, L0_NT, s1));
-  GGMS_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, l0_compact<T, L0_NT, L0_UNROLL>, L0_NT, s2));
+  GGMS_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, (const void*)pv->count, pv->nt, s1));
+  GGMS_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, (const void*)pv->compact, pv->nt, s2));
   *ncta = (uint32_t)(std::max(1, std::min(o1, o2)) * c->sms);
   return GGMS_OK;
 }
@@ -374,7 +400,10 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   int rc = make_plan(&p, n, nk, o);
   if (rc) return rc;
   GGMS_CU(cudaSetDevice(ctx->device));
-  rc = l0_ncta<T>(ctx, p.B, &p.ncta);
+  const PassVariant<T>* pv = pass_variant<T>(o.pass_threads ? o.pass_threads : DEFAULT_PASS_NT,
+                                              o.pass_unroll ? o.pass_unroll : DEFAULT_PASS_UNROLL);
+  if (!pv) return GGMS_E_INVALID_ARG;
+  rc = l0_ncta<T>(ctx, pv, p.B, &p.ncta);
   if (rc) return rc;
   Workspace<K> w0 = layout<K>(p, sizeof(T), nullptr);
   rc = ensure_arena(ctx, w0.bytes);
@@ -441,8 +470,7 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   GGMS_CU(cudaMemsetAsync(w.aflag0, 0, 4ull * (p.B / 32), st));
   prof_rec(prof, 1, st);
   ++ctx->launches;
-  l0_count<T, L0_NT, L0_UNROLL><<<grid_c, L0_NT, l0_count_smem<T>(p.B), st>>>(d_in, n, w.grid, w.C,
-                                                                               w.hist0, w.crow);
+  pv->count<<<grid_c, pv->nt, l0_count_smem<T>(p.B), st>>>(d_in, n, w.grid, w.C, w.hist0, w.crow);
   prof_rec(prof, 2, st);
   ++ctx->launches;
   l0_scan<<<1, 1024, 4u * p.B, st>>>(w.hist0, p.B, w.C);
@@ -461,8 +489,8 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   // ---- PASS 2: compact the buckets that still need refinement
   prof_rec(prof, 3, st);
   ++ctx->launches;
-  l0_compact<T, L0_NT, L0_UNROLL><<<grid_c, L0_NT, l0_compact_smem<T>(p.B), st>>>(
-      d_in, n, w.grid, w.C, w.cmap0, w.crow, w.cand[0], (uint64_t)n);
+  pv->compact<<<grid_c, pv->nt, l0_compact_smem<T>(p.B), st>>>(d_in, n, w.grid, w.C, w.cmap0, w.crow,
+                                                                 w.cand[0], (uint64_t)n);
   prof_rec(prof, 4, st);
   rc = launch_small_select<K>(ctx, w.cand[0], w.segs[1], w.khead[1], w, caps, st);
   if (rc) return rc;

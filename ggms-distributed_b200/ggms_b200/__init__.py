@@ -83,7 +83,8 @@ class Opts(ctypes.Structure):
         ("train_steps", ctypes.c_int32),
         ("ks_on_device", ctypes.c_int32),
         ("out_on_device", ctypes.c_int32),
-        ("keep_levels", ctypes.c_int32),
+        ("pass_threads", ctypes.c_int32),
+        ("pass_unroll", ctypes.c_int32),
         ("stats", ctypes.POINTER(Stats)),
     ]
 

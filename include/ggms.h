@@ -83,7 +83,8 @@ typedef struct ggms_opts {
   int32_t train_steps;          /* optimizer steps for the learned models; 0 = auto */
   int32_t ks_on_device;         /* 1: the k array is device memory */
   int32_t out_on_device;        /* 1: the output array is device memory */
-  int32_t keep_levels;          /* reserved, 0 */
+  int32_t pass_threads;         /* CTA size of the two passes: 256, 512 or 1024; 0 = tuned default */
+  int32_t pass_unroll;          /* 16-byte loads in flight per thread: 2, 4 or 8; 0 = tuned default */
   ggms_stats* stats;            /* optional host pointer */
 } ggms_opts;
 
