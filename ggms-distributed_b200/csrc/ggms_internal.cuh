@@ -103,7 +103,7 @@ constexpr int RADIX_BITS = 11;                  // bits resolved per refinement 
 constexpr int NBIN = 1 << RADIX_BITS;           // 2048 bins per refinement segment
 constexpr int NBIN_WORDS = NBIN / 32;           // active-flag words per segment row
 constexpr int TILE = 16384;                     // elements per refinement work item
-constexpr int ASG_MAXM = 256;                   // max segments of the level-0 assigner
+constexpr int ASG_MAXM = 1024;                  // max segments of a PL model
 constexpr int ASG_CELL_BITS = 12;
 constexpr int ASG_NCELL = 1 << ASG_CELL_BITS;   // uniform lookup cells over the knot range
 constexpr uint32_t K_DONE = 0xFFFFFFFFu;        // k_seg value of a resolved k

@@ -10,7 +10,7 @@
 // passes evaluate.  The model only places buckets: the counting and compaction
 // passes still decide every answer exactly.
 //
-// PL-CDF model (M <= 256 segments between knots at sample quantiles):
+// PL-CDF model (M <= 1024 segments between knots at sample quantiles):
 //   delta_j = softplus(theta_j) > 0,  P_j = sum_{t<j} delta_t,  D = sum_t delta_t
 //   F(s) = (P_j + u(s) * delta_j) / D   for s in segment j, u = (s - x_j)/(x_{j+1} - x_j)
 //   loss = 1/S * sum_i (F(s_i) - y_i)^2,  y_i = (i + 0.5) / S  (sorted sample)
@@ -24,7 +24,7 @@
 
 namespace ggms {
 
-constexpr int PL_M = 256;        // segments of the learned PL model
+constexpr int PL_M = 1024;       // segments of the learned PL model
 constexpr int MLP_H = 32;        // hidden width of the MLP model
 constexpr int MLP_NPARAM = 1153; // 32 + 32 + 32*32 + 32 + 32 + 1
 
@@ -105,8 +105,8 @@ __device__ void pl_stats_block(const K* __restrict__ sorted, uint32_t S, const K
 }
 
 // ------------------------------------------------------------------ forward / backward
-// Run by the first PL_M threads only (8 warps), synchronised with named
-// barrier 1 so the rest of the CTA can wait elsewhere.  Thread j owns segment j.
+// Run by the first PL_NT threads, synchronised with named barrier 1 (with
+// PL_NT == blockDim.x that is the whole CTA).  Thread j owns segment j.
 constexpr int PL_NT = PL_M;
 __device__ __forceinline__ void bar_pl() { asm volatile("bar.sync 1, %0;" ::"n"(PL_NT) : "memory"); }
 

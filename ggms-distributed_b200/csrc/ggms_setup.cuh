@@ -63,11 +63,14 @@ struct CompileSmem {
   uint32_t sub_base[GRID_NC1];  // first sub-cell entry of a split cell (0xFFFFFFFF: not split)
   uint32_t split_cell[GRID_SUBCAP / 2];  // split cells in order (each has >= 2 sub-cells)
   uint32_t split_base[GRID_SUBCAP / 2];
+  uint32_t dev[GRID_NC1];       // max |PL - linear| at the knots inside a cell, in buckets
   uint32_t hist[33];
   uint32_t red[33];
   uint32_t thresh;
   uint32_t cap;
 };
+
+constexpr uint32_t GRID_DEV = 2;  // buckets of model deviation that make a cell worth splitting
 
 // sub-cell bits of a split cell with bucket span sp under depth cap (cap <= sh1)
 __device__ __forceinline__ uint32_t grid_sub_bits(uint32_t sp, int cap) {
@@ -102,16 +105,32 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
     cs.bnd[c] = b;
   }
   if (tid < 33) cs.hist[tid] = 0;
+  for (uint32_t c = tid; c < nc; c += NT) cs.dev[c] = 0;
   __syncthreads();
-  // Split heavy cells so that a sub-cell spans about one bucket: a cell of
-  // bucket span sp gets 2^min(bitlen(sp), cap) sub-cells.  cap is the largest
-  // depth (<= GRID_MAXSB) whose total fits GRID_SUBCAP entries over all cells
-  // with sp >= 4; if even depth 1 does not fit, only the cells with
-  // bitlen(sp) >= t are split (at depth 1), t the smallest value that fits.
-  for (uint32_t c = tid; c < nc; c += NT) {
-    const uint32_t sp = cs.bnd[c + 1] - cs.bnd[c];
-    if (sp >= 4u && sh1 >= 1) atomicAdd(&cs.hist[bitlen(sp)], 1u);
+  // Non-linearity of the model inside each cell: at every interior knot, the
+  // distance (in buckets) between the model and the cell's linear interpolation.
+  for (uint32_t k = 1 + tid; k < a.M; k += NT) {
+    const K xk = a.x[k];
+    const uint32_t c = (uint32_t)((K)(xk - lo) >> sh1);
+    if (c >= nc) continue;
+    const K off = (K)(xk - (K)(lo + ((K)c << sh1)));
+    const float lin = (float)cs.bnd[c] + (float)(cs.bnd[c + 1] - cs.bnd[c]) *
+                                             __fdiv_rn(key_to_float_rn(off), key_to_float_rn(w));
+    const float d = fabsf((float)a.base[k] - lin);
+    atomicMax(&cs.dev[c], (uint32_t)fminf(d, 1.0e9f));
   }
+  __syncthreads();
+  // Split the cells where the model bends (deviation >= GRID_DEV buckets) so
+  // that a sub-cell spans about one bucket: a cell of bucket span sp gets
+  // 2^min(bitlen(sp), cap) sub-cells.  cap is the largest depth (<= GRID_MAXSB)
+  // whose total fits GRID_SUBCAP entries; if even depth 1 does not fit, only the
+  // cells with bitlen(sp) >= t are split (at depth 1), t the smallest that fits.
+  auto wants_split = [&](uint32_t c) -> bool {
+    const uint32_t sp = cs.bnd[c + 1] - cs.bnd[c];
+    return sp >= 4u && sh1 >= 1 && cs.dev[c] >= GRID_DEV;
+  };
+  for (uint32_t c = tid; c < nc; c += NT)
+    if (wants_split(c)) atomicAdd(&cs.hist[bitlen(cs.bnd[c + 1] - cs.bnd[c])], 1u);
   __syncthreads();
   if (tid == 0) {
     uint32_t cap = 0, t = 3;
@@ -141,7 +160,7 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
     const uint32_t c = tid * 2 + k;
     if (c < nc) {
       const uint32_t sp = cs.bnd[c + 1] - cs.bnd[c];
-      if (cap && sp >= 4u && (uint32_t)bitlen(sp) >= thr) sz[k] = 1u << grid_sub_bits(sp, cap);
+      if (cap && wants_split(c) && (uint32_t)bitlen(sp) >= thr) sz[k] = 1u << grid_sub_bits(sp, cap);
     }
   }
   uint32_t total = 0;

@@ -37,6 +37,7 @@ ASSIGNER_SAMPLED = 1
 ASSIGNER_LEARNED_PL = 2
 ASSIGNER_LEARNED_MLP = 3
 ASSIGNER_NAMES = {0: "auto", 1: "sampled", 2: "learned_pl", 3: "learned_mlp"}
+PL_KNOTS = 1024   # segments of the learned piecewise-linear CDF
 
 SUFFIX = {np.dtype(np.float32): "f32", np.dtype(np.float64): "f64",
           np.dtype(np.uint32): "u32", np.dtype(np.int32): "i32"}
@@ -275,11 +276,11 @@ def _fp(a):
 def diag_pl_gradient(sorted_keys: np.ndarray, theta: np.ndarray):
     """GPU loss/gradient of the PL-CDF model; returns (loss, grad[:M], knots[:M+1])."""
     k = np.ascontiguousarray(sorted_keys, dtype=np.uint32)
-    th = np.zeros(256, np.float32)
+    th = np.zeros(PL_KNOTS, np.float32)
     th[:len(theta)] = theta
     loss = np.zeros(1, np.float32)
-    grad = np.zeros(256, np.float32)
-    knots = np.zeros(257, np.uint32)
+    grad = np.zeros(PL_KNOTS, np.float32)
+    knots = np.zeros(PL_KNOTS + 1, np.uint32)
     m = ctypes.c_int(0)
     rc = load().ggms_diag_pl_gradient(_fp(k), len(k), _fp(th), _fp(loss), _fp(grad), _fp(knots),
                                       ctypes.byref(m))

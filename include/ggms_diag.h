@@ -16,9 +16,10 @@ extern "C" {
 #endif
 
 /* PL-CDF model.  sorted_keys: S ascending uint32 keys (host).  The knots are
- * built exactly as the selector builds them (256 quantile knots, equal knots
- * merged); theta: 256 raw parameters (host).  Returns the loss, the gradient
- * w.r.t. theta (first M entries), the M+1 knots and M. */
+ * built exactly as the selector builds them (1024 quantile knots, equal knots
+ * merged); theta: 1024 raw parameters (host).  Returns the loss, the gradient
+ * w.r.t. theta (first M entries; grad holds 1024), the M+1 knots (knots holds
+ * 1025) and M. */
 GGMS_API int ggms_diag_pl_gradient(const uint32_t* sorted_keys, int S, const float* theta,
                                    float* loss, float* grad, uint32_t* knots, int* M);
 

@@ -64,10 +64,10 @@ def test_pl_gradient_matches_cpu(gen):
     v = D.VALUE_GENERATORS[gen](1 << 16, 5)
     keys = np.sort(orc.keys(v))
     g = np.random.default_rng(1)
-    theta = (0.5413 + 0.3 * g.standard_normal(256)).astype(np.float32)
+    theta = (0.5413 + 0.3 * g.standard_normal(G.PL_KNOTS)).astype(np.float32)
     loss, grad, knots = G.diag_pl_gradient(keys, theta)
     M = len(grad)
-    assert 16 <= M <= 256
+    assert 16 <= M <= G.PL_KNOTS
     th = theta[:M]
     ref_loss = pl_loss_cpu(keys, knots, th)
     ref_grad = pl_grad_cpu(keys, knots, th)
