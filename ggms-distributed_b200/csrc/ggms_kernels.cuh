@@ -252,13 +252,14 @@ __device__ void asg_build_from_knots(const K* sorted, const uint32_t* q, const f
       Bs[m] = b;
       ++m;
     }
-    // strictly increasing bases, capped at B-1 from the top
+    // strictly increasing bases in [1, B-1] (the callers keep m <= B - 1 so
+    // this is possible; the final clamp keeps every base in range regardless)
     Bs[0] = 1u;
     for (uint32_t t = 1; t < m; ++t) Bs[t] = max(Bs[t], Bs[t - 1] + 1u);
     Bs[m - 1] = max(Bs[m - 1], B - 1u);
     for (int t = (int)m - 1; t >= 0; --t) {
-      uint32_t cap = (B - 1u) - (uint32_t)((int)m - 1 - t);
-      Bs[t] = min(Bs[t], cap);
+      const long long cap = (long long)B - 1 - ((long long)m - 1 - t);
+      Bs[t] = (uint32_t)max(1LL, min((long long)Bs[t], cap));
     }
     if (m == 1) Bs[0] = 1u;
     Ms = m - 1;
@@ -384,7 +385,7 @@ __global__ __launch_bounds__(NT) void l0_count(const T* __restrict__ in, uint64_
       unpack16<T>(q[u], e);
       uint32_t b[EPV];
 #pragma unroll
-      for (int t = 0; t < EPV; ++t) b[t] = grid_eval<K>(gv, KeyOf<T>::to(e[t]));
+      for (int t = 0; t < EPV; ++t) b[t] = min(grid_eval<K>(gv, KeyOf<T>::to(e[t])), B - 1u);
       bool same = true;
 #pragma unroll
       for (int t = 1; t < EPV; ++t) same = same && (b[t] == b[0]);
@@ -402,14 +403,14 @@ __global__ __launch_bounds__(NT) void l0_count(const T* __restrict__ in, uint64_
     T e[EPV];
     unpack16<T>(ld_stream16(vbase + i * EPV), e);
 #pragma unroll
-    for (int t = 0; t < EPV; ++t) atomicAdd(&h[grid_eval<K>(gv, KeyOf<T>::to(e[t]))], 1u);
+    for (int t = 0; t < EPV; ++t) atomicAdd(&h[min(grid_eval<K>(gv, KeyOf<T>::to(e[t])), B - 1u)], 1u);
   }
   {
     const uint64_t tail0 = head + nvec * EPV;
     const uint64_t nscalar = head + (n - tail0);
     for (uint64_t j = gtid; j < nscalar; j += gstride) {
       const uint64_t idx = j < head ? j : tail0 + (j - head);
-      atomicAdd(&h[grid_eval<K>(gv, KeyOf<T>::to(in[idx]))], 1u);
+      atomicAdd(&h[min(grid_eval<K>(gv, KeyOf<T>::to(in[idx])), B - 1u)], 1u);
     }
   }
   __syncthreads();
@@ -628,7 +629,7 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
 #pragma unroll
       for (int t = 0; t < EPV; ++t) {
         const K key = KeyOf<T>::to(e[t]);
-        const uint32_t b = grid_eval<K>(gv, key);
+        const uint32_t b = min(grid_eval<K>(gv, key), B - 1u);
         if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
       }
     }
@@ -640,7 +641,7 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
 #pragma unroll
     for (int t = 0; t < EPV; ++t) {
       const K key = KeyOf<T>::to(e[t]);
-      const uint32_t b = grid_eval<K>(gv, key);
+      const uint32_t b = min(grid_eval<K>(gv, key), B - 1u);
       if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
     }
   }
@@ -650,7 +651,7 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
     for (uint64_t j = gtid; j < nscalar; j += gstride) {
       const uint64_t idx = j < head ? j : tail0 + (j - head);
       const K key = KeyOf<T>::to(in[idx]);
-      const uint32_t b = grid_eval<K>(gv, key);
+      const uint32_t b = min(grid_eval<K>(gv, key), B - 1u);
       if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
     }
   }

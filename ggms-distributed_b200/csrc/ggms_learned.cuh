@@ -222,7 +222,10 @@ __device__ void pl_set_bases(const float* cdf, Assigner<K>* A, uint32_t* Bs, uin
     Bs[0] = 1u;
     for (uint32_t t = 1; t <= M; ++t) Bs[t] = max(Bs[t], Bs[t - 1] + 1u);
     Bs[M] = max(Bs[M], B - 1u);
-    for (int t = (int)M; t >= 0; --t) Bs[t] = min(Bs[t], (B - 1u) - (M - (uint32_t)t));
+    for (int t = (int)M; t >= 0; --t) {
+      const long long cap = (long long)B - 1 - ((long long)M - t);
+      Bs[t] = (uint32_t)max(1LL, min((long long)Bs[t], cap));
+    }
     if (M == 0) Bs[0] = 1u;
     A->kind = kind;
   }
@@ -250,16 +253,23 @@ struct LearnSmem {
   uint32_t seg_start[PL_M + 1];
 };
 
+// Knots of the learned models: at most B/4 of them (every segment keeps at
+// least a few buckets, and strictly increasing bases fit in [1, B-1]).
+__host__ __device__ constexpr uint32_t pl_knots_for(uint32_t B) {
+  return (B / 4u) < (uint32_t)PL_M ? (B / 4u) : (uint32_t)PL_M;
+}
+
 // Quantile knots: q_j = round(j * (S - 1) / M), initial CDF j / M.
 template <typename K>
 __device__ void pl_knots(const K* sorted, uint32_t S, uint32_t B, uint32_t kind, Assigner<K>* A,
                          LearnSmem<K>& sm) {
-  for (uint32_t j = threadIdx.x; j <= (uint32_t)PL_M; j += blockDim.x) {
-    sm.q[j] = (uint32_t)(((uint64_t)j * (S - 1u) + PL_M / 2) / PL_M);
-    sm.qcdf[j] = (float)j / (float)PL_M;
+  const uint32_t Mq = pl_knots_for(B);
+  for (uint32_t j = threadIdx.x; j <= Mq; j += blockDim.x) {
+    sm.q[j] = (uint32_t)(((uint64_t)j * (S - 1u) + Mq / 2) / Mq);
+    sm.qcdf[j] = (float)j / (float)Mq;
   }
   __syncthreads();
-  asg_build_from_knots<K>(sorted, sm.q, sm.qcdf, PL_M, B, kind, A);
+  asg_build_from_knots<K>(sorted, sm.q, sm.qcdf, Mq, B, kind, A);
   __syncthreads();
 }
 

@@ -89,7 +89,8 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
   const K w = (K)1 << sh1;
   const uint32_t nc = (uint32_t)(span >> sh1) + 1u;        // interior cells
   const bool has_lo = lo >= w;                              // room for a low tail cell
-  const bool has_hi = (K)(KMAX - lo) >= (K)((K)nc << sh1);  // room for a high tail cell
+  // room for a high tail cell: KMAX - lo >= nc * w (computed without overflow)
+  const bool has_hi = ((K)(KMAX - lo) >> sh1) >= (K)nc;
   const uint32_t first = has_lo ? 1u : 0u;
   const K origin = has_lo ? (K)(lo - w) : lo;
   K gmax = KMAX;
@@ -101,8 +102,8 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
   for (uint32_t c = tid; c <= nc; c += NT) {
     uint32_t b;
     if (c < nc) b = asg_eval<K>(a, (K)(lo + ((K)c << sh1)));
-    else b = min(asg_eval<K>(a, hi) + 1u, B - 1u);
-    cs.bnd[c] = b;
+    else b = asg_eval<K>(a, hi) + 1u;
+    cs.bnd[c] = min(b, B - 1u);  // every grid entry stays a valid bucket
   }
   if (tid < 33) cs.hist[tid] = 0;
   for (uint32_t c = tid; c < nc; c += NT) cs.dev[c] = 0;
@@ -220,7 +221,7 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
     auto bnd_at = [&](uint32_t q) -> uint32_t {
       if (q == (1u << sb)) return cs.bnd[c + 1];
       const K off = (K)q << shs;
-      return off > room ? cs.bnd[c + 1] : asg_eval<K>(a, (K)(cell_lo + off));
+      return off > room ? cs.bnd[c + 1] : min(asg_eval<K>(a, (K)(cell_lo + off)), cs.bnd[c + 1]);
     };
     const uint2 e = make_uint2(bnd_at(s), bnd_at(s + 1));
     s2[i] = e;
