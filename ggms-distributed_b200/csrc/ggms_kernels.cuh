@@ -203,104 +203,6 @@ __global__ void asg_merge_rank(const K* __restrict__ chunks, K* sorted, uint32_t
   sorted[rank] = key;
 }
 
-// ------------------------------------------------------------------ assigner build
-// Builds a PL assigner from knot candidates.  The knot keys are
-// sorted[q[j]] for j = 0..Mreq, their target CDF values cdf[j] in [0, 1]
-// (cdf[0] = 0, cdf[Mreq] = 1).  Equal knots (an atom of the sample) are merged;
-// an atom v gets a bucket of its own by an extra knot at v+1.  Bases are made
-// strictly increasing so that distinct knots never share a bucket.
-template <typename K>
-__device__ void asg_build_from_knots(const K* sorted, const uint32_t* q, const float* cdf,
-                                     uint32_t Mreq, uint32_t B, uint32_t kind, Assigner<K>* A) {
-  __shared__ K X[ASG_MAXM + 2];
-  __shared__ uint32_t Bs[ASG_MAXM + 2];
-  __shared__ K XK[ASG_MAXM + 1];
-  __shared__ uint32_t Ms;
-  for (uint32_t j = threadIdx.x; j <= Mreq; j += blockDim.x) XK[j] = sorted[q[j]];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const float span = (float)(B - 2u);
-    uint32_t m = 0;
-    uint32_t prev_b = 1;
-    // dedupe; remember the base at the end of each run of equal knots
-    uint32_t atom_end_b = 0;
-    bool atom = false;
-    for (uint32_t j = 0; j <= Mreq; ++j) {
-      K xk = XK[j];
-      float f = fminf(fmaxf(cdf[j], 0.0f), 1.0f);
-      uint32_t b = 1u + (uint32_t)__float2uint_rn(f * span);
-      if (j == 0) b = 1u;
-      if (j == Mreq) b = B - 1u;
-      b = max(b, prev_b);
-      prev_b = b;
-      if (m > 0 && xk == X[m - 1]) {
-        atom = true;
-        atom_end_b = b;
-        continue;
-      }
-      if (atom && m > 0) {
-        // close the atom at X[m-1]: keys above it start at the run's end base
-        K v = X[m - 1];
-        if (v + 1 < xk && m < ASG_MAXM + 1) {
-          X[m] = v + 1;
-          Bs[m] = max(Bs[m - 1] + 1u, atom_end_b);
-          ++m;
-        }
-        atom = false;
-      }
-      X[m] = xk;
-      Bs[m] = b;
-      ++m;
-    }
-    // strictly increasing bases in [1, B-1] (the callers keep m <= B - 1 so
-    // this is possible; the final clamp keeps every base in range regardless)
-    Bs[0] = 1u;
-    for (uint32_t t = 1; t < m; ++t) Bs[t] = max(Bs[t], Bs[t - 1] + 1u);
-    Bs[m - 1] = max(Bs[m - 1], B - 1u);
-    for (int t = (int)m - 1; t >= 0; --t) {
-      const long long cap = (long long)B - 1 - ((long long)m - 1 - t);
-      Bs[t] = (uint32_t)max(1LL, min((long long)Bs[t], cap));
-    }
-    if (m == 1) Bs[0] = 1u;
-    Ms = m - 1;
-    A->M = m - 1;
-    A->B = B;
-    A->kind = kind;
-    A->loss = 0.0f;
-    const K span_k = X[m - 1] - X[0];
-    const int sh = max(0, bitlen(span_k) - ASG_CELL_BITS);
-    A->csh = (uint32_t)sh;
-    A->ncell = (uint32_t)(span_k >> sh) + 1u;
-  }
-  __syncthreads();
-  const uint32_t M = Ms;
-  for (uint32_t t = threadIdx.x; t <= M; t += blockDim.x) {
-    A->x[t] = X[t];
-    A->base[t] = Bs[t];
-    if (t < M) {
-      float db = (float)(Bs[t + 1] - Bs[t]);
-      float dx = key_to_float_rn((K)(X[t + 1] - X[t]));
-      A->slope[t] = __fdiv_rn(db, dx);
-    }
-  }
-  __syncthreads();
-  // cell index: idx[c] = last segment j <= M-1 whose knot is <= the cell's first key
-  const uint32_t csh = A->csh, ncell = A->ncell;
-  for (uint32_t c = threadIdx.x; c < (uint32_t)ASG_NCELL; c += blockDim.x) {
-    uint32_t j = 0;
-    if (c < ncell && M > 0) {
-      K start = X[0] + ((K)c << csh);
-      uint32_t lo = 0, hi = M - 1;  // largest j in [0, M-1] with X[j] <= start
-      while (lo < hi) {
-        uint32_t mid = (lo + hi + 1) >> 1;
-        if (X[mid] <= start) lo = mid; else hi = mid - 1;
-      }
-      j = lo;
-    }
-    A->idx[c] = (uint16_t)j;
-  }
-}
-
 template <typename K>
 __device__ __forceinline__ AsgView<K> asg_view_global(const Assigner<K>* A) {
   AsgView<K> v;

@@ -52,6 +52,174 @@ __device__ V block_sum(V v, V* red) {
   return tot;
 }
 
+// ------------------------------------------------------------------ PL model build
+// Exclusive prefix max over the block in thread order (identity for thread 0).
+template <typename V>
+__device__ V block_excl_max(V v, V ident, V* red) {
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  V inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const V t = __shfl_up_sync(FULL, inc, o);
+    if ((int)lane >= o) inc = max(inc, t);
+  }
+  V ex = __shfl_up_sync(FULL, inc, 1);
+  if (lane == 0) ex = ident;
+  if (lane == 31) red[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    V w = lane < (blockDim.x >> 5) ? red[lane] : ident;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const V t = __shfl_up_sync(FULL, w, o);
+      if ((int)lane >= o) w = max(w, t);
+    }
+    red[lane] = w;
+  }
+  __syncthreads();
+  const V out = warp ? max(ex, red[warp - 1]) : ex;
+  __syncthreads();
+  return out;
+}
+
+struct BuildSmem {
+  uint32_t jb[ASG_MAXM + 1];    // base of knot candidate j, non-decreasing in j
+  uint32_t rend[ASG_MAXM + 1];  // last candidate of the run of equal knots starting at j
+  uint32_t red_u[32];
+  int32_t red_i[32];
+};
+
+// Builds a PL assigner from knot candidates: candidate j is sorted[q[j]] with
+// target CDF cdf[j] (cdf[0] = 0, cdf[Mreq] = 1), j = 0..Mreq, Mreq <= ASG_MAXM.
+// Runs of equal candidates (an atom of the sample) become one knot; an atom v
+// gets a bucket of its own by an extra knot at v+1 whose base is the base at
+// the run's end.  Bases are then made strictly increasing (distinct knots never
+// share a bucket) and kept in [1, B-1].  Every step is a block-wide prefix
+// scan over the candidates, two per thread; needs blockDim.x == SETUP_NT.
+template <typename K>
+__device__ void asg_build_from_knots(const K* sorted, const uint32_t* q, const float* cdf,
+                                     uint32_t Mreq, uint32_t B, uint32_t kind, Assigner<K>* A) {
+  __shared__ K XK[ASG_MAXM + 1];
+  __shared__ K X[ASG_MAXM + 1];
+  __shared__ uint32_t Bs[ASG_MAXM + 1];
+  __shared__ BuildSmem bs;
+  const uint32_t tid = threadIdx.x;
+  const float span = (float)(B - 2u);
+  // 1. candidate keys and bases; bases made non-decreasing by a prefix max
+  uint32_t b2[2] = {0u, 0u};
+  for (uint32_t k = 0; k < 2; ++k) {
+    const uint32_t j = tid * 2 + k;
+    if (j <= Mreq) {
+      XK[j] = sorted[q[j]];
+      const float f = fminf(fmaxf(cdf[j], 0.0f), 1.0f);
+      uint32_t b = 1u + __float2uint_rn(f * span);
+      if (j == 0) b = 1u;
+      if (j == Mreq) b = B - 1u;
+      b2[k] = b;
+    }
+  }
+  b2[1] = max(b2[1], b2[0]);
+  const uint32_t bex = block_excl_max<uint32_t>(b2[1], 0u, bs.red_u);  // also syncs XK
+  // 2. run starts; every candidate learns its run's start by a prefix max
+  bool start[2];
+  uint32_t rs2[2] = {0u, 0u};
+  for (uint32_t k = 0; k < 2; ++k) {
+    const uint32_t j = tid * 2 + k;
+    start[k] = j <= Mreq && (j == 0 || XK[j] != XK[j - 1]);
+    if (j <= Mreq) bs.jb[j] = max(b2[k], bex);
+    rs2[k] = start[k] ? j : 0u;
+  }
+  rs2[1] = max(rs2[1], rs2[0]);
+  const uint32_t rsex = block_excl_max<uint32_t>(rs2[1], 0u, bs.red_u);
+  for (uint32_t k = 0; k < 2; ++k) {
+    const uint32_t j = tid * 2 + k;
+    const bool end = j <= Mreq && (j == Mreq || XK[j + 1] != XK[j]);
+    if (end) bs.rend[max(k ? rs2[1] : rs2[0], rsex)] = j;
+  }
+  __syncthreads();
+  // 3. emit: a run start gives its knot, plus v+1 after an atom with room above
+  uint32_t emit[2] = {0u, 0u};
+  for (uint32_t k = 0; k < 2; ++k) {
+    const uint32_t j = tid * 2 + k;
+    if (start[k]) {
+      const uint32_t e = bs.rend[j];
+      emit[k] = (e > j && e < Mreq && (K)(XK[j] + 1) < XK[e + 1]) ? 2u : 1u;
+    }
+  }
+  uint32_t m = 0;
+  uint32_t at = block_excl_scan<uint32_t>(emit[0] + emit[1], bs.red_u, &m);
+  for (uint32_t k = 0; k < 2; ++k) {
+    const uint32_t j = tid * 2 + k;
+    if (emit[k]) {
+      X[at] = XK[j];
+      Bs[at] = bs.jb[j];
+      if (emit[k] == 2u) {
+        X[at + 1] = (K)(XK[j] + 1);
+        Bs[at + 1] = max(bs.jb[j] + 1u, bs.jb[bs.rend[j]]);
+      }
+      at += emit[k];
+    }
+  }
+  __syncthreads();
+  // 4. strictly increasing: Bs'[t] = t + max_{t' <= t} (Bs[t'] - t'), Bs'[0] = 1;
+  //    then the last knot at B-1 at least and every knot below the room it leaves
+  int32_t d2[2] = {INT32_MIN, INT32_MIN};
+  for (uint32_t k = 0; k < 2; ++k) {
+    const uint32_t t = tid * 2 + k;
+    if (t < m) d2[k] = ((t == 0) ? 1 : (int32_t)Bs[t]) - (int32_t)t;
+  }
+  d2[1] = max(d2[1], d2[0]);
+  const int32_t dex = block_excl_max<int32_t>(d2[1], INT32_MIN, bs.red_i);
+  for (uint32_t k = 0; k < 2; ++k) {
+    const uint32_t t = tid * 2 + k;
+    if (t < m) {
+      long long b = (long long)max(d2[k], dex) + (long long)t;
+      if (t == m - 1) b = max(b, (long long)B - 1);
+      const long long cap = (long long)B - 1 - ((long long)m - 1 - t);
+      b = max(1LL, min(b, cap));
+      if (m == 1) b = 1;
+      Bs[t] = (uint32_t)b;
+    }
+  }
+  __syncthreads();
+  const uint32_t M = m - 1;
+  const K span_k = X[M] - X[0];
+  const int csh = max(0, bitlen(span_k) - ASG_CELL_BITS);
+  const uint32_t ncell = (uint32_t)(span_k >> csh) + 1u;
+  if (tid == 0) {
+    A->M = M;
+    A->B = B;
+    A->kind = kind;
+    A->loss = 0.0f;
+    A->csh = (uint32_t)csh;
+    A->ncell = ncell;
+  }
+  for (uint32_t t = tid; t <= M; t += blockDim.x) {
+    A->x[t] = X[t];
+    A->base[t] = Bs[t];
+    if (t < M) {
+      const float db = (float)(Bs[t + 1] - Bs[t]);
+      const float dx = key_to_float_rn((K)(X[t + 1] - X[t]));
+      A->slope[t] = __fdiv_rn(db, dx);
+    }
+  }
+  // cell index: idx[c] = last segment j <= M-1 whose knot is <= the cell's first key
+  for (uint32_t c = tid; c < (uint32_t)ASG_NCELL; c += blockDim.x) {
+    uint32_t j = 0;
+    if (c < ncell && M > 0) {
+      const K cstart = X[0] + ((K)c << csh);
+      uint32_t lo = 0, hi = M - 1;  // largest j in [0, M-1] with X[j] <= cstart
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (X[mid] <= cstart) lo = mid; else hi = mid - 1;
+      }
+      j = lo;
+    }
+    A->idx[c] = (uint16_t)j;
+  }
+  __syncthreads();
+}
+
 // ------------------------------------------------------------------ grid compilation
 // Resamples a monotone model (the PL assigner `a`) onto the grid; the heaviest
 // bucket span is at least T (the smallest power of two >= 4x the mean span that
@@ -70,7 +238,7 @@ struct CompileSmem {
   uint32_t cap;
 };
 
-constexpr uint32_t GRID_DEV = 2;  // buckets of model deviation that make a cell worth splitting
+constexpr uint32_t GRID_DEV = 8;  // buckets of model deviation that make a cell worth splitting
 
 // sub-cell bits of a split cell with bucket span sp under depth cap (cap <= sh1)
 __device__ __forceinline__ uint32_t grid_sub_bits(uint32_t sp, int cap) {
