@@ -22,7 +22,9 @@ PKG_ROOT = os.path.dirname(_HERE)
 REPO_ROOT = os.path.dirname(PKG_ROOT)
 LIB_PATH = os.path.join(PKG_ROOT, "lib", "libggms_b200.so")
 HEADER_PATHS = [os.path.join(REPO_ROOT, "include", "ggms.h"),
-                os.path.join(REPO_ROOT, "include", "ggms_diag.h")]
+                os.path.join(REPO_ROOT, "include", "ggms_diag.h"),
+                os.path.join(REPO_ROOT, "include", "ggms_noalloc.h")]
+NOALLOC_MAX_KS = 1024
 
 GGMS_OK = 0
 GGMS_E_INVALID_ARG = 1
@@ -137,6 +139,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ggms_diag_mlp_gradient.argtypes = [vp, vp, vp, vp, vp]
     lib.ggms_diag_fit.restype = i32
     lib.ggms_diag_fit.argtypes = [vp, i32, i32, i32, vp, vp, vp, vp]
+    lib.ggms_multiselect_noalloc_f32.restype = i32
+    lib.ggms_multiselect_noalloc_f32.argtypes = [vp, i64, u32p, ctypes.c_int32, vp, vp]
     _lib = lib
     return lib
 
@@ -255,6 +259,17 @@ def segmented(ctx: Optional[Context], d_ptr: int, seg_off_ptr: int, nseg: int, k
               int(nseg), ctypes.c_void_p(ks_ptr), ctypes.c_void_p(k_off_ptr),
               ctypes.c_void_p(out_ptr), ctypes.byref(opts) if opts is not None else None,
               ctypes.c_void_p(stream))
+
+
+def multiselect_noalloc_f32(d_ptr: int, n: int, ks: np.ndarray, out_ptr: int, stream: int = 0) -> int:
+    """ggms_multiselect_noalloc_f32: float32 vector and output in device memory,
+    ks (1-based k-th largest) in host memory; enqueues on `stream` and returns
+    the status without a host sync."""
+    lib = load()
+    ks = np.ascontiguousarray(ks, dtype=np.uint32)
+    return lib.ggms_multiselect_noalloc_f32(ctypes.c_void_p(d_ptr), int(n),
+                                            ks.ctypes.data_as(ctypes.c_void_p), int(len(ks)),
+                                            ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream))
 
 
 def declared_symbols(paths=None):
