@@ -286,7 +286,9 @@ constexpr int MAX_LEVELS_64 = 6;
 template <typename T>
 static size_t l0_count_smem(uint32_t B) { return GRID_SMEM + (size_t)B * 4u; }
 template <typename T>
-static size_t l0_compact_smem(uint32_t B) { return GRID_SMEM + (MAX_B0 / 32) * 4u + (size_t)B * 4u; }
+static size_t l0_compact_smem(uint32_t B) {
+  return GRID_SMEM + (2 * (MAX_B0 / 32) + 1 + HOT_WORDS) * 4u + (size_t)B * 4u;
+}
 
 // Launch shapes of the two passes (CTA size x 16-byte loads in flight per
 // thread); the default and the autotuner pick among these instantiations.

@@ -478,7 +478,11 @@ __global__ void l0_bases(uint32_t* crow, uint32_t B, uint32_t ncta, const Seg<K>
 // PASS 1; a key whose bucket is copied goes to slot atomicAdd(&cur[b], 1) of
 // this CTA's private range (a shared-memory atomic: no global round trip).
 // A shared bitmask says which buckets are copied (not points, not inactive).
+// Most keys lie in grid cells without a copied bucket: a second bitmask over
+// the grid's top-level cells ("hot" cells) rejects those with one shift and
+// one shared load, before the bucket is computed.
 constexpr uint32_t MAX_B0 = 1u << 15;
+constexpr uint32_t HOT_WORDS = (GRID_T1 + 31) / 32;
 
 template <typename T, int NT, int UNROLL>
 __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint64_t n,
@@ -493,17 +497,56 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
   uint2* s1 = (uint2*)smem;
   uint2* s2 = s1 + GRID_T1;
   uint32_t* amask = (uint32_t*)(smem + GRID_SMEM);  // [MAX_B0 / 32]
-  uint32_t* cur = amask + MAX_B0 / 32;               // [B]
+  uint32_t* wpre = amask + MAX_B0 / 32;              // [MAX_B0 / 32 + 1]: copied buckets before word w
+  uint32_t* hot = wpre + MAX_B0 / 32 + 1;            // [HOT_WORDS]
+  uint32_t* cur = hot + HOT_WORDS;                   // [B]
   const GridView<K> gv = grid_to_smem<K>(G, s1, s2);
-  const uint32_t B = gv.B;
-  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t B = gv.B, ncell = G->ncell;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t* myrow = crow + (size_t)blockIdx.x * B;
-  for (uint32_t w = threadIdx.x >> 5; w < B / 32; w += NT / 32) {
+  for (uint32_t w = warp; w < B / 32; w += NT / 32) {
     const uint32_t b = w * 32 + lane;
     const bool copied = cmap0[b] < CM_POINT;
     if (copied) cur[b] = myrow[b];
     const uint32_t bits = __ballot_sync(FULL, copied);
-    if (lane == 0) amask[w] = bits;
+    if (lane == 0) {
+      amask[w] = bits;
+      wpre[w] = __popc(bits);
+    }
+  }
+  for (uint32_t w = threadIdx.x; w < HOT_WORDS; w += NT) hot[w] = 0u;
+  __syncthreads();
+  if (warp == 0) {  // exclusive prefix of the per-word counts (B / 32 <= 1024 words)
+    uint32_t run = 0;
+    for (uint32_t w0 = 0; w0 < B / 32; w0 += 32) {
+      const uint32_t v = wpre[w0 + lane];
+      uint32_t inc = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(FULL, inc, o);
+        if ((int)lane >= o) inc += t;
+      }
+      wpre[w0 + lane] = run + inc - v;
+      run += __shfl_sync(FULL, inc, 31);
+    }
+    if (lane == 0) wpre[B / 32] = run;
+  }
+  __syncthreads();
+  {
+    // a cell is hot when a copied bucket lies in [bucket of its first key,
+    // bucket of its last key] (the grid is monotone in the key)
+    auto rank = [&](uint32_t b) {  // copied buckets below b, b <= B
+      const uint32_t w = b >> 5;
+      return (b & 31) ? wpre[w] + __popc(amask[w] & ((1u << (b & 31)) - 1u)) : wpre[w];
+    };
+    const K dmax = (K)(gv.gmax - gv.origin);
+    for (uint32_t c = threadIdx.x; c < ncell; c += NT) {
+      const K d0 = (K)c << gv.sh1;
+      const K d1 = (c + 1u < ncell) ? (K)(((K)(c + 1u) << gv.sh1) - 1u) : dmax;
+      const uint32_t lo = min(grid_eval<K>(gv, (K)(gv.origin + d0)), B - 1u);
+      const uint32_t hi = min(grid_eval<K>(gv, (K)(gv.origin + min(d1, dmax))), B - 1u);
+      if (rank(hi + 1u) != rank(lo)) atomicOr(&hot[c >> 5], 1u << (c & 31));
+    }
   }
   __syncthreads();
 
@@ -519,6 +562,11 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
     const uint32_t slot = atomicAdd(&cur[b], 1u);
     if (slot < dst_cap) dst[slot] = key; else overflow = true;
   };
+  auto in_hot = [&](K key) {
+    const K kc = min(max(key, gv.origin), gv.gmax);
+    const uint32_t c = (uint32_t)((K)(kc - gv.origin) >> gv.sh1);
+    return (hot[c >> 5] >> (c & 31)) & 1u;
+  };
 
   for (uint64_t r = 0; r < rounds; ++r, vp += gstride * UNROLL) {
     uint4 q[UNROLL];
@@ -531,8 +579,10 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
 #pragma unroll
       for (int t = 0; t < EPV; ++t) {
         const K key = KeyOf<T>::to(e[t]);
-        const uint32_t b = min(grid_eval<K>(gv, key), B - 1u);
-        if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
+        if (in_hot(key)) {
+          const uint32_t b = min(grid_eval<K>(gv, key), B - 1u);
+          if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
+        }
       }
     }
   }
@@ -543,8 +593,10 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
 #pragma unroll
     for (int t = 0; t < EPV; ++t) {
       const K key = KeyOf<T>::to(e[t]);
-      const uint32_t b = min(grid_eval<K>(gv, key), B - 1u);
-      if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
+      if (in_hot(key)) {
+        const uint32_t b = min(grid_eval<K>(gv, key), B - 1u);
+        if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
+      }
     }
   }
   {
@@ -553,8 +605,10 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
     for (uint64_t j = gtid; j < nscalar; j += gstride) {
       const uint64_t idx = j < head ? j : tail0 + (j - head);
       const K key = KeyOf<T>::to(in[idx]);
-      const uint32_t b = min(grid_eval<K>(gv, key), B - 1u);
-      if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
+      if (in_hot(key)) {
+        const uint32_t b = min(grid_eval<K>(gv, key), B - 1u);
+        if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
+      }
     }
   }
   if (overflow) set_status(C, GGMS_E_INTERNAL);

@@ -212,23 +212,16 @@ __device__ float pl_train_block(const PLStats* st, uint32_t M, uint32_t S, uint3
 // at its knots.  All threads call it.
 template <typename K>
 __device__ void pl_set_bases(const float* cdf, Assigner<K>* A, uint32_t* Bs, uint32_t kind) {
+  __shared__ int32_t red[32];
   const uint32_t M = A->M, B = A->B;
-  if (threadIdx.x == 0) {
-    const float span = (float)(B - 2u);
-    for (uint32_t t = 0; t <= M; ++t) {
-      const float f = fminf(fmaxf(cdf[t], 0.0f), 1.0f);
-      Bs[t] = 1u + __float2uint_rn(f * span);
-    }
-    Bs[0] = 1u;
-    for (uint32_t t = 1; t <= M; ++t) Bs[t] = max(Bs[t], Bs[t - 1] + 1u);
-    Bs[M] = max(Bs[M], B - 1u);
-    for (int t = (int)M; t >= 0; --t) {
-      const long long cap = (long long)B - 1 - ((long long)M - t);
-      Bs[t] = (uint32_t)max(1LL, min((long long)Bs[t], cap));
-    }
-    if (M == 0) Bs[0] = 1u;
-    A->kind = kind;
+  const float span = (float)(B - 2u);
+  for (uint32_t t = threadIdx.x; t <= M; t += blockDim.x) {
+    const float f = fminf(fmaxf(cdf[t], 0.0f), 1.0f);
+    Bs[t] = 1u + __float2uint_rn(f * span);
   }
+  __syncthreads();
+  strict_bases(Bs, M + 1u, B, red);
+  if (threadIdx.x == 0) A->kind = kind;
   __syncthreads();
   for (uint32_t t = threadIdx.x; t <= M; t += blockDim.x) {
     A->base[t] = Bs[t];

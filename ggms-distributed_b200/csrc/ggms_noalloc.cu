@@ -132,7 +132,7 @@ __global__ __launch_bounds__(CNT_NT) void na_count(const float* __restrict__ in,
         const uint32_t u = f32_key(v[j]);
         uint32_t s = 0;
         bool hit = true;
-        if (L > 0) {
+        if constexpr (L > 0) {
           const uint32_t t16 = u >> 16;
           hit = (bmap[t16 >> 5] >> (t16 & 31)) & 1u;
           if (hit) {

@@ -82,6 +82,34 @@ __device__ V block_excl_max(V v, V ident, V* red) {
   return out;
 }
 
+// Makes the bases Bs[0..m) of m knots strictly increasing and keeps them in
+// [1, B-1] (m <= B - 1, m <= 2 * blockDim.x; all threads call it):
+//   Bs[0] = 1;  Bs[t] = max(Bs[t], Bs[t-1] + 1)    (= t + max_{t' <= t} (Bs[t'] - t'))
+//   Bs[m-1] = max(Bs[m-1], B - 1);  Bs[t] = max(1, min(Bs[t], B - 1 - (m - 1 - t)))
+// The running maximum is one block-wide prefix max, two knots per thread.
+__device__ void strict_bases(uint32_t* Bs, uint32_t m, uint32_t B, int32_t* red) {
+  const uint32_t tid = threadIdx.x;
+  int32_t d2[2] = {INT32_MIN, INT32_MIN};
+  for (uint32_t k = 0; k < 2; ++k) {
+    const uint32_t t = tid * 2 + k;
+    if (t < m) d2[k] = ((t == 0) ? 1 : (int32_t)Bs[t]) - (int32_t)t;
+  }
+  d2[1] = max(d2[1], d2[0]);
+  const int32_t dex = block_excl_max<int32_t>(d2[1], INT32_MIN, red);  // syncs: all reads done
+  for (uint32_t k = 0; k < 2; ++k) {
+    const uint32_t t = tid * 2 + k;
+    if (t < m) {
+      long long b = (long long)max(d2[k], dex) + (long long)t;
+      if (t == m - 1) b = max(b, (long long)B - 1);
+      const long long cap = (long long)B - 1 - ((long long)m - 1 - t);
+      b = max(1LL, min(b, cap));
+      if (m == 1) b = 1;
+      Bs[t] = (uint32_t)b;
+    }
+  }
+  __syncthreads();
+}
+
 struct BuildSmem {
   uint32_t jb[ASG_MAXM + 1];    // base of knot candidate j, non-decreasing in j
   uint32_t rend[ASG_MAXM + 1];  // last candidate of the run of equal knots starting at j
@@ -161,27 +189,8 @@ __device__ void asg_build_from_knots(const K* sorted, const uint32_t* q, const f
     }
   }
   __syncthreads();
-  // 4. strictly increasing: Bs'[t] = t + max_{t' <= t} (Bs[t'] - t'), Bs'[0] = 1;
-  //    then the last knot at B-1 at least and every knot below the room it leaves
-  int32_t d2[2] = {INT32_MIN, INT32_MIN};
-  for (uint32_t k = 0; k < 2; ++k) {
-    const uint32_t t = tid * 2 + k;
-    if (t < m) d2[k] = ((t == 0) ? 1 : (int32_t)Bs[t]) - (int32_t)t;
-  }
-  d2[1] = max(d2[1], d2[0]);
-  const int32_t dex = block_excl_max<int32_t>(d2[1], INT32_MIN, bs.red_i);
-  for (uint32_t k = 0; k < 2; ++k) {
-    const uint32_t t = tid * 2 + k;
-    if (t < m) {
-      long long b = (long long)max(d2[k], dex) + (long long)t;
-      if (t == m - 1) b = max(b, (long long)B - 1);
-      const long long cap = (long long)B - 1 - ((long long)m - 1 - t);
-      b = max(1LL, min(b, cap));
-      if (m == 1) b = 1;
-      Bs[t] = (uint32_t)b;
-    }
-  }
-  __syncthreads();
+  // 4. strictly increasing bases in [1, B-1]
+  strict_bases(Bs, m, B, bs.red_i);
   const uint32_t M = m - 1;
   const K span_k = X[M] - X[0];
   const int csh = max(0, bitlen(span_k) - ASG_CELL_BITS);
