@@ -286,8 +286,9 @@ constexpr int MAX_LEVELS_64 = 6;
 template <typename T>
 static size_t l0_count_smem(uint32_t B) { return GRID_SMEM + (size_t)B * 4u; }
 template <typename T>
-static size_t l0_compact_smem(uint32_t B) {
-  return GRID_SMEM + (2 * (MAX_B0 / 32) + 1 + HOT_WORDS) * 4u + (size_t)B * 4u;
+static size_t l0_compact_smem(uint32_t B, int nt) {
+  return GRID_SMEM + (MAX_B0 / 32 + l0_compact_qwords((uint32_t)nt, sizeof(typename KeyOf<T>::K)) + HOT_WORDS) * 4u +
+         (size_t)B * 4u;
 }
 
 // Launch shapes of the two passes (CTA size x 16-byte loads in flight per
@@ -325,7 +326,7 @@ constexpr int DEFAULT_PASS_UNROLL = 4;
 // CTAs as fit on every SM at once for the larger of the two.
 template <typename T>
 static int l0_ncta(Context* c, const PassVariant<T>* pv, uint32_t B, uint32_t* ncta) {
-  const size_t s1 = l0_count_smem<T>(B), s2 = l0_compact_smem<T>(B);
+  const size_t s1 = l0_count_smem<T>(B), s2 = l0_compact_smem<T>(B, pv->nt);
   GGMS_CU(cudaFuncSetAttribute((const void*)pv->count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
   GGMS_CU(cudaFuncSetAttribute((const void*)pv->compact, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
   int o1 = 0, o2 = 0;
@@ -491,7 +492,7 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   // ---- PASS 2: compact the buckets that still need refinement
   prof_rec(prof, 3, st);
   ++ctx->launches;
-  pv->compact<<<grid_c, pv->nt, l0_compact_smem<T>(p.B), st>>>(d_in, n, w.grid, w.C, w.cmap0, w.crow,
+  pv->compact<<<grid_c, pv->nt, l0_compact_smem<T>(p.B, pv->nt), st>>>(d_in, n, w.grid, w.C, w.cmap0, w.crow,
                                                                  w.cand[0], (uint64_t)n);
   prof_rec(prof, 4, st);
   rc = launch_small_select<K>(ctx, w.cand[0], w.segs[1], w.khead[1], w, caps, st);

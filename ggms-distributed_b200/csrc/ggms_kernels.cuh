@@ -481,8 +481,21 @@ __global__ void l0_bases(uint32_t* crow, uint32_t B, uint32_t ncta, const Seg<K>
 // Most keys lie in grid cells without a copied bucket: a second bitmask over
 // the grid's top-level cells ("hot" cells) rejects those with one shift and
 // one shared load, before the bucket is computed.
+// Keys that pass the cell test are queued per warp in shared memory and
+// bucketed 32 at a time, one per lane: the few hot keys are spread over the
+// input, and handling each where it is found would run the long path for
+// every warp that holds one (about half of them at 2% hot keys).
 constexpr uint32_t MAX_B0 = 1u << 15;
 constexpr uint32_t HOT_WORDS = (GRID_T1 + 31) / 32;
+constexpr uint32_t WQ_DEPTH = 64;  // per-warp queue slots: < 32 waiting + 32 appended
+constexpr uint32_t L0_RUNS = 4;    // hot-cell runs tested by key compares (more: the cell bitmask)
+
+// 32-bit words of the region shared by the prologue's prefix table and,
+// afterwards, the per-warp queues.
+__host__ __device__ constexpr uint32_t l0_compact_qwords(uint32_t nt, uint32_t key_bytes) {
+  return (MAX_B0 / 32 + 1) > (nt / 32) * WQ_DEPTH * key_bytes / 4 ? (MAX_B0 / 32 + 1)
+                                                                   : (nt / 32) * WQ_DEPTH * key_bytes / 4;
+}
 
 template <typename T, int NT, int UNROLL>
 __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint64_t n,
@@ -498,7 +511,8 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
   uint2* s2 = s1 + GRID_T1;
   uint32_t* amask = (uint32_t*)(smem + GRID_SMEM);  // [MAX_B0 / 32]
   uint32_t* wpre = amask + MAX_B0 / 32;              // [MAX_B0 / 32 + 1]: copied buckets before word w
-  uint32_t* hot = wpre + MAX_B0 / 32 + 1;            // [HOT_WORDS]
+  constexpr uint32_t QW = l0_compact_qwords(NT, sizeof(K));
+  uint32_t* hot = wpre + QW;                         // [HOT_WORDS]
   uint32_t* cur = hot + HOT_WORDS;                   // [B]
   const GridView<K> gv = grid_to_smem<K>(G, s1, s2);
   const uint32_t B = gv.B, ncell = G->ncell;
@@ -549,6 +563,41 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
     }
   }
   __syncthreads();
+  // Maximal runs of hot cells as key intervals [lo, lo + span]; with at most
+  // L0_RUNS of them the cell test becomes a few compares in registers.
+  __shared__ K run_lo[L0_RUNS], run_span[L0_RUNS];
+  __shared__ uint32_t nruns_s;
+  if (threadIdx.x == 0) {
+    uint32_t nr = 0, start = 0;
+    bool in_run = false;
+    auto record = [&](uint32_t c0, uint32_t c1) {
+      if (nr < L0_RUNS) {
+        const K lo = (c0 == 0) ? (K)0 : (K)(gv.origin + ((K)c0 << gv.sh1));
+        const K hi = (c1 + 1u >= ncell) ? key_max<K>() : (K)(gv.origin + ((K)(c1 + 1u) << gv.sh1) - 1u);
+        run_lo[nr] = lo;
+        run_span[nr] = (K)(hi - lo);
+      }
+      ++nr;
+    };
+    for (uint32_t w = 0; w < HOT_WORDS && nr <= L0_RUNS; ++w) {
+      const uint32_t bits = hot[w];
+      if ((!in_run && bits == 0u) || (in_run && bits == FULL)) continue;
+      for (uint32_t b = 0; b < 32; ++b) {
+        const uint32_t c = w * 32 + b;
+        const bool hb = c < ncell && ((bits >> b) & 1u);
+        if (hb && !in_run) {
+          in_run = true;
+          start = c;
+        } else if (!hb && in_run) {
+          in_run = false;
+          record(start, c - 1u);
+        }
+      }
+    }
+    if (in_run) record(start, ncell - 1u);
+    nruns_s = nr;
+  }
+  __syncthreads();
 
   const uint64_t gtid = (uint64_t)blockIdx.x * NT + threadIdx.x;
   const uint64_t gstride = (uint64_t)gridDim.x * NT;
@@ -568,24 +617,80 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
     return (hot[c >> 5] >> (c & 31)) & 1u;
   };
 
-  for (uint64_t r = 0; r < rounds; ++r, vp += gstride * UNROLL) {
-    uint4 q[UNROLL];
+  auto bucket_and_put = [&](K key) {
+    const uint32_t b = min(grid_eval<K>(gv, key), B - 1u);
+    if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
+  };
+  // the per-warp queue lives where the prefix table was (dead after the prologue)
+  K* wq = reinterpret_cast<K*>(wpre) + (threadIdx.x >> 5) * WQ_DEPTH;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  uint32_t qn = 0;  // warp-uniform
+
+  // every lane runs the same number of rounds, so the warp stays converged
+  auto main_loop = [&](auto&& is_hot) {
+    for (uint64_t r = 0; r < rounds; ++r, vp += gstride * UNROLL) {
+      uint4 q[UNROLL];
 #pragma unroll
-    for (int u = 0; u < UNROLL; ++u) q[u] = ld_stream16(vp + u * gstride);
+      for (int u = 0; u < UNROLL; ++u) q[u] = ld_stream16(vp + u * gstride);
 #pragma unroll
-    for (int u = 0; u < UNROLL; ++u) {
-      T e[EPV];
-      unpack16<T>(q[u], e);
+      for (int u = 0; u < UNROLL; ++u) {
+        T e[EPV];
+        unpack16<T>(q[u], e);
+        K kk[EPV];
+        bool hh[EPV];
+        bool any = false;
 #pragma unroll
-      for (int t = 0; t < EPV; ++t) {
-        const K key = KeyOf<T>::to(e[t]);
-        if (in_hot(key)) {
-          const uint32_t b = min(grid_eval<K>(gv, key), B - 1u);
-          if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
+        for (int t = 0; t < EPV; ++t) {
+          kk[t] = KeyOf<T>::to(e[t]);
+          hh[t] = is_hot(kk[t]);
+          any = any || hh[t];
+        }
+        if (!__any_sync(FULL, any)) continue;
+#pragma unroll
+        for (int t = 0; t < EPV; ++t) {
+          const uint32_t m = __ballot_sync(FULL, hh[t]);
+          if (m) {
+            if (hh[t]) wq[qn + __popc(m & lt_mask)] = kk[t];
+            qn += __popc(m);
+            if (qn >= 32u) {
+              __syncwarp();
+              const K k0 = wq[lane];
+              const K k1 = (lane + 32u < qn) ? wq[lane + 32u] : (K)0;
+              __syncwarp();
+              if (lane + 32u < qn) wq[lane] = k1;
+              qn -= 32u;
+              bucket_and_put(k0);
+            }
+          }
         }
       }
     }
+  };
+  const uint32_t nruns = nruns_s;
+  if (nruns <= 1u) {
+    const K l0 = run_lo[0], s0 = nruns ? run_span[0] : (K)0;
+    if (nruns) main_loop([&](K k) { return (K)(k - l0) <= s0; });
+  } else if (nruns == 2u) {
+    const K l0 = run_lo[0], s0 = run_span[0], l1 = run_lo[1], s1_ = run_span[1];
+    main_loop([&](K k) { return ((K)(k - l0) <= s0) | ((K)(k - l1) <= s1_); });
+  } else if (nruns <= L0_RUNS) {
+    K l[L0_RUNS], sp[L0_RUNS];
+#pragma unroll
+    for (uint32_t r = 0; r < L0_RUNS; ++r) {  // unused slots repeat run 0
+      l[r] = run_lo[r < nruns ? r : 0];
+      sp[r] = run_span[r < nruns ? r : 0];
+    }
+    main_loop([&](K k) {
+      bool h = false;
+#pragma unroll
+      for (uint32_t r = 0; r < L0_RUNS; ++r) h = h | ((K)(k - l[r]) <= sp[r]);
+      return h;
+    });
+  } else {
+    main_loop(in_hot);
   }
+  __syncwarp();
+  if (lane < qn) bucket_and_put(wq[lane]);
   const T* vbase = in + head;
   for (uint64_t i = rounds * gstride * UNROLL + gtid; i < nvec; i += gstride) {
     T e[EPV];
