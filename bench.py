@@ -49,6 +49,14 @@ SEED_KS = 21
 WORKLOAD = "half_normal_f32 n=2^28, 1024 top-1% ks + k=1 + k=n (exact k-th largest)"
 
 
+# DRAM bytes (read + write) per input element of the two passes, from one ncu
+# capture of the same kernels on the same half-normal workload at n = 2^26
+# (profiles/l0_passes_half_normal_f32_n26.md); both passes read the input once,
+# so the traffic of a launch grows in proportion to n.
+PASS_TRAFFIC_PER_ELEM = {"l0_count": (268532992 + 3170560) / 2**26,
+                         "l0_compact": (268843776 + 3119360) / 2**26}
+
+
 def peaks():
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -321,7 +329,10 @@ def run_ours(args):
         "passes": st_auto["full_passes"],
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "bytes_per_launch": bytes_pass,
+                     "traffic": PASS_TRAFFIC_PER_ELEM[dom_name] * N_ELEMS,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at n=2^26, "
+                                       "scaled by n (profiles/l0_passes_half_normal_f32_n26.md)",
+                     "bytes_per_launch": bytes_pass,
                      "pass1_ms": t1, "pass2_ms": t2,
                      "two_pass_frac": 2 * bytes_pass / (ms_step / 1e3) / 1e9 / peak},
         "e2e": {"value": world * N_ELEMS / (ms_e2e / args.steps / 1e3), "unit": "elements/s",
