@@ -14,6 +14,7 @@
 
 #include "ggms_kernels.cuh"
 #include "ggms_learned.cuh"
+#include "ggms_window.cuh"
 #include "../../include/ggms_diag.h"
 
 namespace ggms {
@@ -145,6 +146,7 @@ struct Workspace {
   Assigner<K>* asg;       // [0] sampled, [1] learned (the PL models)
   Grid<K>* grid;          // [0] sampled, [1] learned (what the passes evaluate)
   LearnState* learn;
+  Windows<K>* win;        // PASS 1 windows
   uint32_t* hist0;
   uint32_t* aflag0;
   uint32_t* cmap0;
@@ -174,6 +176,7 @@ struct Plan {
   int assigner;
   int train_steps;
   float bound;
+  float window_z;    // < 0: no PASS 1 windows
   uint64_t seed;
 };
 
@@ -193,6 +196,7 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
   size_t o_asg = b.take(sizeof(Assigner<K>) * 2);
   size_t o_grid = b.take(sizeof(Grid<K>) * 2);
   size_t o_learn = b.take(sizeof(LearnState));
+  size_t o_win = b.take(sizeof(Windows<K>));
   size_t o_h0 = b.take(4ull * p.B);
   size_t o_a0 = b.take(4ull * (p.B / 32));
   size_t o_c0 = b.take(4ull * p.B);
@@ -225,6 +229,7 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
   w.asg = (Assigner<K>*)(base + o_asg);
   w.grid = (Grid<K>*)(base + o_grid);
   w.learn = (LearnState*)(base + o_learn);
+  w.win = (Windows<K>*)(base + o_win);
   w.hist0 = (uint32_t*)(base + o_h0);
   w.aflag0 = (uint32_t*)(base + o_a0);
   w.cmap0 = (uint32_t*)(base + o_c0);
@@ -274,6 +279,7 @@ static int make_plan(Plan* p, uint64_t n, uint32_t nk, const ggms_opts& o) {
   p->cap_tiles = (uint32_t)((n + TILE - 1) / TILE) + p->cap_seg;
   p->train_steps = o.train_steps > 0 ? o.train_steps : 0;
   p->bound = o.imbalance_bound > 0.0f ? o.imbalance_bound : 3.0f;
+  p->window_z = o.window_z == 0.0f ? 8.0f : o.window_z;
   p->seed = o.seed;
   return GGMS_OK;
 }
@@ -284,7 +290,9 @@ constexpr int MAX_LEVELS_32 = 3;
 constexpr int MAX_LEVELS_64 = 6;
 
 template <typename T>
-static size_t l0_count_smem(uint32_t B) { return GRID_SMEM + (size_t)B * 4u; }
+static size_t l0_count_smem(uint32_t B, int nt) {
+  return GRID_SMEM + (size_t)B * 4u + wq_bytes((uint32_t)nt, sizeof(typename KeyOf<T>::K));
+}
 template <typename T>
 static size_t l0_compact_smem(uint32_t B, int nt) {
   return GRID_SMEM + (MAX_B0 / 32 + l0_compact_qwords((uint32_t)nt, sizeof(typename KeyOf<T>::K)) + HOT_WORDS) * 4u +
@@ -297,9 +305,9 @@ template <typename T>
 struct PassVariant {
   using K = typename KeyOf<T>::K;
   int nt, unroll;
-  void (*count)(const T*, uint64_t, const Grid<K>*, const Counters*, uint32_t*, uint32_t*);
-  void (*compact)(const T*, uint64_t, const Grid<K>*, Counters*, const uint32_t*, const uint32_t*, K*,
-                  uint64_t);
+  void (*count)(const T*, uint64_t, const Grid<K>*, const Counters*, const Windows<K>*, uint32_t*, uint32_t*);
+  void (*compact)(const T*, uint64_t, const Grid<K>*, Counters*, const Windows<K>*, const uint32_t*,
+                  const uint32_t*, K*, uint64_t);
 };
 
 template <typename T>
@@ -326,7 +334,7 @@ constexpr int DEFAULT_PASS_UNROLL = 4;
 // CTAs as fit on every SM at once for the larger of the two.
 template <typename T>
 static int l0_ncta(Context* c, const PassVariant<T>* pv, uint32_t B, uint32_t* ncta) {
-  const size_t s1 = l0_count_smem<T>(B), s2 = l0_compact_smem<T>(B, pv->nt);
+  const size_t s1 = l0_count_smem<T>(B, pv->nt), s2 = l0_compact_smem<T>(B, pv->nt);
   GGMS_CU(cudaFuncSetAttribute((const void*)pv->count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
   GGMS_CU(cudaFuncSetAttribute((const void*)pv->compact, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
   int o1 = 0, o2 = 0;
@@ -340,10 +348,12 @@ template <typename K>
 static int setup_attrs() {
   static bool done = false;
   if (done) return GGMS_OK;
-  GGMS_CU(cudaFuncSetAttribute(l0_scan, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  GGMS_CU(cudaFuncSetAttribute(l0_scan<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)(4u * MAX_B0)));
   GGMS_CU(cudaFuncSetAttribute(setup_sampled<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(SetupSmem<K>)));
+  GGMS_CU(cudaFuncSetAttribute(l0_window<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(4u * (MAX_B0 + 1u))));
   done = true;
   return GGMS_OK;
 }
@@ -467,21 +477,31 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     if (rc) return rc;
   }
 
+  // ---- PASS 1 windows
+  if (p.window_z >= 0.0f) {
+    ++ctx->launches;
+    l0_window<K><<<1, WIN_NT, 4u * (p.B + 1u), st>>>(w.samp_sorted, S, w.krank, nk, n, w.grid, w.C,
+                                                      p.window_z, w.win);
+  } else {
+    GGMS_CU(cudaMemsetAsync(w.win, 0, sizeof(Windows<K>), st));
+  }
+
   // ---- PASS 1: count
   const int grid_c = (int)p.ncta;
   GGMS_CU(cudaMemsetAsync(w.hist0, 0, 4ull * p.B, st));
   GGMS_CU(cudaMemsetAsync(w.aflag0, 0, 4ull * (p.B / 32), st));
   prof_rec(prof, 1, st);
   ++ctx->launches;
-  pv->count<<<grid_c, pv->nt, l0_count_smem<T>(p.B), st>>>(d_in, n, w.grid, w.C, w.hist0, w.crow);
+  pv->count<<<grid_c, pv->nt, l0_count_smem<T>(p.B, pv->nt), st>>>(d_in, n, w.grid, w.C, w.win, w.hist0,
+                                                                    w.crow);
   prof_rec(prof, 2, st);
   ++ctx->launches;
-  l0_scan<<<1, 1024, 4u * p.B, st>>>(w.hist0, p.B, w.C);
+  l0_scan<K><<<1, 1024, 4u * p.B, st>>>(w.hist0, p.B, w.C, w.win);
   ++ctx->launches;
   lvl_locate_rows<<<cdiv(nk, 256), 256, 0, st>>>(w.hist0, p.B, nk, w.krank, w.kseg, w.kbin,
                                                    w.aflag0, p.B / 32, w.C);
   ++ctx->launches;
-  l0_children<K><<<cdiv(p.B, 256), 256, 0, st>>>(w.hist0, w.aflag0, p.B, w.grid, w.C, w.cmap0,
+  l0_children<K><<<cdiv(p.B, 256), 256, 0, st>>>(w.hist0, w.aflag0, p.B, w.grid, w.C, w.win, w.cmap0,
                                                    w.segs[1], w.cursor[1], w.tiles[1], w.points,
                                                    w.khead[1], w.smalls, caps);
   ++ctx->launches;
@@ -492,8 +512,8 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   // ---- PASS 2: compact the buckets that still need refinement
   prof_rec(prof, 3, st);
   ++ctx->launches;
-  pv->compact<<<grid_c, pv->nt, l0_compact_smem<T>(p.B, pv->nt), st>>>(d_in, n, w.grid, w.C, w.cmap0, w.crow,
-                                                                 w.cand[0], (uint64_t)n);
+  pv->compact<<<grid_c, pv->nt, l0_compact_smem<T>(p.B, pv->nt), st>>>(d_in, n, w.grid, w.C, w.win, w.cmap0,
+                                                                      w.crow, w.cand[0], (uint64_t)n);
   prof_rec(prof, 4, st);
   rc = launch_small_select<K>(ctx, w.cand[0], w.segs[1], w.khead[1], w, caps, st);
   if (rc) return rc;
@@ -562,6 +582,7 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     s->bucket_max_over_mean = (float)pin_C->max_bucket0 / ((float)n / (float)p.B);
     s->model_imbalance = (p.assigner == GGMS_ASSIGNER_SAMPLED) ? 0.0f : ls.imbalance;
     s->model_loss = (p.assigner == GGMS_ASSIGNER_SAMPLED) ? 0.0f : ls.loss;
+    s->window_runs = (int32_t)pin_C->win_runs;
   }
   if (pin_C->status) return (int)pin_C->status;
   return GGMS_OK;

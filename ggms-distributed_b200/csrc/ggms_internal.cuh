@@ -11,6 +11,7 @@
 //   uint32 : identity
 #pragma once
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 namespace ggms {
@@ -269,8 +270,46 @@ struct Counters {
   unsigned long long cand0;   // elements copied by the level-0 compaction
   unsigned long long refine_elems;
   uint32_t asg_choice;        // index of the assigner in use (0 sampled, 1 learned)
-  uint32_t pad1[7];
+  uint32_t win_runs;          // PASS 1 window runs in use (0: no windows)
+  uint32_t pad1[6];
 };
+
+// PASS 1 windows (l0_window).  From the sample, every requested k gets a
+// range of level-0 buckets that holds it with overwhelming probability; the
+// union of those ranges, merged into at most L0_WIN runs, is where PASS 1
+// computes buckets.  A key outside every run is only counted, per gap between
+// runs, and the gap's count is kept in its first bucket ("gap bucket").  The
+// answers never depend on the prediction: a k that lands in a gap finds the
+// gap bucket, whose segment is then the whole gap.
+constexpr uint32_t L0_WIN = 4;
+template <typename K>
+struct Windows {
+  uint32_t on;                                 // 1: PASS 1 buckets only the runs
+  uint32_t R;                                  // runs, 1..L0_WIN
+  uint32_t cnt;                                // 1: two or more gaps hold keys (PASS 1 counts per run)
+  uint32_t rb0[L0_WIN], rb1[L0_WIN];           // bucket range of run r (ascending, disjoint)
+  uint32_t gb0[L0_WIN + 1], gb1[L0_WIN + 1];   // bucket range of gap g (gb0 > gb1: empty)
+  K lo[L0_WIN], hi[L0_WIN];                    // key range of run r (exactly its buckets' keys)
+};
+
+// Bucket of grid bucket b under windows: b inside a run, else its gap bucket.
+// Monotone non-decreasing in b.
+template <typename K>
+__device__ __forceinline__ uint32_t win_map(const Windows<K>& w, uint32_t b) {
+  for (uint32_t r = 0; r < w.R; ++r)
+    if (b <= w.rb1[r]) return b >= w.rb0[r] ? b : w.gb0[r];
+  return w.gb0[w.R];
+}
+
+// Last bucket of the level-0 segment that starts at bucket b: the gap's last
+// bucket for a gap bucket, b itself otherwise.
+template <typename K>
+__device__ __forceinline__ uint32_t win_end(const Windows<K>& w, uint32_t b) {
+  if (w.on)
+    for (uint32_t g = 0; g <= w.R; ++g)
+      if (b == w.gb0[g] && w.gb0[g] <= w.gb1[g]) return w.gb1[g];
+  return b;
+}
 
 // Capacities of the device-side lists; every append checks them and records
 // GGMS_E_INTERNAL instead of writing out of bounds.

@@ -245,29 +245,144 @@ __device__ __forceinline__ void unpack16(const uint4& q, T (&e)[Vec16<T>::N]) {
   __builtin_memcpy(e, &q, 16);
 }
 
+// Per-warp queues of the passes.  Keys that need the long path (bucket
+// computation) are spread over the input; handling each where it is found
+// would run the long path for every warp that holds one.  They are appended
+// to a per-warp queue in shared memory instead and handled 32 at a time, one
+// per lane.
+constexpr uint32_t WQ_DEPTH = 64;  // per-warp queue slots: < 32 waiting + 32 appended
+
+__host__ __device__ constexpr uint32_t wq_bytes(uint32_t nt, uint32_t key_bytes) {
+  return (nt / 32) * WQ_DEPTH * key_bytes;
+}
+
+// Appends the flagged keys of the warp to its queue (qn: warp-uniform fill).
+// Returns true (for the whole warp) when 32 keys were waiting: they are taken
+// off the queue, one per lane, into *out.  All 32 lanes must call it.
+template <typename K>
+__device__ __forceinline__ bool wq_push(K* wq, uint32_t& qn, bool flag, K key, uint32_t lane, K* out) {
+  const uint32_t m = __ballot_sync(FULL, flag);
+  if (!m) return false;
+  if (flag) wq[qn + __popc(m & ((1u << lane) - 1u))] = key;
+  qn += __popc(m);
+  if (qn < 32u) return false;
+  __syncwarp();
+  *out = wq[lane];
+  const K k1 = (lane + 32u < qn) ? wq[lane + 32u] : (K)0;
+  __syncwarp();
+  if (lane + 32u < qn) wq[lane] = k1;
+  qn -= 32u;
+  return true;
+}
+
+// Key test of the windowed passes: is the key inside one of R key ranges
+// [lo, lo + sp]; with CNT, also count per range the keys below its first key.
+template <typename K, uint32_t R, bool CNT>
+struct RunTest {
+  K lo[R], sp[R];
+  uint32_t bl[R];
+  __device__ __forceinline__ bool operator()(K k) {
+    bool h = false;
+#pragma unroll
+    for (uint32_t r = 0; r < R; ++r) {
+      if (CNT) bl[r] += k < lo[r] ? 1u : 0u;
+      h = h | ((K)(k - lo[r]) <= sp[r]);
+    }
+    return h;
+  }
+};
+
+// The uniform main loop of both passes: `rounds` rounds of UNROLL 16-byte
+// loads per thread, the same number on every lane, so a warp stays converged.
+// Keys that pass test(key) go through the per-warp queue to take(key), 32 at
+// a time; the queue's leftovers (qn < 32) stay for the caller.
+template <typename T, int UNROLL, typename Test, typename Take>
+__device__ __forceinline__ void stream_keys(const uint4* vp, uint64_t rounds, uint64_t step,
+                                            typename KeyOf<T>::K* wq, uint32_t& qn, uint32_t lane,
+                                            Test& test, Take&& take) {
+  using K = typename KeyOf<T>::K;
+  constexpr int EPV = Vec16<T>::N;
+  for (uint64_t r = 0; r < rounds; ++r, vp += step * UNROLL) {
+    uint4 q[UNROLL];
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) q[u] = ld_stream16(vp + u * step);
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) {
+      T e[EPV];
+      unpack16<T>(q[u], e);
+      K kk[EPV];
+      bool hh[EPV];
+      bool any = false;
+#pragma unroll
+      for (int t = 0; t < EPV; ++t) {
+        kk[t] = KeyOf<T>::to(e[t]);
+        hh[t] = test(kk[t]);
+        any = any || hh[t];
+      }
+      if (!__any_sync(FULL, any)) continue;
+#pragma unroll
+      for (int t = 0; t < EPV; ++t) {
+        K k0;
+        if (wq_push(wq, qn, hh[t], kk[t], lane, &k0)) take(k0);
+      }
+    }
+  }
+}
+
+// PASS 1 over windows with R runs (compile-time): the run tests, the per-run
+// counts (CNT) into below[0..R), the keys inside a run to take().
+template <typename T, int UNROLL, uint32_t R, bool CNT, typename Take>
+__device__ __forceinline__ void count_runs(const Windows<typename KeyOf<T>::K>& W, const uint4* vp,
+                                           uint64_t rounds, uint64_t step, typename KeyOf<T>::K* wq,
+                                           uint32_t& qn, uint32_t lane, uint32_t (&below)[L0_WIN],
+                                           Take&& take) {
+  using K = typename KeyOf<T>::K;
+  RunTest<K, R, CNT> t;
+#pragma unroll
+  for (uint32_t r = 0; r < R; ++r) {
+    t.lo[r] = W.lo[r];
+    t.sp[r] = (K)(W.hi[r] - W.lo[r]);
+    t.bl[r] = 0u;
+  }
+  stream_keys<T, UNROLL>(vp, rounds, step, wq, qn, lane, t, take);
+#pragma unroll
+  for (uint32_t r = 0; r < R; ++r) below[r] = t.bl[r];
+}
+
 // PASS 1.  Persistent CTAs; each keeps a shared histogram of the B buckets.
 // At the end a CTA adds its non-zero bins to the global histogram and writes
 // its whole row to crow[blockIdx][*] -- PASS 2 turns those rows into private
 // per-CTA write cursors, so it needs no global atomics.  Element -> CTA
 // assignment is a pure function of (n, grid, NT, UNROLL, input alignment), the
-// same in both passes.  A thread whose vector's elements share a bucket adds
-// once (sorted or clustered data).
+// same in both passes.
+// With windows (Windows::on) only the keys inside a run are bucketed (through
+// the per-warp queue); every key bumps, per run r, a register count of the
+// keys below the run's first key.  At the end the CTA's count of every gap
+// follows -- gap g = below(run g) - below(run g-1) - count(run g-1), the last
+// gap = all - below(last run) - count(last run) -- and goes to the gap's first
+// bucket, so the prefix sums over the buckets stay exact.
 template <typename T, int NT, int UNROLL>
 __global__ __launch_bounds__(NT) void l0_count(const T* __restrict__ in, uint64_t n,
                                               const Grid<typename KeyOf<T>::K>* __restrict__ Gs,
                                               const Counters* __restrict__ C,
+                                              const Windows<typename KeyOf<T>::K>* __restrict__ Wg,
                                               uint32_t* __restrict__ hist0, uint32_t* __restrict__ crow) {
   using K = typename KeyOf<T>::K;
   constexpr int EPV = Vec16<T>::N;
   extern __shared__ __align__(16) uint8_t smem[];
+  __shared__ Windows<K> W;
+  __shared__ uint32_t red[NT / 32][2 * L0_WIN + 1];
   const Grid<K>* G = Gs + C->asg_choice;
   uint2* s1 = (uint2*)smem;
   uint2* s2 = s1 + GRID_T1;
-  uint32_t* h = (uint32_t*)(smem + GRID_SMEM);
+  uint32_t* hs = (uint32_t*)(smem + GRID_SMEM);
   const GridView<K> gv = grid_to_smem<K>(G, s1, s2);
   const uint32_t B = gv.B;
-  for (uint32_t i = threadIdx.x; i < B; i += NT) h[i] = 0u;
+  K* wq = reinterpret_cast<K*>(hs + B) + (threadIdx.x >> 5) * WQ_DEPTH;
+  if (threadIdx.x == 0) W = *Wg;
+  for (uint32_t i = threadIdx.x; i < B; i += NT) hs[i] = 0u;
   __syncthreads();
+  const uint32_t lane = threadIdx.x & 31;
 
   const uint64_t gtid = (uint64_t)blockIdx.x * NT + threadIdx.x;
   const uint64_t gstride = (uint64_t)gridDim.x * NT;
@@ -277,48 +392,139 @@ __global__ __launch_bounds__(NT) void l0_count(const T* __restrict__ in, uint64_
   const uint4* vp = reinterpret_cast<const uint4*>(in + head) + gtid;
   const uint64_t rounds = nvec / (gstride * UNROLL);
 
-  for (uint64_t r = 0; r < rounds; ++r, vp += gstride * UNROLL) {
-    uint4 q[UNROLL];
+  auto bucket = [&](K key) { return min(grid_eval<K>(gv, key), B - 1u); };
+  // windows: this thread's count of keys below each run's first key (only
+  // kept when two or more gaps hold keys, W.cnt)
+  uint32_t below[L0_WIN] = {0u, 0u, 0u, 0u};
+  uint32_t seen = 0;  // keys this thread counted (windows only)
+
+  if (!W.on) {
+    for (uint64_t r = 0; r < rounds; ++r, vp += gstride * UNROLL) {
+      uint4 q[UNROLL];
 #pragma unroll
-    for (int u = 0; u < UNROLL; ++u) q[u] = ld_stream16(vp + u * gstride);
+      for (int u = 0; u < UNROLL; ++u) q[u] = ld_stream16(vp + u * gstride);
 #pragma unroll
-    for (int u = 0; u < UNROLL; ++u) {
-      T e[EPV];
-      unpack16<T>(q[u], e);
-      uint32_t b[EPV];
+      for (int u = 0; u < UNROLL; ++u) {
+        T e[EPV];
+        unpack16<T>(q[u], e);
+        uint32_t b[EPV];
 #pragma unroll
-      for (int t = 0; t < EPV; ++t) b[t] = min(grid_eval<K>(gv, KeyOf<T>::to(e[t])), B - 1u);
-      bool same = true;
+        for (int t = 0; t < EPV; ++t) b[t] = bucket(KeyOf<T>::to(e[t]));
+        bool same = true;
 #pragma unroll
-      for (int t = 1; t < EPV; ++t) same = same && (b[t] == b[0]);
-      if (same) {
-        atomicAdd(&h[b[0]], (uint32_t)EPV);
-      } else {
+        for (int t = 1; t < EPV; ++t) same = same && (b[t] == b[0]);
+        if (same) {
+          atomicAdd(&hs[b[0]], (uint32_t)EPV);
+        } else {
 #pragma unroll
-        for (int t = 0; t < EPV; ++t) atomicAdd(&h[b[t]], 1u);
+          for (int t = 0; t < EPV; ++t) atomicAdd(&hs[b[t]], 1u);
+        }
       }
     }
+  } else {
+    // R runs and (CNT) the per-run counts are compile-time, so that the bounds
+    // and counts stay in registers
+    uint32_t qn = 0;  // warp-uniform queue fill
+    auto take = [&](K k) { atomicAdd(&hs[bucket(k)], 1u); };
+    switch (W.R * 2u + (W.cnt ? 1u : 0u)) {
+      case 2: count_runs<T, UNROLL, 1, false>(W, vp, rounds, gstride, wq, qn, lane, below, take); break;
+      case 3: count_runs<T, UNROLL, 1, true>(W, vp, rounds, gstride, wq, qn, lane, below, take); break;
+      case 4: count_runs<T, UNROLL, 2, false>(W, vp, rounds, gstride, wq, qn, lane, below, take); break;
+      case 5: count_runs<T, UNROLL, 2, true>(W, vp, rounds, gstride, wq, qn, lane, below, take); break;
+      case 6: count_runs<T, UNROLL, 3, false>(W, vp, rounds, gstride, wq, qn, lane, below, take); break;
+      case 7: count_runs<T, UNROLL, 3, true>(W, vp, rounds, gstride, wq, qn, lane, below, take); break;
+      case 8: count_runs<T, UNROLL, 4, false>(W, vp, rounds, gstride, wq, qn, lane, below, take); break;
+      default: count_runs<T, UNROLL, 4, true>(W, vp, rounds, gstride, wq, qn, lane, below, take); break;
+    }
+    seen += (uint32_t)(rounds * UNROLL * EPV);
+    __syncwarp();
+    if (lane < qn) atomicAdd(&hs[bucket(wq[lane])], 1u);
   }
   // the partial last round, then the unaligned head and the tail that does not fill a vector
+  auto tally = [&](K key) {
+    if (!W.on) {
+      atomicAdd(&hs[bucket(key)], 1u);
+      return;
+    }
+    ++seen;
+    bool h = false;
+#pragma unroll
+    for (uint32_t r = 0; r < L0_WIN; ++r) {
+      if (r < W.R) {
+        below[r] += key < W.lo[r] ? 1u : 0u;
+        h = h | ((K)(key - W.lo[r]) <= (K)(W.hi[r] - W.lo[r]));
+      }
+    }
+    if (h) atomicAdd(&hs[bucket(key)], 1u);
+  };
   const T* vbase = in + head;
   for (uint64_t i = rounds * gstride * UNROLL + gtid; i < nvec; i += gstride) {
     T e[EPV];
     unpack16<T>(ld_stream16(vbase + i * EPV), e);
 #pragma unroll
-    for (int t = 0; t < EPV; ++t) atomicAdd(&h[min(grid_eval<K>(gv, KeyOf<T>::to(e[t])), B - 1u)], 1u);
+    for (int t = 0; t < EPV; ++t) tally(KeyOf<T>::to(e[t]));
   }
   {
     const uint64_t tail0 = head + nvec * EPV;
     const uint64_t nscalar = head + (n - tail0);
     for (uint64_t j = gtid; j < nscalar; j += gstride) {
       const uint64_t idx = j < head ? j : tail0 + (j - head);
-      atomicAdd(&h[min(grid_eval<K>(gv, KeyOf<T>::to(in[idx])), B - 1u)], 1u);
+      tally(KeyOf<T>::to(in[idx]));
     }
   }
   __syncthreads();
+  if (W.on) {
+    // this CTA's gap counts into the gaps' first buckets; red[w][*] holds warp
+    // w's sums of: below(run r) for r < L0_WIN, count(run r), keys seen
+#pragma unroll
+    for (uint32_t r = 0; r < L0_WIN; ++r) {
+      uint32_t hot = 0;
+      if (r < W.R)
+        for (uint32_t b = W.rb0[r] + threadIdx.x; b <= W.rb1[r]; b += NT) hot += hs[b];
+      uint32_t x = below[r], y = hot;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        x += __shfl_xor_sync(FULL, x, o);
+        y += __shfl_xor_sync(FULL, y, o);
+      }
+      if (lane == 0) {
+        red[threadIdx.x >> 5][r] = x;
+        red[threadIdx.x >> 5][L0_WIN + r] = y;
+      }
+    }
+    uint32_t z = seen;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) z += __shfl_xor_sync(FULL, z, o);
+    if (lane == 0) red[threadIdx.x >> 5][2 * L0_WIN] = z;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t below[L0_WIN], hot[L0_WIN], all = 0;
+      for (uint32_t r = 0; r < L0_WIN; ++r) below[r] = hot[r] = 0u;
+      for (uint32_t w = 0; w < NT / 32; ++w) {
+        for (uint32_t r = 0; r < L0_WIN; ++r) {
+          below[r] += red[w][r];
+          hot[r] += red[w][L0_WIN + r];
+        }
+        all += red[w][2 * L0_WIN];
+      }
+      const uint32_t R = W.R;
+      uint32_t rest = all;
+      for (uint32_t r = 0; r < R; ++r) rest -= hot[r];
+      for (uint32_t g = 0; g <= R; ++g) {
+        if (W.gb0[g] > W.gb1[g]) continue;  // empty gap
+        uint32_t gap;
+        if (!W.cnt) gap = rest;  // the only gap that holds keys
+        else if (g == 0) gap = below[0];
+        else if (g < R) gap = below[g] - below[g - 1] - hot[g - 1];
+        else gap = all - below[R - 1] - hot[R - 1];
+        if (gap) hs[W.gb0[g]] += gap;
+      }
+    }
+    __syncthreads();
+  }
   uint32_t* row = crow + (size_t)blockIdx.x * B;
   for (uint32_t i = threadIdx.x; i < B; i += NT) {
-    const uint32_t v = h[i];
+    const uint32_t v = hs[i];
     row[i] = v;
     if (v) atomicAdd(&hist0[i], v);
   }
@@ -326,13 +532,27 @@ __global__ __launch_bounds__(NT) void l0_count(const T* __restrict__ in, uint64_
 
 // Inclusive scan of the level-0 counts (one CTA) + the largest bucket.  The
 // counts are staged through shared memory with coalesced loads/stores.
-__global__ __launch_bounds__(1024) void l0_scan(uint32_t* hist0, uint32_t B, Counters* C) {
+// With windows the gap buckets are left out of the largest-bucket statistic
+// (a gap bucket counts a whole gap, not a bucket).
+template <typename K>
+__global__ __launch_bounds__(1024) void l0_scan(uint32_t* hist0, uint32_t B, Counters* C,
+                                                const Windows<K>* __restrict__ Wg) {
   extern __shared__ uint32_t sh_counts[];
   __shared__ uint32_t w[72];
-  for (uint32_t i = threadIdx.x; i < B; i += 1024) sh_counts[i] = hist0[i];
+  __shared__ uint32_t mx;
+  const bool on = Wg->on != 0u;
+  uint32_t m = 0;
+  if (threadIdx.x == 0) mx = 0;
+  for (uint32_t i = threadIdx.x; i < B; i += 1024) {
+    const uint32_t v = hist0[i];
+    sh_counts[i] = v;
+    if (on && win_end<K>(*Wg, i) == i && win_map<K>(*Wg, i) == i) m = max(m, v);
+  }
   __syncthreads();
+  if (on) atomicMax(&mx, m);
   block_inclusive_scan_global<1024>(sh_counts, B, w, &C->max_bucket0);
   for (uint32_t i = threadIdx.x; i < B; i += 1024) hist0[i] = sh_counts[i];
+  if (on && threadIdx.x == 0) C->max_bucket0 = mx;
 }
 
 // Each k finds the bucket holding its rank: the smallest b with I[b] > r.
@@ -364,6 +584,7 @@ __global__ void lvl_locate_rows(const uint32_t* __restrict__ rows, uint32_t row_
 template <typename K>
 __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __restrict__ aflag,
                             uint32_t B, const Grid<K>* __restrict__ Gs, Counters* C,
+                            const Windows<K>* __restrict__ Wg,
                             uint32_t* cmap0, Seg<K>* segs1, uint32_t* cursor1, TileRef* tiles1,
                             K* points, uint32_t* khead1, uint32_t* smalls, Caps caps) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -384,8 +605,10 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
     }
     return lo;
   };
+  // a gap bucket (windows) stands for its whole gap: up to the gap's last bucket
+  const uint32_t e = win_end<K>(*Wg, b);
   const K lo = (b == 0) ? (K)0 : L(b);
-  const K hi = (b == B - 1) ? key_max<K>() : (K)(L(b + 1) - 1);
+  const K hi = (e >= B - 1) ? key_max<K>() : (K)(L(e + 1) - 1);
   atomicAdd(&C->active0, 1u);
   if (lo == hi) {
     uint32_t pid = atomicAdd(&C->npoints, 1u);
@@ -481,13 +704,9 @@ __global__ void l0_bases(uint32_t* crow, uint32_t B, uint32_t ncta, const Seg<K>
 // Most keys lie in grid cells without a copied bucket: a second bitmask over
 // the grid's top-level cells ("hot" cells) rejects those with one shift and
 // one shared load, before the bucket is computed.
-// Keys that pass the cell test are queued per warp in shared memory and
-// bucketed 32 at a time, one per lane: the few hot keys are spread over the
-// input, and handling each where it is found would run the long path for
-// every warp that holds one (about half of them at 2% hot keys).
+// Keys that pass the cell test go through the per-warp queue (wq_push).
 constexpr uint32_t MAX_B0 = 1u << 15;
 constexpr uint32_t HOT_WORDS = (GRID_T1 + 31) / 32;
-constexpr uint32_t WQ_DEPTH = 64;  // per-warp queue slots: < 32 waiting + 32 appended
 constexpr uint32_t L0_RUNS = 4;    // hot-cell runs tested by key compares (more: the cell bitmask)
 
 // 32-bit words of the region shared by the prologue's prefix table and,
@@ -500,12 +719,16 @@ __host__ __device__ constexpr uint32_t l0_compact_qwords(uint32_t nt, uint32_t k
 template <typename T, int NT, int UNROLL>
 __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint64_t n,
                                                 const Grid<typename KeyOf<T>::K>* __restrict__ Gs,
-                                                Counters* C, const uint32_t* __restrict__ cmap0,
+                                                Counters* C,
+                                                const Windows<typename KeyOf<T>::K>* __restrict__ Wg,
+                                                const uint32_t* __restrict__ cmap0,
                                                 const uint32_t* __restrict__ crow,
                                                 typename KeyOf<T>::K* dst, uint64_t dst_cap) {
   using K = typename KeyOf<T>::K;
   constexpr int EPV = Vec16<T>::N;
   extern __shared__ __align__(16) uint8_t smem[];
+  __shared__ Windows<K> W;
+  if (threadIdx.x == 0) W = *Wg;
   const Grid<K>* G = Gs + C->asg_choice;
   uint2* s1 = (uint2*)smem;
   uint2* s2 = s1 + GRID_T1;
@@ -546,9 +769,11 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
     if (lane == 0) wpre[B / 32] = run;
   }
   __syncthreads();
+  // with windows, a key outside every run belongs to its gap's bucket
+  auto bmap = [&](uint32_t b) { return W.on ? win_map(W, b) : b; };
   {
     // a cell is hot when a copied bucket lies in [bucket of its first key,
-    // bucket of its last key] (the grid is monotone in the key)
+    // bucket of its last key] (the grid and bmap are monotone in the key)
     auto rank = [&](uint32_t b) {  // copied buckets below b, b <= B
       const uint32_t w = b >> 5;
       return (b & 31) ? wpre[w] + __popc(amask[w] & ((1u << (b & 31)) - 1u)) : wpre[w];
@@ -557,8 +782,8 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
     for (uint32_t c = threadIdx.x; c < ncell; c += NT) {
       const K d0 = (K)c << gv.sh1;
       const K d1 = (c + 1u < ncell) ? (K)(((K)(c + 1u) << gv.sh1) - 1u) : dmax;
-      const uint32_t lo = min(grid_eval<K>(gv, (K)(gv.origin + d0)), B - 1u);
-      const uint32_t hi = min(grid_eval<K>(gv, (K)(gv.origin + min(d1, dmax))), B - 1u);
+      const uint32_t lo = bmap(min(grid_eval<K>(gv, (K)(gv.origin + d0)), B - 1u));
+      const uint32_t hi = bmap(min(grid_eval<K>(gv, (K)(gv.origin + min(d1, dmax))), B - 1u));
       if (rank(hi + 1u) != rank(lo)) atomicOr(&hot[c >> 5], 1u << (c & 31));
     }
   }
@@ -618,76 +843,32 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
   };
 
   auto bucket_and_put = [&](K key) {
-    const uint32_t b = min(grid_eval<K>(gv, key), B - 1u);
+    const uint32_t b = bmap(min(grid_eval<K>(gv, key), B - 1u));
     if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
   };
   // the per-warp queue lives where the prefix table was (dead after the prologue)
   K* wq = reinterpret_cast<K*>(wpre) + (threadIdx.x >> 5) * WQ_DEPTH;
-  const uint32_t lt_mask = (1u << lane) - 1u;
   uint32_t qn = 0;  // warp-uniform
 
   // every lane runs the same number of rounds, so the warp stays converged
-  auto main_loop = [&](auto&& is_hot) {
-    for (uint64_t r = 0; r < rounds; ++r, vp += gstride * UNROLL) {
-      uint4 q[UNROLL];
-#pragma unroll
-      for (int u = 0; u < UNROLL; ++u) q[u] = ld_stream16(vp + u * gstride);
-#pragma unroll
-      for (int u = 0; u < UNROLL; ++u) {
-        T e[EPV];
-        unpack16<T>(q[u], e);
-        K kk[EPV];
-        bool hh[EPV];
-        bool any = false;
-#pragma unroll
-        for (int t = 0; t < EPV; ++t) {
-          kk[t] = KeyOf<T>::to(e[t]);
-          hh[t] = is_hot(kk[t]);
-          any = any || hh[t];
-        }
-        if (!__any_sync(FULL, any)) continue;
-#pragma unroll
-        for (int t = 0; t < EPV; ++t) {
-          const uint32_t m = __ballot_sync(FULL, hh[t]);
-          if (m) {
-            if (hh[t]) wq[qn + __popc(m & lt_mask)] = kk[t];
-            qn += __popc(m);
-            if (qn >= 32u) {
-              __syncwarp();
-              const K k0 = wq[lane];
-              const K k1 = (lane + 32u < qn) ? wq[lane + 32u] : (K)0;
-              __syncwarp();
-              if (lane + 32u < qn) wq[lane] = k1;
-              qn -= 32u;
-              bucket_and_put(k0);
-            }
-          }
-        }
-      }
-    }
-  };
   const uint32_t nruns = nruns_s;
-  if (nruns <= 1u) {
-    const K l0 = run_lo[0], s0 = nruns ? run_span[0] : (K)0;
-    if (nruns) main_loop([&](K k) { return (K)(k - l0) <= s0; });
-  } else if (nruns == 2u) {
-    const K l0 = run_lo[0], s0 = run_span[0], l1 = run_lo[1], s1_ = run_span[1];
-    main_loop([&](K k) { return ((K)(k - l0) <= s0) | ((K)(k - l1) <= s1_); });
-  } else if (nruns <= L0_RUNS) {
-    K l[L0_RUNS], sp[L0_RUNS];
+  auto runs = [&](auto rc) {
+    constexpr uint32_t R = decltype(rc)::value;
+    RunTest<K, R, false> t;
 #pragma unroll
-    for (uint32_t r = 0; r < L0_RUNS; ++r) {  // unused slots repeat run 0
-      l[r] = run_lo[r < nruns ? r : 0];
-      sp[r] = run_span[r < nruns ? r : 0];
+    for (uint32_t r = 0; r < R; ++r) {
+      t.lo[r] = run_lo[r];
+      t.sp[r] = run_span[r];
     }
-    main_loop([&](K k) {
-      bool h = false;
-#pragma unroll
-      for (uint32_t r = 0; r < L0_RUNS; ++r) h = h | ((K)(k - l[r]) <= sp[r]);
-      return h;
-    });
-  } else {
-    main_loop(in_hot);
+    stream_keys<T, UNROLL>(vp, rounds, gstride, wq, qn, lane, t, bucket_and_put);
+  };
+  switch (nruns) {
+    case 0: break;  // nothing to copy
+    case 1: runs(std::integral_constant<uint32_t, 1>{}); break;
+    case 2: runs(std::integral_constant<uint32_t, 2>{}); break;
+    case 3: runs(std::integral_constant<uint32_t, 3>{}); break;
+    case 4: runs(std::integral_constant<uint32_t, 4>{}); break;
+    default: stream_keys<T, UNROLL>(vp, rounds, gstride, wq, qn, lane, in_hot, bucket_and_put); break;
   }
   __syncwarp();
   if (lane < qn) bucket_and_put(wq[lane]);
@@ -698,10 +879,7 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
 #pragma unroll
     for (int t = 0; t < EPV; ++t) {
       const K key = KeyOf<T>::to(e[t]);
-      if (in_hot(key)) {
-        const uint32_t b = min(grid_eval<K>(gv, key), B - 1u);
-        if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
-      }
+      if (in_hot(key)) bucket_and_put(key);
     }
   }
   {
@@ -710,10 +888,7 @@ __global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint6
     for (uint64_t j = gtid; j < nscalar; j += gstride) {
       const uint64_t idx = j < head ? j : tail0 + (j - head);
       const K key = KeyOf<T>::to(in[idx]);
-      if (in_hot(key)) {
-        const uint32_t b = min(grid_eval<K>(gv, key), B - 1u);
-        if ((amask[b >> 5] >> (b & 31)) & 1u) put(b, key);
-      }
+      if (in_hot(key)) bucket_and_put(key);
     }
   }
   if (overflow) set_status(C, GGMS_E_INTERNAL);

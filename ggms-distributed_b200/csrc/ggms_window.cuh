@@ -1,0 +1,161 @@
+// ggms_window.cuh -- PASS 1 windows: where the requested ks can lie.
+//
+// The reference counts every element into its bucket before it knows which
+// buckets matter (DistributedSMOS/bucketMultiselect.cu:135-210, 664-679).
+// Here the sorted sample already says roughly where each k lies: if the k-th
+// key has ascending rank r, the number of sample keys below it is binomial
+// (S, q = (r + 1/2) / n), so the key lies between the sample keys at positions
+// S q -+ m, m = z sqrt(S q (1 - q)) + z + 2, except with a probability far
+// below 10^-12 for z = 8.  Every k thus gets a range of level-0 buckets; their
+// union, merged into at most L0_WIN runs, is the only place PASS 1 computes
+// buckets.  Keys elsewhere are counted per gap between runs (a few compares),
+// so when the ks are clustered most of the input skips the bucket
+// computation entirely.  Nothing here decides an answer: a k outside every
+// run lands in a gap bucket, whose segment is then the whole gap.
+#pragma once
+#include "ggms_setup.cuh"
+
+namespace ggms {
+
+constexpr uint32_t WIN_MAXRAW = 64;    // runs before merging; more: no windows
+constexpr uint32_t WIN_MERGE = 64;     // runs closer than this many buckets merge
+constexpr uint32_t WIN_NT = 1024;
+
+// One CTA.  Dynamic shared memory: (B + 1) int32.
+template <typename K>
+__global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted, uint32_t S,
+                                                   const uint32_t* __restrict__ krank, uint32_t nk,
+                                                   uint64_t n, const Grid<K>* __restrict__ Gs,
+                                                   Counters* C, float z, Windows<K>* W) {
+  extern __shared__ int32_t cover[];  // difference array, then coverage, of the B buckets
+  __shared__ uint32_t red[33];
+  __shared__ uint32_t rs[WIN_MAXRAW], re[WIN_MAXRAW];
+  __shared__ Windows<K> sw;
+  const uint32_t tid = threadIdx.x;
+  const GridView<K> gv = grid_view_global<K>(Gs + C->asg_choice);
+  const uint32_t B = gv.B;
+  for (uint32_t b = tid; b <= B; b += WIN_NT) cover[b] = 0;
+  __syncthreads();
+  // 1. bucket range of every k
+  for (uint32_t i = tid; i < nk; i += WIN_NT) {
+    const double q = ((double)krank[i] + 0.5) / (double)n;
+    const double pos = q * (double)S;
+    const double m = (double)z * sqrt((double)S * q * (1.0 - q)) + (double)z + 2.0;
+    const double a = floor(pos - m), c = ceil(pos + m);
+    const K klo = a < 0.0 ? (K)0 : sorted[min((uint32_t)a, S - 1u)];
+    const K khi = c > (double)(S - 1u) ? key_max<K>() : sorted[(uint32_t)c];
+    const uint32_t b0 = min(grid_eval<K>(gv, klo), B - 1u);
+    const uint32_t b1 = min(grid_eval<K>(gv, khi), B - 1u);
+    atomicAdd(&cover[b0], 1);
+    atomicAdd(&cover[b1 + 1u], -1);
+  }
+  __syncthreads();
+  // 2. coverage: prefix sum of the difference array, a contiguous chunk per thread
+  const uint32_t chunk = (B + WIN_NT - 1u) / WIN_NT;
+  const uint32_t c0 = min(tid * chunk, B), c1 = min(c0 + chunk, B);
+  int32_t part = 0;
+  for (uint32_t b = c0; b < c1; ++b) part += cover[b];
+  uint32_t tot_u = 0;
+  const int32_t before = (int32_t)block_excl_scan<uint32_t>((uint32_t)part, red, &tot_u);
+  {
+    int32_t run = before;
+    for (uint32_t b = c0; b < c1; ++b) {
+      run += cover[b];
+      cover[b] = run;  // this thread's chunk only: no other thread reads it yet
+    }
+  }
+  __syncthreads();
+  // 3. raw runs of covered buckets, numbered in bucket order (run j is the
+  //    j-th start and the j-th end)
+  auto is_start = [&](uint32_t b) { return cover[b] > 0 && (b == 0 || cover[b - 1] <= 0); };
+  auto is_end = [&](uint32_t b) { return cover[b] > 0 && (b + 1u == B || cover[b + 1] <= 0); };
+  uint32_t nst = 0, nen = 0;
+  for (uint32_t b = c0; b < c1; ++b) {
+    nst += is_start(b);
+    nen += is_end(b);
+  }
+  uint32_t nraw = 0, nraw2 = 0;
+  uint32_t at = block_excl_scan<uint32_t>(nst, red, &nraw);
+  uint32_t ate = block_excl_scan<uint32_t>(nen, red, &nraw2);
+  for (uint32_t b = c0; b < c1; ++b) {
+    if (is_start(b)) {
+      if (at < WIN_MAXRAW) rs[at] = b;
+      ++at;
+    }
+    if (is_end(b)) {
+      if (ate < WIN_MAXRAW) re[ate] = b;
+      ++ate;
+    }
+  }
+  __syncthreads();
+  // 4. merge close runs; decide
+  if (tid == 0) {
+    sw.on = 0;
+    sw.R = 0;
+    sw.cnt = 0;
+    uint32_t R = 0, hot = 0;
+    if (nraw >= 1 && nraw <= WIN_MAXRAW && nraw2 == nraw) {
+      uint32_t cs = rs[0], ce = re[0];
+      bool ok = true;
+      for (uint32_t i = 1; i <= nraw && ok; ++i) {
+        if (i < nraw && rs[i] - ce - 1u < WIN_MERGE) {
+          ce = re[i];
+          continue;
+        }
+        if (R == L0_WIN) { ok = false; break; }
+        sw.rb0[R] = cs;
+        sw.rb1[R] = ce;
+        hot += ce - cs + 1u;
+        ++R;
+        if (i < nraw) { cs = rs[i]; ce = re[i]; }
+      }
+      if (ok && hot <= B / 4u) {
+        sw.on = 1;
+        sw.R = R;
+        // buckets below the smallest key's or above the largest key's never
+        // hold a key: a gap made only of those is empty
+        const uint32_t bmin = min(grid_eval<K>(gv, (K)0), B - 1u);
+        const uint32_t bmax = min(grid_eval<K>(gv, key_max<K>()), B - 1u);
+        for (uint32_t g = 0; g <= R; ++g) {
+          // gap g lies between run g-1 and run g; gb0 > gb1 marks an empty gap
+          const uint32_t g0 = g == 0 ? 0u : sw.rb1[g - 1] + 1u;
+          const uint32_t g1 = g == R ? B : sw.rb0[g];  // one past the gap's last bucket
+          const bool holds = g0 < g1 && g0 <= bmax && g1 > bmin;
+          sw.gb0[g] = holds ? g0 : B;
+          sw.gb1[g] = holds ? g1 - 1u : 0u;
+        }
+        uint32_t ne = 0;
+        for (uint32_t g = 0; g <= R; ++g) ne += sw.gb0[g] <= sw.gb1[g] ? 1u : 0u;
+        sw.cnt = ne >= 2u ? 1u : 0u;
+      }
+    }
+  }
+  __syncthreads();
+  // 5. key range of each run: [L(rb0), L(rb1 + 1) - 1], L(x) = smallest key with bucket >= x
+  if (sw.on && tid < 2u * sw.R) {
+    const uint32_t r = tid >> 1;
+    const bool upper = tid & 1u;
+    const uint32_t target = upper ? sw.rb1[r] + 1u : sw.rb0[r];
+    K v;
+    if (!upper && target == 0u) {
+      v = (K)0;
+    } else if (upper && target >= B) {
+      v = key_max<K>();
+    } else {
+      K lo = 0, hi = key_max<K>();
+      while (lo < hi) {
+        const K mid = lo + ((hi - lo) >> 1);
+        if (min(grid_eval<K>(gv, mid), B - 1u) >= target) hi = mid; else lo = mid + 1;
+      }
+      v = upper ? (lo == 0 ? (K)0 : (K)(lo - 1u)) : lo;
+    }
+    if (upper) sw.hi[r] = v; else sw.lo[r] = v;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    *W = sw;
+    C->win_runs = sw.on ? sw.R : 0u;
+  }
+}
+
+}  // namespace ggms

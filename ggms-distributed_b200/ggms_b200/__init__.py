@@ -66,11 +66,11 @@ class Stats(ctypes.Structure):
         ("bucket_max_over_mean", ctypes.c_float),
         ("model_imbalance", ctypes.c_float),
         ("model_loss", ctypes.c_float),
-        ("reserved", ctypes.c_float),
+        ("window_runs", ctypes.c_int32),
     ]
 
     def as_dict(self):
-        d = {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+        d = {f: getattr(self, f) for f, _ in self._fields_}
         d["assigner_used"] = ASSIGNER_NAMES.get(self.assigner_used, self.assigner_used)
         return d
 
@@ -88,6 +88,8 @@ class Opts(ctypes.Structure):
         ("out_on_device", ctypes.c_int32),
         ("pass_threads", ctypes.c_int32),
         ("pass_unroll", ctypes.c_int32),
+        ("window_z", ctypes.c_float),
+        ("reserved0", ctypes.c_int32),
         ("stats", ctypes.POINTER(Stats)),
     ]
 

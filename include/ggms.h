@@ -70,7 +70,7 @@ typedef struct ggms_stats {
   float bucket_max_over_mean;   /* level-0 occupancy: max bucket / (n / num_buckets) */
   float model_imbalance;        /* max/mean of the model's buckets on its own sample (learned) */
   float model_loss;             /* final training loss of the learned model */
-  float reserved;
+  int32_t window_runs;          /* PASS 1 windows: bucket runs PASS 1 bucketed (0: every key bucketed) */
 } ggms_stats;
 
 typedef struct ggms_opts {
@@ -85,6 +85,9 @@ typedef struct ggms_opts {
   int32_t out_on_device;        /* 1: the output array is device memory */
   int32_t pass_threads;         /* CTA size of the two passes: 256, 512 or 1024; 0 = tuned default */
   int32_t pass_unroll;          /* 16-byte loads in flight per thread: 2, 4 or 8; 0 = tuned default */
+  float window_z;               /* PASS 1 windows: safety margin of the predicted k positions in
+                                   binomial standard deviations; 0 = 8; < 0 = no windows */
+  int32_t reserved0;
   ggms_stats* stats;            /* optional host pointer */
 } ggms_opts;
 

@@ -1,0 +1,81 @@
+"""PASS 1 windows: bit-exact answers whether the predicted k positions hold or not.
+
+With clustered ks (the top 1% of ranks plus k = 1 and k = n) PASS 1 buckets only
+the runs of buckets the sample predicts for the ks and counts every other key per
+gap.  The answers must not depend on the prediction: the tests compare with the
+CPU oracle with the default margin, with a margin far too small (many ks then land
+in a gap, whose whole key range becomes their segment) and with windows off.
+"""
+import numpy as np
+import pytest
+
+import ggms_b200 as G
+import ggms_oracle as orc
+from ggms_b200 import datagen as D
+from conftest import to_device
+
+pytestmark = pytest.mark.gpu
+
+N = (1 << 22) + 5
+
+CASES = [
+    ("half_normal_f32", np.float32),
+    ("cauchy_f32", np.float32),
+    ("distinct256_f32", np.float32),
+    ("normal_f64", np.float64),
+    ("uniform_u32", np.uint32),
+    ("sorted_desc_u32", np.uint32),
+]
+
+
+@pytest.mark.parametrize("gen,dtype", CASES)
+@pytest.mark.parametrize("assigner", [G.ASSIGNER_SAMPLED, G.ASSIGNER_AUTO])
+@pytest.mark.parametrize("window_z", [0.0, 0.001, -1.0])
+def test_windows_exact(ctx, gen, dtype, assigner, window_z):
+    v = D.VALUE_GENERATORS[gen](N, 5)
+    assert v.dtype == dtype
+    ks = D.ks_top1pct(N, 1024, 6)
+    exp = orc.select(v, ks)
+    d = to_device(v)
+    out, st = G.select(ctx, d.data_ptr(), N, ks, dtype, assigner=assigner, stats=True,
+                       window_z=window_z)
+    np.testing.assert_array_equal(orc.bits(out), orc.bits(exp))
+    if window_z < 0:
+        assert st["window_runs"] == 0
+    elif window_z == 0.0 and gen != "distinct256_f32":
+        # clustered ks: the default margin keeps windows on (top run + the minimum's run)
+        assert 1 <= st["window_runs"] <= 4, st
+
+
+@pytest.mark.parametrize("window_z", [0.0, 0.001])
+def test_windows_extremes_and_middle(ctx, window_z):
+    """Runs at both ends and in the middle, with a duplicate k."""
+    n = N
+    v = D.VALUE_GENERATORS["normal_f32"](n, 9)
+    mid = n // 2
+    ks = np.array([1, 2, 3, mid, mid + 1, mid + 1, n - 2, n - 1, n], dtype=np.uint32)
+    d = to_device(v)
+    out, st = G.select(ctx, d.data_ptr(), n, ks, np.float32, stats=True, window_z=window_z)
+    np.testing.assert_array_equal(orc.bits(out), orc.bits(orc.select(v, ks)))
+    if window_z == 0.0:
+        assert st["window_runs"] == 3, st
+
+
+def test_windows_off_when_ks_spread(ctx):
+    """ks spread over all ranks cover every bucket: windows stay off."""
+    v = D.VALUE_GENERATORS["uniform_f32"](N, 11)
+    ks = D.ks_uniform(N, 1000, 12)
+    d = to_device(v)
+    out, st = G.select(ctx, d.data_ptr(), N, ks, np.float32, stats=True)
+    np.testing.assert_array_equal(orc.bits(out), orc.bits(orc.select(v, ks)))
+    assert st["window_runs"] == 0
+
+
+def test_windows_topk(ctx):
+    n = N
+    v = D.VALUE_GENERATORS["half_normal_f32"](n, 13)
+    d = to_device(v)
+    K = 4096
+    out = G.topk(ctx, d.data_ptr(), n, K, np.float32)
+    exp = np.sort(v)[::-1][:K]
+    np.testing.assert_array_equal(orc.bits(out), orc.bits(exp))
