@@ -353,7 +353,7 @@ static int setup_attrs() {
   GGMS_CU(cudaFuncSetAttribute(setup_sampled<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(SetupSmem<K>)));
   GGMS_CU(cudaFuncSetAttribute(l0_window<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)(4u * (MAX_B0 + 1u))));
+                               (int)l0_window_smem<K>(MAX_B0)));
   done = true;
   return GGMS_OK;
 }
@@ -473,15 +473,16 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
                                                                &w.grid[0]);
   if (p.assigner != GGMS_ASSIGNER_SAMPLED) {
     rc = learn_and_choose<K>(p.assigner, w.samp_sorted, S, p.B, p.train_steps, p.bound, w.asg,
-                             w.grid, w.learn, &w.C->asg_choice, st, &ctx->launches);
+                             w.grid, w.learn, &w.C->asg_choice, w.krank, nk, n, p.window_z, st,
+                             &ctx->launches);
     if (rc) return rc;
   }
 
   // ---- PASS 1 windows
   if (p.window_z >= 0.0f) {
     ++ctx->launches;
-    l0_window<K><<<1, WIN_NT, 4u * (p.B + 1u), st>>>(w.samp_sorted, S, w.krank, nk, n, w.grid, w.C,
-                                                      p.window_z, w.win);
+    l0_window<K><<<1, WIN_NT, l0_window_smem<K>(p.B), st>>>(w.samp_sorted, S, w.krank, nk, n, w.grid,
+                                                             w.C, p.window_z, w.win);
   } else {
     GGMS_CU(cudaMemsetAsync(w.win, 0, sizeof(Windows<K>), st));
   }
@@ -844,7 +845,7 @@ static int fit(const uint32_t* keys, int S, int kind, int steps, float* l0, floa
   setup_sampled<uint32_t><<<1, SETUP_NT, sizeof(SetupSmem<uint32_t>)>>>(k, (uint32_t)S, B, &As[0], &Gs[0]);
   long long launches = 0;
   rc = learn_and_choose<uint32_t>(kind, k, (uint32_t)S, B, steps, 1e30f, As, Gs, L, (uint32_t*)dc.p,
-                                  0, &launches);
+                                  nullptr, 0u, 0ull, -1.0f, 0, &launches);
   if (rc) return rc;
   GGMS_CU(cudaDeviceSynchronize());
   LearnState hl;

@@ -540,13 +540,23 @@ __global__ __launch_bounds__(1024) void l0_scan(uint32_t* hist0, uint32_t B, Cou
   extern __shared__ uint32_t sh_counts[];
   __shared__ uint32_t w[72];
   __shared__ uint32_t mx;
-  const bool on = Wg->on != 0u;
+  __shared__ Windows<K> W;
+  if (threadIdx.x == 0) {
+    W = *Wg;
+    mx = 0;
+  }
+  __syncthreads();
+  const bool on = W.on != 0u;
   uint32_t m = 0;
-  if (threadIdx.x == 0) mx = 0;
   for (uint32_t i = threadIdx.x; i < B; i += 1024) {
     const uint32_t v = hist0[i];
     sh_counts[i] = v;
-    if (on && win_end<K>(*Wg, i) == i && win_map<K>(*Wg, i) == i) m = max(m, v);
+    if (on) {
+      bool gap = false;
+#pragma unroll
+      for (uint32_t g = 0; g <= L0_WIN; ++g) gap = gap || (g <= W.R && i == W.gb0[g]);
+      if (!gap) m = max(m, v);
+    }
   }
   __syncthreads();
   if (on) atomicMax(&mx, m);

@@ -42,7 +42,8 @@ struct LearnState {
   uint32_t M;                    // segments actually used
   uint32_t steps;
   uint32_t choice;               // 1 learned accepted, 0 fell back to sampled
-  uint32_t pad[2];
+  uint32_t focus_points;         // breakpoints of the bucket focus (2: none)
+  uint32_t pad[1];
   // MLP parameters (see ggms_mlp.cuh)
   float mlp_params[MLP_NPARAM + 3];
   float mlp_loss;
@@ -211,12 +212,14 @@ __device__ float pl_train_block(const PLStats* st, uint32_t M, uint32_t S, uint3
 // New bases (strictly increasing) and slopes of a PL assigner from CDF values
 // at its knots.  All threads call it.
 template <typename K>
-__device__ void pl_set_bases(const float* cdf, Assigner<K>* A, uint32_t* Bs, uint32_t kind) {
+__device__ void pl_set_bases(const float* cdf, Assigner<K>* A, uint32_t* Bs, uint32_t kind,
+                             const Warp* wp = nullptr) {
   __shared__ int32_t red[32];
   const uint32_t M = A->M, B = A->B;
   const float span = (float)(B - 2u);
   for (uint32_t t = threadIdx.x; t <= M; t += blockDim.x) {
-    const float f = fminf(fmaxf(cdf[t], 0.0f), 1.0f);
+    float f = fminf(fmaxf(cdf[t], 0.0f), 1.0f);
+    if (wp && wp->n > 2u) f = warp_fwd(*wp, f);  // focus the buckets on the ks' windows
     Bs[t] = 1u + __float2uint_rn(f * span);
   }
   __syncthreads();
@@ -268,16 +271,19 @@ __device__ void pl_knots(const K* sorted, uint32_t S, uint32_t B, uint32_t kind,
 
 // Final stage shared by both learned models: compile the PL assigner A into
 // the grid G, measure it on the sample and decide learned vs sampled.
+// The learned grid is used when its imbalance is within the bound, or when the
+// sampled grid G0 (measured the same way on the same sample) is worse still.
+// A focused model is measured in CDF space before its warp.
 template <typename K>
 __device__ void learned_finish(const K* sorted, uint32_t S, uint32_t B, uint32_t kind, float bound,
-                               Assigner<K>* A, Grid<K>* G, LearnState* L, uint32_t* choice,
-                               LearnSmem<K>& sm) {
+                               Assigner<K>* A, Grid<K>* G, const Grid<K>* G0, LearnState* L,
+                               uint32_t* choice, LearnSmem<K>& sm, const Warp* wp = nullptr) {
   const AsgView<K> av = asg_copy<K>(A, sm.su.asg);
   const GridView<K> gv = grid_compile<K>(av, B, kind, G, sm.su.s1, sm.su.s2, sm.su.cs);
-  const float qv = grid_measure<K>(gv, sorted, S, sm.su.hist256);
+  const float qv = grid_measure<K>(gv, sorted, S, sm.su.hist256, wp);
   if (threadIdx.x == 0) {
     G->quality = qv;
-    const uint32_t c = (qv <= bound) ? 1u : 0u;
+    const uint32_t c = (qv <= bound || qv < G0->quality) ? 1u : 0u;
     *choice = c;
     L->choice = c;
     L->imbalance = qv;
@@ -287,13 +293,20 @@ __device__ void learned_finish(const K* sorted, uint32_t S, uint32_t B, uint32_t
 // The whole learned-PL setup in one CTA: knots -> statistics -> training ->
 // bases -> grid -> occupancy -> choice (grid 1 if within the bound, else the
 // sampled grid 0 stays in use).
+// With window_z >= 0 the bases are focused on the ks' windows (build_warp):
+// krank[0..nk) are the ks' ascending ranks among n keys.
 template <typename K>
 __global__ __launch_bounds__(SETUP_NT) void setup_learned_pl(const K* __restrict__ sorted, uint32_t S,
                                                             uint32_t B, uint32_t steps, float lr,
                                                             float bound, Assigner<K>* A, Grid<K>* G,
-                                                            LearnState* L, uint32_t* choice) {
+                                                            const Grid<K>* G0, LearnState* L,
+                                                            uint32_t* choice,
+                                                            const uint32_t* __restrict__ krank,
+                                                            uint32_t nk, uint64_t n, float window_z) {
   extern __shared__ __align__(16) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
+  __shared__ Warp wsh;
+  __shared__ uint32_t wred[33];
   pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, A, sm);
   const uint32_t M = A->M;
   pl_stats_block<K>(sorted, S, A->x, M, sm.st, sm.seg_start);
@@ -308,8 +321,18 @@ __global__ __launch_bounds__(SETUP_NT) void setup_learned_pl(const K* __restrict
     }
   }
   __syncthreads();
-  pl_set_bases<K>(sm.cdf, A, sm.Bs, GGMS_ASSIGNER_LEARNED_PL);
-  learned_finish<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, bound, A, G, L, choice, sm);
+  if (window_z >= 0.0f) {
+    // the statistics are dead after training: their space holds the bins
+    build_warp(krank, nk, n, S, window_z, L0_WIN, reinterpret_cast<int32_t*>(sm.st), wred, &wsh);
+  } else if (threadIdx.x == 0) {
+    wsh.n = 2;
+    wsh.p[0] = wsh.w[0] = 0.0f;
+    wsh.p[1] = wsh.w[1] = 1.0f;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) L->focus_points = wsh.n;
+  pl_set_bases<K>(sm.cdf, A, sm.Bs, GGMS_ASSIGNER_LEARNED_PL, &wsh);
+  learned_finish<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, bound, A, G, G0, L, choice, sm, &wsh);
 }
 
 // Gradient probe (diagnostics): knots and statistics as above, then one
@@ -343,7 +366,8 @@ namespace ggms {
 template <typename K>
 static int learn_and_choose(int kind, const K* sorted, uint32_t S, uint32_t B, int steps_opt,
                             float bound, Assigner<K>* As, Grid<K>* Gs, LearnState* L,
-                            uint32_t* choice, cudaStream_t st, long long* launches) {
+                            uint32_t* choice, const uint32_t* krank, uint32_t nk, uint64_t n,
+                            float window_z, cudaStream_t st, long long* launches) {
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(setup_learned_pl<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -357,7 +381,8 @@ static int learn_and_choose(int kind, const K* sorted, uint32_t S, uint32_t B, i
   } else {
     const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 16u;
     setup_learned_pl<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, steps, 0.02f, bound,
-                                                                    &As[1], &Gs[1], L, choice);
+                                                                    &As[1], &Gs[1], &Gs[0], L, choice,
+                                                                    krank, nk, n, window_z);
     *launches += 1;
   }
   return cudaGetLastError() == cudaSuccess ? GGMS_OK : GGMS_E_CUDA;

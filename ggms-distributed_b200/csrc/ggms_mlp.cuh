@@ -310,7 +310,8 @@ __global__ __launch_bounds__(SETUP_NT) void setup_mlp_finish(const K* __restrict
   mlp_eval_knots<K>(P, A, (float*)sm.Bs, sm.cdf);
   for (uint32_t j = threadIdx.x; j <= A->M; j += blockDim.x) L->cdf[j] = sm.cdf[j];
   pl_set_bases<K>(sm.cdf, A, sm.Bs, GGMS_ASSIGNER_LEARNED_MLP);
-  learned_finish<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_MLP, bound, A, G, L, choice, sm);
+  // G is the learned slot of the grid pair: G - 1 is the sampled grid
+  learned_finish<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_MLP, bound, A, G, G - 1, L, choice, sm);
 }
 
 template <typename K>

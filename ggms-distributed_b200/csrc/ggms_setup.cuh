@@ -422,6 +422,129 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
   return v;
 }
 
+// ------------------------------------------------------------------ bucket focus
+// A monotone piecewise-linear map of CDF space onto itself, w(0) = 0,
+// w(1) = 1: a learned model places bucket boundaries at w(F(key)) instead of
+// F(key).  With the ks clustered, the CDF ranges that can hold a k (the same
+// windows PASS 1 uses) get most of the buckets and the gaps between them the
+// rest, so the buckets that hold a k are far smaller and the candidates far
+// fewer.  Identity (n = 2 points) when the ks are spread out.
+constexpr uint32_t WARP_PTS = 2 * 4 + 2;   // two breakpoints per run (<= 4 runs) + the ends
+constexpr uint32_t FOCUS_BINS = 4096;     // resolution of the windows in CDF space
+constexpr float FOCUS_GAPS = 0.125f;      // share of the buckets for the gaps between runs
+
+struct Warp {
+  uint32_t n;              // breakpoints, 2..WARP_PTS
+  float p[WARP_PTS];       // CDF values, increasing from 0 to 1
+  float w[WARP_PTS];       // their images, increasing from 0 to 1
+};
+
+__device__ __forceinline__ float warp_fwd(const Warp& W, float p) {
+  p = fminf(fmaxf(p, 0.0f), 1.0f);
+  for (uint32_t i = 1; i < W.n; ++i)
+    if (p <= W.p[i] || i + 1 == W.n) {
+      const float d = W.p[i] - W.p[i - 1];
+      return d > 0.0f ? W.w[i - 1] + (W.w[i] - W.w[i - 1]) * __fdiv_rn(p - W.p[i - 1], d) : W.w[i];
+    }
+  return 1.0f;
+}
+__device__ __forceinline__ float warp_inv(const Warp& W, float y) {
+  y = fminf(fmaxf(y, 0.0f), 1.0f);
+  for (uint32_t i = 1; i < W.n; ++i)
+    if (y <= W.w[i] || i + 1 == W.n) {
+      const float d = W.w[i] - W.w[i - 1];
+      return d > 0.0f ? W.p[i - 1] + (W.p[i] - W.p[i - 1]) * __fdiv_rn(y - W.w[i - 1], d) : W.p[i];
+    }
+  return 1.0f;
+}
+
+// Builds the warp from the ks (ascending ranks krank[0..nk) of n keys) and the
+// sample size S.  The window of a k in CDF space is [pos - m, pos + m] / S with
+// pos = S (r + 1/2) / n and m = z sqrt(S q (1 - q)) + z + 2 (the PASS 1 window
+// rule); windows are rasterised onto FOCUS_BINS bins, merged across gaps
+// narrower than FOCUS_BINS / 256 bins, and used when they form at most
+// `maxruns` runs covering at most a quarter of the CDF.  All threads call it;
+// bins holds FOCUS_BINS + 1 ints of shared scratch.
+__device__ void build_warp(const uint32_t* __restrict__ krank, uint32_t nk, uint64_t n, uint32_t S,
+                           float z, uint32_t maxruns, int32_t* bins, uint32_t* red, Warp* out) {
+  const uint32_t tid = threadIdx.x, NT = blockDim.x;
+  for (uint32_t b = tid; b <= FOCUS_BINS; b += NT) bins[b] = 0;
+  __syncthreads();
+  for (uint32_t i = tid; i < nk; i += NT) {
+    const double q = ((double)krank[i] + 0.5) / (double)n;
+    const double m = (double)z * sqrt((double)S * q * (1.0 - q)) + (double)z + 2.0;
+    const double a = q - m / (double)S, c = q + m / (double)S;
+    const uint32_t b0 = a <= 0.0 ? 0u : min((uint32_t)(a * FOCUS_BINS), FOCUS_BINS - 1u);
+    const uint32_t b1 = c >= 1.0 ? FOCUS_BINS - 1u : min((uint32_t)(c * FOCUS_BINS), FOCUS_BINS - 1u);
+    atomicAdd(&bins[b0], 1);
+    atomicAdd(&bins[b1 + 1u], -1);
+  }
+  __syncthreads();
+  // coverage: prefix sum, a contiguous chunk per thread
+  const uint32_t chunk = (FOCUS_BINS + NT - 1u) / NT;
+  const uint32_t c0 = min(tid * chunk, FOCUS_BINS), c1 = min(c0 + chunk, FOCUS_BINS);
+  int32_t part = 0;
+  for (uint32_t b = c0; b < c1; ++b) part += bins[b];
+  uint32_t tot = 0;
+  int32_t run = (int32_t)block_excl_scan<uint32_t>((uint32_t)part, red, &tot);
+  for (uint32_t b = c0; b < c1; ++b) {
+    run += bins[b];
+    bins[b] = run;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    // runs of covered bins, merged across narrow gaps (serial: <= 4096 bins)
+    constexpr uint32_t MERGE = FOCUS_BINS / 256u;
+    uint32_t rs[4], re[4], R = 0, cov = 0;
+    bool ok = true;
+    uint32_t b = 0;
+    while (b < FOCUS_BINS && ok) {
+      if (bins[b] <= 0) { ++b; continue; }
+      uint32_t e = b;
+      while (e + 1u < FOCUS_BINS && bins[e + 1u] > 0) ++e;
+      if (R > 0 && b - re[R - 1] - 1u < MERGE) {
+        re[R - 1] = e;
+      } else if (R < 4u && R < maxruns) {
+        rs[R] = b;
+        re[R] = e;
+        ++R;
+      } else {
+        ok = false;
+      }
+      b = e + 1u;
+    }
+    for (uint32_t r = 0; r < R; ++r) cov += re[r] - rs[r] + 1u;
+    Warp W;
+    W.n = 2;
+    W.p[0] = 0.0f; W.w[0] = 0.0f;
+    W.p[1] = 1.0f; W.w[1] = 1.0f;
+    if (ok && R > 0 && cov <= FOCUS_BINS / 4u) {
+      const float P = (float)cov / (float)FOCUS_BINS;  // CDF mass of the runs
+      const float gap_share = (P < 1.0f) ? FOCUS_GAPS : 0.0f;
+      const float run_slope = (1.0f - gap_share) / P, gap_slope = gap_share / (1.0f - P);
+      uint32_t k = 0;
+      float pp = 0.0f, ww = 0.0f;
+      W.p[k] = 0.0f; W.w[k] = 0.0f; ++k;
+      for (uint32_t r = 0; r < R; ++r) {
+        const float a = (float)rs[r] / (float)FOCUS_BINS, c = (float)(re[r] + 1u) / (float)FOCUS_BINS;
+        if (a > pp) {  // gap before run r
+          ww += (a - pp) * gap_slope;
+          pp = a;
+          W.p[k] = pp; W.w[k] = fminf(ww, 1.0f); ++k;
+        }
+        ww += (c - pp) * run_slope;
+        pp = c;
+        W.p[k] = pp; W.w[k] = fminf(ww, 1.0f); ++k;
+      }
+      if (pp < 1.0f) { W.p[k] = 1.0f; W.w[k] = 1.0f; ++k; }
+      W.w[k - 1] = 1.0f;
+      W.n = k;
+    }
+    *out = W;
+  }
+  __syncthreads();
+}
+
 // Occupancy of the grid's buckets on the (sorted) sample, over 256 groups of
 // buckets: max / mean.
 // At most GRID_MEASURE_N samples are used (a strided subsample of the sorted
@@ -429,7 +552,8 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
 constexpr uint32_t GRID_MEASURE_N = 16384;
 
 template <typename K>
-__device__ float grid_measure(const GridView<K>& g, const K* sorted_all, uint32_t S_all, uint32_t* hist256) {
+__device__ float grid_measure(const GridView<K>& g, const K* sorted_all, uint32_t S_all, uint32_t* hist256,
+                              const Warp* wp = nullptr) {
   const uint32_t stride = S_all > GRID_MEASURE_N ? S_all / GRID_MEASURE_N : 1u;
   const uint32_t S = S_all / stride;
   for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) hist256[i] = 0;
@@ -449,7 +573,16 @@ __device__ float grid_measure(const GridView<K>& g, const K* sorted_all, uint32_
     for (int u = 0; u < 4; ++u) {
       const uint32_t i = base + u * NTh + threadIdx.x;
       const bool ok = i < S;
-      const uint32_t grp = ok ? (uint32_t)(((uint64_t)grid_eval<K>(g, v[u]) * 256u) / g.B) : 0xFFFFFFFFu;
+      uint32_t grp = 0xFFFFFFFFu;
+      if (ok) {
+        const uint32_t b = grid_eval<K>(g, v[u]);
+        if (wp && wp->n > 2u) {  // a focused model: measure in the CDF space before the warp
+          const float y = ((float)b - 0.5f) / (float)(g.B - 2u);
+          grp = min((uint32_t)(warp_inv(*wp, y) * 256.0f), 255u);
+        } else {
+          grp = (uint32_t)(((uint64_t)b * 256u) / g.B);
+        }
+      }
       const uint32_t g0 = __shfl_sync(FULL, grp, 0);
       const uint32_t okm = __ballot_sync(FULL, ok);
       if (__all_sync(FULL, !ok || grp == g0)) {

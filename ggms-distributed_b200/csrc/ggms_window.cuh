@@ -7,7 +7,8 @@
 // (S, q = (r + 1/2) / n), so the key lies between the sample keys at positions
 // S q -+ m, m = z sqrt(S q (1 - q)) + z + 2, except with a probability far
 // below 10^-12 for z = 8.  Every k thus gets a range of level-0 buckets; their
-// union, merged into at most L0_WIN runs, is the only place PASS 1 computes
+// union, merged across gaps that hold under 1/256 of the sample into at most
+// L0_WIN runs holding at most a quarter of it, is the only place PASS 1 computes
 // buckets.  Keys elsewhere are counted per gap between runs (a few compares),
 // so when the ks are clustered most of the input skips the bucket
 // computation entirely.  Nothing here decides an answer: a k outside every
@@ -18,22 +19,36 @@
 namespace ggms {
 
 constexpr uint32_t WIN_MAXRAW = 64;    // runs before merging; more: no windows
-constexpr uint32_t WIN_MERGE = 64;     // runs closer than this many buckets merge
 constexpr uint32_t WIN_NT = 1024;
 
-// One CTA.  Dynamic shared memory: (B + 1) int32.
+constexpr uint32_t WIN_IDX = 64;  // every WIN_IDX-th sample key is kept in shared memory
+
+template <typename K>
+__host__ __device__ constexpr size_t l0_window_smem(uint32_t B) {
+  return GRID_SMEM + sizeof(K) * (65536u / WIN_IDX) + 4u * ((size_t)B + 1u);
+}
+
+// One CTA.  Dynamic shared memory: l0_window_smem<K>(B) -- the grid (every
+// search below evaluates it many times), a coarse index of the sample, and the
+// (B + 1)-entry coverage array.
 template <typename K>
 __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted, uint32_t S,
                                                    const uint32_t* __restrict__ krank, uint32_t nk,
                                                    uint64_t n, const Grid<K>* __restrict__ Gs,
                                                    Counters* C, float z, Windows<K>* W) {
-  extern __shared__ int32_t cover[];  // difference array, then coverage, of the B buckets
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint2* s1 = reinterpret_cast<uint2*>(smem);
+  uint2* s2 = s1 + GRID_T1;
+  K* sidx = reinterpret_cast<K*>(smem + GRID_SMEM);                 // sorted[j * WIN_IDX]
+  int32_t* cover = reinterpret_cast<int32_t*>(sidx + 65536u / WIN_IDX);  // difference array, then coverage
   __shared__ uint32_t red[33];
-  __shared__ uint32_t rs[WIN_MAXRAW], re[WIN_MAXRAW];
+  __shared__ uint32_t rs[WIN_MAXRAW], re[WIN_MAXRAW], ss[WIN_MAXRAW], se[WIN_MAXRAW];
   __shared__ Windows<K> sw;
   const uint32_t tid = threadIdx.x;
-  const GridView<K> gv = grid_view_global<K>(Gs + C->asg_choice);
+  const GridView<K> gv = grid_to_smem<K>(Gs + C->asg_choice, s1, s2);
   const uint32_t B = gv.B;
+  const uint32_t nidx = (S + WIN_IDX - 1u) / WIN_IDX;  // S <= 65536
+  for (uint32_t j = tid; j < nidx; j += WIN_NT) sidx[j] = sorted[j * WIN_IDX];
   for (uint32_t b = tid; b <= B; b += WIN_NT) cover[b] = 0;
   __syncthreads();
   // 1. bucket range of every k
@@ -88,34 +103,58 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
     }
   }
   __syncthreads();
-  // 4. merge close runs; decide
+  // 4. sample positions of the raw runs: [ss, se) = the sample keys whose
+  //    bucket lies in the run (binary search over the sorted sample)
+  if (tid < 2u * min(nraw, WIN_MAXRAW)) {
+    const uint32_t j = tid >> 1;
+    const uint32_t target = (tid & 1u) ? re[j] + 1u : rs[j];  // first sample with bucket >= target
+    // coarse: the first indexed key with bucket >= target, in shared memory;
+    // then within the WIN_IDX keys before it, in global memory
+    uint32_t lo = 0, hi = nidx;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (min(grid_eval<K>(gv, sidx[mid]), B - 1u) >= target) hi = mid; else lo = mid + 1;
+    }
+    hi = min(lo * WIN_IDX, S);
+    lo = lo ? (lo - 1u) * WIN_IDX + 1u : 0u;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (min(grid_eval<K>(gv, sorted[mid]), B - 1u) >= target) hi = mid; else lo = mid + 1;
+    }
+    if (tid & 1u) se[j] = lo; else ss[j] = lo;
+  }
+  __syncthreads();
+  // 5. merge runs across gaps that hold under 1/256 of the sample; decide:
+  //    at most L0_WIN runs holding at most a quarter of the sample
   if (tid == 0) {
     sw.on = 0;
     sw.R = 0;
     sw.cnt = 0;
     uint32_t R = 0, hot = 0;
     if (nraw >= 1 && nraw <= WIN_MAXRAW && nraw2 == nraw) {
-      uint32_t cs = rs[0], ce = re[0];
+      uint32_t cs = rs[0], ce = re[0], cse = se[0], css = ss[0];
       bool ok = true;
       for (uint32_t i = 1; i <= nraw && ok; ++i) {
-        if (i < nraw && rs[i] - ce - 1u < WIN_MERGE) {
+        if (i < nraw && (ss[i] - cse) * 256u < S) {
           ce = re[i];
+          cse = se[i];
           continue;
         }
         if (R == L0_WIN) { ok = false; break; }
         sw.rb0[R] = cs;
         sw.rb1[R] = ce;
-        hot += ce - cs + 1u;
+        hot += cse - css;
         ++R;
-        if (i < nraw) { cs = rs[i]; ce = re[i]; }
+        if (i < nraw) { cs = rs[i]; ce = re[i]; css = ss[i]; cse = se[i]; }
       }
-      if (ok && hot <= B / 4u) {
+      if (ok && hot * 4u <= S) {
         sw.on = 1;
         sw.R = R;
         // buckets below the smallest key's or above the largest key's never
         // hold a key: a gap made only of those is empty
         const uint32_t bmin = min(grid_eval<K>(gv, (K)0), B - 1u);
         const uint32_t bmax = min(grid_eval<K>(gv, key_max<K>()), B - 1u);
+        uint32_t ne = 0;
         for (uint32_t g = 0; g <= R; ++g) {
           // gap g lies between run g-1 and run g; gb0 > gb1 marks an empty gap
           const uint32_t g0 = g == 0 ? 0u : sw.rb1[g - 1] + 1u;
@@ -123,15 +162,14 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
           const bool holds = g0 < g1 && g0 <= bmax && g1 > bmin;
           sw.gb0[g] = holds ? g0 : B;
           sw.gb1[g] = holds ? g1 - 1u : 0u;
+          ne += holds ? 1u : 0u;
         }
-        uint32_t ne = 0;
-        for (uint32_t g = 0; g <= R; ++g) ne += sw.gb0[g] <= sw.gb1[g] ? 1u : 0u;
         sw.cnt = ne >= 2u ? 1u : 0u;
       }
     }
   }
   __syncthreads();
-  // 5. key range of each run: [L(rb0), L(rb1 + 1) - 1], L(x) = smallest key with bucket >= x
+  // 6. key range of each run: [L(rb0), L(rb1 + 1) - 1], L(x) = smallest key with bucket >= x
   if (sw.on && tid < 2u * sw.R) {
     const uint32_t r = tid >> 1;
     const bool upper = tid & 1u;

@@ -79,3 +79,22 @@ def test_windows_topk(ctx):
     out = G.topk(ctx, d.data_ptr(), n, K, np.float32)
     exp = np.sort(v)[::-1][:K]
     np.testing.assert_array_equal(orc.bits(out), orc.bits(exp))
+
+
+def test_focused_buckets_cut_candidates(ctx):
+    """With clustered ks the learned model spends most buckets on the ks' windows:
+    the buckets that hold a k are smaller, so PASS 2 copies fewer candidates."""
+    n = 1 << 24
+    v = D.VALUE_GENERATORS["half_normal_f32"](n, 21)
+    ks = D.ks_top1pct(n, 1024, 21)
+    d = to_device(v)
+    exp = orc.select(v, ks)
+    res = {}
+    for z in (0.0, -1.0):
+        out, st = G.select(ctx, d.data_ptr(), n, ks, np.float32, assigner=G.ASSIGNER_LEARNED_PL,
+                           stats=True, window_z=z)
+        np.testing.assert_array_equal(orc.bits(out), orc.bits(exp))
+        assert st["assigner_used"] == "learned_pl", st
+        res[z] = st
+    assert res[0.0]["window_runs"] >= 1
+    assert res[0.0]["candidates"] * 3 < res[-1.0]["candidates"], res
