@@ -245,6 +245,11 @@ __device__ __forceinline__ void unpack16(const uint4& q, T (&e)[Vec16<T>::N]) {
   __builtin_memcpy(e, &q, 16);
 }
 
+// The passes run 1024 threads per SM at least (2 CTAs of 512, 4 of 256, 1 of
+// 1024): the register budget is 64 per thread, which the launch bounds state
+// so that the compiler neither exceeds it nor spills well below it.
+#define PASS_MIN_CTAS(nt) ((nt) >= 1024 ? 1 : 1024 / (nt))
+
 // Per-warp queues of the passes.  Keys that need the long path (bucket
 // computation) are spread over the input; handling each where it is found
 // would run the long path for every warp that holds one.  They are appended
@@ -362,7 +367,7 @@ __device__ __forceinline__ void count_runs(const Windows<typename KeyOf<T>::K>& 
 // gap = all - below(last run) - count(last run) -- and goes to the gap's first
 // bucket, so the prefix sums over the buckets stay exact.
 template <typename T, int NT, int UNROLL>
-__global__ __launch_bounds__(NT) void l0_count(const T* __restrict__ in, uint64_t n,
+__global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_count(const T* __restrict__ in, uint64_t n,
                                               const Grid<typename KeyOf<T>::K>* __restrict__ Gs,
                                               const Counters* __restrict__ C,
                                               const Windows<typename KeyOf<T>::K>* __restrict__ Wg,
@@ -727,7 +732,7 @@ __host__ __device__ constexpr uint32_t l0_compact_qwords(uint32_t nt, uint32_t k
 }
 
 template <typename T, int NT, int UNROLL>
-__global__ __launch_bounds__(NT) void l0_compact(const T* __restrict__ in, uint64_t n,
+__global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __restrict__ in, uint64_t n,
                                                 const Grid<typename KeyOf<T>::K>* __restrict__ Gs,
                                                 Counters* C,
                                                 const Windows<typename KeyOf<T>::K>* __restrict__ Wg,

@@ -55,53 +55,47 @@ __device__ __forceinline__ float softplusf(float x) {
 __device__ __forceinline__ float sigmoidf_(float x) { return 1.0f / (1.0f + expf(-x)); }
 
 // ------------------------------------------------------------------ statistics
-// Per-segment sufficient statistics of the sorted sample; warp w handles
-// segments w, w + nwarps, ... (fixed summation order: deterministic).
+// Per-segment sufficient statistics of the sorted sample.  Thread j handles
+// segment j alone, in sample order (a fixed summation order: deterministic);
+// its samples are contiguous, so the loads stream from L2.  The segment bounds
+// come from one search per knot, first over every 64th sample key kept in
+// shared memory, then over the 64 keys between two of them.
+constexpr uint32_t PL_IDX = 64;
+
 template <typename K>
 __device__ void pl_stats_block(const K* __restrict__ sorted, uint32_t S, const K* x, uint32_t M,
                                PLStats* st, uint32_t* seg_start) {
-  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  // first sample of every segment: one binary search per knot, all in parallel
+  // the statistics array is free until the end: its front holds the index
+  K* sidx = reinterpret_cast<K*>(st);
+  const uint32_t nidx = (S + PL_IDX - 1u) / PL_IDX;  // S <= 65536: <= 1024 keys
+  for (uint32_t j = threadIdx.x; j < nidx; j += blockDim.x) sidx[j] = sorted[j * PL_IDX];
+  __syncthreads();
+  // first sample of every segment (the last segment also takes s == x_M)
   for (uint32_t j = threadIdx.x; j <= M; j += blockDim.x) {
-    uint32_t lo = 0, hi = S;
-    if (j == M) {
-      lo = S;  // the last segment also takes s == x_M
-    } else {
+    uint32_t lo = S;
+    if (j < M) {
       const K v = x[j];
-      while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (sorted[m] < v) lo = m + 1; else hi = m; }
+      uint32_t a = 0, b = nidx;  // first indexed key >= v
+      while (a < b) { const uint32_t m = (a + b) >> 1; if (sidx[m] < v) a = m + 1; else b = m; }
+      uint32_t hi = min(a * PL_IDX, S);
+      lo = a ? (a - 1u) * PL_IDX + 1u : 0u;
+      while (lo < hi) { const uint32_t m = (lo + hi) >> 1; if (sorted[m] < v) lo = m + 1; else hi = m; }
     }
     seg_start[j] = lo;
   }
   __syncthreads();
-  for (uint32_t j = warp; j < M; j += nw) {
+  for (uint32_t j = threadIdx.x; j < M; j += blockDim.x) {
     const K xj = x[j], xn = x[j + 1];
     const uint32_t i0 = seg_start[j], i1 = seg_start[j + 1];
     const float width = key_to_float_rn((K)(xn - xj));
     double n = 0, su = 0, su2 = 0, sy = 0, syu = 0, sy2 = 0;
-    for (uint32_t i = i0 + lane; i < i1; i += 128) {  // four independent loads in flight
-      K v[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) v[q] = (i + 32 * q < i1) ? sorted[i + 32 * q] : xj;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const uint32_t ii = i + 32 * q;
-        if (ii < i1) {
-          const float u = fminf(__fdiv_rn(key_to_float_rn((K)(v[q] - xj)), width), 1.0f);
-          const double y = ((double)ii + 0.5) / (double)S;
-          n += 1.0; su += u; su2 += (double)u * u; sy += y; syu += y * u; sy2 += y * y;
-        }
-      }
+#pragma unroll 4
+    for (uint32_t i = i0; i < i1; ++i) {
+      const float u = fminf(__fdiv_rn(key_to_float_rn((K)(sorted[i] - xj)), width), 1.0f);
+      const double y = ((double)i + 0.5) / (double)S;
+      n += 1.0; su += u; su2 += (double)u * u; sy += y; syu += y * u; sy2 += y * y;
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      n += __shfl_xor_sync(FULL, n, o);
-      su += __shfl_xor_sync(FULL, su, o);
-      su2 += __shfl_xor_sync(FULL, su2, o);
-      sy += __shfl_xor_sync(FULL, sy, o);
-      syu += __shfl_xor_sync(FULL, syu, o);
-      sy2 += __shfl_xor_sync(FULL, sy2, o);
-    }
-    if (lane == 0) st[j] = PLStats{n, su, su2, sy, syu, sy2};
+    st[j] = PLStats{n, su, su2, sy, syu, sy2};
   }
 }
 
@@ -323,7 +317,7 @@ __global__ __launch_bounds__(SETUP_NT) void setup_learned_pl(const K* __restrict
   __syncthreads();
   if (window_z >= 0.0f) {
     // the statistics are dead after training: their space holds the bins
-    build_warp(krank, nk, n, S, window_z, L0_WIN, reinterpret_cast<int32_t*>(sm.st), wred, &wsh);
+    build_warp(krank, nk, n, S, window_z, L0_WIN, reinterpret_cast<uint32_t*>(sm.st), wred, &wsh);
   } else if (threadIdx.x == 0) {
     wsh.n = 2;
     wsh.p[0] = wsh.w[0] = 0.0f;
@@ -379,7 +373,7 @@ static int learn_and_choose(int kind, const K* sorted, uint32_t S, uint32_t B, i
     int rc = mlp_fit_and_compile<K>(sorted, S, B, steps_opt, bound, As, Gs, L, choice, st, launches);
     if (rc) return rc;
   } else {
-    const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 16u;
+    const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 4u;
     setup_learned_pl<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, steps, 0.02f, bound,
                                                                     &As[1], &Gs[1], &Gs[0], L, choice,
                                                                     krank, nk, n, window_z);

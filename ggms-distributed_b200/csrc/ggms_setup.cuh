@@ -422,6 +422,54 @@ __device__ GridView<K> grid_compile(const AsgView<K>& a, uint32_t B, uint32_t ki
   return v;
 }
 
+// ------------------------------------------------------------------ interval bitmaps
+// Sets bits [b0, b1] of a bitmap in shared memory (concurrent callers OK).
+__device__ __forceinline__ void bits_mark(uint32_t* bm, uint32_t b0, uint32_t b1) {
+  const uint32_t w0 = b0 >> 5, w1 = b1 >> 5;
+  const uint32_t lo = ~0u << (b0 & 31);
+  const uint32_t hi = (b1 & 31) == 31u ? ~0u : ((2u << (b1 & 31)) - 1u);
+  if (w0 == w1) {
+    atomicOr(&bm[w0], lo & hi);
+    return;
+  }
+  atomicOr(&bm[w0], lo);
+  for (uint32_t w = w0 + 1u; w < w1; ++w) atomicOr(&bm[w], ~0u);
+  atomicOr(&bm[w1], hi);
+}
+
+// Maximal runs of set bits of a bitmap of `words` words (<= blockDim.x), in
+// order: run j is [rs[j], re[j]] for j < min(total, cap).  Returns the number
+// of runs.  All threads call it.
+__device__ uint32_t bitmap_runs(const uint32_t* bm, uint32_t words, uint32_t* rs, uint32_t* re,
+                                uint32_t cap, uint32_t* red) {
+  const uint32_t i = threadIdx.x;
+  uint32_t st = 0, en = 0;
+  if (i < words) {
+    const uint32_t w = bm[i];
+    const uint32_t prev_top = i ? bm[i - 1] >> 31 : 0u;
+    const uint32_t next_low = i + 1u < words ? bm[i + 1u] & 1u : 0u;
+    st = w & ~((w << 1) | prev_top);
+    en = w & ~((w >> 1) | (next_low << 31));
+  }
+  uint32_t total = 0, total2 = 0;
+  uint32_t a = block_excl_scan<uint32_t>((uint32_t)__popc(st), red, &total);
+  uint32_t b = block_excl_scan<uint32_t>((uint32_t)__popc(en), red, &total2);
+  while (st) {
+    const uint32_t bit = __ffs(st) - 1u;
+    if (a < cap) rs[a] = i * 32u + bit;
+    ++a;
+    st &= st - 1u;
+  }
+  while (en) {
+    const uint32_t bit = __ffs(en) - 1u;
+    if (b < cap) re[b] = i * 32u + bit;
+    ++b;
+    en &= en - 1u;
+  }
+  __syncthreads();
+  return total;
+}
+
 // ------------------------------------------------------------------ bucket focus
 // A monotone piecewise-linear map of CDF space onto itself, w(0) = 0,
 // w(1) = 1: a learned model places bucket boundaries at w(F(key)) instead of
@@ -461,14 +509,19 @@ __device__ __forceinline__ float warp_inv(const Warp& W, float y) {
 // Builds the warp from the ks (ascending ranks krank[0..nk) of n keys) and the
 // sample size S.  The window of a k in CDF space is [pos - m, pos + m] / S with
 // pos = S (r + 1/2) / n and m = z sqrt(S q (1 - q)) + z + 2 (the PASS 1 window
-// rule); windows are rasterised onto FOCUS_BINS bins, merged across gaps
-// narrower than FOCUS_BINS / 256 bins, and used when they form at most
-// `maxruns` runs covering at most a quarter of the CDF.  All threads call it;
-// bins holds FOCUS_BINS + 1 ints of shared scratch.
+// rule); windows are rasterised onto a bitmap of FOCUS_BINS bins, merged
+// across gaps narrower than FOCUS_BINS / 256 bins, and used when they form at
+// most `maxruns` runs covering at most a quarter of the CDF.  All threads call
+// it (blockDim.x >= FOCUS_BINS / 32); scratch holds FOCUS_BINS / 32 + 128
+// words of shared memory.
 __device__ void build_warp(const uint32_t* __restrict__ krank, uint32_t nk, uint64_t n, uint32_t S,
-                           float z, uint32_t maxruns, int32_t* bins, uint32_t* red, Warp* out) {
+                           float z, uint32_t maxruns, uint32_t* scratch, uint32_t* red, Warp* out) {
+  constexpr uint32_t WORDS = FOCUS_BINS / 32u, CAP = 64;
+  uint32_t* bm = scratch;              // [WORDS] covered bins
+  uint32_t* rs = scratch + WORDS;      // [CAP] raw run starts
+  uint32_t* re = rs + CAP;             // [CAP] raw run ends
   const uint32_t tid = threadIdx.x, NT = blockDim.x;
-  for (uint32_t b = tid; b <= FOCUS_BINS; b += NT) bins[b] = 0;
+  for (uint32_t w = tid; w < WORDS; w += NT) bm[w] = 0u;
   __syncthreads();
   for (uint32_t i = tid; i < nk; i += NT) {
     const double q = ((double)krank[i] + 0.5) / (double)n;
@@ -476,44 +529,27 @@ __device__ void build_warp(const uint32_t* __restrict__ krank, uint32_t nk, uint
     const double a = q - m / (double)S, c = q + m / (double)S;
     const uint32_t b0 = a <= 0.0 ? 0u : min((uint32_t)(a * FOCUS_BINS), FOCUS_BINS - 1u);
     const uint32_t b1 = c >= 1.0 ? FOCUS_BINS - 1u : min((uint32_t)(c * FOCUS_BINS), FOCUS_BINS - 1u);
-    atomicAdd(&bins[b0], 1);
-    atomicAdd(&bins[b1 + 1u], -1);
+    bits_mark(bm, b0, b1);
   }
   __syncthreads();
-  // coverage: prefix sum, a contiguous chunk per thread
-  const uint32_t chunk = (FOCUS_BINS + NT - 1u) / NT;
-  const uint32_t c0 = min(tid * chunk, FOCUS_BINS), c1 = min(c0 + chunk, FOCUS_BINS);
-  int32_t part = 0;
-  for (uint32_t b = c0; b < c1; ++b) part += bins[b];
-  uint32_t tot = 0;
-  int32_t run = (int32_t)block_excl_scan<uint32_t>((uint32_t)part, red, &tot);
-  for (uint32_t b = c0; b < c1; ++b) {
-    run += bins[b];
-    bins[b] = run;
-  }
-  __syncthreads();
+  const uint32_t nraw = bitmap_runs(bm, WORDS, rs, re, CAP, red);
   if (tid == 0) {
-    // runs of covered bins, merged across narrow gaps (serial: <= 4096 bins)
+    // merge runs across narrow gaps
     constexpr uint32_t MERGE = FOCUS_BINS / 256u;
-    uint32_t rs[4], re[4], R = 0, cov = 0;
-    bool ok = true;
-    uint32_t b = 0;
-    while (b < FOCUS_BINS && ok) {
-      if (bins[b] <= 0) { ++b; continue; }
-      uint32_t e = b;
-      while (e + 1u < FOCUS_BINS && bins[e + 1u] > 0) ++e;
-      if (R > 0 && b - re[R - 1] - 1u < MERGE) {
-        re[R - 1] = e;
+    uint32_t frs[4], fre[4], R = 0, cov = 0;
+    bool ok = nraw >= 1u && nraw <= CAP;
+    for (uint32_t j = 0; j < nraw && ok; ++j) {
+      if (R > 0 && rs[j] - fre[R - 1] - 1u < MERGE) {
+        fre[R - 1] = re[j];
       } else if (R < 4u && R < maxruns) {
-        rs[R] = b;
-        re[R] = e;
+        frs[R] = rs[j];
+        fre[R] = re[j];
         ++R;
       } else {
         ok = false;
       }
-      b = e + 1u;
     }
-    for (uint32_t r = 0; r < R; ++r) cov += re[r] - rs[r] + 1u;
+    for (uint32_t r = 0; r < R; ++r) cov += fre[r] - frs[r] + 1u;
     Warp W;
     W.n = 2;
     W.p[0] = 0.0f; W.w[0] = 0.0f;
@@ -526,7 +562,7 @@ __device__ void build_warp(const uint32_t* __restrict__ krank, uint32_t nk, uint
       float pp = 0.0f, ww = 0.0f;
       W.p[k] = 0.0f; W.w[k] = 0.0f; ++k;
       for (uint32_t r = 0; r < R; ++r) {
-        const float a = (float)rs[r] / (float)FOCUS_BINS, c = (float)(re[r] + 1u) / (float)FOCUS_BINS;
+        const float a = (float)frs[r] / (float)FOCUS_BINS, c = (float)(fre[r] + 1u) / (float)FOCUS_BINS;
         if (a > pp) {  // gap before run r
           ww += (a - pp) * gap_slope;
           pp = a;

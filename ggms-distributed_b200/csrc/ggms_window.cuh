@@ -25,12 +25,12 @@ constexpr uint32_t WIN_IDX = 64;  // every WIN_IDX-th sample key is kept in shar
 
 template <typename K>
 __host__ __device__ constexpr size_t l0_window_smem(uint32_t B) {
-  return GRID_SMEM + sizeof(K) * (65536u / WIN_IDX) + 4u * ((size_t)B + 1u);
+  return GRID_SMEM + sizeof(K) * (65536u / WIN_IDX) + 4u * ((size_t)B / 32u);
 }
 
 // One CTA.  Dynamic shared memory: l0_window_smem<K>(B) -- the grid (every
-// search below evaluates it many times), a coarse index of the sample, and the
-// (B + 1)-entry coverage array.
+// search below evaluates it many times), a coarse index of the sample, and a
+// bitmap of the B buckets.
 template <typename K>
 __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted, uint32_t S,
                                                    const uint32_t* __restrict__ krank, uint32_t nk,
@@ -39,8 +39,8 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
   extern __shared__ __align__(16) uint8_t smem[];
   uint2* s1 = reinterpret_cast<uint2*>(smem);
   uint2* s2 = s1 + GRID_T1;
-  K* sidx = reinterpret_cast<K*>(smem + GRID_SMEM);                 // sorted[j * WIN_IDX]
-  int32_t* cover = reinterpret_cast<int32_t*>(sidx + 65536u / WIN_IDX);  // difference array, then coverage
+  K* sidx = reinterpret_cast<K*>(smem + GRID_SMEM);                         // sorted[j * WIN_IDX]
+  uint32_t* bm = reinterpret_cast<uint32_t*>(sidx + 65536u / WIN_IDX);      // buckets some k may hold
   __shared__ uint32_t red[33];
   __shared__ uint32_t rs[WIN_MAXRAW], re[WIN_MAXRAW], ss[WIN_MAXRAW], se[WIN_MAXRAW];
   __shared__ Windows<K> sw;
@@ -49,9 +49,9 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
   const uint32_t B = gv.B;
   const uint32_t nidx = (S + WIN_IDX - 1u) / WIN_IDX;  // S <= 65536
   for (uint32_t j = tid; j < nidx; j += WIN_NT) sidx[j] = sorted[j * WIN_IDX];
-  for (uint32_t b = tid; b <= B; b += WIN_NT) cover[b] = 0;
+  for (uint32_t w = tid; w < B / 32u; w += WIN_NT) bm[w] = 0u;
   __syncthreads();
-  // 1. bucket range of every k
+  // 1. bucket range of every k, marked in the bitmap
   for (uint32_t i = tid; i < nk; i += WIN_NT) {
     const double q = ((double)krank[i] + 0.5) / (double)n;
     const double pos = q * (double)S;
@@ -61,49 +61,13 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
     const K khi = c > (double)(S - 1u) ? key_max<K>() : sorted[(uint32_t)c];
     const uint32_t b0 = min(grid_eval<K>(gv, klo), B - 1u);
     const uint32_t b1 = min(grid_eval<K>(gv, khi), B - 1u);
-    atomicAdd(&cover[b0], 1);
-    atomicAdd(&cover[b1 + 1u], -1);
+    bits_mark(bm, b0, b1);
   }
   __syncthreads();
-  // 2. coverage: prefix sum of the difference array, a contiguous chunk per thread
-  const uint32_t chunk = (B + WIN_NT - 1u) / WIN_NT;
-  const uint32_t c0 = min(tid * chunk, B), c1 = min(c0 + chunk, B);
-  int32_t part = 0;
-  for (uint32_t b = c0; b < c1; ++b) part += cover[b];
-  uint32_t tot_u = 0;
-  const int32_t before = (int32_t)block_excl_scan<uint32_t>((uint32_t)part, red, &tot_u);
-  {
-    int32_t run = before;
-    for (uint32_t b = c0; b < c1; ++b) {
-      run += cover[b];
-      cover[b] = run;  // this thread's chunk only: no other thread reads it yet
-    }
-  }
-  __syncthreads();
-  // 3. raw runs of covered buckets, numbered in bucket order (run j is the
-  //    j-th start and the j-th end)
-  auto is_start = [&](uint32_t b) { return cover[b] > 0 && (b == 0 || cover[b - 1] <= 0); };
-  auto is_end = [&](uint32_t b) { return cover[b] > 0 && (b + 1u == B || cover[b + 1] <= 0); };
-  uint32_t nst = 0, nen = 0;
-  for (uint32_t b = c0; b < c1; ++b) {
-    nst += is_start(b);
-    nen += is_end(b);
-  }
-  uint32_t nraw = 0, nraw2 = 0;
-  uint32_t at = block_excl_scan<uint32_t>(nst, red, &nraw);
-  uint32_t ate = block_excl_scan<uint32_t>(nen, red, &nraw2);
-  for (uint32_t b = c0; b < c1; ++b) {
-    if (is_start(b)) {
-      if (at < WIN_MAXRAW) rs[at] = b;
-      ++at;
-    }
-    if (is_end(b)) {
-      if (ate < WIN_MAXRAW) re[ate] = b;
-      ++ate;
-    }
-  }
-  __syncthreads();
-  // 4. sample positions of the raw runs: [ss, se) = the sample keys whose
+  // 2. raw runs of marked buckets, in bucket order (B / 32 <= 1024 words)
+  const uint32_t nraw = bitmap_runs(bm, B / 32u, rs, re, WIN_MAXRAW, red);
+  const uint32_t nraw2 = nraw;
+  // 3. sample positions of the raw runs: [ss, se) = the sample keys whose
   //    bucket lies in the run (binary search over the sorted sample)
   if (tid < 2u * min(nraw, WIN_MAXRAW)) {
     const uint32_t j = tid >> 1;
@@ -124,7 +88,7 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
     if (tid & 1u) se[j] = lo; else ss[j] = lo;
   }
   __syncthreads();
-  // 5. merge runs across gaps that hold under 1/256 of the sample; decide:
+  // 4. merge runs across gaps that hold under 1/256 of the sample; decide:
   //    at most L0_WIN runs holding at most a quarter of the sample
   if (tid == 0) {
     sw.on = 0;
@@ -169,7 +133,7 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
     }
   }
   __syncthreads();
-  // 6. key range of each run: [L(rb0), L(rb1 + 1) - 1], L(x) = smallest key with bucket >= x
+  // 5. key range of each run: [L(rb0), L(rb1 + 1) - 1], L(x) = smallest key with bucket >= x
   if (sw.on && tid < 2u * sw.R) {
     const uint32_t r = tid >> 1;
     const bool upper = tid & 1u;
