@@ -261,9 +261,9 @@ static int make_plan(Plan* p, uint64_t n, uint32_t nk, const ggms_opts& o) {
   p->nk = nk;
   uint32_t B = (uint32_t)o.num_buckets;
   if (B == 0) {
-    // about 2^11 elements per bucket, between 2^10 and 2^14 buckets
+    // about 2^11 elements per bucket, between 2^10 and 2^13 buckets
     B = pow2_floor(std::max<uint64_t>(n >> 11, 1));
-    B = std::min<uint32_t>(std::max<uint32_t>(B, 1u << 10), 1u << 14);
+    B = std::min<uint32_t>(std::max<uint32_t>(B, 1u << 10), 1u << 13);
   }
   if (B < (1u << 10) || B > (1u << 15) || (B & (B - 1))) return GGMS_E_INVALID_ARG;
   p->B = B;
@@ -326,7 +326,7 @@ static const PassVariant<T>* pass_variant(int nt, int unroll) {
   return nullptr;
 }
 
-constexpr int DEFAULT_PASS_NT = 512;
+constexpr int DEFAULT_PASS_NT = 1024;
 constexpr int DEFAULT_PASS_UNROLL = 4;
 
 // The two passes must split the input among CTAs identically (PASS 2 writes
@@ -772,10 +772,11 @@ struct DevBuf {
 
 static int pl_gradient(const uint32_t* keys, int S, const float* theta, float* loss, float* grad,
                        uint32_t* knots, int* Mout) {
-  if (!keys || S < 2 || !theta || !loss || !grad) return GGMS_E_INVALID_ARG;
-  DevBuf dk, da, dt, dout;
+  if (!keys || S < 2 || S > 65536 || !theta || !loss || !grad) return GGMS_E_INVALID_ARG;
+  DevBuf dk, da, dt, dout, dl;
   GGMS_CU(cudaMalloc(&dk.p, 4ull * S));
   GGMS_CU(cudaMalloc(&da.p, sizeof(Assigner<uint32_t>)));
+  GGMS_CU(cudaMalloc(&dl.p, sizeof(LearnState)));
   GGMS_CU(cudaMalloc(&dt.p, 4ull * PL_M));
   GGMS_CU(cudaMalloc(&dout.p, 4ull * (PL_M + 1)));
   GGMS_CU(cudaMemcpy(dk.p, keys, 4ull * S, cudaMemcpyHostToDevice));
@@ -783,10 +784,17 @@ static int pl_gradient(const uint32_t* keys, int S, const float* theta, float* l
   auto* A = (Assigner<uint32_t>*)da.p;
   float* dloss = (float*)dout.p;
   float* dgrad = dloss + 1;
+  auto* L = (LearnState*)dl.p;
   GGMS_CU(cudaFuncSetAttribute(pl_grad_probe<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(LearnSmem<uint32_t>)));
-  pl_grad_probe<uint32_t><<<1, SETUP_NT, sizeof(LearnSmem<uint32_t>)>>>(
-      (const uint32_t*)dk.p, (uint32_t)S, 1u << 14, (const float*)dt.p, A, dloss, dgrad);
+  GGMS_CU(cudaFuncSetAttribute(setup_pl_knots<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(LearnSmem<uint32_t>)));
+  // the same three kernels as training: knots, statistics, forward/backward
+  setup_pl_knots<uint32_t><<<1, SETUP_NT, sizeof(LearnSmem<uint32_t>)>>>((const uint32_t*)dk.p,
+                                                                          (uint32_t)S, 1u << 14, A);
+  pl_stats_grid<uint32_t><<<(PL_M + 31) / 32, 1024>>>((const uint32_t*)dk.p, (uint32_t)S, A, L);
+  pl_grad_probe<uint32_t><<<1, SETUP_NT, sizeof(LearnSmem<uint32_t>)>>>(A, (uint32_t)S, L,
+                                                                         (const float*)dt.p, dloss, dgrad);
   GGMS_CU(cudaDeviceSynchronize());
   Assigner<uint32_t> h;
   GGMS_CU(cudaMemcpy(&h, A, sizeof(h), cudaMemcpyDeviceToHost));

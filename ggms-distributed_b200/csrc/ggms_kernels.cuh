@@ -179,25 +179,39 @@ __global__ __launch_bounds__(NT) void asg_sort_chunks(const K* __restrict__ in, 
 }
 
 // Stable merge of G sorted chunks by ranking: each key counts the keys before
-// it in every other chunk (ties go to the lower chunk).
+// it in every other chunk (ties go to the lower chunk).  Every CTA first keeps
+// every MR_IDX-th key of every chunk in shared memory, so each count is a
+// search over those (shared memory) and then over MR_IDX keys (global).
+constexpr uint32_t MR_IDX = 64;
+
 template <typename K>
-__global__ void asg_merge_rank(const K* __restrict__ chunks, K* sorted, uint32_t S, uint32_t CH) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= S) return;
+__global__ __launch_bounds__(256) void asg_merge_rank(const K* __restrict__ chunks, K* sorted, uint32_t S,
+                                                     uint32_t CH) {
+  __shared__ K idx[65536u / MR_IDX];  // S <= 65536
   const uint32_t G = (S + CH - 1) / CH;
+  const uint32_t per = CH / MR_IDX;  // index entries per chunk (CH is a multiple of MR_IDX)
+  for (uint32_t j = threadIdx.x; j < G * per; j += blockDim.x) {
+    const uint32_t pos = j * MR_IDX;
+    idx[j] = pos < S ? chunks[pos] : key_max<K>();
+  }
+  __syncthreads();
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S) return;
   const uint32_t c = i / CH, p = i % CH;
   const K key = chunks[i];
   uint32_t rank = p;
   for (uint32_t c2 = 0; c2 < G; ++c2) {
     if (c2 == c) continue;
     const K* a = chunks + (size_t)c2 * CH;
-    uint32_t len = min(CH, S - c2 * CH);
-    uint32_t lo = 0, hi = len;
-    if (c2 < c) {  // upper bound
-      while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (a[m] <= key) lo = m + 1; else hi = m; }
-    } else {       // lower bound
-      while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (a[m] < key) lo = m + 1; else hi = m; }
-    }
+    const K* ai = idx + c2 * per;
+    const uint32_t len = min(CH, S - c2 * CH);
+    const bool upper = c2 < c;  // keys <= key (upper bound) or < key (lower bound) come before
+    auto before = [&](K v) { return upper ? v <= key : v < key; };
+    uint32_t lo = 0, hi = (len + MR_IDX - 1u) / MR_IDX;  // first index entry not before key
+    while (lo < hi) { const uint32_t m = (lo + hi) >> 1; if (before(ai[m])) lo = m + 1; else hi = m; }
+    hi = min(lo * MR_IDX, len);
+    lo = lo ? (lo - 1u) * MR_IDX + 1u : 0u;
+    while (lo < hi) { const uint32_t m = (lo + hi) >> 1; if (before(a[m])) lo = m + 1; else hi = m; }
     rank += lo;
   }
   sorted[rank] = key;

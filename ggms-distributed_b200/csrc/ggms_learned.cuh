@@ -44,6 +44,7 @@ struct LearnState {
   uint32_t choice;               // 1 learned accepted, 0 fell back to sampled
   uint32_t focus_points;         // breakpoints of the bucket focus (2: none)
   uint32_t pad[1];
+  PLStats st[PL_M];              // per-segment statistics (pl_stats_grid -> training)
   // MLP parameters (see ggms_mlp.cuh)
   float mlp_params[MLP_NPARAM + 3];
   float mlp_loss;
@@ -55,48 +56,62 @@ __device__ __forceinline__ float softplusf(float x) {
 __device__ __forceinline__ float sigmoidf_(float x) { return 1.0f / (1.0f + expf(-x)); }
 
 // ------------------------------------------------------------------ statistics
-// Per-segment sufficient statistics of the sorted sample.  Thread j handles
-// segment j alone, in sample order (a fixed summation order: deterministic);
-// its samples are contiguous, so the loads stream from L2.  The segment bounds
-// come from one search per knot, first over every 64th sample key kept in
-// shared memory, then over the 64 keys between two of them.
+// Per-segment sufficient statistics of the sorted sample, one warp per
+// segment over many CTAs: the lanes stride the segment's samples (coalesced),
+// each lane sums in sample order and the warp reduces in a fixed shape
+// (deterministic).  A segment's first sample is found by one search per
+// bound, first over every PL_IDX-th sample key kept in shared memory, then
+// over the PL_IDX keys between two of them.  Grid: ceil(PL_M / 32) CTAs of
+// 1024 threads; segments past A->M return.
 constexpr uint32_t PL_IDX = 64;
 
 template <typename K>
-__device__ void pl_stats_block(const K* __restrict__ sorted, uint32_t S, const K* x, uint32_t M,
-                               PLStats* st, uint32_t* seg_start) {
-  // the statistics array is free until the end: its front holds the index
-  K* sidx = reinterpret_cast<K*>(st);
-  const uint32_t nidx = (S + PL_IDX - 1u) / PL_IDX;  // S <= 65536: <= 1024 keys
+__global__ __launch_bounds__(1024) void pl_stats_grid(const K* __restrict__ sorted, uint32_t S,
+                                                     const Assigner<K>* __restrict__ A, LearnState* L) {
+  __shared__ K sidx[65536u / PL_IDX];
+  const uint32_t M = A->M;
+  const uint32_t nidx = (S + PL_IDX - 1u) / PL_IDX;  // S <= 65536
   for (uint32_t j = threadIdx.x; j < nidx; j += blockDim.x) sidx[j] = sorted[j * PL_IDX];
   __syncthreads();
-  // first sample of every segment (the last segment also takes s == x_M)
-  for (uint32_t j = threadIdx.x; j <= M; j += blockDim.x) {
-    uint32_t lo = S;
-    if (j < M) {
-      const K v = x[j];
-      uint32_t a = 0, b = nidx;  // first indexed key >= v
-      while (a < b) { const uint32_t m = (a + b) >> 1; if (sidx[m] < v) a = m + 1; else b = m; }
-      uint32_t hi = min(a * PL_IDX, S);
-      lo = a ? (a - 1u) * PL_IDX + 1u : 0u;
-      while (lo < hi) { const uint32_t m = (lo + hi) >> 1; if (sorted[m] < v) lo = m + 1; else hi = m; }
-    }
-    seg_start[j] = lo;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (j >= M) return;
+  uint32_t bound = S;  // lane 0: first sample of segment j; lane 1: of segment j + 1
+  if (lane < 2u && j + lane < M) {
+    const K v = A->x[j + lane];
+    uint32_t a = 0, b = nidx;  // first indexed key >= v
+    while (a < b) { const uint32_t m = (a + b) >> 1; if (sidx[m] < v) a = m + 1; else b = m; }
+    uint32_t hi = min(a * PL_IDX, S), lo = a ? (a - 1u) * PL_IDX + 1u : 0u;
+    while (lo < hi) { const uint32_t m = (lo + hi) >> 1; if (sorted[m] < v) lo = m + 1; else hi = m; }
+    bound = lo;
   }
+  const uint32_t i0 = __shfl_sync(FULL, bound, 0), i1 = __shfl_sync(FULL, bound, 1);
+  const K xj = A->x[j], xn = A->x[j + 1];
+  const float width = key_to_float_rn((K)(xn - xj));
+  double n = 0, su = 0, su2 = 0, sy = 0, syu = 0, sy2 = 0;
+  for (uint32_t i = i0 + lane; i < i1; i += 32) {
+    const float u = fminf(__fdiv_rn(key_to_float_rn((K)(sorted[i] - xj)), width), 1.0f);
+    const double y = ((double)i + 0.5) / (double)S;
+    n += 1.0; su += u; su2 += (double)u * u; sy += y; syu += y * u; sy2 += y * y;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    n += __shfl_xor_sync(FULL, n, o);
+    su += __shfl_xor_sync(FULL, su, o);
+    su2 += __shfl_xor_sync(FULL, su2, o);
+    sy += __shfl_xor_sync(FULL, sy, o);
+    syu += __shfl_xor_sync(FULL, syu, o);
+    sy2 += __shfl_xor_sync(FULL, sy2, o);
+  }
+  if (lane == 0) L->st[j] = PLStats{n, su, su2, sy, syu, sy2};
+}
+
+// The statistics into shared memory for training (all threads call it).
+__device__ __forceinline__ void pl_stats_load(const LearnState* L, uint32_t M, PLStats* st) {
+  const double* src = reinterpret_cast<const double*>(L->st);
+  double* dst = reinterpret_cast<double*>(st);
+  for (uint32_t i = threadIdx.x; i < 6u * M; i += blockDim.x) dst[i] = src[i];
   __syncthreads();
-  for (uint32_t j = threadIdx.x; j < M; j += blockDim.x) {
-    const K xj = x[j], xn = x[j + 1];
-    const uint32_t i0 = seg_start[j], i1 = seg_start[j + 1];
-    const float width = key_to_float_rn((K)(xn - xj));
-    double n = 0, su = 0, su2 = 0, sy = 0, syu = 0, sy2 = 0;
-#pragma unroll 4
-    for (uint32_t i = i0; i < i1; ++i) {
-      const float u = fminf(__fdiv_rn(key_to_float_rn((K)(sorted[i] - xj)), width), 1.0f);
-      const double y = ((double)i + 0.5) / (double)S;
-      n += 1.0; su += u; su2 += (double)u * u; sy += y; syu += y * u; sy2 += y * y;
-    }
-    st[j] = PLStats{n, su, su2, sy, syu, sy2};
-  }
 }
 
 // ------------------------------------------------------------------ forward / backward
@@ -287,8 +302,19 @@ __device__ void learned_finish(const K* sorted, uint32_t S, uint32_t B, uint32_t
 // The whole learned-PL setup in one CTA: knots -> statistics -> training ->
 // bases -> grid -> occupancy -> choice (grid 1 if within the bound, else the
 // sampled grid 0 stays in use).
-// With window_z >= 0 the bases are focused on the ks' windows (build_warp):
-// krank[0..nk) are the ks' ascending ranks among n keys.
+// Knots of the learned PL model (one CTA): quantile knots, deduplicated.
+template <typename K>
+__global__ __launch_bounds__(SETUP_NT) void setup_pl_knots(const K* __restrict__ sorted, uint32_t S,
+                                                          uint32_t B, Assigner<K>* A) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
+  pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, A, sm);
+}
+
+// Training and compilation of the learned PL model (one CTA), after
+// setup_pl_knots and pl_stats_grid.  With window_z >= 0 the bases are focused
+// on the ks' windows (build_warp): krank[0..nk) are the ks' ascending ranks
+// among n keys.
 template <typename K>
 __global__ __launch_bounds__(SETUP_NT) void setup_learned_pl(const K* __restrict__ sorted, uint32_t S,
                                                             uint32_t B, uint32_t steps, float lr,
@@ -301,10 +327,8 @@ __global__ __launch_bounds__(SETUP_NT) void setup_learned_pl(const K* __restrict
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
   __shared__ Warp wsh;
   __shared__ uint32_t wred[33];
-  pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, A, sm);
-  const uint32_t M = A->M;
-  pl_stats_block<K>(sorted, S, A->x, M, sm.st, sm.seg_start);
-  __syncthreads();
+  const uint32_t M = A->M;  // knots: setup_pl_knots; statistics: pl_stats_grid
+  pl_stats_load(L, M, sm.st);
   if (threadIdx.x < PL_NT) {
     const float loss = pl_train_block(sm.st, M, S, steps, lr, sm.red, sm.cdf, &L->loss_init,
                                       L->theta, L->grad);
@@ -329,19 +353,17 @@ __global__ __launch_bounds__(SETUP_NT) void setup_learned_pl(const K* __restrict
   learned_finish<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, bound, A, G, G0, L, choice, sm, &wsh);
 }
 
-// Gradient probe (diagnostics): knots and statistics as above, then one
-// forward/backward at the given theta.
+// Gradient probe (diagnostics): after setup_pl_knots and pl_stats_grid, one
+// forward/backward at the given theta -- the kernels training uses.
 template <typename K>
-__global__ __launch_bounds__(SETUP_NT) void pl_grad_probe(const K* __restrict__ sorted, uint32_t S,
-                                                         uint32_t B, const float* __restrict__ theta_in,
-                                                         Assigner<K>* A, float* loss_out,
-                                                         float* grad_out) {
+__global__ __launch_bounds__(SETUP_NT) void pl_grad_probe(const Assigner<K>* __restrict__ A, uint32_t S,
+                                                         const LearnState* L,
+                                                         const float* __restrict__ theta_in,
+                                                         float* loss_out, float* grad_out) {
   extern __shared__ __align__(16) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
-  pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, A, sm);
   const uint32_t M = A->M;
-  pl_stats_block<K>(sorted, S, A->x, M, sm.st, sm.seg_start);
-  __syncthreads();
+  pl_stats_load(L, M, sm.st);
   if (threadIdx.x < PL_NT) {
     float g = 0.0f;
     const float th = threadIdx.x < M ? theta_in[threadIdx.x] : 0.0f;
@@ -365,6 +387,8 @@ static int learn_and_choose(int kind, const K* sorted, uint32_t S, uint32_t B, i
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(setup_learned_pl<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(LearnSmem<K>)) != cudaSuccess ||
+        cudaFuncSetAttribute(setup_pl_knots<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(LearnSmem<K>)) != cudaSuccess)
       return GGMS_E_CUDA;
     attr = true;
@@ -374,10 +398,12 @@ static int learn_and_choose(int kind, const K* sorted, uint32_t S, uint32_t B, i
     if (rc) return rc;
   } else {
     const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 4u;
+    setup_pl_knots<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, &As[1]);
+    pl_stats_grid<K><<<(PL_M + 31) / 32, 1024, 0, st>>>(sorted, S, &As[1], L);
     setup_learned_pl<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, steps, 0.02f, bound,
                                                                     &As[1], &Gs[1], &Gs[0], L, choice,
                                                                     krank, nk, n, window_z);
-    *launches += 1;
+    *launches += 3;
   }
   return cudaGetLastError() == cudaSuccess ? GGMS_OK : GGMS_E_CUDA;
 }

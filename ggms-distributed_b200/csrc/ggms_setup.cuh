@@ -437,6 +437,36 @@ __device__ __forceinline__ void bits_mark(uint32_t* bm, uint32_t b0, uint32_t b1
   atomicOr(&bm[w1], hi);
 }
 
+// Coverage of intervals given as a difference array cnt[0..nb] (+1 at each
+// interval's first bin, -1 one past its last; nb a multiple of blockDim.x):
+// bm gets one bit per bin, set where the coverage is > 0.  Warp w scans bins
+// [w * nb / nwarps, (w + 1) * nb / nwarps) row by row (32 bins per row, one per
+// lane: no bank conflicts).  All threads call it.
+__device__ void coverage_bitmap(const int32_t* cnt, uint32_t nb, uint32_t* bm, uint32_t* red) {
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const uint32_t per = nb / nw, base = warp * per;
+  int32_t part = 0;
+  for (uint32_t r = 0; r < per; r += 32) part += cnt[base + r + lane];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(FULL, part, o);
+  uint32_t tot = 0;
+  // block-exclusive prefix of the warp sums (lane 0 of warp w contributes part_w)
+  int32_t run = (int32_t)block_excl_scan<uint32_t>(lane == 0 ? (uint32_t)part : 0u, red, &tot);
+  run = __shfl_sync(FULL, run, 0);
+  for (uint32_t r = 0; r < per; r += 32) {
+    int32_t v = cnt[base + r + lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t t = __shfl_up_sync(FULL, v, o);
+      if ((int)lane >= o) v += t;
+    }
+    const uint32_t bits = __ballot_sync(FULL, run + v > 0);
+    if (lane == 0) bm[(base + r) >> 5] = bits;
+    run += __shfl_sync(FULL, v, 31);
+  }
+  __syncthreads();
+}
+
 // Maximal runs of set bits of a bitmap of `words` words (<= blockDim.x), in
 // order: run j is [rs[j], re[j]] for j < min(total, cap).  Returns the number
 // of runs.  All threads call it.

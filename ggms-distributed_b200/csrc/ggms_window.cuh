@@ -25,12 +25,12 @@ constexpr uint32_t WIN_IDX = 64;  // every WIN_IDX-th sample key is kept in shar
 
 template <typename K>
 __host__ __device__ constexpr size_t l0_window_smem(uint32_t B) {
-  return GRID_SMEM + sizeof(K) * (65536u / WIN_IDX) + 4u * ((size_t)B / 32u);
+  return GRID_SMEM + sizeof(K) * (65536u / WIN_IDX) + 4u * ((size_t)B / 32u) + 4u * ((size_t)B + 1u);
 }
 
 // One CTA.  Dynamic shared memory: l0_window_smem<K>(B) -- the grid (every
-// search below evaluates it many times), a coarse index of the sample, and a
-// bitmap of the B buckets.
+// search below evaluates it many times), a coarse index of the sample, a
+// bitmap of the B buckets and a difference array over them.
 template <typename K>
 __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted, uint32_t S,
                                                    const uint32_t* __restrict__ krank, uint32_t nk,
@@ -47,11 +47,12 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
   const uint32_t tid = threadIdx.x;
   const GridView<K> gv = grid_to_smem<K>(Gs + C->asg_choice, s1, s2);
   const uint32_t B = gv.B;
+  int32_t* cnt = reinterpret_cast<int32_t*>(bm + B / 32u);  // difference array [B + 1]
   const uint32_t nidx = (S + WIN_IDX - 1u) / WIN_IDX;  // S <= 65536
   for (uint32_t j = tid; j < nidx; j += WIN_NT) sidx[j] = sorted[j * WIN_IDX];
-  for (uint32_t w = tid; w < B / 32u; w += WIN_NT) bm[w] = 0u;
+  for (uint32_t b = tid; b <= B; b += WIN_NT) cnt[b] = 0;
   __syncthreads();
-  // 1. bucket range of every k, marked in the bitmap
+  // 1. bucket range of every k, as +1 / -1 in the difference array
   for (uint32_t i = tid; i < nk; i += WIN_NT) {
     const double q = ((double)krank[i] + 0.5) / (double)n;
     const double pos = q * (double)S;
@@ -61,10 +62,12 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
     const K khi = c > (double)(S - 1u) ? key_max<K>() : sorted[(uint32_t)c];
     const uint32_t b0 = min(grid_eval<K>(gv, klo), B - 1u);
     const uint32_t b1 = min(grid_eval<K>(gv, khi), B - 1u);
-    bits_mark(bm, b0, b1);
+    atomicAdd(&cnt[b0], 1);
+    atomicAdd(&cnt[b1 + 1u], -1);
   }
   __syncthreads();
-  // 2. raw runs of marked buckets, in bucket order (B / 32 <= 1024 words)
+  // 2. buckets some k may hold, then their runs in bucket order (B / 32 <= 1024 words)
+  coverage_bitmap(cnt, B, bm, red);
   const uint32_t nraw = bitmap_runs(bm, B / 32u, rs, re, WIN_MAXRAW, red);
   const uint32_t nraw2 = nraw;
   // 3. sample positions of the raw runs: [ss, se) = the sample keys whose
