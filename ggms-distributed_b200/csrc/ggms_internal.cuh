@@ -287,6 +287,7 @@ struct Windows {
   uint32_t on;                                 // 1: PASS 1 buckets only the runs
   uint32_t R;                                  // runs, 1..L0_WIN
   uint32_t cnt;                                // 1: two or more gaps hold keys (PASS 1 counts per run)
+  uint32_t tight;                              // 1: the runs hold at most 1/64 of the sample
   uint32_t rb0[L0_WIN], rb1[L0_WIN];           // bucket range of run r (ascending, disjoint)
   uint32_t gb0[L0_WIN + 1], gb1[L0_WIN + 1];   // bucket range of gap g (gb0 > gb1: empty)
   K lo[L0_WIN], hi[L0_WIN];                    // key range of run r (exactly its buckets' keys)

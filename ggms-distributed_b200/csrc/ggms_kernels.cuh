@@ -879,24 +879,38 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
   K* wq = reinterpret_cast<K*>(wpre) + (threadIdx.x >> 5) * WQ_DEPTH;
   uint32_t qn = 0;  // warp-uniform
 
-  // every lane runs the same number of rounds, so the warp stays converged
+  // every lane runs the same number of rounds, so the warp stays converged.
+  // With windows and no gap bucket to copy, every copied bucket lies inside a
+  // window run: when the runs are narrow (tight), their key ranges (few, known
+  // exactly) are the test.
+  bool use_win = W.on != 0u && W.tight != 0u;
+  for (uint32_t g = 0; g <= L0_WIN && use_win; ++g)
+    if (g <= W.R && W.gb0[g] <= W.gb1[g] && ((amask[W.gb0[g] >> 5] >> (W.gb0[g] & 31)) & 1u))
+      use_win = false;
   const uint32_t nruns = nruns_s;
-  auto runs = [&](auto rc) {
+  auto runs = [&](auto rc, bool win) {
     constexpr uint32_t R = decltype(rc)::value;
     RunTest<K, R, false> t;
 #pragma unroll
     for (uint32_t r = 0; r < R; ++r) {
-      t.lo[r] = run_lo[r];
-      t.sp[r] = run_span[r];
+      t.lo[r] = win ? W.lo[r] : run_lo[r];
+      t.sp[r] = win ? (K)(W.hi[r] - W.lo[r]) : run_span[r];
     }
     stream_keys<T, UNROLL>(vp, rounds, gstride, wq, qn, lane, t, bucket_and_put);
   };
-  switch (nruns) {
+  if (use_win) {
+    switch (W.R) {
+      case 1: runs(std::integral_constant<uint32_t, 1>{}, true); break;
+      case 2: runs(std::integral_constant<uint32_t, 2>{}, true); break;
+      case 3: runs(std::integral_constant<uint32_t, 3>{}, true); break;
+      default: runs(std::integral_constant<uint32_t, 4>{}, true); break;
+    }
+  } else switch (nruns) {
     case 0: break;  // nothing to copy
-    case 1: runs(std::integral_constant<uint32_t, 1>{}); break;
-    case 2: runs(std::integral_constant<uint32_t, 2>{}); break;
-    case 3: runs(std::integral_constant<uint32_t, 3>{}); break;
-    case 4: runs(std::integral_constant<uint32_t, 4>{}); break;
+    case 1: runs(std::integral_constant<uint32_t, 1>{}, false); break;
+    case 2: runs(std::integral_constant<uint32_t, 2>{}, false); break;
+    case 3: runs(std::integral_constant<uint32_t, 3>{}, false); break;
+    case 4: runs(std::integral_constant<uint32_t, 4>{}, false); break;
     default: stream_keys<T, UNROLL>(vp, rounds, gstride, wq, qn, lane, in_hot, bucket_and_put); break;
   }
   __syncwarp();

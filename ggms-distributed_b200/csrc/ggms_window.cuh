@@ -97,6 +97,7 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
     sw.on = 0;
     sw.R = 0;
     sw.cnt = 0;
+    sw.tight = 0;
     uint32_t R = 0, hot = 0;
     if (nraw >= 1 && nraw <= WIN_MAXRAW && nraw2 == nraw) {
       uint32_t cs = rs[0], ce = re[0], cse = se[0], css = ss[0];
@@ -132,6 +133,7 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
           ne += holds ? 1u : 0u;
         }
         sw.cnt = ne >= 2u ? 1u : 0u;
+        sw.tight = hot * 64u <= S ? 1u : 0u;
       }
     }
   }
