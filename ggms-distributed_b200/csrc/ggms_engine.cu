@@ -11,6 +11,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <vector>
 
 #include "ggms_kernels.cuh"
 #include "ggms_learned.cuh"
@@ -34,6 +35,18 @@ struct Context {
   bool profile = false;
   cudaEvent_t ev[RING][6] = {};
   int ring_head = 0, ring_count = 0;
+  // captured CUDA graphs of repeated calls (same arguments, same workspace)
+  struct Graph {
+    uint64_t key[16];
+    cudaGraphExec_t exec = nullptr;  // null: seen once, not captured yet
+    long long launches = 0;
+    uint64_t used = 0;
+  };
+  static constexpr size_t GRAPHS = 8;
+  std::vector<Graph> graphs;
+  uint64_t clock = 0;
+  cudaStream_t capture = nullptr;  // private stream the graphs are captured on
+  cudaEvent_t pin_busy = nullptr;  // recorded after the last call's uploads from the pinned buffer
 };
 
 static int cuda_status(cudaError_t e) {
@@ -101,6 +114,10 @@ static void destroy_context(Context* c) {
   for (int i = 0; i < Context::RING; ++i)
     for (int j = 0; j < 6; ++j)
       if (c->ev[i][j]) cudaEventDestroy(c->ev[i][j]);
+  for (auto& g : c->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (c->capture) cudaStreamDestroy(c->capture);
+  if (c->pin_busy) cudaEventDestroy(c->pin_busy);
   cudaSetDevice(prev);
   delete c;
 }
@@ -284,6 +301,74 @@ static int make_plan(Plan* p, uint64_t n, uint32_t nk, const ggms_opts& o) {
   return GGMS_OK;
 }
 
+static inline uint32_t float_bits(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  return u;
+}
+
+// ------------------------------------------------------------------ CUDA graphs
+// A call whose kernel sequence and arguments repeat (same pointers, sizes,
+// options and workspace) is captured into a CUDA graph the second time it is
+// seen and replayed from then on: one graph launch instead of ~30 kernel
+// launches.  `enqueue(stream)` must issue only stream-ordered work (no host
+// sync, no allocation).  The first call of a key runs directly, which also
+// sets the kernels' attributes before any capture.  A failed capture falls
+// back to running directly.
+template <typename F>
+static int run_graphed(Context* c, const uint64_t* key, int nkey, cudaStream_t st, F&& enqueue) {
+  auto same = [&](const Context::Graph& g) {
+    for (int i = 0; i < 16; ++i)
+      if (g.key[i] != (i < nkey ? key[i] : 0ull)) return false;
+    return true;
+  };
+  Context::Graph* hit = nullptr;
+  for (auto& g : c->graphs)
+    if (same(g)) hit = &g;
+  if (hit && hit->exec) {
+    hit->used = ++c->clock;
+    GGMS_CU(cudaGraphLaunch(hit->exec, st));
+    c->launches += hit->launches;
+    return GGMS_OK;
+  }
+  if (!hit) {  // first sighting: remember the key (evicting the least recently used), run directly
+    if (c->graphs.size() >= Context::GRAPHS) {
+      auto lru = std::min_element(c->graphs.begin(), c->graphs.end(),
+                                  [](const Context::Graph& a, const Context::Graph& b) { return a.used < b.used; });
+      if (lru->exec) cudaGraphExecDestroy(lru->exec);
+      c->graphs.erase(lru);
+    }
+    Context::Graph g;
+    for (int i = 0; i < 16; ++i) g.key[i] = i < nkey ? key[i] : 0ull;
+    g.used = ++c->clock;
+    c->graphs.push_back(g);
+    return enqueue(st);
+  }
+  // second sighting: capture, then launch
+  if (!c->capture) GGMS_CU(cudaStreamCreateWithFlags(&c->capture, cudaStreamNonBlocking));
+  const long long before = c->launches;
+  if (cudaStreamBeginCapture(c->capture, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return enqueue(st);
+  const int rc = enqueue(c->capture);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c->capture, &graph);
+  cudaGraphExec_t exec = nullptr;
+  const bool ok = rc == GGMS_OK && e == cudaSuccess && graph &&
+                  cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+  if (graph) cudaGraphDestroy(graph);
+  const long long captured = c->launches - before;  // kernels the graph holds
+  c->launches = before;
+  if (!ok) {
+    cudaGetLastError();
+    return enqueue(st);
+  }
+  hit->exec = exec;
+  hit->launches = captured;
+  hit->used = ++c->clock;
+  GGMS_CU(cudaGraphLaunch(exec, st));
+  c->launches += captured;
+  return GGMS_OK;
+}
+
 // ------------------------------------------------------------------ kernel configs
 constexpr int LV_NT = 256;
 constexpr int MAX_LEVELS_32 = 3;
@@ -432,136 +517,165 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   uint8_t* pin_out = pin_k + (host_k ? ((4ull * nk + 63) & ~(size_t)63) : 0);
 
   const Caps caps{p.cap_seg, p.cap_tiles, p.nk, (uint32_t)(SMALL_SMEM / sizeof(K))};
-  cudaEvent_t* prof = prof_slot(ctx);
-  prof_rec(prof, 0, st);
-  GGMS_CU(cudaMemsetAsync(w.C, 0, sizeof(Counters), st));
-  const uint32_t* d_k = ks;
   if (host_k && !topk) {
+    // host side, every call: the previous call's upload from the same pinned
+    // buffer may still be queued (calls with device-resident answers return
+    // without a sync), so wait for it first
+    if (ctx->pin_busy) GGMS_CU(cudaEventSynchronize(ctx->pin_busy));
     memcpy(pin_k, ks, 4ull * nk);
-    GGMS_CU(cudaMemcpyAsync(w.kin, pin_k, 4ull * nk, cudaMemcpyHostToDevice, st));
-    d_k = w.kin;
   }
-  ++ctx->launches;
-  if (topk)
-    k_init_topk<<<cdiv(nk, 256), 256, 0, st>>>(nk, n, w.krank, w.kseg);
-  else
-    k_init_single<<<cdiv(nk, 256), 256, 0, st>>>(d_k, nk, n, w.krank, w.kseg, w.C);
+  cudaEvent_t* prof = prof_slot(ctx);
+  // the stream-ordered part: captured once and replayed when the call repeats
+  auto enqueue = [&](cudaStream_t s) -> int {
+    prof_rec(prof, 0, s);
+    GGMS_CU(cudaMemsetAsync(w.C, 0, sizeof(Counters), s));
+    const uint32_t* d_k = ks;
+    if (host_k && !topk) {
+      GGMS_CU(cudaMemcpyAsync(w.kin, pin_k, 4ull * nk, cudaMemcpyHostToDevice, s));
+      d_k = w.kin;
+    }
+    ++ctx->launches;
+    if (topk)
+      k_init_topk<<<cdiv(nk, 256), 256, 0, s>>>(nk, n, w.krank, w.kseg);
+    else
+      k_init_single<<<cdiv(nk, 256), 256, 0, s>>>(d_k, nk, n, w.krank, w.kseg, w.C);
 
-  // ---- level-0 assigner
-  const uint32_t S = p.S;
-  ++ctx->launches;
-  asg_sample<T><<<cdiv(S, 256), 256, 0, st>>>(d_in, n, S, p.seed, w.samp_raw);
-  if (S <= 1024) {
+    // ---- level-0 assigner
+    const uint32_t S = p.S;
     ++ctx->launches;
-    asg_sort_chunks<K, 1024, 1024><<<1, 1024, 0, st>>>(w.samp_raw, w.samp_sorted, S);
-  } else if (S <= 2048) {
-    ++ctx->launches;
-    asg_sort_chunks<K, 2048, 1024><<<1, 1024, 0, st>>>(w.samp_raw, w.samp_sorted, S);
-  } else if (S <= 4096) {
-    ++ctx->launches;
-    asg_sort_chunks<K, 4096, 1024><<<1, 1024, 0, st>>>(w.samp_raw, w.samp_sorted, S);
-  } else {
-    ++ctx->launches;
-    asg_sort_chunks<K, 4096, 1024><<<S / 4096, 1024, 0, st>>>(w.samp_raw, w.samp_tmp, S);
-    ++ctx->launches;
-    asg_merge_rank<K><<<cdiv(S, 256), 256, 0, st>>>(w.samp_tmp, w.samp_sorted, S, 4096u);
-  }
-  rc = setup_attrs<K>();
-  if (rc) return rc;
-  ++ctx->launches;
-  setup_sampled<K><<<1, SETUP_NT, sizeof(SetupSmem<K>), st>>>(w.samp_sorted, S, p.B, &w.asg[0],
-                                                               &w.grid[0]);
-  if (p.assigner != GGMS_ASSIGNER_SAMPLED) {
-    rc = learn_and_choose<K>(p.assigner, w.samp_sorted, S, p.B, p.train_steps, p.bound, w.asg,
-                             w.grid, w.learn, &w.C->asg_choice, w.krank, nk, n, p.window_z, st,
-                             &ctx->launches);
-    if (rc) return rc;
-  }
-
-  // ---- PASS 1 windows
-  if (p.window_z >= 0.0f) {
-    ++ctx->launches;
-    l0_window<K><<<1, WIN_NT, l0_window_smem<K>(p.B), st>>>(w.samp_sorted, S, w.krank, nk, n, w.grid,
-                                                             w.C, p.window_z, w.win);
-  } else {
-    GGMS_CU(cudaMemsetAsync(w.win, 0, sizeof(Windows<K>), st));
-  }
-
-  // ---- PASS 1: count
-  const int grid_c = (int)p.ncta;
-  GGMS_CU(cudaMemsetAsync(w.hist0, 0, 4ull * p.B, st));
-  GGMS_CU(cudaMemsetAsync(w.aflag0, 0, 4ull * (p.B / 32), st));
-  prof_rec(prof, 1, st);
-  ++ctx->launches;
-  pv->count<<<grid_c, pv->nt, l0_count_smem<T>(p.B, pv->nt), st>>>(d_in, n, w.grid, w.C, w.win, w.hist0,
-                                                                    w.crow);
-  prof_rec(prof, 2, st);
-  ++ctx->launches;
-  l0_scan<K><<<1, 1024, 4u * p.B, st>>>(w.hist0, p.B, w.C, w.win);
-  ++ctx->launches;
-  lvl_locate_rows<<<cdiv(nk, 256), 256, 0, st>>>(w.hist0, p.B, nk, w.krank, w.kseg, w.kbin,
-                                                   w.aflag0, p.B / 32, w.C);
-  ++ctx->launches;
-  l0_children<K><<<cdiv(p.B, 256), 256, 0, st>>>(w.hist0, w.aflag0, p.B, w.grid, w.C, w.win, w.cmap0,
-                                                   w.segs[1], w.cursor[1], w.tiles[1], w.points,
-                                                   w.khead[1], w.smalls, caps);
-  ++ctx->launches;
-  lvl_relabel<K><<<cdiv(nk, 256), 256, 0, st>>>(w.cmap0, p.B, nk, w.kbin, w.kseg, w.kkey,
-                                                  w.points, w.C, w.segs[1], w.khead[1], w.knext);
-  ++ctx->launches;
-  l0_bases<K><<<ctx->sms * 4, 256, 0, st>>>(w.crow, p.B, p.ncta, w.segs[1], w.C, caps);
-  // ---- PASS 2: compact the buckets that still need refinement
-  prof_rec(prof, 3, st);
-  ++ctx->launches;
-  pv->compact<<<grid_c, pv->nt, l0_compact_smem<T>(p.B, pv->nt), st>>>(d_in, n, w.grid, w.C, w.win, w.cmap0,
-                                                                      w.crow, w.cand[0], (uint64_t)n);
-  prof_rec(prof, 4, st);
-  rc = launch_small_select<K>(ctx, w.cand[0], w.segs[1], w.khead[1], w, caps, st);
-  if (rc) return rc;
-
-  // ---- refinement levels over candidates
-  const int maxlev = (sizeof(K) == 4) ? MAX_LEVELS_32 : MAX_LEVELS_64;
-  const int lv_grid = ctx->sms * 8;
-  const int seg_grid = std::min<int>((int)p.cap_seg, ctx->sms * 2);
-  for (int l = 1; l <= maxlev; ++l) {
-    const int pp = l & 1, q = pp ^ 1;
-    const K* src = w.cand[(l - 1) & 1];
-    K* dst = w.cand[l & 1];
-    ++ctx->launches;
-    lvl_prep<<<ctx->sms * 2, 256, 0, st>>>(w.rows[pp], w.aflag[pp], w.C, pp, caps);
-    ++ctx->launches;
-    lvl_count<K, LV_NT><<<lv_grid, LV_NT, 0, st>>>(src, w.segs[pp], w.tiles[pp], w.C, pp, w.rows[pp], caps);
-    ++ctx->launches;
-    lvl_scan<<<seg_grid, 1024, 0, st>>>(w.rows[pp], w.C, pp, caps);
-    ++ctx->launches;
-    lvl_locate_rows<<<cdiv(nk, 256), 256, 0, st>>>(w.rows[pp], NBIN, nk, w.krank, w.kseg, w.kbin,
-                                                     w.aflag[pp], NBIN_WORDS, w.C);
-    ++ctx->launches;
-    lvl_children<K, 1024><<<seg_grid, 1024, 0, st>>>(w.rows[pp], w.aflag[pp], w.segs[pp], w.C, pp,
-                                                     w.segs[q], w.cursor[q], w.tiles[q], w.points,
-                                                     w.khead[q], w.smalls, caps);
-    ++ctx->launches;
-    lvl_relabel<K><<<cdiv(nk, 256), 256, 0, st>>>(w.rows[pp], NBIN, nk, w.kbin, w.kseg, w.kkey,
-                                                    w.points, w.C, w.segs[q], w.khead[q], w.knext);
-    if (l < maxlev) {
+    asg_sample<T><<<cdiv(S, 256), 256, 0, s>>>(d_in, n, S, p.seed, w.samp_raw);
+    if (S <= 1024) {
       ++ctx->launches;
-      lvl_compact<K, LV_NT><<<lv_grid, LV_NT, 0, st>>>(src, w.segs[pp], w.tiles[pp], w.C, pp,
-                                                       w.rows[pp], w.segs[q], w.cursor[q], dst, caps);
-      rc = launch_small_select<K>(ctx, dst, w.segs[q], w.khead[q], w, caps, st);
+      asg_sort_chunks<K, 1024, 1024><<<1, 1024, 0, s>>>(w.samp_raw, w.samp_sorted, S);
+    } else if (S <= 2048) {
+      ++ctx->launches;
+      asg_sort_chunks<K, 2048, 1024><<<1, 1024, 0, s>>>(w.samp_raw, w.samp_sorted, S);
+    } else if (S <= 4096) {
+      ++ctx->launches;
+      asg_sort_chunks<K, 4096, 1024><<<1, 1024, 0, s>>>(w.samp_raw, w.samp_sorted, S);
+    } else {
+      ++ctx->launches;
+      asg_sort_chunks<K, 4096, 1024><<<S / 4096, 1024, 0, s>>>(w.samp_raw, w.samp_tmp, S);
+      ++ctx->launches;
+      asg_merge_rank<K><<<cdiv(S, 256), 256, 0, s>>>(w.samp_tmp, w.samp_sorted, S, 4096u);
+    }
+    rc = setup_attrs<K>();
+    if (rc) return rc;
+    ++ctx->launches;
+    setup_sampled<K><<<1, SETUP_NT, sizeof(SetupSmem<K>), s>>>(w.samp_sorted, S, p.B, &w.asg[0],
+                                                                 &w.grid[0]);
+    if (p.assigner != GGMS_ASSIGNER_SAMPLED) {
+      rc = learn_and_choose<K>(p.assigner, w.samp_sorted, S, p.B, p.train_steps, p.bound, w.asg,
+                               w.grid, w.learn, &w.C->asg_choice, w.krank, nk, n, p.window_z, s,
+                               &ctx->launches);
       if (rc) return rc;
     }
-  }
 
-  // ---- answers
-  T* d_out = host_out ? (T*)w.out_dev : out;
-  ++ctx->launches;
-  write_out<T><<<cdiv(nk, 256), 256, 0, st>>>(w.kkey, w.kseg, nk, d_out, w.C);
-  GGMS_CU(cudaGetLastError());
-  if (host_out) GGMS_CU(cudaMemcpyAsync(pin_out, d_out, sizeof(T) * nk, cudaMemcpyDeviceToHost, st));
-  prof_rec(prof, 5, st);
+    // ---- PASS 1 windows
+    if (p.window_z >= 0.0f) {
+      ++ctx->launches;
+      l0_window<K><<<1, WIN_NT, l0_window_smem<K>(p.B), s>>>(w.samp_sorted, S, w.krank, nk, n, w.grid,
+                                                               w.C, p.window_z, w.win);
+    } else {
+      GGMS_CU(cudaMemsetAsync(w.win, 0, sizeof(Windows<K>), s));
+    }
+
+    // ---- PASS 1: count
+    const int grid_c = (int)p.ncta;
+    GGMS_CU(cudaMemsetAsync(w.hist0, 0, 4ull * p.B, s));
+    GGMS_CU(cudaMemsetAsync(w.aflag0, 0, 4ull * (p.B / 32), s));
+    prof_rec(prof, 1, s);
+    ++ctx->launches;
+    pv->count<<<grid_c, pv->nt, l0_count_smem<T>(p.B, pv->nt), s>>>(d_in, n, w.grid, w.C, w.win, w.hist0,
+                                                                      w.crow);
+    prof_rec(prof, 2, s);
+    ++ctx->launches;
+    l0_scan<K><<<1, 1024, 4u * p.B, s>>>(w.hist0, p.B, w.C, w.win);
+    ++ctx->launches;
+    lvl_locate_rows<<<cdiv(nk, 256), 256, 0, s>>>(w.hist0, p.B, nk, w.krank, w.kseg, w.kbin,
+                                                     w.aflag0, p.B / 32, w.C);
+    ++ctx->launches;
+    l0_children<K><<<cdiv(p.B, 256), 256, 0, s>>>(w.hist0, w.aflag0, p.B, w.grid, w.C, w.win, w.cmap0,
+                                                     w.segs[1], w.cursor[1], w.tiles[1], w.points,
+                                                     w.khead[1], w.smalls, caps);
+    ++ctx->launches;
+    lvl_relabel<K><<<cdiv(nk, 256), 256, 0, s>>>(w.cmap0, p.B, nk, w.kbin, w.kseg, w.kkey,
+                                                    w.points, w.C, w.segs[1], w.khead[1], w.knext);
+    ++ctx->launches;
+    l0_bases<K><<<ctx->sms * 4, 256, 0, s>>>(w.crow, p.B, p.ncta, w.segs[1], w.C, caps);
+    // ---- PASS 2: compact the buckets that still need refinement
+    prof_rec(prof, 3, s);
+    ++ctx->launches;
+    pv->compact<<<grid_c, pv->nt, l0_compact_smem<T>(p.B, pv->nt), s>>>(d_in, n, w.grid, w.C, w.win, w.cmap0,
+                                                                        w.crow, w.cand[0], (uint64_t)n);
+    prof_rec(prof, 4, s);
+    rc = launch_small_select<K>(ctx, w.cand[0], w.segs[1], w.khead[1], w, caps, s);
+    if (rc) return rc;
+
+    // ---- refinement levels over candidates
+    const int maxlev = (sizeof(K) == 4) ? MAX_LEVELS_32 : MAX_LEVELS_64;
+    const int lv_grid = ctx->sms * 8;
+    const int seg_grid = std::min<int>((int)p.cap_seg, ctx->sms * 2);
+    for (int l = 1; l <= maxlev; ++l) {
+      const int pp = l & 1, q = pp ^ 1;
+      const K* src = w.cand[(l - 1) & 1];
+      K* dst = w.cand[l & 1];
+      ++ctx->launches;
+      lvl_prep<<<ctx->sms * 2, 256, 0, s>>>(w.rows[pp], w.aflag[pp], w.C, pp, caps);
+      ++ctx->launches;
+      lvl_count<K, LV_NT><<<lv_grid, LV_NT, 0, s>>>(src, w.segs[pp], w.tiles[pp], w.C, pp, w.rows[pp], caps);
+      ++ctx->launches;
+      lvl_scan<<<seg_grid, 1024, 0, s>>>(w.rows[pp], w.C, pp, caps);
+      ++ctx->launches;
+      lvl_locate_rows<<<cdiv(nk, 256), 256, 0, s>>>(w.rows[pp], NBIN, nk, w.krank, w.kseg, w.kbin,
+                                                       w.aflag[pp], NBIN_WORDS, w.C);
+      ++ctx->launches;
+      lvl_children<K, 1024><<<seg_grid, 1024, 0, s>>>(w.rows[pp], w.aflag[pp], w.segs[pp], w.C, pp,
+                                                       w.segs[q], w.cursor[q], w.tiles[q], w.points,
+                                                       w.khead[q], w.smalls, caps);
+      ++ctx->launches;
+      lvl_relabel<K><<<cdiv(nk, 256), 256, 0, s>>>(w.rows[pp], NBIN, nk, w.kbin, w.kseg, w.kkey,
+                                                      w.points, w.C, w.segs[q], w.khead[q], w.knext);
+      if (l < maxlev) {
+        ++ctx->launches;
+        lvl_compact<K, LV_NT><<<lv_grid, LV_NT, 0, s>>>(src, w.segs[pp], w.tiles[pp], w.C, pp,
+                                                         w.rows[pp], w.segs[q], w.cursor[q], dst, caps);
+        rc = launch_small_select<K>(ctx, dst, w.segs[q], w.khead[q], w, caps, s);
+        if (rc) return rc;
+      }
+    }
+
+    // ---- answers
+    T* d_out = host_out ? (T*)w.out_dev : out;
+    ++ctx->launches;
+    write_out<T><<<cdiv(nk, 256), 256, 0, s>>>(w.kkey, w.kseg, nk, d_out, w.C);
+    if (cudaGetLastError() != cudaSuccess) return GGMS_E_CUDA;
+    if (host_out) GGMS_CU(cudaMemcpyAsync(pin_out, d_out, sizeof(T) * nk, cudaMemcpyDeviceToHost, s));
+    if (host_out || o.stats) GGMS_CU(cudaMemcpyAsync(pin_C, w.C, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+    prof_rec(prof, 5, s);
+    return GGMS_OK;
+  };
+  if (o.stats || prof) {
+    rc = enqueue(st);
+  } else {
+    const uint64_t key[] = {0x51Eull + sizeof(T) + (topk ? 256u : 0u) + (std::is_signed<T>::value ? 16u : 0u) +
+                                (std::is_floating_point<T>::value ? 32u : 0u),
+                            (uint64_t)(uintptr_t)d_in, n, host_k ? 1ull : (uint64_t)(uintptr_t)ks, nk,
+                            host_out ? 1ull : (uint64_t)(uintptr_t)out,
+                            (uint64_t)p.assigner | ((uint64_t)p.B << 8) | ((uint64_t)p.S << 24),
+                            p.seed, (uint64_t)(uint32_t)p.train_steps | ((uint64_t)pv->nt << 32),
+                            (uint64_t)pv->unroll | ((uint64_t)float_bits(p.bound) << 8),
+                            (uint64_t)float_bits(p.window_z), (uint64_t)(uintptr_t)ctx->arena,
+                            (uint64_t)(uintptr_t)ctx->pinned};
+    rc = run_graphed(ctx, key, (int)(sizeof(key) / sizeof(key[0])), st, enqueue);
+  }
+  if (rc) return rc;
+  if (host_k && !topk) {
+    if (!ctx->pin_busy) GGMS_CU(cudaEventCreateWithFlags(&ctx->pin_busy, cudaEventDisableTiming));
+    GGMS_CU(cudaEventRecord(ctx->pin_busy, st));
+  }
   const bool need_sync = host_out || o.stats;
   if (!need_sync) return GGMS_OK;
-  GGMS_CU(cudaMemcpyAsync(pin_C, w.C, sizeof(Counters), cudaMemcpyDeviceToHost, st));
   GGMS_CU(cudaStreamSynchronize(st));
   if (host_out) memcpy(out, pin_out, sizeof(T) * nk);
   if (o.stats) {
@@ -579,7 +693,7 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     s->active_buckets = (int32_t)pin_C->active0;
     s->point_buckets = (int32_t)pin_C->point0;
     s->small_segments = (int32_t)pin_C->small_segs;
-    s->sample_size = (int32_t)S;
+    s->sample_size = (int32_t)p.S;
     s->bucket_max_over_mean = (float)pin_C->max_bucket0 / ((float)n / (float)p.B);
     s->model_imbalance = (p.assigner == GGMS_ASSIGNER_SAMPLED) ? 0.0f : ls.imbalance;
     s->model_loss = (p.assigner == GGMS_ASSIGNER_SAMPLED) ? 0.0f : ls.loss;
@@ -678,57 +792,70 @@ static int run_segmented(Context* ctx, const T* d_in, const int64_t* seg_off, in
   if (rc) return rc;
   Workspace<K> w = layout<K>(p, sizeof(T), ctx->arena);
   const Caps caps{p.cap_seg, p.cap_tiles, p.nk, (uint32_t)(SMALL_SMEM / sizeof(K))};
-  GGMS_CU(cudaMemsetAsync(w.C, 0, sizeof(Counters), st));
-  ++ctx->launches;
-  k_init_seg<<<cdiv(nk, 256), 256, 0, st>>>(ks, nk, seg_off, k_off, nseg, w.krank, w.kseg, w.C);
-  ++ctx->launches;
-  seg_init<K><<<cdiv(nseg, 256), 256, 0, st>>>(seg_off, nseg, k_off, w.segs[0], w.tiles[0], w.C);
-  ++ctx->launches;
-  seg_set_count<<<1, 1, 0, st>>>(w.C, nseg);
-  const int maxlev = (sizeof(K) == 4) ? 3 : 6;  // radix shifts 21,10,0 / 53,42,31,20,9,0
-  const int lv_grid = ctx->sms * 8;
-  const int seg_grid = ctx->sms * 2;
-  for (int l = 0; l < maxlev; ++l) {
-    const int pp = l & 1, q = pp ^ 1;
-    K* dst = w.cand[l & 1];
+  // the stream-ordered part: captured once and replayed when the call repeats
+  auto enqueue = [&](cudaStream_t s) -> int {
+    GGMS_CU(cudaMemsetAsync(w.C, 0, sizeof(Counters), s));
     ++ctx->launches;
-    lvl_prep<<<ctx->sms * 2, 256, 0, st>>>(w.rows[pp], w.aflag[pp], w.C, pp, caps);
-    if (l == 0) {
-        ++ctx->launches;
-        lvl_count<T, LV_NT><<<lv_grid, LV_NT, 0, st>>>(d_in, w.segs[pp], w.tiles[pp], w.C, pp, w.rows[pp], caps);
-      } else {
-        ++ctx->launches;
-        lvl_count<K, LV_NT><<<lv_grid, LV_NT, 0, st>>>(w.cand[(l - 1) & 1], w.segs[pp], w.tiles[pp],
-                                                       w.C, pp, w.rows[pp], caps);
-      }
+    k_init_seg<<<cdiv(nk, 256), 256, 0, s>>>(ks, nk, seg_off, k_off, nseg, w.krank, w.kseg, w.C);
     ++ctx->launches;
-    lvl_scan<<<seg_grid, 1024, 0, st>>>(w.rows[pp], w.C, pp, caps);
+    seg_init<K><<<cdiv(nseg, 256), 256, 0, s>>>(seg_off, nseg, k_off, w.segs[0], w.tiles[0], w.C);
     ++ctx->launches;
-    lvl_locate_rows<<<cdiv(nk, 256), 256, 0, st>>>(w.rows[pp], NBIN, nk, w.krank, w.kseg, w.kbin,
-                                                     w.aflag[pp], NBIN_WORDS, w.C);
-    ++ctx->launches;
-    lvl_children<K, 1024><<<seg_grid, 1024, 0, st>>>(w.rows[pp], w.aflag[pp], w.segs[pp], w.C, pp,
-                                                     w.segs[q], w.cursor[q], w.tiles[q], w.points,
-                                                     w.khead[q], w.smalls, caps);
-    ++ctx->launches;
-    lvl_relabel<K><<<cdiv(nk, 256), 256, 0, st>>>(w.rows[pp], NBIN, nk, w.kbin, w.kseg, w.kkey,
-                                                    w.points, w.C, w.segs[q], w.khead[q], w.knext);
-    if (l + 1 < maxlev) {
+    seg_set_count<<<1, 1, 0, s>>>(w.C, nseg);
+    const int maxlev = (sizeof(K) == 4) ? 3 : 6;  // radix shifts 21,10,0 / 53,42,31,20,9,0
+    const int lv_grid = ctx->sms * 8;
+    const int seg_grid = ctx->sms * 2;
+    for (int l = 0; l < maxlev; ++l) {
+      const int pp = l & 1, q = pp ^ 1;
+      K* dst = w.cand[l & 1];
       ++ctx->launches;
-      if (l == 0)
-        lvl_compact<T, LV_NT><<<lv_grid, LV_NT, 0, st>>>(d_in, w.segs[pp], w.tiles[pp], w.C, pp,
-                                                         w.rows[pp], w.segs[q], w.cursor[q], dst, caps);
-      else
-        lvl_compact<K, LV_NT><<<lv_grid, LV_NT, 0, st>>>(w.cand[(l - 1) & 1], w.segs[pp], w.tiles[pp],
-                                                         w.C, pp, w.rows[pp], w.segs[q], w.cursor[q],
-                                                         dst, caps);
-      rc = launch_small_select<K>(ctx, dst, w.segs[q], w.khead[q], w, caps, st);
-      if (rc) return rc;
+      lvl_prep<<<ctx->sms * 2, 256, 0, s>>>(w.rows[pp], w.aflag[pp], w.C, pp, caps);
+      if (l == 0) {
+          ++ctx->launches;
+          lvl_count<T, LV_NT><<<lv_grid, LV_NT, 0, s>>>(d_in, w.segs[pp], w.tiles[pp], w.C, pp, w.rows[pp], caps);
+        } else {
+          ++ctx->launches;
+          lvl_count<K, LV_NT><<<lv_grid, LV_NT, 0, s>>>(w.cand[(l - 1) & 1], w.segs[pp], w.tiles[pp],
+                                                         w.C, pp, w.rows[pp], caps);
+        }
+      ++ctx->launches;
+      lvl_scan<<<seg_grid, 1024, 0, s>>>(w.rows[pp], w.C, pp, caps);
+      ++ctx->launches;
+      lvl_locate_rows<<<cdiv(nk, 256), 256, 0, s>>>(w.rows[pp], NBIN, nk, w.krank, w.kseg, w.kbin,
+                                                       w.aflag[pp], NBIN_WORDS, w.C);
+      ++ctx->launches;
+      lvl_children<K, 1024><<<seg_grid, 1024, 0, s>>>(w.rows[pp], w.aflag[pp], w.segs[pp], w.C, pp,
+                                                       w.segs[q], w.cursor[q], w.tiles[q], w.points,
+                                                       w.khead[q], w.smalls, caps);
+      ++ctx->launches;
+      lvl_relabel<K><<<cdiv(nk, 256), 256, 0, s>>>(w.rows[pp], NBIN, nk, w.kbin, w.kseg, w.kkey,
+                                                      w.points, w.C, w.segs[q], w.khead[q], w.knext);
+      if (l + 1 < maxlev) {
+        ++ctx->launches;
+        if (l == 0)
+          lvl_compact<T, LV_NT><<<lv_grid, LV_NT, 0, s>>>(d_in, w.segs[pp], w.tiles[pp], w.C, pp,
+                                                           w.rows[pp], w.segs[q], w.cursor[q], dst, caps);
+        else
+          lvl_compact<K, LV_NT><<<lv_grid, LV_NT, 0, s>>>(w.cand[(l - 1) & 1], w.segs[pp], w.tiles[pp],
+                                                           w.C, pp, w.rows[pp], w.segs[q], w.cursor[q],
+                                                           dst, caps);
+        rc = launch_small_select<K>(ctx, dst, w.segs[q], w.khead[q], w, caps, s);
+        if (rc) return rc;
+      }
     }
+    ++ctx->launches;
+    write_out<T><<<cdiv(nk, 256), 256, 0, s>>>(w.kkey, w.kseg, nk, out, w.C);
+  return cudaGetLastError() == cudaSuccess ? GGMS_OK : GGMS_E_CUDA;
+  };
+  if (o.stats || ctx->profile) {
+    rc = enqueue(st);
+  } else {
+    const uint64_t key[] = {0x5E6ull + sizeof(T), (uint64_t)(uintptr_t)d_in, (uint64_t)(uintptr_t)seg_off, nseg,
+                            (uint64_t)(uintptr_t)ks, (uint64_t)(uintptr_t)k_off, (uint64_t)(uintptr_t)out, n,
+                            nk, (uint64_t)(uintptr_t)ctx->arena, (uint64_t)std::is_signed<T>::value,
+                            (uint64_t)std::is_floating_point<T>::value};
+    rc = run_graphed(ctx, key, (int)(sizeof(key) / sizeof(key[0])), st, enqueue);
   }
-  ++ctx->launches;
-  write_out<T><<<cdiv(nk, 256), 256, 0, st>>>(w.kkey, w.kseg, nk, out, w.C);
-  GGMS_CU(cudaGetLastError());
+  if (rc) return rc;
   if (o.stats) {
     Counters hc;
     GGMS_CU(cudaMemcpyAsync(&hc, w.C, sizeof(Counters), cudaMemcpyDeviceToHost, st));
