@@ -30,6 +30,7 @@ struct Context {
   size_t pinned_bytes = 0;
   std::mutex mu;
   long long launches = 0;          // kernels launched by this context
+  long long graph_launches = 0;    // calls replayed from a captured CUDA graph
   // profiling: events around pass 1, pass 2 and the whole call (ring of calls)
   static constexpr int RING = 256;
   bool profile = false;
@@ -47,6 +48,12 @@ struct Context {
   uint64_t clock = 0;
   cudaStream_t capture = nullptr;  // private stream the graphs are captured on
   cudaEvent_t pin_busy = nullptr;  // recorded after the last call's uploads from the pinned buffer
+  // autotuner: launch shapes and bucket counts picked per shape class
+  struct Tuned {
+    uint64_t key[4];
+    int B, nt, unroll, lv_mult;
+  };
+  std::vector<Tuned> tuned;
 };
 
 static int cuda_status(cudaError_t e) {
@@ -329,6 +336,7 @@ static int run_graphed(Context* c, const uint64_t* key, int nkey, cudaStream_t s
     hit->used = ++c->clock;
     GGMS_CU(cudaGraphLaunch(hit->exec, st));
     c->launches += hit->launches;
+    ++c->graph_launches;
     return GGMS_OK;
   }
   if (!hit) {  // first sighting: remember the key (evicting the least recently used), run directly
@@ -366,6 +374,7 @@ static int run_graphed(Context* c, const uint64_t* key, int nkey, cudaStream_t s
   hit->used = ++c->clock;
   GGMS_CU(cudaGraphLaunch(exec, st));
   c->launches += captured;
+  ++c->graph_launches;
   return GGMS_OK;
 }
 
@@ -703,6 +712,89 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   return GGMS_OK;
 }
 
+// ------------------------------------------------------------------ autotuner
+// With opts->autotune set and the bucket count and pass shape left to the
+// library, the first call of a shape class (type, log2 n, log2 K, assigner,
+// where ks and answers live) times every candidate on the caller's own data --
+// each candidate a full, correct call: 1 warm-up + 2 timed with CUDA events on
+// the caller's stream -- and keeps the fastest in the context; later calls of
+// the class use it.  The batched path tunes the CTAs per SM of its level
+// kernels the same way (class: type, log2 n, log2 K, log2 segments).
+static const Context::Tuned* tuned_find(Context* c, const uint64_t* key) {
+  for (const auto& t : c->tuned)
+    if (!memcmp(t.key, key, sizeof(t.key))) return &t;
+  return nullptr;
+}
+
+static int bitlen64(uint64_t v) {
+  int b = 0;
+  while (v) { ++b; v >>= 1; }
+  return b;
+}
+
+template <typename F>
+static int time_calls(cudaStream_t st, F&& call, float* ms) {
+  int rc = call();  // warm-up (and graph capture of repeated calls)
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  GGMS_CU(cudaEventCreate(&e0));
+  GGMS_CU(cudaEventCreate(&e1));
+  GGMS_CU(cudaEventRecord(e0, st));
+  for (int i = 0; i < 2 && !rc; ++i) rc = call();
+  GGMS_CU(cudaEventRecord(e1, st));
+  GGMS_CU(cudaEventSynchronize(e1));
+  cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
+template <typename T>
+static int run_single_tuned(Context* c, const T* d_in, uint64_t n, const uint32_t* ks, uint64_t nk, T* out,
+                            const ggms_opts& o, cudaStream_t st, bool topk = false) {
+  if (!o.autotune || o.num_buckets || o.pass_threads || o.pass_unroll || n == 0 || nk == 0)
+    return run_single<T>(c, d_in, n, ks, nk, out, o, st, topk);
+  const uint64_t key[4] = {sizeof(T) | (std::is_signed<T>::value ? 16u : 0u) |
+                               (std::is_floating_point<T>::value ? 32u : 0u) | (topk ? 64u : 0u),
+                           (uint64_t)bitlen64(n) | ((uint64_t)bitlen64(nk) << 8),
+                           (uint64_t)o.assigner | ((uint64_t)o.ks_on_device << 8) | ((uint64_t)o.out_on_device << 9),
+                           (uint64_t)float_bits(o.window_z)};
+  ggms_opts b = o;
+  b.autotune = 0;
+  if (const Context::Tuned* t = tuned_find(c, key)) {
+    b.num_buckets = t->B;
+    b.pass_threads = t->nt;
+    b.pass_unroll = t->unroll;
+    return run_single<T>(c, d_in, n, ks, nk, out, b, st, topk);
+  }
+  static const int Bs[] = {4096, 8192, 16384};
+  static const int shapes[][2] = {{1024, 4}, {512, 4}, {512, 8}};
+  float best = 3.4e38f;
+  Context::Tuned pick{{key[0], key[1], key[2], key[3]}, 8192, 1024, 4, 8};
+  for (int B : Bs) {
+    for (const auto& sh : shapes) {
+      ggms_opts t = b;
+      t.num_buckets = B;
+      t.pass_threads = sh[0];
+      t.pass_unroll = sh[1];
+      float ms = 0.0f;
+      const int rc = time_calls(st, [&] { return run_single<T>(c, d_in, n, ks, nk, out, t, st, topk); }, &ms);
+      if (rc) return rc;
+      if (ms < best) {
+        best = ms;
+        pick.B = B;
+        pick.nt = sh[0];
+        pick.unroll = sh[1];
+      }
+    }
+  }
+  c->tuned.push_back(pick);
+  b.num_buckets = pick.B;
+  b.pass_threads = pick.nt;
+  b.pass_unroll = pick.unroll;
+  return run_single<T>(c, d_in, n, ks, nk, out, b, st, topk);
+}
+
 template <typename T>
 static int dropin(const T* d_vector, int length, const uint32_t* kVals, int numKs, T* outputs) {
   if (length <= 0 || numKs < 0) return GGMS_E_INVALID_ARG;
@@ -731,7 +823,7 @@ static int topk_call(ggms_context* cx, const T* d_in, int64_t n, int64_t K, T* o
     if (rc) return rc;
   }
   std::lock_guard<std::mutex> lk(c->mu);
-  return run_single<T>(c, d_in, (uint64_t)n, nullptr, (uint64_t)K, out, o, (cudaStream_t)stream, true);
+  return run_single_tuned<T>(c, d_in, (uint64_t)n, nullptr, (uint64_t)K, out, o, (cudaStream_t)stream, true);
 }
 
 template <typename T>
@@ -750,7 +842,7 @@ static int ex(ggms_context* cx, const T* d_in, int64_t n, const uint32_t* ks, in
     if (rc) return rc;
   }
   std::lock_guard<std::mutex> lk(c->mu);
-  return run_single<T>(c, d_in, (uint64_t)n, ks, (uint64_t)nk, out, o, (cudaStream_t)stream);
+  return run_single_tuned<T>(c, d_in, (uint64_t)n, ks, (uint64_t)nk, out, o, (cudaStream_t)stream);
 }
 
 
@@ -760,7 +852,7 @@ static int ex(ggms_context* cx, const T* d_in, int64_t n, const uint32_t* ks, in
 template <typename T>
 static int run_segmented(Context* ctx, const T* d_in, const int64_t* seg_off, int64_t nseg64,
                          const uint32_t* ks, const int64_t* k_off, T* out, const ggms_opts& o,
-                         cudaStream_t st) {
+                         cudaStream_t st, int lv_mult = 8) {
   using K = typename KeyOf<T>::K;
   if (!d_in || !seg_off || !k_off || nseg64 <= 0 || nseg64 > (1 << 30)) return GGMS_E_INVALID_ARG;
   if ((uintptr_t)d_in % sizeof(T) != 0) return GGMS_E_INVALID_ARG;
@@ -802,7 +894,7 @@ static int run_segmented(Context* ctx, const T* d_in, const int64_t* seg_off, in
     ++ctx->launches;
     seg_set_count<<<1, 1, 0, s>>>(w.C, nseg);
     const int maxlev = (sizeof(K) == 4) ? 3 : 6;  // radix shifts 21,10,0 / 53,42,31,20,9,0
-    const int lv_grid = ctx->sms * 8;
+    const int lv_grid = ctx->sms * lv_mult;
     const int seg_grid = ctx->sms * 2;
     for (int l = 0; l < maxlev; ++l) {
       const int pp = l & 1, q = pp ^ 1;
@@ -852,7 +944,7 @@ static int run_segmented(Context* ctx, const T* d_in, const int64_t* seg_off, in
     const uint64_t key[] = {0x5E6ull + sizeof(T), (uint64_t)(uintptr_t)d_in, (uint64_t)(uintptr_t)seg_off, nseg,
                             (uint64_t)(uintptr_t)ks, (uint64_t)(uintptr_t)k_off, (uint64_t)(uintptr_t)out, n,
                             nk, (uint64_t)(uintptr_t)ctx->arena, (uint64_t)std::is_signed<T>::value,
-                            (uint64_t)std::is_floating_point<T>::value};
+                            (uint64_t)std::is_floating_point<T>::value, (uint64_t)lv_mult};
     rc = run_graphed(ctx, key, (int)(sizeof(key) / sizeof(key[0])), st, enqueue);
   }
   if (rc) return rc;
@@ -867,6 +959,42 @@ static int run_segmented(Context* ctx, const T* d_in, const int64_t* seg_off, in
     if (hc.status) return (int)hc.status;
   }
   return GGMS_OK;
+}
+
+template <typename T>
+static int run_segmented_tuned(Context* c, const T* d_in, const int64_t* seg_off, int64_t nseg,
+                               const uint32_t* ks, const int64_t* k_off, T* out, const ggms_opts& o,
+                               cudaStream_t st) {
+  if (!o.autotune || o.stats) return run_segmented<T>(c, d_in, seg_off, nseg, ks, k_off, out, o, st);
+  // the class needs n and K: read the totals (run_segmented reads them again)
+  int64_t h[2] = {0, 0};
+  if (nseg <= 0 || !seg_off || !k_off) return GGMS_E_INVALID_ARG;
+  GGMS_CU(cudaSetDevice(c->device));
+  GGMS_CU(cudaMemcpyAsync(&h[0], seg_off + nseg, 8, cudaMemcpyDeviceToHost, st));
+  GGMS_CU(cudaMemcpyAsync(&h[1], k_off + nseg, 8, cudaMemcpyDeviceToHost, st));
+  GGMS_CU(cudaStreamSynchronize(st));
+  const uint64_t key[4] = {0x5E60000ull | sizeof(T) | (std::is_floating_point<T>::value ? 32u : 0u),
+                           (uint64_t)bitlen64((uint64_t)std::max<int64_t>(h[0], 0)) |
+                               ((uint64_t)bitlen64((uint64_t)std::max<int64_t>(h[1], 0)) << 8) |
+                               ((uint64_t)bitlen64((uint64_t)nseg) << 16),
+                           0ull, 0ull};
+  if (const Context::Tuned* t = tuned_find(c, key))
+    return run_segmented<T>(c, d_in, seg_off, nseg, ks, k_off, out, o, st, t->lv_mult);
+  static const int mults[] = {4, 8, 16};
+  float best = 3.4e38f;
+  Context::Tuned pick{{key[0], key[1], key[2], key[3]}, 0, 0, 0, 8};
+  for (int m : mults) {
+    float ms = 0.0f;
+    const int rc = time_calls(st, [&] { return run_segmented<T>(c, d_in, seg_off, nseg, ks, k_off, out, o, st, m); },
+                              &ms);
+    if (rc) return rc;
+    if (ms < best) {
+      best = ms;
+      pick.lv_mult = m;
+    }
+  }
+  c->tuned.push_back(pick);
+  return run_segmented<T>(c, d_in, seg_off, nseg, ks, k_off, out, o, st, pick.lv_mult);
 }
 
 template <typename T>
@@ -885,7 +1013,7 @@ static int segmented(ggms_context* cx, const T* d_in, const int64_t* seg_off, in
     if (rc) return rc;
   }
   std::lock_guard<std::mutex> lk(c->mu);
-  return run_segmented<T>(c, d_in, seg_off, nseg, ks, k_off, out, o, (cudaStream_t)stream);
+  return run_segmented_tuned<T>(c, d_in, seg_off, nseg, ks, k_off, out, o, (cudaStream_t)stream);
 }
 
 
@@ -1085,6 +1213,13 @@ int64_t ggms_context_launches(ggms_context* ctx) {
   Context* c = (Context*)ctx;
   if (!c) return -1;
   return (int64_t)c->launches;
+}
+
+int64_t ggms_context_graph_launches(ggms_context* ctx) {
+  Context* c = (Context*)ctx;
+  if (!c) return -1;
+  std::lock_guard<std::mutex> lk(c->mu);
+  return c->graph_launches;
 }
 
 #define GGMS_DROPIN(NAME, T)                                                                 \

@@ -89,7 +89,7 @@ class Opts(ctypes.Structure):
         ("pass_threads", ctypes.c_int32),
         ("pass_unroll", ctypes.c_int32),
         ("window_z", ctypes.c_float),
-        ("reserved0", ctypes.c_int32),
+        ("autotune", ctypes.c_int32),
         ("stats", ctypes.POINTER(Stats)),
     ]
 
@@ -135,6 +135,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ggms_context_pass_times.argtypes = [vp, vp, vp, vp, i32]
     lib.ggms_context_launches.restype = i64
     lib.ggms_context_launches.argtypes = [vp]
+    lib.ggms_context_graph_launches.restype = i64
+    lib.ggms_context_graph_launches.argtypes = [vp]
     lib.ggms_diag_pl_gradient.restype = i32
     lib.ggms_diag_pl_gradient.argtypes = [vp, i32, vp, vp, vp, vp, vp]
     lib.ggms_diag_mlp_gradient.restype = i32

@@ -87,7 +87,9 @@ typedef struct ggms_opts {
   int32_t pass_unroll;          /* 16-byte loads in flight per thread: 2, 4 or 8; 0 = tuned default */
   float window_z;               /* PASS 1 windows: safety margin of the predicted k positions in
                                    binomial standard deviations; 0 = 8; < 0 = no windows */
-  int32_t reserved0;
+  int32_t autotune;             /* 1: when num_buckets and the pass shape are left at 0, the first call of a
+                                   shape class times the candidates on the caller's data and the context
+                                   keeps the fastest (the batched path tunes its level kernels' CTAs) */
   ggms_stats* stats;            /* optional host pointer */
 } ggms_opts;
 
@@ -116,6 +118,11 @@ GGMS_API int ggms_context_profile(ggms_context* ctx, int enable);
 GGMS_API int ggms_context_pass_times(ggms_context* ctx, float* pass1_ms, float* pass2_ms,
                                      float* call_ms, int max);
 GGMS_API int64_t ggms_context_launches(ggms_context* ctx);
+/* Calls of this context that ran as a replay of a captured CUDA graph: a call
+ * whose arguments, options and workspace repeat is captured the second time
+ * it is seen (on a private stream) and replayed from then on; statistics and
+ * profiling calls always run directly. */
+GGMS_API int64_t ggms_context_graph_launches(ggms_context* ctx);
 
 /* ---- drop-in entry points: the reference's wrapper signatures in C spelling ----
  * d_vector: device memory, `length` elements, never modified (the reference's
