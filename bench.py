@@ -263,12 +263,18 @@ def run_ours(args):
             if not np.array_equal(got.view(np.uint32), exp.view(np.uint32)):
                 raise SystemExit(f"answers differ from the oracle (assigner {a})")
 
-    # value: device-resident, learned (auto) assigner; pass times on the same stream
-    lib.ggms_context_profile(ctx.ptr, 1)
+    # value: device-resident, learned (auto) assigner.  Repeated calls replay a
+    # captured CUDA graph (the second call captures it), as in a real loop.
     launches0 = lib.ggms_context_launches(ctx.ptr)
+    graphs0 = lib.ggms_context_graph_launches(ctx.ptr)
     with Clocks(local) as clk:
         ms = time_loop(call(G.ASSIGNER_AUTO), args.steps, args.warmup, stream, world, dev)
     launches = (lib.ggms_context_launches(ctx.ptr) - launches0) * args.steps // (args.steps + args.warmup)
+    graph_calls = lib.ggms_context_graph_launches(ctx.ptr) - graphs0
+    # pass times: the same calls with the profiling hooks on (events around the
+    # passes on the call's stream; such calls run without the graph)
+    lib.ggms_context_profile(ctx.ptr, 1)
+    time_loop(call(G.ASSIGNER_AUTO), args.steps, args.warmup, stream, world, dev)
     cnt = args.steps + args.warmup
     p1 = (ctypes.c_float * cnt)()
     p2 = (ctypes.c_float * cnt)()
@@ -345,6 +351,7 @@ def run_ours(args):
                     "stats": st_samp},
         "stats": st_auto,
         "gpu_launches": int(launches),
+        "graph_replays": int(graph_calls),
         "clocks": clk.summary(),
     }
     if rank == 0 and not args.no_cpu:

@@ -48,6 +48,7 @@ struct Context {
   uint64_t clock = 0;
   cudaStream_t capture = nullptr;  // private stream the graphs are captured on
   cudaEvent_t pin_busy = nullptr;  // recorded after the last call's uploads from the pinned buffer
+  cudaStream_t body = nullptr;     // private stream the conditional level bodies are captured on
   // autotuner: launch shapes and bucket counts picked per shape class
   struct Tuned {
     uint64_t key[4];
@@ -125,6 +126,7 @@ static void destroy_context(Context* c) {
     if (g.exec) cudaGraphExecDestroy(g.exec);
   if (c->capture) cudaStreamDestroy(c->capture);
   if (c->pin_busy) cudaEventDestroy(c->pin_busy);
+  if (c->body) cudaStreamDestroy(c->body);
   cudaSetDevice(prev);
   delete c;
 }
@@ -375,6 +377,43 @@ static int run_graphed(Context* c, const uint64_t* key, int nkey, cudaStream_t s
   GGMS_CU(cudaGraphLaunch(exec, st));
   c->launches += captured;
   ++c->graph_launches;
+  return GGMS_OK;
+}
+
+// One refinement level.  Captured into a graph, it becomes an IF node whose
+// condition lvl_gate sets on the device: once a level finds no segment, it
+// and every later level cost nothing.  Run directly, the level's kernels are
+// launched as they are (each returns at once when there is no work).
+template <typename F>
+static int enqueue_level(Context* c, cudaStream_t s, Counters* C, int p, F&& body) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  GGMS_CU(cudaStreamIsCapturing(s, &cs));
+  if (cs != cudaStreamCaptureStatusActive) return body(s);
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  GGMS_CU(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+  cudaGraphConditionalHandle h;
+  GGMS_CU(cudaGraphConditionalHandleCreate(&h, g, 0u, cudaGraphCondAssignDefault));
+  ++c->launches;
+  lvl_gate<<<1, 1, 0, s>>>(C, p, h);
+  GGMS_CU(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeIf;
+  np.conditional.size = 1;
+  cudaGraphNode_t cn;
+  GGMS_CU(cudaGraphAddNode(&cn, g, deps, nd, &np));
+  if (!c->body) GGMS_CU(cudaStreamCreateWithFlags(&c->body, cudaStreamNonBlocking));
+  GGMS_CU(cudaStreamBeginCaptureToGraph(c->body, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal));
+  const int rc = body(c->body);
+  cudaGraph_t out = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c->body, &out);
+  if (rc) return rc;
+  GGMS_CU(e);
+  GGMS_CU(cudaStreamUpdateCaptureDependencies(s, &cn, 1, cudaStreamSetCaptureDependencies));
   return GGMS_OK;
 }
 
@@ -629,6 +668,7 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
       const int pp = l & 1, q = pp ^ 1;
       const K* src = w.cand[(l - 1) & 1];
       K* dst = w.cand[l & 1];
+      rc = enqueue_level(ctx, s, w.C, pp, [&](cudaStream_t s) -> int {
       ++ctx->launches;
       lvl_prep<<<ctx->sms * 2, 256, 0, s>>>(w.rows[pp], w.aflag[pp], w.C, pp, caps);
       ++ctx->launches;
@@ -649,9 +689,11 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
         ++ctx->launches;
         lvl_compact<K, LV_NT><<<lv_grid, LV_NT, 0, s>>>(src, w.segs[pp], w.tiles[pp], w.C, pp,
                                                          w.rows[pp], w.segs[q], w.cursor[q], dst, caps);
-        rc = launch_small_select<K>(ctx, dst, w.segs[q], w.khead[q], w, caps, s);
-        if (rc) return rc;
+        return launch_small_select<K>(ctx, dst, w.segs[q], w.khead[q], w, caps, s);
       }
+      return GGMS_OK;
+      });
+      if (rc) return rc;
     }
 
     // ---- answers

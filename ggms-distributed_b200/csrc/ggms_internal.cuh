@@ -271,7 +271,8 @@ struct Counters {
   unsigned long long refine_elems;
   uint32_t asg_choice;        // index of the assigner in use (0 sampled, 1 learned)
   uint32_t win_runs;          // PASS 1 window runs in use (0: no windows)
-  uint32_t pad1[6];
+  uint32_t done;              // a refinement level found no segment: later levels are skipped
+  uint32_t pad1[5];
 };
 
 // PASS 1 windows (l0_window).  From the sample, every requested k gets a

@@ -941,6 +941,13 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
 // Level l works on the segments of pool p = l & 1 and creates children in pool
 // q = p ^ 1.  Keys are read from `src` and children are written to `dst`.
 
+// Gate of a refinement level inside a captured CUDA graph: the level (an IF
+// node) runs only while every level so far had segments to refine.
+__global__ void lvl_gate(Counters* C, int p, cudaGraphConditionalHandle h) {
+  if (C->nsegs[p] == 0u) C->done = 1u;
+  cudaGraphSetConditional(h, C->done ? 0u : 1u);
+}
+
 // zero this level's histogram rows / flags; reset the child pool's counters
 __global__ void lvl_prep(uint32_t* rows, uint32_t* aflag, Counters* C, int p, Caps caps) {
   const uint32_t ns = min(C->nsegs[p], caps.segs);

@@ -101,3 +101,21 @@ def test_autotune_segmented_stays_exact(ctx):
         assert rc == 0
         torch.cuda.synchronize()
         np.testing.assert_array_equal(orc.bits(out.cpu().numpy()), orc.bits(exp))
+
+
+@pytest.mark.parametrize("gen,assigner", [("normal_f32", G.ASSIGNER_SAMPLED), ("distinct256_f32", G.ASSIGNER_AUTO)])
+def test_replayed_graph_runs_refinement_levels_when_needed(ctx, gen, assigner):
+    """Spread ks and duplicates make segments too big for the shared-memory select, so
+    refinement levels must run inside the replayed graph (their IF nodes open)."""
+    import torch
+    n = 1 << 23
+    d = to_device(D.VALUE_GENERATORS[gen](n, 1))
+    for call in range(4):
+        v = D.VALUE_GENERATORS[gen](n, 50 + call)
+        d.copy_(torch.from_numpy(v))
+        ks = D.ks_uniform(n, 4096, 60 + call)
+        out, st = None, None
+        out = G.select(ctx, d.data_ptr(), n, ks, np.float32, assigner=assigner)
+        np.testing.assert_array_equal(orc.bits(out), orc.bits(orc.select(v, ks)), err_msg=f"call {call}")
+    _, st = G.select(ctx, d.data_ptr(), n, ks, np.float32, assigner=assigner, stats=True)
+    assert st["levels"] >= 1, st
