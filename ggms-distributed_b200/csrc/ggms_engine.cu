@@ -49,6 +49,8 @@ struct Context {
   cudaStream_t capture = nullptr;  // private stream the graphs are captured on
   cudaEvent_t pin_busy = nullptr;  // recorded after the last call's uploads from the pinned buffer
   cudaStream_t body = nullptr;     // private stream the conditional level bodies are captured on
+  cudaStream_t side = nullptr;     // the sampled assigner's build, next to the learned one
+  cudaEvent_t fork = nullptr, join = nullptr;
   // autotuner: launch shapes and bucket counts picked per shape class
   struct Tuned {
     uint64_t key[4];
@@ -127,6 +129,9 @@ static void destroy_context(Context* c) {
   if (c->capture) cudaStreamDestroy(c->capture);
   if (c->pin_busy) cudaEventDestroy(c->pin_busy);
   if (c->body) cudaStreamDestroy(c->body);
+  if (c->side) cudaStreamDestroy(c->side);
+  if (c->fork) cudaEventDestroy(c->fork);
+  if (c->join) cudaEventDestroy(c->join);
   cudaSetDevice(prev);
   delete c;
 }
@@ -609,13 +614,25 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     }
     rc = setup_attrs<K>();
     if (rc) return rc;
-    ++ctx->launches;
-    setup_sampled<K><<<1, SETUP_NT, sizeof(SetupSmem<K>), s>>>(w.samp_sorted, S, p.B, &w.asg[0],
-                                                                 &w.grid[0]);
-    if (p.assigner != GGMS_ASSIGNER_SAMPLED) {
+    if (p.assigner == GGMS_ASSIGNER_SAMPLED) {
+      ++ctx->launches;
+      setup_sampled<K><<<1, SETUP_NT, sizeof(SetupSmem<K>), s>>>(w.samp_sorted, S, p.B, &w.asg[0],
+                                                                   &w.grid[0]);
+    } else {
+      // the sampled grid (fallback and judge) is built on a side stream while
+      // the learned model's knots and statistics are computed: fork and join
+      if (!ctx->side) GGMS_CU(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+      if (!ctx->fork) GGMS_CU(cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming));
+      if (!ctx->join) GGMS_CU(cudaEventCreateWithFlags(&ctx->join, cudaEventDisableTiming));
+      GGMS_CU(cudaEventRecord(ctx->fork, s));
+      GGMS_CU(cudaStreamWaitEvent(ctx->side, ctx->fork, 0));
+      ++ctx->launches;
+      setup_sampled<K><<<1, SETUP_NT, sizeof(SetupSmem<K>), ctx->side>>>(w.samp_sorted, S, p.B, &w.asg[0],
+                                                                           &w.grid[0]);
+      GGMS_CU(cudaEventRecord(ctx->join, ctx->side));
       rc = learn_and_choose<K>(p.assigner, w.samp_sorted, S, p.B, p.train_steps, p.bound, w.asg,
                                w.grid, w.learn, &w.C->asg_choice, w.krank, nk, n, p.window_z, s,
-                               &ctx->launches);
+                               &ctx->launches, ctx->join);
       if (rc) return rc;
     }
 

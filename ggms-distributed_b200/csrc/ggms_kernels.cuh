@@ -616,13 +616,18 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
                             const Windows<K>* __restrict__ Wg,
                             uint32_t* cmap0, Seg<K>* segs1, uint32_t* cursor1, TileRef* tiles1,
                             K* points, uint32_t* khead1, uint32_t* smalls, Caps caps) {
+  // the key-range searches below evaluate the grid ~64 times per bucket: keep
+  // it in shared memory (every thread helps load it before any returns)
+  __shared__ uint2 s1[GRID_T1];
+  __shared__ uint2 s2[GRID_SUBCAP];
+  const GridView<K> gv = grid_to_smem<K>(Gs + C->asg_choice, s1, s2);
+  __syncthreads();
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= B) return;
   if (!((aflag[b >> 5] >> (b & 31)) & 1u)) {
     cmap0[b] = CM_NONE;
     return;
   }
-  const GridView<K> gv = grid_view_global<K>(Gs + C->asg_choice);
   const uint32_t start = b ? I[b - 1] : 0u;
   const uint32_t cnt = I[b] - start;
   // key range of bucket b: [L(b), L(b+1) - 1], L(x) = smallest key with eval >= x

@@ -383,7 +383,8 @@ template <typename K>
 static int learn_and_choose(int kind, const K* sorted, uint32_t S, uint32_t B, int steps_opt,
                             float bound, Assigner<K>* As, Grid<K>* Gs, LearnState* L,
                             uint32_t* choice, const uint32_t* krank, uint32_t nk, uint64_t n,
-                            float window_z, cudaStream_t st, long long* launches) {
+                            float window_z, cudaStream_t st, long long* launches,
+                            cudaEvent_t sampled_done = nullptr) {
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(setup_learned_pl<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -394,12 +395,16 @@ static int learn_and_choose(int kind, const K* sorted, uint32_t S, uint32_t B, i
     attr = true;
   }
   if (kind == GGMS_ASSIGNER_LEARNED_MLP) {
-    int rc = mlp_fit_and_compile<K>(sorted, S, B, steps_opt, bound, As, Gs, L, choice, st, launches);
+    int rc = mlp_fit_and_compile<K>(sorted, S, B, steps_opt, bound, As, Gs, L, choice, st, launches,
+                                    sampled_done);
     if (rc) return rc;
   } else {
     const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 4u;
     setup_pl_knots<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, &As[1]);
     pl_stats_grid<K><<<(PL_M + 31) / 32, 1024, 0, st>>>(sorted, S, &As[1], L);
+    // the choice compares with the sampled grid: wait for it (it may be built
+    // on another stream, concurrently with the knots and the statistics)
+    if (sampled_done && cudaStreamWaitEvent(st, sampled_done, 0) != cudaSuccess) return GGMS_E_CUDA;
     setup_learned_pl<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, steps, 0.02f, bound,
                                                                     &As[1], &Gs[1], &Gs[0], L, choice,
                                                                     krank, nk, n, window_z);

@@ -317,7 +317,7 @@ __global__ __launch_bounds__(SETUP_NT) void setup_mlp_finish(const K* __restrict
 template <typename K>
 static int mlp_fit_and_compile(const K* sorted, uint32_t S, uint32_t B, int steps_opt, float bound,
                                Assigner<K>* As, Grid<K>* Gs, LearnState* L, uint32_t* choice,
-                               cudaStream_t st, long long* launches) {
+                               cudaStream_t st, long long* launches, cudaEvent_t sampled_done) {
   static bool attr_set = false;
   if (!attr_set) {
     if (cudaFuncSetAttribute(mlp_train<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -334,6 +334,7 @@ static int mlp_fit_and_compile(const K* sorted, uint32_t S, uint32_t B, int step
   setup_mlp_begin<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, &As[1], P);
   mlp_train<K><<<MLP_CTAS, MLP_NT, sizeof(MlpSmem), st>>>(sorted, S, &As[1], L, P, steps, 0.05f,
                                                           nullptr, nullptr, nullptr);
+  if (sampled_done && cudaStreamWaitEvent(st, sampled_done, 0) != cudaSuccess) return GGMS_E_CUDA;
   setup_mlp_finish<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, bound, P, &As[1],
                                                                   &Gs[1], L, choice);
   *launches += 3;
