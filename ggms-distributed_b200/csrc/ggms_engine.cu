@@ -190,6 +190,10 @@ struct Workspace {
   uint32_t* khead[2];     // per segment: head of its k list (small segments)
   uint32_t* knext;        // per k: next k in its segment's list
   uint32_t* smalls;       // ids of the small segments the current level created
+  uint32_t* tinies;       // ids of the tiny segments the current level created
+  uint32_t* bigs[2];      // per pool: the segments a level refines (batched level 0: quantile ones)
+  K* qtab;                // ... their boundaries [cap_q][QB]
+  uint16_t* qdir;         // ... their directories [cap_q][QDS]
   K* points;
   K* cand[2];
   void* out_dev;
@@ -209,6 +213,7 @@ struct Plan {
   float bound;
   float window_z;    // < 0: no PASS 1 windows
   uint64_t seed;
+  uint32_t cap_q;    // batched path: caller segments with quantile bins (0: single path)
 };
 
 template <typename K>
@@ -235,6 +240,11 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
   size_t o_segs[2], o_cur[2], o_tiles[2], o_rows[2], o_af[2], o_cand[2], o_kh[2];
   size_t o_knext = b.take(4ull * p.nk);
   size_t o_smalls = b.take(4ull * p.cap_seg);
+  size_t o_tinies = b.take(4ull * p.cap_seg);
+  size_t o_bigs[2];
+  for (int i = 0; i < 2; ++i) o_bigs[i] = b.take(4ull * p.cap_seg);
+  size_t o_qtab = b.take(sizeof(K) * QB * p.cap_q);
+  size_t o_qdir = b.take(2ull * QDS * p.cap_q);
   for (int i = 0; i < 2; ++i) {
     o_kh[i] = b.take(4ull * p.cap_seg);
     o_segs[i] = b.take(sizeof(Seg<K>) * p.cap_seg);
@@ -276,6 +286,10 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
   }
   w.knext = (uint32_t*)(base + o_knext);
   w.smalls = (uint32_t*)(base + o_smalls);
+  w.tinies = (uint32_t*)(base + o_tinies);
+  for (int i = 0; i < 2; ++i) w.bigs[i] = (uint32_t*)(base + o_bigs[i]);
+  w.qtab = (K*)(base + o_qtab);
+  w.qdir = (uint16_t*)(base + o_qdir);
   w.points = (K*)(base + o_pts);
   w.out_dev = (void*)(base + o_out);
   return w;
@@ -312,6 +326,7 @@ static int make_plan(Plan* p, uint64_t n, uint32_t nk, const ggms_opts& o) {
   p->bound = o.imbalance_bound > 0.0f ? o.imbalance_bound : 3.0f;
   p->window_z = o.window_z == 0.0f ? 8.0f : o.window_z;
   p->seed = o.seed;
+  p->cap_q = 0;
   return GGMS_OK;
 }
 
@@ -498,19 +513,26 @@ static int setup_attrs() {
 
 constexpr int SS_NT = 512;
 
-template <typename K>
-static int launch_small_select(Context* ctx, const K* src, const Seg<K>* segs_q, const uint32_t* khead_q,
-                               const Workspace<K>& w, const Caps& caps, cudaStream_t st) {
+template <typename InT, typename K = typename KeyOf<InT>::K>
+static int launch_small_select(Context* ctx, const InT* src, const Seg<K>* segs_q, const uint32_t* khead_q,
+                               const Workspace<K>& w, const Caps& caps, cudaStream_t st,
+                               const int64_t* k_off = nullptr) {
   static bool attr = false;
   const size_t sm = SMALL_SMEM + (size_t)SS_GROUP * 256 * 4;
   if (!attr) {
-    GGMS_CU(cudaFuncSetAttribute(small_select<K, SS_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    GGMS_CU(cudaFuncSetAttribute(small_select<InT, SS_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)sm));
     attr = true;
   }
   ++ctx->launches;
-  small_select<K, SS_NT><<<ctx->sms * 2, SS_NT, sm, st>>>(src, segs_q, w.smalls, w.C, khead_q, w.knext,
-                                                          w.krank, w.kseg, w.kkey, caps.small_keys, caps);
+  small_select<InT, SS_NT><<<ctx->sms * 2, SS_NT, sm, st>>>(src, segs_q, w.smalls, w.C, khead_q, w.knext,
+                                                            k_off, w.krank, w.kseg, w.kkey, caps.small_keys,
+                                                            caps);
+  if (caps.tiny_keys) {
+    ++ctx->launches;
+    tiny_select<InT, TS_NT><<<ctx->sms * 8, TS_NT, 0, st>>>(src, segs_q, w.tinies, w.C, khead_q, w.knext,
+                                                            k_off, w.krank, w.kseg, w.kkey, caps);
+  }
   return GGMS_OK;
 }
 
@@ -569,7 +591,7 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   uint8_t* pin_k = pin + ((sizeof(Counters) + 63) & ~(size_t)63);
   uint8_t* pin_out = pin_k + (host_k ? ((4ull * nk + 63) & ~(size_t)63) : 0);
 
-  const Caps caps{p.cap_seg, p.cap_tiles, p.nk, (uint32_t)(SMALL_SMEM / sizeof(K))};
+  const Caps caps{p.cap_seg, p.cap_tiles, p.nk, (uint32_t)(SMALL_SMEM / sizeof(K)), 0u};
   if (host_k && !topk) {
     // host side, every call: the previous call's upload from the same pinned
     // buffer may still be queued (calls with device-resident answers return
@@ -662,7 +684,7 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     ++ctx->launches;
     l0_children<K><<<cdiv(p.B, 256), 256, 0, s>>>(w.hist0, w.aflag0, p.B, w.grid, w.C, w.win, w.cmap0,
                                                      w.segs[1], w.cursor[1], w.tiles[1], w.points,
-                                                     w.khead[1], w.smalls, caps);
+                                                     w.khead[1], w.smalls, w.bigs[1], caps);
     ++ctx->launches;
     lvl_relabel<K><<<cdiv(nk, 256), 256, 0, s>>>(w.cmap0, p.B, nk, w.kbin, w.kseg, w.kkey,
                                                     w.points, w.C, w.segs[1], w.khead[1], w.knext);
@@ -687,25 +709,28 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
       K* dst = w.cand[l & 1];
       rc = enqueue_level(ctx, s, w.C, pp, [&](cudaStream_t s) -> int {
       ++ctx->launches;
-      lvl_prep<<<ctx->sms * 2, 256, 0, s>>>(w.rows[pp], w.aflag[pp], w.C, pp, caps);
+      lvl_prep<<<ctx->sms * 2, 256, 0, s>>>(w.rows[pp], w.aflag[pp], w.bigs[pp], w.C, pp, caps);
       ++ctx->launches;
-      lvl_count<K, LV_NT><<<lv_grid, LV_NT, 0, s>>>(src, w.segs[pp], w.tiles[pp], w.C, pp, w.rows[pp], caps);
+      lvl_count<K, LV_NT><<<lv_grid, LV_NT, 0, s>>>(src, w.segs[pp], w.tiles[pp], w.C, pp, w.rows[pp], caps,
+                                                     nullptr, nullptr);
       ++ctx->launches;
-      lvl_scan<<<seg_grid, 1024, 0, s>>>(w.rows[pp], w.C, pp, caps);
+      lvl_scan<<<seg_grid, 1024, 0, s>>>(w.rows[pp], w.bigs[pp], w.C, pp, caps);
       ++ctx->launches;
       lvl_locate_rows<<<cdiv(nk, 256), 256, 0, s>>>(w.rows[pp], NBIN, nk, w.krank, w.kseg, w.kbin,
                                                        w.aflag[pp], NBIN_WORDS, w.C);
       ++ctx->launches;
       lvl_children<K, 1024><<<seg_grid, 1024, 0, s>>>(w.rows[pp], w.aflag[pp], w.segs[pp], w.C, pp,
                                                        w.segs[q], w.cursor[q], w.tiles[q], w.points,
-                                                       w.khead[q], w.smalls, caps);
+                                                       w.khead[q], w.smalls, w.tinies, w.bigs[pp],
+                                                       w.bigs[q], caps, nullptr);
       ++ctx->launches;
       lvl_relabel<K><<<cdiv(nk, 256), 256, 0, s>>>(w.rows[pp], NBIN, nk, w.kbin, w.kseg, w.kkey,
                                                       w.points, w.C, w.segs[q], w.khead[q], w.knext);
       if (l < maxlev) {
         ++ctx->launches;
         lvl_compact<K, LV_NT><<<lv_grid, LV_NT, 0, s>>>(src, w.segs[pp], w.tiles[pp], w.C, pp,
-                                                         w.rows[pp], w.segs[q], w.cursor[q], dst, caps);
+                                                         w.rows[pp], w.segs[q], w.cursor[q], dst, caps,
+                                                         nullptr, nullptr);
         return launch_small_select<K>(ctx, dst, w.segs[q], w.khead[q], w, caps, s);
       }
       return GGMS_OK;
@@ -906,8 +931,11 @@ static int ex(ggms_context* cx, const T* d_in, int64_t n, const uint32_t* ks, in
 
 
 // ------------------------------------------------------------------ batched segmented path
-// Level 0 is a radix level over each caller segment (no per-segment sampling
-// yet); every level runs over all segments at once.
+// Every caller segment that holds a k: small ones are finished straight from
+// the input (one warp or one CTA each); the others get sample-quantile bins at
+// level 0, and the children of those bins go through radix levels (or
+// straight to the warp / CTA finishers) -- every level runs over all segments
+// at once.
 template <typename T>
 static int run_segmented(Context* ctx, const T* d_in, const int64_t* seg_off, int64_t nseg64,
                          const uint32_t* ks, const int64_t* k_off, T* out, const ggms_opts& o,
@@ -936,59 +964,79 @@ static int run_segmented(Context* ctx, const T* d_in, const int64_t* seg_off, in
   Plan p;
   int rc = make_plan(&p, n, nk, oo);
   if (rc) return rc;
+  const uint32_t small_keys = (uint32_t)(SMALL_SMEM / sizeof(K));
   p.cap_seg = std::max<uint32_t>(nk, nseg) + 1;
   p.cap_tiles = (uint32_t)((n + TILE - 1) / TILE) + p.cap_seg;
+  p.cap_q = (uint32_t)std::min<uint64_t>(nseg, n / (small_keys + 1ull)) + 1;
   Workspace<K> w0 = layout<K>(p, sizeof(T), nullptr);
   rc = ensure_arena(ctx, w0.bytes);
   if (rc) return rc;
   Workspace<K> w = layout<K>(p, sizeof(T), ctx->arena);
-  const Caps caps{p.cap_seg, p.cap_tiles, p.nk, (uint32_t)(SMALL_SMEM / sizeof(K))};
+  const Caps caps{p.cap_seg, p.cap_tiles, p.nk, small_keys, tiny_keys<K>()};
   // the stream-ordered part: captured once and replayed when the call repeats
   auto enqueue = [&](cudaStream_t s) -> int {
     GGMS_CU(cudaMemsetAsync(w.C, 0, sizeof(Counters), s));
     ++ctx->launches;
-    k_init_seg<<<cdiv(nk, 256), 256, 0, s>>>(ks, nk, seg_off, k_off, nseg, w.krank, w.kseg, w.C);
-    ++ctx->launches;
-    seg_init<K><<<cdiv(nseg, 256), 256, 0, s>>>(seg_off, nseg, k_off, w.segs[0], w.tiles[0], w.C);
+    seg_init<K><<<cdiv(nseg, 256), 256, 0, s>>>(seg_off, nseg, k_off, w.segs[0], w.tiles[0], w.khead[0],
+                                                 w.smalls, w.tinies, w.bigs[0], p.cap_q, w.C, caps);
     ++ctx->launches;
     seg_set_count<<<1, 1, 0, s>>>(w.C, nseg);
-    const int maxlev = (sizeof(K) == 4) ? 3 : 6;  // radix shifts 21,10,0 / 53,42,31,20,9,0
+    ++ctx->launches;
+    k_init_seg<K><<<cdiv(nk, 256), 256, 0, s>>>(ks, nk, seg_off, k_off, nseg, w.segs[0], w.khead[0], w.knext,
+                                                 w.krank, w.kseg, w.C);
+    // small caller segments, straight from the input
+    rc = launch_small_select<T>(ctx, d_in, w.segs[0], w.khead[0], w, caps, s, k_off);
+    if (rc) return rc;
+    ++ctx->launches;
+    seg_sample<T><<<ctx->sms * 2, 1024, 0, s>>>(d_in, w.segs[0], w.bigs[0], w.C, p.cap_q, w.qtab, w.qdir,
+                                                 p.seed ^ 0x5E6A11ull);
+    // level 0 over the input with quantile bins; then radix levels over candidates
+    // (a child range of up to 2^bits keys needs ceil(bits / 11) more levels)
+    const int maxlev = 1 + (KeyBits<K>::value + RADIX_BITS - 1) / RADIX_BITS;
     const int lv_grid = ctx->sms * lv_mult;
     const int seg_grid = ctx->sms * 2;
     for (int l = 0; l < maxlev; ++l) {
       const int pp = l & 1, q = pp ^ 1;
       K* dst = w.cand[l & 1];
+      const K* src = w.cand[(l + 1) & 1];  // the previous level's candidates (l >= 1)
       ++ctx->launches;
-      lvl_prep<<<ctx->sms * 2, 256, 0, s>>>(w.rows[pp], w.aflag[pp], w.C, pp, caps);
-      if (l == 0) {
-          ++ctx->launches;
-          lvl_count<T, LV_NT><<<lv_grid, LV_NT, 0, s>>>(d_in, w.segs[pp], w.tiles[pp], w.C, pp, w.rows[pp], caps);
-        } else {
-          ++ctx->launches;
-          lvl_count<K, LV_NT><<<lv_grid, LV_NT, 0, s>>>(w.cand[(l - 1) & 1], w.segs[pp], w.tiles[pp],
-                                                         w.C, pp, w.rows[pp], caps);
-        }
+      lvl_prep<<<ctx->sms * 2, 256, 0, s>>>(w.rows[pp], w.aflag[pp], w.bigs[pp], w.C, pp, caps);
       ++ctx->launches;
-      lvl_scan<<<seg_grid, 1024, 0, s>>>(w.rows[pp], w.C, pp, caps);
+      if (l == 0)
+        lvl_count<T, LV_NT, true><<<lv_grid, LV_NT, 0, s>>>(d_in, w.segs[pp], w.tiles[pp], w.C, pp, w.rows[pp],
+                                                             caps, w.qtab, w.qdir);
+      else
+        lvl_count<K, LV_NT><<<lv_grid, LV_NT, 0, s>>>(src, w.segs[pp], w.tiles[pp], w.C, pp, w.rows[pp], caps,
+                                                       nullptr, nullptr);
+      ++ctx->launches;
+      lvl_scan<<<seg_grid, 1024, 0, s>>>(w.rows[pp], w.bigs[pp], w.C, pp, caps);
       ++ctx->launches;
       lvl_locate_rows<<<cdiv(nk, 256), 256, 0, s>>>(w.rows[pp], NBIN, nk, w.krank, w.kseg, w.kbin,
                                                        w.aflag[pp], NBIN_WORDS, w.C);
       ++ctx->launches;
-      lvl_children<K, 1024><<<seg_grid, 1024, 0, s>>>(w.rows[pp], w.aflag[pp], w.segs[pp], w.C, pp,
-                                                       w.segs[q], w.cursor[q], w.tiles[q], w.points,
-                                                       w.khead[q], w.smalls, caps);
+      if (l == 0)
+        lvl_children<K, 1024, true><<<seg_grid, 1024, 0, s>>>(w.rows[pp], w.aflag[pp], w.segs[pp], w.C, pp,
+                                                               w.segs[q], w.cursor[q], w.tiles[q], w.points,
+                                                               w.khead[q], w.smalls, w.tinies, w.bigs[pp],
+                                                               w.bigs[q], caps, w.qtab);
+      else
+        lvl_children<K, 1024><<<seg_grid, 1024, 0, s>>>(w.rows[pp], w.aflag[pp], w.segs[pp], w.C, pp,
+                                                         w.segs[q], w.cursor[q], w.tiles[q], w.points,
+                                                         w.khead[q], w.smalls, w.tinies, w.bigs[pp],
+                                                         w.bigs[q], caps, nullptr);
       ++ctx->launches;
       lvl_relabel<K><<<cdiv(nk, 256), 256, 0, s>>>(w.rows[pp], NBIN, nk, w.kbin, w.kseg, w.kkey,
                                                       w.points, w.C, w.segs[q], w.khead[q], w.knext);
       if (l + 1 < maxlev) {
         ++ctx->launches;
         if (l == 0)
-          lvl_compact<T, LV_NT><<<lv_grid, LV_NT, 0, s>>>(d_in, w.segs[pp], w.tiles[pp], w.C, pp,
-                                                           w.rows[pp], w.segs[q], w.cursor[q], dst, caps);
+          lvl_compact<T, LV_NT, true><<<lv_grid, LV_NT, 0, s>>>(d_in, w.segs[pp], w.tiles[pp], w.C, pp,
+                                                                 w.rows[pp], w.segs[q], w.cursor[q], dst, caps,
+                                                                 w.qtab, w.qdir);
         else
-          lvl_compact<K, LV_NT><<<lv_grid, LV_NT, 0, s>>>(w.cand[(l - 1) & 1], w.segs[pp], w.tiles[pp],
-                                                           w.C, pp, w.rows[pp], w.segs[q], w.cursor[q],
-                                                           dst, caps);
+          lvl_compact<K, LV_NT><<<lv_grid, LV_NT, 0, s>>>(src, w.segs[pp], w.tiles[pp], w.C, pp,
+                                                           w.rows[pp], w.segs[q], w.cursor[q], dst, caps,
+                                                           nullptr, nullptr);
         rc = launch_small_select<K>(ctx, dst, w.segs[q], w.khead[q], w, caps, s);
         if (rc) return rc;
       }

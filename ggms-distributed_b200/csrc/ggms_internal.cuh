@@ -272,7 +272,9 @@ struct Counters {
   uint32_t asg_choice;        // index of the assigner in use (0 sampled, 1 learned)
   uint32_t win_runs;          // PASS 1 window runs in use (0: no windows)
   uint32_t done;              // a refinement level found no segment: later levels are skipped
-  uint32_t pad1[5];
+  uint32_t ntiny;             // tiny segments created by the current level (batched path)
+  uint32_t nbig[2];           // segments of pool p that a level refines (listed in bigs[p])
+  uint32_t pad1[2];
 };
 
 // PASS 1 windows (l0_window).  From the sample, every requested k gets a
@@ -320,6 +322,23 @@ struct Caps {
   uint32_t tiles;
   uint32_t points;
   uint32_t small_keys;        // a child with at most this many keys is finished by small_select
+  uint32_t tiny_keys;         // ... and with at most this many by tiny_select (one warp); 0: never
 };
+
+// Level 0 of the batched path: a caller segment too large for small_select
+// gets QB bins whose boundaries are every second key of a sorted sample of
+// QSAMP of its keys (equal-mass bins whatever the distribution), and a
+// directory of QD cells, uniform in key over the sample's range, that gives
+// for each cell the boundaries below its first key -- a key's bin is then a
+// short search between two directory entries.
+constexpr uint32_t QB = NBIN;                   // bins (QB - 1 boundaries)
+constexpr uint32_t QSAMP = 2 * QB;              // sampled keys per segment
+constexpr int QD_BITS = 12;
+constexpr uint32_t QD = 1u << QD_BITS;          // directory cells
+constexpr uint32_t QDS = QD + 8;                // directory stride (QD + 1 entries, 16-byte rows)
+
+// Keys of one tiny segment (a warp's shared-memory slice of 8 KB).
+template <typename K>
+__host__ __device__ constexpr uint32_t tiny_keys() { return 8192u / (uint32_t)sizeof(K); }
 
 }  // namespace ggms

@@ -615,7 +615,7 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
                             uint32_t B, const Grid<K>* __restrict__ Gs, Counters* C,
                             const Windows<K>* __restrict__ Wg,
                             uint32_t* cmap0, Seg<K>* segs1, uint32_t* cursor1, TileRef* tiles1,
-                            K* points, uint32_t* khead1, uint32_t* smalls, Caps caps) {
+                            K* points, uint32_t* khead1, uint32_t* smalls, uint32_t* bigs1, Caps caps) {
   // the key-range searches below evaluate the grid ~64 times per bucket: keep
   // it in shared memory (every thread helps load it before any returns)
   __shared__ uint2 s1[GRID_T1];
@@ -672,6 +672,8 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
     if (si < caps.segs) smalls[si] = id; else set_status(C, GGMS_E_INTERNAL);
     return;
   }
+  const uint32_t bi = atomicAdd(&C->nbig[1], 1u);
+  if (bi < caps.segs) bigs1[bi] = id; else set_status(C, GGMS_E_INTERNAL);
   const uint32_t nt = (cnt + TILE - 1) / TILE;
   const uint32_t t0 = atomicAdd(&C->ntiles[1], nt);
   if (t0 + nt > caps.tiles || t0 + nt < t0) { set_status(C, GGMS_E_INTERNAL); return; }
@@ -803,6 +805,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
     if (lane == 0) wpre[B / 32] = run;
   }
   __syncthreads();
+  const uint32_t ncopied = wpre[B / 32];  // read before the queues reuse the table
   // with windows, a key outside every run belongs to its gap's bucket
   auto bmap = [&](uint32_t b) { return W.on ? win_map(W, b) : b; };
   {
@@ -903,7 +906,39 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
     }
     stream_keys<T, UNROLL>(vp, rounds, gstride, wq, qn, lane, t, bucket_and_put);
   };
-  if (use_win) {
+  // Most buckets copied: every key takes the long path anyway, so the queue
+  // only serialises it; each lane buckets its keys directly, all EPV of a
+  // vector at once (independent lookups in flight).
+  auto dense = [&]() {
+    constexpr int DU = UNROLL < 4 ? UNROLL : 4;  // vectors in flight (the same elements as PASS 1)
+    const uint4* dp = vp;
+    for (uint64_t r = 0; r < rounds; ++r, dp += gstride * UNROLL) {
+#pragma unroll
+      for (int u0 = 0; u0 < UNROLL; u0 += DU) {
+      uint4 q[DU];
+#pragma unroll
+      for (int u = 0; u < DU; ++u) q[u] = ld_stream16(dp + (u0 + u) * gstride);
+#pragma unroll
+      for (int u = 0; u < DU; ++u) {
+        T e[EPV];
+        unpack16<T>(q[u], e);
+        K kk[EPV];
+        uint32_t b[EPV];
+#pragma unroll
+        for (int t = 0; t < EPV; ++t) {
+          kk[t] = KeyOf<T>::to(e[t]);
+          b[t] = bmap(min(grid_eval<K>(gv, kk[t]), B - 1u));
+        }
+#pragma unroll
+        for (int t = 0; t < EPV; ++t)
+          if ((amask[b[t] >> 5] >> (b[t] & 31)) & 1u) put(b[t], kk[t]);
+      }
+      }
+    }
+  };
+  if (!use_win && nruns > L0_RUNS && ncopied * 2u >= B) {
+    dense();
+  } else if (use_win) {
     switch (W.R) {
       case 1: runs(std::integral_constant<uint32_t, 1>{}, true); break;
       case 2: runs(std::integral_constant<uint32_t, 2>{}, true); break;
@@ -949,49 +984,158 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
 // Gate of a refinement level inside a captured CUDA graph: the level (an IF
 // node) runs only while every level so far had segments to refine.
 __global__ void lvl_gate(Counters* C, int p, cudaGraphConditionalHandle h) {
-  if (C->nsegs[p] == 0u) C->done = 1u;
+  if (C->nbig[p] == 0u) C->done = 1u;
   cudaGraphSetConditional(h, C->done ? 0u : 1u);
 }
 
-// zero this level's histogram rows / flags; reset the child pool's counters
-__global__ void lvl_prep(uint32_t* rows, uint32_t* aflag, Counters* C, int p, Caps caps) {
-  const uint32_t ns = min(C->nsegs[p], caps.segs);
-  const size_t words = (size_t)ns * NBIN;
-  const size_t fw = (size_t)ns * NBIN_WORDS;
-  const size_t gt = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const size_t gs = (size_t)gridDim.x * blockDim.x;
-  for (size_t i = gt; i < words; i += gs) rows[i] = 0u;
-  for (size_t i = gt; i < fw; i += gs) aflag[i] = 0u;
-  if (gt == 0) {
+// zero this level's histogram rows / flags (segments that small_select or
+// tiny_select finished have none); reset the child pool's counters
+__global__ void lvl_prep(uint32_t* rows, uint32_t* aflag, const uint32_t* __restrict__ bigs, Counters* C,
+                         int p, Caps caps) {
+  const uint32_t nb = min(C->nbig[p], caps.segs);
+  for (uint32_t j = blockIdx.x; j < nb; j += gridDim.x) {
+    const uint32_t sid = bigs[j];
+    uint32_t* row = rows + (size_t)sid * NBIN;
+    for (uint32_t i = threadIdx.x; i < NBIN; i += blockDim.x) row[i] = 0u;
+    for (uint32_t i = threadIdx.x; i < NBIN_WORDS; i += blockDim.x) aflag[(size_t)sid * NBIN_WORDS + i] = 0u;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
     C->nsegs[p ^ 1] = 0u;
     C->ntiles[p ^ 1] = 0u;
+    C->nbig[p ^ 1] = 0u;
     C->nsmall = 0u;
-    if (ns) C->levels_run += 1u;
+    C->ntiny = 0u;
+    if (nb) C->levels_run += 1u;
+  }
+}
+
+// Bin of a key in a quantile segment: the number of boundaries <= key.  The
+// directory cell of the key bounds the search: boundaries before qd[c] lie
+// below the cell's first key, those from qd[c + 1] on above its last.
+template <typename K>
+__device__ __forceinline__ uint32_t qbin(K key, K kmin, uint32_t dsh, const K* qb, const uint16_t* qd) {
+  const K d = key > kmin ? (K)(key - kmin) : (K)0;
+  const K cc = d >> dsh;
+  const uint32_t c = cc < (K)QD ? (uint32_t)cc : QD - 1u;
+  uint32_t lo = qd[c], hi = qd[c + 1];
+  while (lo < hi) {
+    const uint32_t m = (lo + hi) >> 1;
+    if (qb[m] <= key) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+
+// Boundaries and directory of quantile segment q into shared memory.
+template <typename K>
+__device__ __forceinline__ void qtab_to_smem(const K* __restrict__ qtab, const uint16_t* __restrict__ qdir,
+                                             uint32_t q, K* qb, uint16_t* qd) {
+  const K* tb = qtab + (size_t)q * QB;
+  for (uint32_t i = threadIdx.x; i < QB; i += blockDim.x) qb[i] = tb[i];
+  const uint4* dr = reinterpret_cast<const uint4*>(qdir + (size_t)q * QDS);
+  uint4* dd = reinterpret_cast<uint4*>(qd);
+  for (uint32_t i = threadIdx.x; i < QDS / 8; i += blockDim.x) dd[i] = dr[i];
+}
+
+// Sample-quantile bins of the batched level 0: one CTA per large caller
+// segment draws QSAMP keys (one from each of QSAMP equal strata, at a hashed
+// offset inside it), sorts them, and writes the QB - 1 boundaries and the
+// directory; the segment's lo / shift become the directory's origin / cell
+// shift and pad its table index.
+template <typename T>
+__global__ __launch_bounds__(1024) void seg_sample(const T* __restrict__ in, Seg<typename KeyOf<T>::K>* segs0,
+                                                   const uint32_t* __restrict__ qsegs,
+                                                   const Counters* __restrict__ C, uint32_t cap_q,
+                                                   typename KeyOf<T>::K* qtab, uint16_t* qdir, uint64_t seed) {
+  using K = typename KeyOf<T>::K;
+  __shared__ K sv[QSAMP];
+  const uint32_t tid = threadIdx.x;
+  const uint32_t nq = min(C->nbig[0], cap_q);
+  for (uint32_t q = blockIdx.x; q < nq; q += gridDim.x) {
+    const uint32_t sid = qsegs[q];
+    Seg<K> s = segs0[sid];
+    for (uint32_t i = tid; i < QSAMP; i += 1024) {
+      const uint64_t a = (uint64_t)s.cnt * i / QSAMP, b = (uint64_t)s.cnt * (i + 1) / QSAMP;
+      const uint64_t h = mix64(seed ^ ((uint64_t)sid << 32) ^ i);
+      const uint64_t pos = b > a ? a + h % (b - a) : a;
+      sv[i] = KeyOf<T>::to(in[s.off + pos]);
+    }
+    __syncthreads();
+    for (uint32_t kk = 2; kk <= QSAMP; kk <<= 1) {
+      for (uint32_t jj = kk >> 1; jj > 0; jj >>= 1) {
+        for (uint32_t i = tid; i < QSAMP; i += 1024) {
+          const uint32_t ixj = i ^ jj;
+          if (ixj > i) {
+            const K a = sv[i], b = sv[ixj];
+            if ((a > b) == ((i & kk) == 0)) { sv[i] = b; sv[ixj] = a; }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    K* tb = qtab + (size_t)q * QB;
+    for (uint32_t j = tid; j < QB; j += 1024) tb[j] = (j + 1 < QB) ? sv[2 * j + 2] : key_max<K>();
+    const K kmin = sv[0], kmax = sv[QSAMP - 1];
+    const uint32_t dsh = (uint32_t)max(0, bitlen((K)(kmax - kmin)) - QD_BITS);
+    uint16_t* dr = qdir + (size_t)q * QDS;
+    for (uint32_t c = tid; c < QDS; c += 1024) {
+      uint32_t v = QB - 1u;  // past the range (or padding): every boundary is below
+      const K off = (K)((K)c << dsh);
+      if (c < QD && ((off >> dsh) == (K)c) && off <= (K)(key_max<K>() - kmin)) {
+        const K start = (K)(kmin + off);
+        uint32_t lo = 0, hi = QB - 1u;  // boundaries j < lo are < start
+        while (lo < hi) {
+          const uint32_t m = (lo + hi) >> 1;
+          if (sv[2 * m + 2] < start) lo = m + 1; else hi = m;
+        }
+        v = lo;
+      }
+      dr[c] = (uint16_t)v;
+    }
+    if (tid == 0) {
+      s.lo = kmin;
+      s.shift = dsh;
+      s.pad = q;
+      segs0[sid] = s;
+    }
+    __syncthreads();
   }
 }
 
 // Histogram of radix bins, one tile of one segment per iteration.
-template <typename InT, int NT>
+// Q: the level's segments have quantile bins (batched level 0), else radix
+// bins (key - lo) >> shift.
+template <typename InT, int NT, bool Q = false>
 __global__ __launch_bounds__(NT) void lvl_count(const InT* __restrict__ src,
                                                const Seg<typename KeyOf<InT>::K>* __restrict__ segs,
                                                const TileRef* __restrict__ tiles,
-                                               Counters* C, int p, uint32_t* rows, Caps caps) {
+                                               Counters* C, int p, uint32_t* rows, Caps caps,
+                                               const typename KeyOf<InT>::K* __restrict__ qtab,
+                                               const uint16_t* __restrict__ qdir) {
   using K = typename KeyOf<InT>::K;
   __shared__ uint32_t h[NBIN];
+  __shared__ __align__(16) K qb[Q ? QB : 1];
+  __shared__ __align__(16) uint16_t qd[Q ? QDS : 8];
   const uint32_t nt = min(C->ntiles[p], caps.tiles);
   const uint32_t ns = min(C->nsegs[p], caps.segs);
+  uint32_t loaded = 0xFFFFFFFFu;  // quantile table in shared memory
   for (uint32_t t = blockIdx.x; t < nt; t += gridDim.x) {
     const TileRef tr = tiles[t];
     if (tr.seg >= ns) continue;  // only after a capacity error (status already set)
     const Seg<K> s = segs[tr.seg];
+    if (Q && s.pad != loaded) {  // the previous tile ended with a barrier
+      qtab_to_smem<K>(qtab, qdir, s.pad, qb, qd);
+      loaded = s.pad;
+    }
     for (uint32_t i = threadIdx.x; i < NBIN; i += NT) h[i] = 0u;
     __syncthreads();
     const uint64_t beg = s.off + (uint64_t)tr.no * TILE;
     const uint64_t end = min(beg + TILE, s.off + s.cnt);
     for (uint64_t i = beg + threadIdx.x; i < end; i += NT) {
       K key = KeyOf<InT>::to(src[i]);
-      uint32_t bin = (uint32_t)((K)(key - s.lo) >> s.shift);
-      atomicAdd(&h[min(bin, (uint32_t)NBIN - 1u)], 1u);
+      uint32_t bin;
+      if (Q) bin = qbin<K>(key, s.lo, s.shift, qb, qd);
+      else bin = min((uint32_t)((K)(key - s.lo) >> s.shift), (uint32_t)NBIN - 1u);
+      atomicAdd(&h[bin], 1u);
     }
     __syncthreads();
     uint32_t* row = rows + (size_t)tr.seg * NBIN;
@@ -1004,26 +1148,28 @@ __global__ __launch_bounds__(NT) void lvl_count(const InT* __restrict__ src,
   }
 }
 
-__global__ __launch_bounds__(1024) void lvl_scan(uint32_t* rows, const Counters* __restrict__ C, int p,
-                                                  Caps caps) {
+__global__ __launch_bounds__(1024) void lvl_scan(uint32_t* rows, const uint32_t* __restrict__ bigs,
+                                                  const Counters* __restrict__ C, int p, Caps caps) {
   __shared__ uint32_t w[72];
-  const uint32_t ns = min(C->nsegs[p], caps.segs);
-  for (uint32_t s = blockIdx.x; s < ns; s += gridDim.x)
-    block_inclusive_scan_global<1024>(rows + (size_t)s * NBIN, NBIN, w, nullptr);
+  const uint32_t nb = min(C->nbig[p], caps.segs);
+  for (uint32_t j = blockIdx.x; j < nb; j += gridDim.x)
+    block_inclusive_scan_global<1024>(rows + (size_t)bigs[j] * NBIN, NBIN, w, nullptr);
 }
 
 // Active bins of each segment -> child segments (pool q) or points.  One CTA
 // per segment; the row holding the inclusive counts is overwritten by the
 // child map (each entry read before any is written).
-template <typename K, int NT>
+template <typename K, int NT, bool Q = false>
 __global__ __launch_bounds__(NT) void lvl_children(uint32_t* rows, const uint32_t* __restrict__ aflag,
                                                   const Seg<K>* __restrict__ segs, Counters* C, int p,
                                                   Seg<K>* segs_q, uint32_t* cursor_q, TileRef* tiles_q,
                                                   K* points, uint32_t* khead_q, uint32_t* smalls,
-                                                  Caps caps) {
+                                                  uint32_t* tinies, const uint32_t* __restrict__ bigs,
+                                                  uint32_t* bigs_q, Caps caps, const K* __restrict__ qtab) {
   constexpr int PER = NBIN / NT;
-  const uint32_t ns = min(C->nsegs[p], caps.segs);
-  for (uint32_t sid = blockIdx.x; sid < ns; sid += gridDim.x) {
+  const uint32_t nb = min(C->nbig[p], caps.segs);
+  for (uint32_t j = blockIdx.x; j < nb; j += gridDim.x) {
+    const uint32_t sid = bigs[j];
     const Seg<K> s = segs[sid];
     if (s.small) continue;  // finished by small_select
     uint32_t* I = rows + (size_t)sid * NBIN;
@@ -1036,9 +1182,20 @@ __global__ __launch_bounds__(NT) void lvl_children(uint32_t* rows, const uint32_
       if (!((F[b >> 5] >> (b & 31)) & 1u)) continue;
       const uint32_t start = b ? I[b - 1] : 0u;
       const uint32_t cnt = I[b] - start;
-      const K blo = s.lo + ((K)b << s.shift);
-      const K width_m1 = (K)(((K)1 << s.shift) - 1);
-      K bhi = (key_max<K>() - blo < width_m1) ? key_max<K>() : (K)(blo + width_m1);
+      K blo, bhi;
+      if (Q) {  // [boundary b - 1, boundary b - 1]; the outer bins reach the ends of the key space
+        const K* tb = qtab + (size_t)s.pad * QB;
+        blo = b ? tb[b - 1] : (K)0;
+        bhi = (b + 1u < QB) ? (K)(tb[b] - 1u) : key_max<K>();
+        if (b + 1u < QB && tb[b] <= blo) {  // an empty bin cannot hold a k
+          set_status(C, GGMS_E_INTERNAL);
+          continue;
+        }
+      } else {
+        blo = s.lo + ((K)b << s.shift);
+        const K width_m1 = (K)(((K)1 << s.shift) - 1);
+        bhi = (key_max<K>() - blo < width_m1) ? key_max<K>() : (K)(blo + width_m1);
+      }
       if (bhi > s.hi) bhi = s.hi;
       if (blo == bhi) {
         uint32_t pid = atomicAdd(&C->npoints, 1u);
@@ -1062,10 +1219,13 @@ __global__ __launch_bounds__(NT) void lvl_children(uint32_t* rows, const uint32_
       khead_q[id] = K_NIL;
       out[u] = id;
       if (c.small) {
-        const uint32_t si = atomicAdd(&C->nsmall, 1u);
-        if (si < caps.segs) smalls[si] = id; else set_status(C, GGMS_E_INTERNAL);
+        const bool tiny = cnt <= caps.tiny_keys;
+        const uint32_t si = atomicAdd(tiny ? &C->ntiny : &C->nsmall, 1u);
+        if (si < caps.segs) (tiny ? tinies : smalls)[si] = id; else set_status(C, GGMS_E_INTERNAL);
         continue;
       }
+      const uint32_t bi = atomicAdd(&C->nbig[p ^ 1], 1u);
+      if (bi < caps.segs) bigs_q[bi] = id; else set_status(C, GGMS_E_INTERNAL);
       const uint32_t nt = (cnt + TILE - 1) / TILE;
       const uint32_t t0 = atomicAdd(&C->ntiles[p ^ 1], nt);
       if (t0 + nt > caps.tiles || t0 + nt < t0) { set_status(C, GGMS_E_INTERNAL); continue; }
@@ -1079,7 +1239,7 @@ __global__ __launch_bounds__(NT) void lvl_children(uint32_t* rows, const uint32_
 }
 
 // Copies each key whose bin became a child segment into that child's region.
-template <typename InT, int NT>
+template <typename InT, int NT, bool Q = false>
 __global__ __launch_bounds__(NT) void lvl_compact(const InT* __restrict__ src,
                                                  const Seg<typename KeyOf<InT>::K>* __restrict__ segs,
                                                  const TileRef* __restrict__ tiles,
@@ -1087,44 +1247,62 @@ __global__ __launch_bounds__(NT) void lvl_compact(const InT* __restrict__ src,
                                                  const uint32_t* __restrict__ rows,
                                                  const Seg<typename KeyOf<InT>::K>* __restrict__ segs_q,
                                                  uint32_t* cursor_q, typename KeyOf<InT>::K* dst,
-                                                 Caps caps) {
+                                                 Caps caps, const typename KeyOf<InT>::K* __restrict__ qtab,
+                                                 const uint16_t* __restrict__ qdir) {
   using K = typename KeyOf<InT>::K;
   __shared__ uint32_t cm[NBIN];
+  __shared__ __align__(16) K qb[Q ? QB : 1];
+  __shared__ __align__(16) uint16_t qd[Q ? QDS : 8];
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t nt = min(C->ntiles[p], caps.tiles);
   const uint32_t ns = min(C->nsegs[p], caps.segs);
+  uint32_t loaded = 0xFFFFFFFFu;  // segment whose child map (and table) is in shared memory
   for (uint32_t t = blockIdx.x; t < nt; t += gridDim.x) {
     const TileRef tr = tiles[t];
     if (tr.seg >= ns) continue;  // only after a capacity error (status already set)
     const Seg<K> s = segs[tr.seg];
-    const uint32_t* row = rows + (size_t)tr.seg * NBIN;
-    for (uint32_t i = threadIdx.x; i < NBIN; i += NT) cm[i] = row[i];
+    if (tr.seg != loaded) {  // the previous tile ended with a barrier
+      const uint32_t* row = rows + (size_t)tr.seg * NBIN;
+      for (uint32_t i = threadIdx.x; i < NBIN; i += NT) cm[i] = row[i];
+      if (Q) qtab_to_smem<K>(qtab, qdir, s.pad, qb, qd);
+      loaded = tr.seg;
+    }
     __syncthreads();
     const uint64_t beg = s.off + (uint64_t)tr.no * TILE;
     const uint64_t end = min(beg + TILE, s.off + s.cnt);
-    const uint64_t span = ((end - beg + NT - 1) / NT) * NT;
-    for (uint64_t o = threadIdx.x; o < span; o += NT) {
-      const uint64_t i = beg + o;
-      const bool valid = i < end;
-      K key = 0;
-      uint32_t c = CM_NONE;
-      if (valid) {
-        key = KeyOf<InT>::to(src[i]);
-        uint32_t bin = (uint32_t)((K)(key - s.lo) >> s.shift);
-        c = cm[min(bin, (uint32_t)NBIN - 1u)];
+    constexpr int U = 4;  // loads in flight per thread before the warp-synchronous part
+    const uint64_t span = ((end - beg + NT * U - 1) / (NT * U)) * (NT * U);
+    for (uint64_t o = threadIdx.x; o < span; o += NT * U) {
+      K kk[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const uint64_t i = beg + o + (uint64_t)u * NT;
+        kk[u] = i < end ? KeyOf<InT>::to(src[i]) : (K)0;
       }
-      const bool hit = valid && c < CM_POINT;
-      const uint32_t hm = __ballot_sync(FULL, hit);
-      if (hm && hit) {
-        const uint32_t peers = __match_any_sync(hm, c);
-        const int leader = __ffs(peers) - 1;
-        uint32_t basepos = 0;
-        if ((int)lane == leader) basepos = atomicAdd(&cursor_q[c], (uint32_t)__popc(peers));
-        basepos = __shfl_sync(peers, basepos, leader);
-        const uint32_t slot = basepos + __popc(peers & lanemask_lt());
-        const Seg<K>& sg = segs_q[c];
-        if (slot < sg.cnt) dst[sg.off + slot] = key;
-        else set_status(const_cast<Counters*>(C), GGMS_E_INTERNAL);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const bool valid = beg + o + (uint64_t)u * NT < end;
+        const K key = kk[u];
+        uint32_t c = CM_NONE;
+        if (valid) {
+          uint32_t bin;
+          if (Q) bin = qbin<K>(key, s.lo, s.shift, qb, qd);
+          else bin = min((uint32_t)((K)(key - s.lo) >> s.shift), (uint32_t)NBIN - 1u);
+          c = cm[bin];
+        }
+        const bool hit = valid && c < CM_POINT;
+        const uint32_t hm = __ballot_sync(FULL, hit);
+        if (hm && hit) {
+          const uint32_t peers = __match_any_sync(hm, c);
+          const int leader = __ffs(peers) - 1;
+          uint32_t basepos = 0;
+          if ((int)lane == leader) basepos = atomicAdd(&cursor_q[c], (uint32_t)__popc(peers));
+          basepos = __shfl_sync(peers, basepos, leader);
+          const uint32_t slot = basepos + __popc(peers & lanemask_lt());
+          const Seg<K>& sg = segs_q[c];
+          if (slot < sg.cnt) dst[sg.off + slot] = key;
+          else set_status(const_cast<Counters*>(C), GGMS_E_INTERNAL);
+        }
       }
     }
     __syncthreads();
@@ -1144,21 +1322,24 @@ constexpr int SS_GROUP = 16;
 constexpr int SS_MAXK = 256;
 constexpr int SS_SORT_ABOVE = 64;   // more ks than this in one segment: bitonic sort instead
 
-template <typename K, int NT>
-__global__ __launch_bounds__(NT) void small_select(const K* __restrict__ src,
-                                                  const Seg<K>* __restrict__ segs_q,
+template <typename InT, int NT>
+__global__ __launch_bounds__(NT) void small_select(const InT* __restrict__ src,
+                                                  const Seg<typename KeyOf<InT>::K>* __restrict__ segs_q,
                                                   const uint32_t* __restrict__ smalls,
                                                   const Counters* __restrict__ C_,
                                                   const uint32_t* __restrict__ khead_q,
                                                   const uint32_t* __restrict__ knext,
+                                                  const int64_t* __restrict__ k_off,
                                                   const uint32_t* __restrict__ k_rank, uint32_t* k_seg,
-                                                  K* k_key, uint32_t small_keys, Caps caps) {
+                                                  typename KeyOf<InT>::K* k_key, uint32_t small_keys,
+                                                  Caps caps) {
+  using K = typename KeyOf<InT>::K;
   Counters* C = const_cast<Counters*>(C_);
   extern __shared__ __align__(16) uint8_t smem[];
   K* vals = (K*)smem;
   uint32_t* hist = (uint32_t*)(smem + SMALL_SMEM);           // [SS_GROUP][256]
   __shared__ uint32_t kid[SS_MAXK];
-  __shared__ uint32_t nk_s, next_s;
+  __shared__ uint32_t nk_s, next_s, kend_s;
   __shared__ uint32_t rk[SS_GROUP];
   __shared__ K pk[SS_GROUP];
   __shared__ K upk[SS_GROUP];       // distinct prefixes of the current round
@@ -1176,7 +1357,7 @@ __global__ __launch_bounds__(NT) void small_select(const K* __restrict__ src,
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const uint32_t i = i0 + q * NT;
-        v[q] = i < cnt ? src[s.off + i] : s.lo;
+        v[q] = i < cnt ? KeyOf<InT>::to(src[s.off + i]) : s.lo;
       }
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
@@ -1186,11 +1367,27 @@ __global__ __launch_bounds__(NT) void small_select(const K* __restrict__ src,
     }
     const int bits = bitlen((K)(s.hi - s.lo));
     bool sorted_seg = false;
-    if (tid == 0) next_s = khead_q[id];
+    if (tid == 0) {  // the ks: the segment's list, or (k_off: a caller segment) its k range
+      if (k_off) {
+        const uint32_t k0 = (uint32_t)k_off[id], k1 = (uint32_t)k_off[id + 1];
+        next_s = k0 < k1 ? k0 : K_NIL;
+        kend_s = k1;
+      } else {
+        next_s = khead_q[id];
+      }
+    }
     __syncthreads();
     while (next_s != K_NIL) {
       __syncthreads();
-      if (tid == 0) {  // collect up to SS_MAXK ks from the list
+      if (k_off) {  // the next up to SS_MAXK ks of the range
+        const uint32_t k0 = next_s, m = min((uint32_t)SS_MAXK, kend_s - k0);
+        for (uint32_t j = tid; j < m; j += NT) kid[j] = k0 + j;
+        __syncthreads();
+        if (tid == 0) {
+          nk_s = m;
+          next_s = (k0 + m < kend_s) ? k0 + m : K_NIL;
+        }
+      } else if (tid == 0) {  // collect up to SS_MAXK ks from the list
         uint32_t k = next_s, m = 0;
         while (k != K_NIL && m < (uint32_t)SS_MAXK) { kid[m++] = k; k = knext[k]; }
         nk_s = m;
@@ -1309,13 +1506,177 @@ __global__ __launch_bounds__(NT) void small_select(const K* __restrict__ src,
   }
 }
 
+// One warp finishes a whole tiny segment (at most tiny_keys<K>() keys, as
+// offsets from its lo, in the warp's slice of shared memory).  With few ks: per
+// k, a radix select with 8-bit digits from the top of the segment's range (one
+// warp-private 256-bin histogram per digit).  With more than TS_SORT_ABOVE ks
+// (caller segments of the batched path): the slice is bitonic-sorted once and
+// the lanes read their ks' answers from it.  The ks come from the segment's
+// list, or (k_off given: the segments are the caller's) from its k range.
+constexpr int TS_NT = 128;
+constexpr uint32_t TS_SORT_ABOVE = 8;
+
+template <typename K>
+__device__ __forceinline__ K warp_radix_select(const K* v, uint32_t cnt, int bits, uint32_t r, uint32_t* h,
+                                               uint32_t lane, bool* ok) {
+  K pre = 0;
+  for (int top = bits; top > 0;) {
+    const int width = min(8, top);
+    const int sh = top - width;
+    const uint32_t dmask = (1u << width) - 1u;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) h[lane * 8 + q] = 0u;
+    __syncwarp();
+    for (uint32_t i = lane; i < cnt; i += 32) {
+      const K x = v[i];
+      if ((((x ^ pre) >> sh) >> width) == 0) atomicAdd(&h[(uint32_t)(x >> sh) & dmask], 1u);
+    }
+    __syncwarp();
+    uint32_t c8[8], sum = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) { c8[q] = h[lane * 8 + q]; sum += c8[q]; }
+    uint32_t inc = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t tt = __shfl_up_sync(FULL, inc, o);
+      if ((int)lane >= o) inc += tt;
+    }
+    const uint32_t before = inc - sum;
+    const bool mine = before <= r && r < inc;
+    const uint32_t who = __ballot_sync(FULL, mine);
+    uint32_t d = 0, nr = 0;
+    if (mine) {
+      uint32_t cum = before;
+      d = lane * 8 + 7;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        if (r < cum + c8[q]) { d = lane * 8 + q; break; }
+        cum += c8[q];
+      }
+      nr = r - cum;
+    }
+    const int owner = who ? __ffs(who) - 1 : 0;
+    d = __shfl_sync(FULL, d, owner);
+    nr = __shfl_sync(FULL, nr, owner);
+    __syncwarp();  // every lane has read the histogram before the next digit clears it
+    if (!who) {    // rank beyond the segment (warp-uniform)
+      *ok = false;
+      return pre;
+    }
+    r = nr;
+    pre = pre | ((K)d << sh);
+    top = sh;
+  }
+  *ok = true;
+  return pre;
+}
+
+template <typename InT, int NT>
+__global__ __launch_bounds__(NT) void tiny_select(const InT* __restrict__ src,
+                                                 const Seg<typename KeyOf<InT>::K>* __restrict__ segs_q,
+                                                 const uint32_t* __restrict__ tinies,
+                                                 const Counters* __restrict__ C_,
+                                                 const uint32_t* __restrict__ khead_q,
+                                                 const uint32_t* __restrict__ knext,
+                                                 const int64_t* __restrict__ k_off,
+                                                 const uint32_t* __restrict__ k_rank, uint32_t* k_seg,
+                                                 typename KeyOf<InT>::K* k_key, Caps caps) {
+  using K = typename KeyOf<InT>::K;
+  constexpr uint32_t TK = tiny_keys<K>();
+  constexpr int NW = NT / 32;
+  __shared__ K buf[NW][TK];
+  __shared__ uint32_t hist[NW][256];
+  Counters* C = const_cast<Counters*>(C_);
+  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  K* v = buf[wid];
+  uint32_t* h = hist[wid];
+  const uint32_t nt = min(C->ntiny, caps.segs);
+  for (uint32_t t = blockIdx.x * NW + wid; t < nt; t += gridDim.x * NW) {
+    const uint32_t id = tinies[t];
+    const Seg<K> s = segs_q[id];
+    const uint32_t cnt = s.cnt;
+    if (cnt > TK) {  // cannot happen: tiny segments are created with cnt <= tiny_keys
+      if (lane == 0) set_status(C, GGMS_E_INTERNAL);
+      continue;
+    }
+    for (uint32_t i0 = lane; i0 < cnt; i0 += 32 * 8) {  // eight independent loads in flight
+      K x[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const uint32_t i = i0 + q * 32;
+        x[q] = i < cnt ? KeyOf<InT>::to(src[s.off + i]) : s.lo;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const uint32_t i = i0 + q * 32;
+        if (i < cnt) v[i] = (K)(x[q] - s.lo);
+      }
+    }
+    __syncwarp();
+    const int bits = bitlen((K)(s.hi - s.lo));
+    if (k_off) {
+      const int64_t k0 = k_off[id], k1 = k_off[id + 1];
+      if ((uint64_t)(k1 - k0) > TS_SORT_ABOVE) {
+        uint32_t N = 32;
+        while (N < cnt) N <<= 1;
+        for (uint32_t i = cnt + lane; i < N; i += 32) v[i] = key_max<K>();
+        __syncwarp();
+        for (uint32_t kk = 2; kk <= N; kk <<= 1) {
+          for (uint32_t jj = kk >> 1; jj > 0; jj >>= 1) {
+            for (uint32_t i = lane; i < N; i += 32) {
+              const uint32_t ixj = i ^ jj;
+              if (ixj > i) {
+                const K a = v[i], b = v[ixj];
+                if ((a > b) == ((i & kk) == 0)) { v[i] = b; v[ixj] = a; }
+              }
+            }
+            __syncwarp();
+          }
+        }
+        for (int64_t k = k0 + lane; k < k1; k += 32) {
+          if (k_seg[k] == K_DONE) continue;  // an invalid k (status already set)
+          const uint32_t r = k_rank[k];
+          if (r < cnt) k_key[k] = (K)(s.lo + v[r]); else set_status(C, GGMS_E_INTERNAL);
+          k_seg[k] = K_DONE;
+        }
+      } else {
+        for (int64_t k = k0; k < k1; ++k) {
+          if (k_seg[k] == K_DONE) continue;  // warp-uniform
+          bool ok = false;
+          const uint32_t r = k_rank[k];
+          const K pre = r < cnt ? warp_radix_select<K>(v, cnt, bits, r, h, lane, &ok) : (K)0;
+          if (lane == 0) {
+            if (ok) k_key[k] = (K)(s.lo + pre); else set_status(C, GGMS_E_INTERNAL);
+            k_seg[k] = K_DONE;
+          }
+        }
+      }
+    } else {
+      for (uint32_t k = khead_q[id]; k != K_NIL; k = knext[k]) {
+        bool ok = false;
+        const uint32_t r = k_rank[k];
+        const K pre = r < cnt ? warp_radix_select<K>(v, cnt, bits, r, h, lane, &ok) : (K)0;
+        if (lane == 0) {
+          if (ok) k_key[k] = (K)(s.lo + pre); else set_status(C, GGMS_E_INTERNAL);
+          k_seg[k] = K_DONE;
+        }
+      }
+    }
+    __syncwarp();  // the slice is reloaded by the warp's next segment
+    if (lane == 0) atomicAdd(&C->small_segs, 1u);
+  }
+}
+
 // ------------------------------------------------------------------ batched segments
-// Level 0 of the batched mode: every caller segment that holds a k becomes a
-// radix segment over the whole key space (top 11 key bits first).
+// Level 0 of the batched mode.  A caller segment that holds a k is finished
+// directly from the input when it is small (tiny_select for tiny ones,
+// small_select otherwise); a larger one gets quantile bins (seg_sample fills
+// its table) and tiles for the level-0 count.
 template <typename K>
 __global__ void seg_init(const int64_t* __restrict__ seg_off, uint32_t nseg,
                          const int64_t* __restrict__ k_off, Seg<K>* segs0, TileRef* tiles0,
-                         Counters* C) {
+                         uint32_t* khead0, uint32_t* smalls, uint32_t* tinies, uint32_t* bigs0,
+                         uint32_t cap_q, Counters* C, Caps caps) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nseg) return;
   const int64_t a = seg_off[s], b = seg_off[s + 1];
@@ -1324,23 +1685,49 @@ __global__ void seg_init(const int64_t* __restrict__ seg_off, uint32_t nseg,
   d.cnt = (b > a) ? (uint32_t)(b - a) : 0u;
   d.lo = 0;
   d.hi = key_max<K>();
-  d.shift = (uint32_t)(KeyBits<K>::value - RADIX_BITS);
+  d.shift = 0u;
   d.small = 0u;
   d.pad = 0u;
-  segs0[s] = d;
+  khead0[s] = K_NIL;
   if (b < a) set_status(C, GGMS_E_INVALID_ARG);
-  if (k_off[s + 1] == k_off[s] || d.cnt == 0) return;  // nothing to select here
+  if (k_off[s + 1] == k_off[s] || d.cnt == 0) {  // nothing to select here
+    d.small = 1u;  // no row, no tiles
+    segs0[s] = d;
+    return;
+  }
+  if (d.cnt <= caps.small_keys) {
+    d.small = 1u;
+    segs0[s] = d;
+    const bool tiny = d.cnt <= caps.tiny_keys;
+    const uint32_t si = atomicAdd(tiny ? &C->ntiny : &C->nsmall, 1u);
+    if (si < caps.segs) (tiny ? tinies : smalls)[si] = s; else set_status(C, GGMS_E_INTERNAL);
+    return;
+  }
+  const uint32_t q = atomicAdd(&C->nbig[0], 1u);  // its quantile table: q
+  if (q < caps.segs) bigs0[q] = s;
+  if (q >= cap_q) {  // cannot happen: cap_q bounds the segments above small_keys
+    set_status(C, GGMS_E_INTERNAL);
+    d.small = 1u;
+    segs0[s] = d;
+    return;
+  }
+  d.pad = q;
+  segs0[s] = d;
   const uint32_t nt = (d.cnt + TILE - 1) / TILE;
   const uint32_t t0 = atomicAdd(&C->ntiles[0], nt);
+  if (t0 + nt > caps.tiles) { set_status(C, GGMS_E_INTERNAL); return; }
   for (uint32_t t = 0; t < nt; ++t) tiles0[t0 + t] = TileRef{s, t};
 }
 
 __global__ void seg_set_count(Counters* C, uint32_t nseg) { C->nsegs[0] = nseg; }
 
-// k i belongs to the segment s with k_off[s] <= i < k_off[s+1].
+// k i belongs to the segment s with k_off[s] <= i < k_off[s+1]; the ks of a
+// segment that is finished directly go on its list.
+template <typename K>
 __global__ void k_init_seg(const uint32_t* __restrict__ ks, uint32_t nk,
                            const int64_t* __restrict__ seg_off, const int64_t* __restrict__ k_off,
-                           uint32_t nseg, uint32_t* k_rank, uint32_t* k_seg, Counters* C) {
+                           uint32_t nseg, const Seg<K>* __restrict__ segs0, uint32_t* khead0,
+                           uint32_t* knext, uint32_t* k_rank, uint32_t* k_seg, Counters* C) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nk) return;
   uint32_t lo = 0, hi = nseg - 1;  // largest s with k_off[s] <= i
@@ -1358,6 +1745,7 @@ __global__ void k_init_seg(const uint32_t* __restrict__ ks, uint32_t nk,
   }
   k_rank[i] = (uint32_t)(len - k);
   k_seg[i] = lo;
+  if (segs0[lo].small) knext[i] = atomicExch(&khead0[lo], i);  // lock-free push
 }
 
 // ------------------------------------------------------------------ outputs
