@@ -182,6 +182,8 @@ struct Workspace {
   uint32_t* aflag0;
   uint32_t* cmap0;
   uint32_t* crow;         // per-CTA bucket counts of PASS 1 -> per-CTA cursors of PASS 2
+  uint32_t* ic;           // coarse mode: inclusive counts of the NGRP groups
+  uint32_t* aflagc;       // coarse mode: groups holding a k
   Seg<K>* segs[2];
   uint32_t* cursor[2];
   TileRef* tiles[2];
@@ -237,6 +239,8 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
   size_t o_a0 = b.take(4ull * (p.B / 32));
   size_t o_c0 = b.take(4ull * p.B);
   size_t o_crow = b.take(4ull * p.B * (p.ncta ? p.ncta : 1));
+  size_t o_ic = b.take(4ull * NGRP);
+  size_t o_afc = b.take(4ull * (NGRP / 32));
   size_t o_segs[2], o_cur[2], o_tiles[2], o_rows[2], o_af[2], o_cand[2], o_kh[2];
   size_t o_knext = b.take(4ull * p.nk);
   size_t o_smalls = b.take(4ull * p.cap_seg);
@@ -275,6 +279,8 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
   w.aflag0 = (uint32_t*)(base + o_a0);
   w.cmap0 = (uint32_t*)(base + o_c0);
   w.crow = (uint32_t*)(base + o_crow);
+  w.ic = (uint32_t*)(base + o_ic);
+  w.aflagc = (uint32_t*)(base + o_afc);
   for (int i = 0; i < 2; ++i) {
     w.segs[i] = (Seg<K>*)(base + o_segs[i]);
     w.cursor[i] = (uint32_t*)(base + o_cur[i]);
@@ -447,6 +453,11 @@ static size_t l0_count_smem(uint32_t B, int nt) {
   return GRID_SMEM + (size_t)B * 4u + wq_bytes((uint32_t)nt, sizeof(typename KeyOf<T>::K));
 }
 template <typename T>
+static size_t l0_coarse_smem(int nt, int unroll) {
+  const size_t ch = (size_t)nt * (unroll < 4 ? unroll : 4) * (16 / sizeof(T));
+  return GRID_SMEM + ch * (sizeof(typename KeyOf<T>::K) + 1);
+}
+template <typename T>
 static size_t l0_compact_smem(uint32_t B, int nt) {
   return GRID_SMEM + (MAX_B0 / 32 + l0_compact_qwords((uint32_t)nt, sizeof(typename KeyOf<T>::K)) + HOT_WORDS) * 4u +
          (size_t)B * 4u;
@@ -461,18 +472,19 @@ struct PassVariant {
   void (*count)(const T*, uint64_t, const Grid<K>*, const Counters*, const Windows<K>*, uint32_t*, uint32_t*);
   void (*compact)(const T*, uint64_t, const Grid<K>*, Counters*, const Windows<K>*, const uint32_t*,
                   const uint32_t*, K*, uint64_t);
+  void (*coarse)(const T*, uint64_t, const Grid<K>*, Counters*, const uint32_t*, const uint32_t*, K*, uint64_t);
 };
 
 template <typename T>
 static const PassVariant<T>* pass_variant(int nt, int unroll) {
   static const PassVariant<T> v[] = {
-      {256, 4, l0_count<T, 256, 4>, l0_compact<T, 256, 4>},
-      {256, 8, l0_count<T, 256, 8>, l0_compact<T, 256, 8>},
-      {512, 2, l0_count<T, 512, 2>, l0_compact<T, 512, 2>},
-      {512, 4, l0_count<T, 512, 4>, l0_compact<T, 512, 4>},
-      {512, 8, l0_count<T, 512, 8>, l0_compact<T, 512, 8>},
-      {1024, 2, l0_count<T, 1024, 2>, l0_compact<T, 1024, 2>},
-      {1024, 4, l0_count<T, 1024, 4>, l0_compact<T, 1024, 4>},
+      {256, 4, l0_count<T, 256, 4>, l0_compact<T, 256, 4>, l0_compact_coarse<T, 256, 4>},
+      {256, 8, l0_count<T, 256, 8>, l0_compact<T, 256, 8>, l0_compact_coarse<T, 256, 8>},
+      {512, 2, l0_count<T, 512, 2>, l0_compact<T, 512, 2>, l0_compact_coarse<T, 512, 2>},
+      {512, 4, l0_count<T, 512, 4>, l0_compact<T, 512, 4>, l0_compact_coarse<T, 512, 4>},
+      {512, 8, l0_count<T, 512, 8>, l0_compact<T, 512, 8>, l0_compact_coarse<T, 512, 8>},
+      {1024, 2, l0_count<T, 1024, 2>, l0_compact<T, 1024, 2>, l0_compact_coarse<T, 1024, 2>},
+      {1024, 4, l0_count<T, 1024, 4>, l0_compact<T, 1024, 4>, l0_compact_coarse<T, 1024, 4>},
   };
   for (const auto& x : v)
     if (x.nt == nt && x.unroll == unroll) return &x;
@@ -488,12 +500,15 @@ constexpr int DEFAULT_PASS_UNROLL = 4;
 template <typename T>
 static int l0_ncta(Context* c, const PassVariant<T>* pv, uint32_t B, uint32_t* ncta) {
   const size_t s1 = l0_count_smem<T>(B, pv->nt), s2 = l0_compact_smem<T>(B, pv->nt);
+  const size_t s3 = l0_coarse_smem<T>(pv->nt, pv->unroll);
   GGMS_CU(cudaFuncSetAttribute((const void*)pv->count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
   GGMS_CU(cudaFuncSetAttribute((const void*)pv->compact, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
-  int o1 = 0, o2 = 0;
+  GGMS_CU(cudaFuncSetAttribute((const void*)pv->coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s3));
+  int o1 = 0, o2 = 0, o3 = 0;
   GGMS_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, (const void*)pv->count, pv->nt, s1));
   GGMS_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, (const void*)pv->compact, pv->nt, s2));
-  *ncta = (uint32_t)(std::max(1, std::min(o1, o2)) * c->sms);
+  GGMS_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o3, (const void*)pv->coarse, pv->nt, s3));
+  *ncta = (uint32_t)(std::max(1, std::min(std::min(o1, o2), o3)) * c->sms);
   return GGMS_OK;
 }
 
@@ -681,10 +696,15 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     ++ctx->launches;
     lvl_locate_rows<<<cdiv(nk, 256), 256, 0, s>>>(w.hist0, p.B, nk, w.krank, w.kseg, w.kbin,
                                                      w.aflag0, p.B / 32, w.C);
+    // most buckets hold a k: copy groups of buckets instead (coarse mode)
+    ++ctx->launches;
+    l0_mode<K><<<1, 256, 0, s>>>(w.hist0, w.aflag0, p.B, w.win, w.C, w.ic, w.aflagc);
+    ++ctx->launches;
+    l0_coarsen_ks<<<cdiv(nk, 256), 256, 0, s>>>(w.hist0, p.B, nk, w.krank, w.kseg, w.kbin, w.aflagc, w.C);
     ++ctx->launches;
     l0_children<K><<<cdiv(p.B, 256), 256, 0, s>>>(w.hist0, w.aflag0, p.B, w.grid, w.C, w.win, w.cmap0,
                                                      w.segs[1], w.cursor[1], w.tiles[1], w.points,
-                                                     w.khead[1], w.smalls, w.bigs[1], caps);
+                                                     w.khead[1], w.smalls, w.bigs[1], caps, w.ic, w.aflagc);
     ++ctx->launches;
     lvl_relabel<K><<<cdiv(nk, 256), 256, 0, s>>>(w.cmap0, p.B, nk, w.kbin, w.kseg, w.kkey,
                                                     w.points, w.C, w.segs[1], w.khead[1], w.knext);
@@ -695,6 +715,9 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     ++ctx->launches;
     pv->compact<<<grid_c, pv->nt, l0_compact_smem<T>(p.B, pv->nt), s>>>(d_in, n, w.grid, w.C, w.win, w.cmap0,
                                                                         w.crow, w.cand[0], (uint64_t)n);
+    ++ctx->launches;  // one of the two PASS-2 kernels returns at once
+    pv->coarse<<<grid_c, pv->nt, l0_coarse_smem<T>(pv->nt, pv->unroll), s>>>(d_in, n, w.grid, w.C, w.cmap0,
+                                                                              w.crow, w.cand[0], (uint64_t)n);
     prof_rec(prof, 4, s);
     rc = launch_small_select<K>(ctx, w.cand[0], w.segs[1], w.khead[1], w, caps, s);
     if (rc) return rc;

@@ -274,7 +274,8 @@ struct Counters {
   uint32_t done;              // a refinement level found no segment: later levels are skipped
   uint32_t ntiny;             // tiny segments created by the current level (batched path)
   uint32_t nbig[2];           // segments of pool p that a level refines (listed in bigs[p])
-  uint32_t pad1[2];
+  uint32_t coarse;            // level 0 copies NGRP groups of buckets (most buckets hold a k)
+  uint32_t pad1[1];
 };
 
 // PASS 1 windows (l0_window).  From the sample, every requested k gets a
@@ -336,6 +337,15 @@ constexpr uint32_t QSAMP = 2 * QB;              // sampled keys per segment
 constexpr int QD_BITS = 12;
 constexpr uint32_t QD = 1u << QD_BITS;          // directory cells
 constexpr uint32_t QDS = QD + 8;                // directory stride (QD + 1 entries, 16-byte rows)
+
+// Coarse level 0 (single vector, most buckets hold a k): NGRP groups of
+// 2^coarse_shift(B) consecutive buckets (B a power of two >= 2 * NGRP).
+constexpr uint32_t NGRP = 256;
+__host__ __device__ __forceinline__ uint32_t coarse_shift(uint32_t B) {
+  uint32_t l = 0;
+  while ((2u << l) <= B) ++l;  // log2(B)
+  return l > 8u ? l - 8u : 0u;
+}
 
 // Keys of one tiny segment (a warp's shared-memory slice of 8 KB).
 template <typename K>

@@ -610,12 +610,15 @@ __global__ void lvl_locate_rows(const uint32_t* __restrict__ rows, uint32_t row_
 }
 
 // Active level-0 buckets -> refinement segments (or points).  One thread per bucket.
+// In the coarse mode (C->coarse) the children are the NGRP groups of 2^gsh
+// consecutive buckets instead (counts from ic, flags from aflagc).
 template <typename K>
 __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __restrict__ aflag,
                             uint32_t B, const Grid<K>* __restrict__ Gs, Counters* C,
                             const Windows<K>* __restrict__ Wg,
                             uint32_t* cmap0, Seg<K>* segs1, uint32_t* cursor1, TileRef* tiles1,
-                            K* points, uint32_t* khead1, uint32_t* smalls, uint32_t* bigs1, Caps caps) {
+                            K* points, uint32_t* khead1, uint32_t* smalls, uint32_t* bigs1, Caps caps,
+                            const uint32_t* __restrict__ ic, const uint32_t* __restrict__ aflagc) {
   // the key-range searches below evaluate the grid ~64 times per bucket: keep
   // it in shared memory (every thread helps load it before any returns)
   __shared__ uint2 s1[GRID_T1];
@@ -623,13 +626,15 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
   const GridView<K> gv = grid_to_smem<K>(Gs + C->asg_choice, s1, s2);
   __syncthreads();
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= B) return;
-  if (!((aflag[b >> 5] >> (b & 31)) & 1u)) {
+  const bool coarse = C->coarse != 0u;
+  const uint32_t gsh = coarse_shift(B);
+  if (b >= (coarse ? NGRP : B)) return;
+  if (!(((coarse ? aflagc : aflag)[b >> 5] >> (b & 31)) & 1u)) {
     cmap0[b] = CM_NONE;
     return;
   }
-  const uint32_t start = b ? I[b - 1] : 0u;
-  const uint32_t cnt = I[b] - start;
+  const uint32_t start = b ? (coarse ? ic : I)[b - 1] : 0u;
+  const uint32_t cnt = (coarse ? ic : I)[b] - start;
   // key range of bucket b: [L(b), L(b+1) - 1], L(x) = smallest key with eval >= x
   auto L = [&](uint32_t target) -> K {
     K lo = 0, hi = key_max<K>();
@@ -639,9 +644,11 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
     }
     return lo;
   };
-  // a gap bucket (windows) stands for its whole gap: up to the gap's last bucket
-  const uint32_t e = win_end<K>(*Wg, b);
-  const K lo = (b == 0) ? (K)0 : L(b);
+  // a gap bucket (windows) stands for its whole gap: up to the gap's last bucket;
+  // a group, for its buckets [b << gsh, (b + 1) << gsh)
+  const uint32_t b0 = coarse ? b << gsh : b;
+  const uint32_t e = coarse ? ((b + 1u) << gsh) - 1u : win_end<K>(*Wg, b);
+  const K lo = (b0 == 0) ? (K)0 : L(b0);
   const K hi = (e >= B - 1) ? key_max<K>() : (K)(L(e + 1) - 1);
   atomicAdd(&C->active0, 1u);
   if (lo == hi) {
@@ -661,7 +668,7 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
   s.hi = hi;
   s.shift = (uint32_t)max(0, bitlen((K)(hi - lo)) - RADIX_BITS);
   s.small = cnt <= caps.small_keys ? 1u : 0u;
-  s.pad = b;  // the level-0 bucket (l0_bases needs it)
+  s.pad = b;  // the level-0 bucket or group (l0_bases needs it)
   segs1[id] = s;
   cursor1[id] = 0u;
   khead1[id] = K_NIL;
@@ -714,13 +721,23 @@ __global__ void l0_bases(uint32_t* crow, uint32_t B, uint32_t ncta, const Seg<K>
                          const Counters* __restrict__ C, Caps caps) {
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   const uint32_t ns = min(C->nsegs[1], caps.segs);
+  const bool coarse = C->coarse != 0u;
+  const uint32_t gsh = coarse_shift(B);
   for (uint32_t id = warp; id < ns; id += (gridDim.x * blockDim.x) >> 5) {
     const Seg<K> s = segs1[id];
-    const uint32_t b = s.pad;  // the level-0 bucket this child came from
+    // the level-0 bucket this child came from (coarse: the first bucket of its
+    // group, whose column then holds the group's cursors)
+    const uint32_t b = coarse ? s.pad << gsh : s.pad;
     uint64_t run = s.off;
     for (uint32_t g0 = 0; g0 < ncta; g0 += 32) {
       const uint32_t g = g0 + lane;
-      const uint32_t v = g < ncta ? crow[(size_t)g * B + b] : 0u;
+      uint32_t v = 0u;
+      if (g < ncta) {
+        if (coarse)
+          for (uint32_t j = 0; j < (1u << gsh); ++j) v += crow[(size_t)g * B + b + j];
+        else
+          v = crow[(size_t)g * B + b];
+      }
       uint32_t inc = v;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
@@ -762,6 +779,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
                                                 typename KeyOf<T>::K* dst, uint64_t dst_cap) {
   using K = typename KeyOf<T>::K;
   constexpr int EPV = Vec16<T>::N;
+  if (C->coarse) return;  // l0_compact_coarse copies this call's groups
   extern __shared__ __align__(16) uint8_t smem[];
   __shared__ Windows<K> W;
   if (threadIdx.x == 0) W = *Wg;
@@ -972,6 +990,209 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
       const uint64_t idx = j < head ? j : tail0 + (j - head);
       const K key = KeyOf<T>::to(in[idx]);
       if (in_hot(key)) bucket_and_put(key);
+    }
+  }
+  if (overflow) set_status(C, GGMS_E_INTERNAL);
+}
+
+// ------------------------------------------------------------------ coarse level 0
+// When most buckets hold a k (many ks spread over all ranks), copying key by
+// key into ~B per-CTA bucket ranges is a scatter of 4-byte stores over the
+// whole candidate buffer, which runs far below the memory's bandwidth.  The
+// coarse mode copies NGRP groups of consecutive buckets instead (equal mass,
+// since the buckets are), and PASS 2 sorts each chunk of a CTA's keys by group
+// in shared memory first, so that the stores leave as contiguous runs.  The
+// refinement levels then split the groups.
+// Decided on the device after PASS 1: windows off and at least half the
+// buckets flagged.
+template <typename K>
+__global__ void l0_mode(const uint32_t* __restrict__ I, const uint32_t* __restrict__ aflag0, uint32_t B,
+                        const Windows<K>* __restrict__ Wg, Counters* C, uint32_t* ic, uint32_t* aflagc) {
+  __shared__ uint32_t tot;
+  if (threadIdx.x == 0) tot = 0u;
+  __syncthreads();
+  uint32_t a = 0;
+  for (uint32_t w = threadIdx.x; w < B / 32; w += blockDim.x) a += __popc(aflag0[w]);
+  atomicAdd(&tot, a);
+  __syncthreads();
+  const uint32_t gsh = coarse_shift(B);
+  if (threadIdx.x == 0) C->coarse = (!Wg->on && tot * 2u >= B) ? 1u : 0u;
+  for (uint32_t g = threadIdx.x; g < NGRP; g += blockDim.x) ic[g] = I[((g + 1u) << gsh) - 1u];
+  for (uint32_t w = threadIdx.x; w < NGRP / 32; w += blockDim.x) aflagc[w] = 0u;
+}
+
+// Coarse mode: a k's bucket becomes its group, its rank one inside the group.
+__global__ void l0_coarsen_ks(const uint32_t* __restrict__ I, uint32_t B, uint32_t nk, uint32_t* k_rank,
+                              const uint32_t* __restrict__ k_seg, uint32_t* k_bin, uint32_t* aflagc,
+                              const Counters* __restrict__ C) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nk || !C->coarse || k_seg[i] == K_DONE) return;
+  const uint32_t gsh = coarse_shift(B);
+  const uint32_t b = k_bin[i], g = b >> gsh, g0 = g << gsh;
+  k_rank[i] += (b ? I[b - 1] : 0u) - (g0 ? I[g0 - 1] : 0u);
+  k_bin[i] = g;
+  atomicOr(&aflagc[g >> 5], 1u << (g & 31));
+}
+
+// Keys of one PASS-2 chunk of the coarse mode: up to 4 vectors per thread.
+template <typename T, int NT, int UNROLL>
+__host__ __device__ constexpr uint32_t coarse_chunk() {
+  return (uint32_t)NT * (UNROLL < 4 ? UNROLL : 4) * Vec16<T>::N;
+}
+
+// PASS 2 of the coarse mode.  Same element -> CTA assignment as PASS 1; CTA
+// c's range of group g starts at crow[c][g << gsh] (l0_bases).  Per chunk: the
+// group of every key (bucket >> gsh), its rank among the chunk's keys of that
+// group (a shared atomic), a scan of the NGRP counts, the keys into shared
+// memory in group order, then thread i stores staged key i -- consecutive
+// threads, consecutive addresses inside a group's run.
+template <typename T, int NT, int UNROLL>
+__global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact_coarse(const T* __restrict__ in, uint64_t n,
+                                                       const Grid<typename KeyOf<T>::K>* __restrict__ Gs,
+                                                       Counters* C, const uint32_t* __restrict__ cmap0,
+                                                       const uint32_t* __restrict__ crow,
+                                                       typename KeyOf<T>::K* dst, uint64_t dst_cap) {
+  using K = typename KeyOf<T>::K;
+  constexpr int EPV = Vec16<T>::N;
+  constexpr int DU = UNROLL < 4 ? UNROLL : 4;
+  constexpr uint32_t CH = coarse_chunk<T, NT, UNROLL>();
+  constexpr uint32_t NONE = 0xFFFFFFFFu;
+  static_assert(CH <= 65536u, "chunk ranks are 16-bit");
+  if (!C->coarse) return;  // l0_compact copies this call's buckets
+  extern __shared__ __align__(16) uint8_t smem[];
+  __shared__ uint32_t gbase[NGRP], hist[NGRP], off[NGRP], cflag[NGRP / 32];
+  __shared__ uint32_t total_s;
+  const Grid<K>* G = Gs + C->asg_choice;
+  uint2* s1 = (uint2*)smem;
+  uint2* s2 = s1 + GRID_T1;
+  K* stg = (K*)(smem + GRID_SMEM);
+  uint8_t* sg = (uint8_t*)(stg + CH);
+  const GridView<K> gv = grid_to_smem<K>(G, s1, s2);
+  const uint32_t B = gv.B, gsh = coarse_shift(B);
+  const uint32_t tid = threadIdx.x, lane = tid & 31;
+  if (tid < NGRP / 32) cflag[tid] = 0u;
+  __syncthreads();
+  for (uint32_t g = tid; g < NGRP; g += NT) {
+    hist[g] = 0u;
+    const bool copied = cmap0[g] < CM_POINT;
+    gbase[g] = copied ? crow[(size_t)blockIdx.x * B + (g << gsh)] : 0u;
+    if (copied) atomicOr(&cflag[g >> 5], 1u << (g & 31));
+  }
+  __syncthreads();
+  auto group = [&](K key) -> uint32_t {
+    const uint32_t g = min(grid_eval<K>(gv, key), B - 1u) >> gsh;
+    return ((cflag[g >> 5] >> (g & 31)) & 1u) ? g : NONE;
+  };
+
+  const uint64_t gtid = (uint64_t)blockIdx.x * NT + tid;
+  const uint64_t gstride = (uint64_t)gridDim.x * NT;
+  uint64_t head = ((16u - (uint32_t)((uintptr_t)in & 15u)) & 15u) / sizeof(T);
+  if (head > n) head = n;
+  const uint64_t nvec = (n - head) / EPV;
+  const uint4* vp = reinterpret_cast<const uint4*>(in + head) + gtid;
+  const uint64_t rounds = nvec / (gstride * UNROLL);
+  bool overflow = false;
+  // chunk c: DU vectors of round c / CPR; the next chunk's loads are issued
+  // before this chunk's barriers, so they are in flight while it is staged
+  constexpr int CPR = UNROLL / DU;
+  const uint64_t nch = rounds * CPR;
+  auto chunk_ptr = [&](uint64_t c) {
+    return vp + (c / CPR) * gstride * UNROLL + (uint64_t)((int)(c % CPR) * DU) * gstride;
+  };
+  uint4 q[DU];
+  if (nch) {
+    const uint4* p0 = chunk_ptr(0);
+#pragma unroll
+    for (int u = 0; u < DU; ++u) q[u] = ld_stream16(p0 + u * gstride);
+  }
+  for (uint64_t c = 0; c < nch; ++c) {
+    {
+      uint32_t pk[DU * EPV];  // (group << 16) | rank inside the chunk's group, or NONE
+#pragma unroll
+      for (int u = 0; u < DU; ++u) {
+        T e[EPV];
+        unpack16<T>(q[u], e);
+        uint32_t g[EPV];
+#pragma unroll
+        for (int t = 0; t < EPV; ++t) g[t] = group(KeyOf<T>::to(e[t]));
+#pragma unroll
+        for (int t = 0; t < EPV; ++t)
+          pk[u * EPV + t] = g[t] == NONE ? NONE : (g[t] << 16) | atomicAdd(&hist[g[t]], 1u);
+      }
+      uint4 qn[DU];
+      if (c + 1 < nch) {
+        const uint4* pn = chunk_ptr(c + 1);
+#pragma unroll
+        for (int u = 0; u < DU; ++u) qn[u] = ld_stream16(pn + u * gstride);
+      }
+      __syncthreads();
+      if (tid < 32) {  // exclusive scan of the NGRP counts, 8 per lane
+        uint32_t c8[NGRP / 32], sum = 0;
+#pragma unroll
+        for (int j = 0; j < (int)(NGRP / 32); ++j) { c8[j] = hist[lane * (NGRP / 32) + j]; sum += c8[j]; }
+        uint32_t inc = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t t = __shfl_up_sync(FULL, inc, o);
+          if ((int)lane >= o) inc += t;
+        }
+        uint32_t run = inc - sum;
+#pragma unroll
+        for (int j = 0; j < (int)(NGRP / 32); ++j) { off[lane * (NGRP / 32) + j] = run; run += c8[j]; }
+        if (lane == 31) total_s = inc;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < DU; ++u) {
+        T e[EPV];
+        unpack16<T>(q[u], e);
+#pragma unroll
+        for (int t = 0; t < EPV; ++t) {
+          const uint32_t x = pk[u * EPV + t];
+          if (x != NONE) {
+            const uint32_t g = x >> 16, pos = off[g] + (x & 0xFFFFu);
+            stg[pos] = KeyOf<T>::to(e[t]);
+            sg[pos] = (uint8_t)g;
+          }
+        }
+      }
+      __syncthreads();
+      const uint32_t tot = total_s;
+      for (uint32_t i = tid; i < tot; i += NT) {
+        const uint32_t g = sg[i];
+        const uint64_t slot = (uint64_t)gbase[g] + (i - off[g]);
+        if (slot < dst_cap) dst[slot] = stg[i]; else overflow = true;
+      }
+      __syncthreads();
+      for (uint32_t g = tid; g < NGRP; g += NT) {
+        gbase[g] += hist[g];
+        hist[g] = 0u;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < DU; ++u) q[u] = qn[u];
+    }
+  }
+  // the partial last round, the unaligned head and the tail: one key at a time
+  auto put = [&](K key) {
+    const uint32_t g = group(key);
+    if (g == NONE) return;
+    const uint32_t slot = atomicAdd(&gbase[g], 1u);
+    if (slot < dst_cap) dst[slot] = key; else overflow = true;
+  };
+  const T* vbase = in + head;
+  for (uint64_t i = rounds * gstride * UNROLL + gtid; i < nvec; i += gstride) {
+    T e[EPV];
+    unpack16<T>(ld_stream16(vbase + i * EPV), e);
+#pragma unroll
+    for (int t = 0; t < EPV; ++t) put(KeyOf<T>::to(e[t]));
+  }
+  {
+    const uint64_t tail0 = head + nvec * EPV;
+    const uint64_t nscalar = head + (n - tail0);
+    for (uint64_t j = gtid; j < nscalar; j += gstride) {
+      const uint64_t idx = j < head ? j : tail0 + (j - head);
+      put(KeyOf<T>::to(in[idx]));
     }
   }
   if (overflow) set_status(C, GGMS_E_INTERNAL);
