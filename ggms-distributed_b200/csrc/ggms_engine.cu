@@ -990,7 +990,7 @@ static int run_segmented(Context* ctx, const T* d_in, const int64_t* seg_off, in
   const uint32_t small_keys = (uint32_t)(SMALL_SMEM / sizeof(K));
   p.cap_seg = std::max<uint32_t>(nk, nseg) + 1;
   p.cap_tiles = (uint32_t)((n + TILE - 1) / TILE) + p.cap_seg;
-  p.cap_q = (uint32_t)std::min<uint64_t>(nseg, n / (small_keys + 1ull)) + 1;
+  p.cap_q = (uint32_t)std::min<uint64_t>(nseg, n / QSAMP) + 1;
   Workspace<K> w0 = layout<K>(p, sizeof(T), nullptr);
   rc = ensure_arena(ctx, w0.bytes);
   if (rc) return rc;

@@ -1351,12 +1351,22 @@ __global__ __launch_bounds__(NT) void lvl_count(const InT* __restrict__ src,
     __syncthreads();
     const uint64_t beg = s.off + (uint64_t)tr.no * TILE;
     const uint64_t end = min(beg + TILE, s.off + s.cnt);
-    for (uint64_t i = beg + threadIdx.x; i < end; i += NT) {
-      K key = KeyOf<InT>::to(src[i]);
-      uint32_t bin;
-      if (Q) bin = qbin<K>(key, s.lo, s.shift, qb, qd);
-      else bin = min((uint32_t)((K)(key - s.lo) >> s.shift), (uint32_t)NBIN - 1u);
-      atomicAdd(&h[bin], 1u);
+    constexpr int U = 8;  // independent loads in flight per thread
+    for (uint64_t o = beg + threadIdx.x; o < end; o += (uint64_t)NT * U) {
+      K kk[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const uint64_t i = o + (uint64_t)u * NT;
+        kk[u] = i < end ? KeyOf<InT>::to(src[i]) : (K)0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (o + (uint64_t)u * NT >= end) break;
+        uint32_t bin;
+        if (Q) bin = qbin<K>(kk[u], s.lo, s.shift, qb, qd);
+        else bin = min((uint32_t)((K)(kk[u] - s.lo) >> s.shift), (uint32_t)NBIN - 1u);
+        atomicAdd(&h[bin], 1u);
+      }
     }
     __syncthreads();
     uint32_t* row = rows + (size_t)tr.seg * NBIN;
@@ -1891,8 +1901,9 @@ __global__ __launch_bounds__(NT) void tiny_select(const InT* __restrict__ src,
 // ------------------------------------------------------------------ batched segments
 // Level 0 of the batched mode.  A caller segment that holds a k is finished
 // directly from the input when it is small (tiny_select for tiny ones,
-// small_select otherwise); a larger one gets quantile bins (seg_sample fills
-// its table) and tiles for the level-0 count.
+// small_select below QSAMP keys); a larger one gets quantile bins (seg_sample
+// fills its table) and tiles for the level-0 count -- its children then hold
+// about 1/QB of it, mostly a single k each.
 template <typename K>
 __global__ void seg_init(const int64_t* __restrict__ seg_off, uint32_t nseg,
                          const int64_t* __restrict__ k_off, Seg<K>* segs0, TileRef* tiles0,
@@ -1916,7 +1927,7 @@ __global__ void seg_init(const int64_t* __restrict__ seg_off, uint32_t nseg,
     segs0[s] = d;
     return;
   }
-  if (d.cnt <= caps.small_keys) {
+  if (d.cnt <= caps.tiny_keys || d.cnt < QSAMP) {
     d.small = 1u;
     segs0[s] = d;
     const bool tiny = d.cnt <= caps.tiny_keys;
@@ -1926,7 +1937,7 @@ __global__ void seg_init(const int64_t* __restrict__ seg_off, uint32_t nseg,
   }
   const uint32_t q = atomicAdd(&C->nbig[0], 1u);  // its quantile table: q
   if (q < caps.segs) bigs0[q] = s;
-  if (q >= cap_q) {  // cannot happen: cap_q bounds the segments above small_keys
+  if (q >= cap_q) {  // cannot happen: cap_q bounds the segments of QSAMP keys or more
     set_status(C, GGMS_E_INTERNAL);
     d.small = 1u;
     segs0[s] = d;

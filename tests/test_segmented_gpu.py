@@ -70,3 +70,33 @@ def test_topk(ctx, dtype, n, K):
     got = G.topk(ctx, d.data_ptr(), n, K, dtype)
     exp = orc.select(v, np.arange(1, K + 1, dtype=np.uint32))
     np.testing.assert_array_equal(orc.bits(got), orc.bits(exp))
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.uint32])
+def test_segmented_size_classes(ctx, dtype):
+    """Segments at the borders of the finishing classes (warp <= 2048 keys,
+    CTA below 4096, sample-quantile bins from 4096 on), sorted, constant and
+    heavily duplicated ones, each with its extreme ks and a run of ks."""
+    g = np.random.default_rng(17)
+    lens = [2047, 2048, 2049, 4095, 4096, 4097, 65536, 300001, 1 << 20]
+    parts, ks_l = [], []
+    for i, ln in enumerate(lens):
+        if i % 3 == 0:
+            v = np.sort(g.integers(0, 1 << 31, size=ln)).astype(np.uint32)[::-1]  # sorted descending
+        elif i % 3 == 1:
+            v = g.integers(0, 7, size=ln).astype(np.uint32)  # 7 distinct values
+        else:
+            v = g.integers(0, 1 << 32, size=ln, dtype=np.uint64).astype(np.uint32)
+        if dtype == np.float32:
+            v = (v.astype(np.float64) / 1000.0 - 5e5).astype(np.float32)
+        parts.append(v)
+        k = np.concatenate([[1, ln, (ln + 1) // 2], g.integers(1, ln + 1, size=40), np.arange(1, 20)])
+        ks_l.append(k.astype(np.uint32))
+    parts.append(np.full(5000, 3, dtype=np.uint32).astype(dtype))  # constant segment
+    ks_l.append(np.array([1, 2500, 5000], np.uint32))
+    vals = np.concatenate(parts).astype(dtype)
+    seg_off = np.concatenate([[0], np.cumsum([len(p) for p in parts])]).astype(np.int64)
+    k_off = np.concatenate([[0], np.cumsum([len(k) for k in ks_l])]).astype(np.int64)
+    ks = np.concatenate(ks_l).astype(np.uint32)
+    got = run_segmented(ctx, vals, seg_off, ks, k_off)
+    np.testing.assert_array_equal(orc.bits(got), orc.bits(orc.select_segmented(vals, seg_off, ks, k_off)))
