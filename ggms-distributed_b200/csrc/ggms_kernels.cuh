@@ -1822,57 +1822,89 @@ __global__ __launch_bounds__(NT) void tiny_select(const InT* __restrict__ src,
   K* v = buf[wid];
   uint32_t* h = hist[wid];
   const uint32_t nt = min(C->ntiny, caps.segs);
-  for (uint32_t t = blockIdx.x * NW + wid; t < nt; t += gridDim.x * NW) {
-    const uint32_t id = tinies[t];
-    const Seg<K> s = segs_q[id];
-    const uint32_t cnt = s.cnt;
-    if (cnt > TK) {  // cannot happen: tiny segments are created with cnt <= tiny_keys
-      if (lane == 0) set_status(C, GGMS_E_INTERNAL);
-      continue;
+  // a warp takes up to 32 list entries at a time (fewer when the list is short,
+  // so that every warp gets work): lane j loads entry j's descriptor and k-list
+  // head -- the chain of dependent loads is paid once per batch -- then the warp
+  // finishes the segments one by one
+  const uint32_t nwarps = gridDim.x * NW;
+  const uint32_t batch = max(1u, min(32u, nt / nwarps));
+  for (uint32_t t0 = (blockIdx.x * NW + wid) * batch; t0 < nt; t0 += nwarps * batch) {
+    const uint32_t tj = t0 + lane;
+    uint32_t pid = 0u, pkh = K_NIL;
+    Seg<K> ps{};
+    if (lane < batch && tj < nt) {
+      pid = tinies[tj];
+      ps = segs_q[pid];
+      if (!k_off) pkh = khead_q[pid];
     }
-    for (uint32_t i0 = lane; i0 < cnt; i0 += 32 * 8) {  // eight independent loads in flight
-      K x[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const uint32_t i = i0 + q * 32;
-        x[q] = i < cnt ? KeyOf<InT>::to(src[s.off + i]) : s.lo;
+    const uint32_t nb = min(batch, nt - t0);
+    for (uint32_t j = 0; j < nb; ++j) {
+      const uint32_t id = __shfl_sync(FULL, pid, j);
+      Seg<K> s;
+      s.off = __shfl_sync(FULL, ps.off, j);
+      s.cnt = __shfl_sync(FULL, ps.cnt, j);
+      s.lo = __shfl_sync(FULL, ps.lo, j);
+      s.hi = __shfl_sync(FULL, ps.hi, j);
+      const uint32_t khead = __shfl_sync(FULL, pkh, j);
+      const uint32_t cnt = s.cnt;
+      if (cnt > TK) {  // cannot happen: tiny segments are created with cnt <= tiny_keys
+        if (lane == 0) set_status(C, GGMS_E_INTERNAL);
+        continue;
       }
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const uint32_t i = i0 + q * 32;
-        if (i < cnt) v[i] = (K)(x[q] - s.lo);
+      for (uint32_t i0 = lane; i0 < cnt; i0 += 32 * 8) {  // eight independent loads in flight
+        K x[8];
+  #pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const uint32_t i = i0 + q * 32;
+          x[q] = i < cnt ? KeyOf<InT>::to(src[s.off + i]) : s.lo;
+        }
+  #pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const uint32_t i = i0 + q * 32;
+          if (i < cnt) v[i] = (K)(x[q] - s.lo);
+        }
       }
-    }
-    __syncwarp();
-    const int bits = bitlen((K)(s.hi - s.lo));
-    if (k_off) {
-      const int64_t k0 = k_off[id], k1 = k_off[id + 1];
-      if ((uint64_t)(k1 - k0) > TS_SORT_ABOVE) {
-        uint32_t N = 32;
-        while (N < cnt) N <<= 1;
-        for (uint32_t i = cnt + lane; i < N; i += 32) v[i] = key_max<K>();
-        __syncwarp();
-        for (uint32_t kk = 2; kk <= N; kk <<= 1) {
-          for (uint32_t jj = kk >> 1; jj > 0; jj >>= 1) {
-            for (uint32_t i = lane; i < N; i += 32) {
-              const uint32_t ixj = i ^ jj;
-              if (ixj > i) {
-                const K a = v[i], b = v[ixj];
-                if ((a > b) == ((i & kk) == 0)) { v[i] = b; v[ixj] = a; }
+      __syncwarp();
+      const int bits = bitlen((K)(s.hi - s.lo));
+      if (k_off) {
+        const int64_t k0 = k_off[id], k1 = k_off[id + 1];
+        if ((uint64_t)(k1 - k0) > TS_SORT_ABOVE) {
+          uint32_t N = 32;
+          while (N < cnt) N <<= 1;
+          for (uint32_t i = cnt + lane; i < N; i += 32) v[i] = key_max<K>();
+          __syncwarp();
+          for (uint32_t kk = 2; kk <= N; kk <<= 1) {
+            for (uint32_t jj = kk >> 1; jj > 0; jj >>= 1) {
+              for (uint32_t i = lane; i < N; i += 32) {
+                const uint32_t ixj = i ^ jj;
+                if (ixj > i) {
+                  const K a = v[i], b = v[ixj];
+                  if ((a > b) == ((i & kk) == 0)) { v[i] = b; v[ixj] = a; }
+                }
               }
+              __syncwarp();
             }
-            __syncwarp();
+          }
+          for (int64_t k = k0 + lane; k < k1; k += 32) {
+            if (k_seg[k] == K_DONE) continue;  // an invalid k (status already set)
+            const uint32_t r = k_rank[k];
+            if (r < cnt) k_key[k] = (K)(s.lo + v[r]); else set_status(C, GGMS_E_INTERNAL);
+            k_seg[k] = K_DONE;
+          }
+        } else {
+          for (int64_t k = k0; k < k1; ++k) {
+            if (k_seg[k] == K_DONE) continue;  // warp-uniform
+            bool ok = false;
+            const uint32_t r = k_rank[k];
+            const K pre = r < cnt ? warp_radix_select<K>(v, cnt, bits, r, h, lane, &ok) : (K)0;
+            if (lane == 0) {
+              if (ok) k_key[k] = (K)(s.lo + pre); else set_status(C, GGMS_E_INTERNAL);
+              k_seg[k] = K_DONE;
+            }
           }
         }
-        for (int64_t k = k0 + lane; k < k1; k += 32) {
-          if (k_seg[k] == K_DONE) continue;  // an invalid k (status already set)
-          const uint32_t r = k_rank[k];
-          if (r < cnt) k_key[k] = (K)(s.lo + v[r]); else set_status(C, GGMS_E_INTERNAL);
-          k_seg[k] = K_DONE;
-        }
       } else {
-        for (int64_t k = k0; k < k1; ++k) {
-          if (k_seg[k] == K_DONE) continue;  // warp-uniform
+        for (uint32_t k = khead; k != K_NIL; k = knext[k]) {
           bool ok = false;
           const uint32_t r = k_rank[k];
           const K pre = r < cnt ? warp_radix_select<K>(v, cnt, bits, r, h, lane, &ok) : (K)0;
@@ -1882,19 +1914,9 @@ __global__ __launch_bounds__(NT) void tiny_select(const InT* __restrict__ src,
           }
         }
       }
-    } else {
-      for (uint32_t k = khead_q[id]; k != K_NIL; k = knext[k]) {
-        bool ok = false;
-        const uint32_t r = k_rank[k];
-        const K pre = r < cnt ? warp_radix_select<K>(v, cnt, bits, r, h, lane, &ok) : (K)0;
-        if (lane == 0) {
-          if (ok) k_key[k] = (K)(s.lo + pre); else set_status(C, GGMS_E_INTERNAL);
-          k_seg[k] = K_DONE;
-        }
-      }
+      __syncwarp();  // the slice is reloaded by the warp's next segment
     }
-    __syncwarp();  // the slice is reloaded by the warp's next segment
-    if (lane == 0) atomicAdd(&C->small_segs, 1u);
+    if (lane == 0) atomicAdd(&C->small_segs, nb);
   }
 }
 
