@@ -692,15 +692,14 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
                                                                       w.crow);
     prof_rec(prof, 2, s);
     ++ctx->launches;
-    l0_scan<K><<<1, 1024, 4u * p.B, s>>>(w.hist0, p.B, w.C, w.win);
+    l0_scan<K><<<1, 1024, 4u * p.B, s>>>(w.hist0, p.B, w.C, w.win, w.aflagc);
     ++ctx->launches;
     lvl_locate_rows<<<cdiv(nk, 256), 256, 0, s>>>(w.hist0, p.B, nk, w.krank, w.kseg, w.kbin,
                                                      w.aflag0, p.B / 32, w.C);
     // most buckets hold a k: copy groups of buckets instead (coarse mode)
     ++ctx->launches;
-    l0_mode<K><<<1, 256, 0, s>>>(w.hist0, w.aflag0, p.B, w.win, w.C, w.ic, w.aflagc);
-    ++ctx->launches;
-    l0_coarsen_ks<<<cdiv(nk, 256), 256, 0, s>>>(w.hist0, p.B, nk, w.krank, w.kseg, w.kbin, w.aflagc, w.C);
+    l0_mode_ks<K><<<cdiv(nk, 256), 256, 0, s>>>(w.hist0, w.aflag0, p.B, w.win, w.C, w.ic, w.aflagc, nk, w.krank,
+                                                 w.kseg, w.kbin);
     ++ctx->launches;
     l0_children<K><<<cdiv(p.B, 256), 256, 0, s>>>(w.hist0, w.aflag0, p.B, w.grid, w.C, w.win, w.cmap0,
                                                      w.segs[1], w.cursor[1], w.tiles[1], w.points,

@@ -172,7 +172,11 @@ __global__ __launch_bounds__(NT) void asg_sort_chunks(const K* __restrict__ in, 
           }
         }
       }
-      __syncthreads();
+      // a stage with j < 32 pairs keys of one warp only (i and i ^ j belong to
+      // lanes l and l ^ j): a warp barrier suffices unless the next stage
+      // reaches across warps
+      const uint32_t nj = j > 1 ? (j >> 1) : k;  // the next stage's j
+      if (nj >= 32u || (j == 1 && k == (uint32_t)CH)) __syncthreads(); else __syncwarp();
     }
   }
   for (uint32_t i = threadIdx.x; i < cnt; i += NT) out[base + i] = s[i];
@@ -555,7 +559,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_count(const T* __res
 // (a gap bucket counts a whole gap, not a bucket).
 template <typename K>
 __global__ __launch_bounds__(1024) void l0_scan(uint32_t* hist0, uint32_t B, Counters* C,
-                                                const Windows<K>* __restrict__ Wg) {
+                                                const Windows<K>* __restrict__ Wg, uint32_t* aflagc) {
   extern __shared__ uint32_t sh_counts[];
   __shared__ uint32_t w[72];
   __shared__ uint32_t mx;
@@ -564,6 +568,7 @@ __global__ __launch_bounds__(1024) void l0_scan(uint32_t* hist0, uint32_t B, Cou
     W = *Wg;
     mx = 0;
   }
+  if (threadIdx.x < NGRP / 32) aflagc[threadIdx.x] = 0u;  // the coarse mode's group flags
   __syncthreads();
   const bool on = W.on != 0u;
   uint32_t m = 0;
@@ -1003,11 +1008,14 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
 // since the buckets are), and PASS 2 sorts each chunk of a CTA's keys by group
 // in shared memory first, so that the stores leave as contiguous runs.  The
 // refinement levels then split the groups.
-// Decided on the device after PASS 1: windows off and at least half the
-// buckets flagged.
+// Decided on the device after PASS 1 (windows off and at least half the
+// buckets flagged), by every CTA of l0_mode_ks for itself; CTA 0 records it
+// and the groups' inclusive counts.  In the coarse mode a k's bucket becomes
+// its group and its rank one inside the group.
 template <typename K>
-__global__ void l0_mode(const uint32_t* __restrict__ I, const uint32_t* __restrict__ aflag0, uint32_t B,
-                        const Windows<K>* __restrict__ Wg, Counters* C, uint32_t* ic, uint32_t* aflagc) {
+__global__ void l0_mode_ks(const uint32_t* __restrict__ I, const uint32_t* __restrict__ aflag0, uint32_t B,
+                           const Windows<K>* __restrict__ Wg, Counters* C, uint32_t* ic, uint32_t* aflagc,
+                           uint32_t nk, uint32_t* k_rank, const uint32_t* __restrict__ k_seg, uint32_t* k_bin) {
   __shared__ uint32_t tot;
   if (threadIdx.x == 0) tot = 0u;
   __syncthreads();
@@ -1015,19 +1023,14 @@ __global__ void l0_mode(const uint32_t* __restrict__ I, const uint32_t* __restri
   for (uint32_t w = threadIdx.x; w < B / 32; w += blockDim.x) a += __popc(aflag0[w]);
   atomicAdd(&tot, a);
   __syncthreads();
+  const bool coarse = !Wg->on && tot * 2u >= B;
   const uint32_t gsh = coarse_shift(B);
-  if (threadIdx.x == 0) C->coarse = (!Wg->on && tot * 2u >= B) ? 1u : 0u;
-  for (uint32_t g = threadIdx.x; g < NGRP; g += blockDim.x) ic[g] = I[((g + 1u) << gsh) - 1u];
-  for (uint32_t w = threadIdx.x; w < NGRP / 32; w += blockDim.x) aflagc[w] = 0u;
-}
-
-// Coarse mode: a k's bucket becomes its group, its rank one inside the group.
-__global__ void l0_coarsen_ks(const uint32_t* __restrict__ I, uint32_t B, uint32_t nk, uint32_t* k_rank,
-                              const uint32_t* __restrict__ k_seg, uint32_t* k_bin, uint32_t* aflagc,
-                              const Counters* __restrict__ C) {
+  if (blockIdx.x == 0) {
+    if (threadIdx.x == 0) C->coarse = coarse ? 1u : 0u;
+    for (uint32_t g = threadIdx.x; g < NGRP; g += blockDim.x) ic[g] = I[((g + 1u) << gsh) - 1u];
+  }
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nk || !C->coarse || k_seg[i] == K_DONE) return;
-  const uint32_t gsh = coarse_shift(B);
+  if (!coarse || i >= nk || k_seg[i] == K_DONE) return;
   const uint32_t b = k_bin[i], g = b >> gsh, g0 = g << gsh;
   k_rank[i] += (b ? I[b - 1] : 0u) - (g0 ? I[g0 - 1] : 0u);
   k_bin[i] = g;
@@ -1277,7 +1280,7 @@ __global__ __launch_bounds__(1024) void seg_sample(const T* __restrict__ in, Seg
     for (uint32_t i = tid; i < QSAMP; i += 1024) {
       const uint64_t a = (uint64_t)s.cnt * i / QSAMP, b = (uint64_t)s.cnt * (i + 1) / QSAMP;
       const uint64_t h = mix64(seed ^ ((uint64_t)sid << 32) ^ i);
-      const uint64_t pos = b > a ? a + h % (b - a) : a;
+      const uint64_t pos = a + (((h >> 32) * (b - a)) >> 32);  // in [a, b) (b - a < 2^32), or a
       sv[i] = KeyOf<T>::to(in[s.off + pos]);
     }
     __syncthreads();
@@ -1290,7 +1293,9 @@ __global__ __launch_bounds__(1024) void seg_sample(const T* __restrict__ in, Seg
             if ((a > b) == ((i & kk) == 0)) { sv[i] = b; sv[ixj] = a; }
           }
         }
-        __syncthreads();
+        // stages with jj < 32 stay inside a warp (i and i ^ jj: lanes l, l ^ jj)
+        const uint32_t nj = jj > 1 ? (jj >> 1) : kk;
+        if (nj >= 32u || (jj == 1 && kk == QSAMP)) __syncthreads(); else __syncwarp();
       }
     }
     K* tb = qtab + (size_t)q * QB;
