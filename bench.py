@@ -53,8 +53,8 @@ WORKLOAD = "half_normal_f32 n=2^28, 1024 top-1% ks + k=1 + k=n (exact k-th large
 # capture of the same kernels on the same half-normal workload at n = 2^26
 # (profiles/l0_passes_half_normal_f32_n26.md); both passes read the input once,
 # so the traffic of a launch grows in proportion to n.
-PASS_TRAFFIC_PER_ELEM = {"l0_count": (268579840 + 3201024) / 2**26,
-                         "l0_compact": (271807744 + 3438080) / 2**26}
+PASS_TRAFFIC_PER_ELEM = {"l0_count": (268580096 + 3641344) / 2**26,
+                         "l0_compact": (271806720 + 3763712) / 2**26}
 
 
 def peaks():
