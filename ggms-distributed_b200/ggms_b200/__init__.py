@@ -23,7 +23,8 @@ REPO_ROOT = os.path.dirname(PKG_ROOT)
 LIB_PATH = os.path.join(PKG_ROOT, "lib", "libggms_b200.so")
 HEADER_PATHS = [os.path.join(REPO_ROOT, "include", "ggms.h"),
                 os.path.join(REPO_ROOT, "include", "ggms_diag.h"),
-                os.path.join(REPO_ROOT, "include", "ggms_noalloc.h")]
+                os.path.join(REPO_ROOT, "include", "ggms_noalloc.h"),
+                os.path.join(REPO_ROOT, "include", "ggms_generate.h")]
 NOALLOC_MAX_KS = 1024
 
 GGMS_OK = 0
@@ -145,6 +146,10 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ggms_diag_fit.argtypes = [vp, i32, i32, i32, vp, vp, vp, vp]
     lib.ggms_multiselect_noalloc_f32.restype = i32
     lib.ggms_multiselect_noalloc_f32.argtypes = [vp, i64, u32p, ctypes.c_int32, vp, vp]
+    for suf in ("f32", "f64", "u32"):
+        fn = getattr(lib, f"ggms_generate_{suf}")
+        fn.restype = i32
+        fn.argtypes = [vp, i64, i32, ctypes.c_uint64, vp]
     _lib = lib
     return lib
 
@@ -274,6 +279,19 @@ def multiselect_noalloc_f32(d_ptr: int, n: int, ks: np.ndarray, out_ptr: int, st
     return lib.ggms_multiselect_noalloc_f32(ctypes.c_void_p(d_ptr), int(n),
                                             ks.ctypes.data_as(ctypes.c_void_p), int(len(ks)),
                                             ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream))
+
+
+def generate(d_ptr: int, n: int, dtype, kind: int, seed: int, stream: int = 0) -> int:
+    """ggms_generate_<suffix>: fill n elements at device pointer d_ptr with the
+    reference's generator number `kind` of that value type (float32, float64 or
+    uint32); enqueued on `stream`, returns the status without a host sync."""
+    lib = load()
+    suf = _suffix(dtype)
+    if suf == "i32":
+        raise TypeError("no generator table for int32")
+    return getattr(lib, f"ggms_generate_{suf}")(ctypes.c_void_p(d_ptr), int(n), int(kind),
+                                                ctypes.c_uint64(seed & (2**64 - 1)),
+                                                ctypes.c_void_p(stream))
 
 
 def declared_symbols(paths=None):

@@ -41,3 +41,19 @@ def test_default_opts_layout():
     assert o.assigner == ggms_b200.ASSIGNER_AUTO
 
 
+
+
+def test_generate_rejects_before_launch():
+    """Argument checks of the device generators return before any CUDA call."""
+    lib = ggms_b200.load()
+    fake = ctypes.c_void_p(0x1000)            # never dereferenced: every case returns early
+    for suf, kinds in (("f32", 10), ("f64", 3), ("u32", 3)):
+        fn = getattr(lib, f"ggms_generate_{suf}")
+        assert fn(None, 16, 0, 1, None) == 1
+        assert fn(fake, 0, 0, 1, None) == 1
+        assert fn(fake, 16, -1, 1, None) == 1
+        assert fn(fake, 16, kinds, 1, None) == 1
+    assert lib.ggms_generate_f32(fake, 16, 2, 1, None) == 5      # KILLER FLOATS
+    assert lib.ggms_generate_f64(fake, 16, 2, 1, None) == 5      # KILLER DOUBLES
+    assert lib.ggms_generate_f32(fake, (1 << 32) + 1, 8, 1, None) == 5
+    assert lib.ggms_generate_u32(fake, (1 << 32) + 1, 1, 1, None) == 5
