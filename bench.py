@@ -130,11 +130,15 @@ def workload():
 
 
 def run_kernels_only(args):
-    """Short fixed run for profilers: a few device-resident calls per assigner."""
+    """Short fixed run for profilers: a few device-resident calls per assigner.
+    --spread-ks swaps the clustered ks for 1024 ks uniform over all ranks."""
     import torch
     import ggms_b200 as G
+    from ggms_b200 import datagen as D
     torch.cuda.set_device(0)
     v, ks = workload()
+    if args.spread_ks:
+        ks = D.ks_uniform(N_ELEMS, NK_TOP, SEED_KS)
     d_v = torch.from_numpy(v).cuda()
     d_k = torch.from_numpy(ks.view(np.int32)).cuda()
     d_out = torch.empty(len(ks), dtype=torch.float32, device="cuda")
@@ -412,6 +416,8 @@ def main():
     ap.add_argument("--n-log2", type=int, default=28, help="vector length (profiling runs only)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="a few device-resident calls and exit (for profilers); no JSON line")
+    ap.add_argument("--spread-ks", action="store_true",
+                    help="with --kernels-only: 1024 ks uniform over all ranks instead of the top 1%%")
     args = ap.parse_args()
     global N_ELEMS
     N_ELEMS = 1 << args.n_log2
