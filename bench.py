@@ -34,6 +34,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -72,7 +73,8 @@ class Clocks:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join(REPO, "gpurun_out", f"clocks_gpu{index}.csv")
+        self.path = os.path.join(os.environ.get("GGMS_CLOCKS_DIR", tempfile.gettempdir()),
+                                 f"ggms_clocks_gpu{index}.csv")
 
     def __enter__(self):
         try:

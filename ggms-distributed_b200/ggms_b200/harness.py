@@ -19,7 +19,7 @@ post-processing reads our rows unchanged:
   name, k-distribution name, then `name,time,` per algorithm run, then the
   mismatch count.
 * `compare_multiselect`: the driver.  Algorithm 0 is sort-and-choose on the GPU
-  (torch's sort of the order-preserving keys; it only judges the others),
+  (torch's sort of the order-preserving keys; it only checks the others),
   algorithms 1 and 2 are this library's `bucketMultiselect` and `iterativeSMOS`
   drop-in entry points, timed like the reference's timing functions
   (DS/iterativeSMOSTimingFunctions.cu:134-156, 207-229): the vector is already on the

@@ -93,8 +93,8 @@ def test_csv_row_layout():
 
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64, np.uint32, np.int32])
-def test_sort_and_choose_judge_order(dtype):
-    """The harness's judge (algorithm 0) on CPU tensors: the k-th largest under the
+def test_sort_and_choose_checker_order(dtype):
+    """The harness's checker (algorithm 0) on CPU tensors: the k-th largest under the
     total order -NaN < -Inf < ... < -0 < +0 < ... < +Inf < +NaN, as bit patterns."""
     import torch
     g = np.random.default_rng(1)

@@ -1,6 +1,6 @@
 """The comparison harness on the GPU: every generator of every value type and every
 k distribution through this library's bucketMultiselect and iterativeSMOS entry
-points, judged by sort-and-choose (DS/compareIterativeSMOS.cu:50-245); the rows it
+points, checked against sort-and-choose (DS/compareIterativeSMOS.cu:50-245); the rows it
 appends have the reference's layout."""
 import os
 import sys
