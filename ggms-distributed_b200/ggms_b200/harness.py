@@ -399,3 +399,65 @@ __all__ = [
     "K_GENERATORS", "generators_for", "csv_row", "error_lines", "compare_multiselect",
     "run_tests",
 ]
+
+
+# ------------------------------------------------------------------ command line
+_TYPES = (("float", np.float32), ("double", np.float64), ("uint", np.uint32))
+_QUESTIONS = ("type (0-float 1-double 2-uint)", "distribution type", "K distribution type",
+              "start power", "stop power", "start number of K values",
+              "number of K values to jump by", "stop number of K values",
+              "number of tests to run per K")
+
+
+def parse_answers(tokens: Sequence[str]) -> dict:
+    """The nine answers of the reference's interactive `main`
+    (DS/compareIterativeSMOS.cu:316-338), in its order: type, distribution, k
+    distribution, start power, stop power, start K, K jump, stop K, tests per K."""
+    if len(tokens) < 9:
+        raise ValueError(f"expected 9 answers ({', '.join(_QUESTIONS)}), got {len(tokens)}")
+    t, g, kd, p0, p1, k0, kj, k1, nt = (int(x) for x in tokens[:9])
+    if not 0 <= t < len(_TYPES):
+        raise ValueError("type must be 0 (float), 1 (double) or 2 (uint)")
+    if not 0 <= g < len(generators_for(_TYPES[t][1])) or not 0 <= kd < len(K_GENERATORS):
+        raise ValueError("generator or k distribution out of range")
+    if not (0 < p0 <= p1 <= 40 and 0 < k0 <= k1 and kj > 0 and nt > 0):
+        raise ValueError("powers, K counts, jump and test count must be positive and ordered")
+    return dict(type=t, generator=g, k_distribution=kd, start_power=p0, stop_power=p1,
+                start_k=k0, k_jump=kj, stop_k=k1, tests=nt)
+
+
+def file_name(a: dict, host: str, when: str) -> str:
+    """The reference's results file name (DS/compareIterativeSMOS.cu:355-359)."""
+    tname, dt = _TYPES[a["type"]]
+    return (f"{tname} {generators_for(dt)[a['generator']][0]} "
+            f"k-dist:{K_GENERATORS[a['k_distribution']][0]} 2^{a['start_power']} to 2^{a['stop_power']} "
+            f"({a['start_k']}:{a['k_jump']}:{a['stop_k']}) {a['tests']}-tests on {host} at {when}")
+
+
+def main(argv: Optional[Sequence[str]] = None) -> int:
+    """`python -m ggms_b200.harness [9 answers] [--csv PATH] [--seed S]`; without the
+    answers on the command line they are read from standard input, one per line, in
+    the order the reference's harness asks for them."""
+    import argparse
+    import socket
+    import sys
+    import time as _time
+
+    ap = argparse.ArgumentParser(description="compare the selectors the way compareIterativeSMOS does")
+    ap.add_argument("answers", nargs="*", help="; ".join(_QUESTIONS))
+    ap.add_argument("--csv", default=None, help="results file (default: the reference's file name)")
+    ap.add_argument("--seed", type=int, default=0)
+    args = ap.parse_args(argv)
+    tokens = list(args.answers) or sys.stdin.read().split()
+    a = parse_answers(tokens)
+    path = args.csv or file_name(a, socket.gethostname()[:20], _time.asctime())
+    print(f"File Name: {path} ")
+    runs = run_tests(_TYPES[a["type"]][1], a["generator"], path, a["start_power"], a["stop_power"],
+                     a["tests"], a["k_distribution"], a["start_k"], a["stop_k"], a["k_jump"], seed=args.seed)
+    bad = sum(sum(r["flags"]) for r in runs)
+    print(f"{len(runs)} comparisons, {bad} wrong answers")
+    return 1 if bad else 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -119,3 +119,18 @@ def test_sort_and_choose_checker_order(dtype):
         key = bits
     srt = bits[np.argsort(key, kind="stable")]
     assert np.array_equal(got.view(ib), srt[n - ks.astype(np.int64)])
+
+
+def test_command_line_answers_and_file_name():
+    a = H.parse_answers("0 0 1 20 26 101 1 101 5".split())
+    assert a == dict(type=0, generator=0, k_distribution=1, start_power=20, stop_power=26,
+                     start_k=101, k_jump=1, stop_k=101, tests=5)
+    assert H.file_name(a, "box", "Thu Dec  3 10:00:00 2026") == (
+        "float UNIFORM FLOATS k-dist:Uniform Ks 2^20 to 2^26 (101:1:101) 5-tests on box at "
+        "Thu Dec  3 10:00:00 2026")
+    d = H.parse_answers(["1", "2", "3", "10", "12", "9", "9", "27", "1"])
+    assert H.file_name(d, "h", "t").startswith("double KILLER DOUBLES k-dist:Cluster Ks 2^10 to 2^12 (9:9:27)")
+    for bad in ("3 0 0 20 26 1 1 1 1", "0 10 0 20 26 1 1 1 1", "0 0 5 20 26 1 1 1 1",
+                "0 0 0 26 20 1 1 1 1", "0 0 0 20 26 5 0 9 1", "0 0 0 20 26 1 1 1"):
+        with pytest.raises(ValueError):
+            H.parse_answers(bad.split())
