@@ -57,3 +57,18 @@ def test_generate_rejects_before_launch():
     assert lib.ggms_generate_f64(fake, 16, 2, 1, None) == 5      # KILLER DOUBLES
     assert lib.ggms_generate_f32(fake, (1 << 32) + 1, 8, 1, None) == 5
     assert lib.ggms_generate_u32(fake, (1 << 32) + 1, 1, 1, None) == 5
+
+
+def test_package_never_reaches_the_oracle():
+    """The product (the CUDA library and its Python binding) has no path to the CPU
+    oracle: no import of it, no load of its library, no link against it."""
+    pkg = os.path.dirname(ggms_b200.__file__)
+    csrc = os.path.join(os.path.dirname(pkg), "csrc")
+    files = [os.path.join(pkg, f) for f in os.listdir(pkg) if f.endswith(".py")]
+    files += [os.path.join(csrc, f) for f in os.listdir(csrc)]
+    files.append(os.path.join(os.path.dirname(pkg), "Makefile"))
+    for path in files:
+        with open(path) as f:
+            txt = f.read()
+        for needle in ("ggms_oracle", "libggms_ref", "oracle/"):
+            assert needle not in txt, (path, needle)
