@@ -1,167 +1,24 @@
-// ggms_engine.cu -- host orchestration and the C ABI (include/ggms.h).
+// ggms_engine.cuh -- host orchestration of one call: the single-vector path
+// (run_single), the batched segmented path (run_segmented), the autotuner and
+// the entry-point bodies.
 //
 // One call = one stream-ordered sequence of kernels over a cached workspace:
 // no host round trip between the passes, no allocation on the steady path,
 // one H2D of the ks and one D2H of the answers when those live in host memory.
 // (The reference does ~12 cudaMalloc/cudaFree and ~10 blocking copies per
 // call: DistributedSMOS/bucketMultiselect.cu:583-606, 625-638, 805-845.)
-#include <algorithm>
-#include <cstdio>
-#include <cstdlib>
-#include <cstring>
-#include <mutex>
-#include <new>
-#include <vector>
-
+//
+// Each translation unit that includes this header defines GGMS_TU first and
+// instantiates the templates for its own value types: the kernels (and the
+// once-per-kernel attribute flags next to their launches) then belong to that
+// unit alone, and the units compile in parallel.
+#pragma once
+#include "ggms_host.cuh"
 #include "ggms_kernels.cuh"
 #include "ggms_learned.cuh"
 #include "ggms_window.cuh"
-#include "../../include/ggms_diag.h"
 
-namespace ggms {
-
-// ------------------------------------------------------------------ context
-struct Context {
-  int device = 0;
-  int sms = 148;
-  uint8_t* arena = nullptr;
-  size_t arena_bytes = 0;
-  uint8_t* pinned = nullptr;
-  size_t pinned_bytes = 0;
-  std::mutex mu;
-  long long launches = 0;          // kernels launched by this context
-  long long graph_launches = 0;    // calls replayed from a captured CUDA graph
-  // profiling: events around pass 1, pass 2 and the whole call (ring of calls)
-  static constexpr int RING = 256;
-  bool profile = false;
-  cudaEvent_t ev[RING][6] = {};
-  int ring_head = 0, ring_count = 0;
-  // captured CUDA graphs of repeated calls (same arguments, same workspace)
-  struct Graph {
-    uint64_t key[16];
-    cudaGraphExec_t exec = nullptr;  // null: seen once, not captured yet
-    long long launches = 0;
-    uint64_t used = 0;
-  };
-  static constexpr size_t GRAPHS = 8;
-  std::vector<Graph> graphs;
-  uint64_t clock = 0;
-  cudaStream_t capture = nullptr;  // private stream the graphs are captured on
-  cudaEvent_t pin_busy = nullptr;  // recorded after the last call's uploads from the pinned buffer
-  cudaStream_t body = nullptr;     // private stream the conditional level bodies are captured on
-  cudaStream_t side = nullptr;     // the sampled assigner's build, next to the learned one
-  cudaEvent_t fork = nullptr, join = nullptr;
-  // autotuner: launch shapes and bucket counts picked per shape class
-  struct Tuned {
-    uint64_t key[4];
-    int B, nt, unroll, lv_mult;
-  };
-  std::vector<Tuned> tuned;
-};
-
-static int cuda_status(cudaError_t e) {
-  if (e == cudaSuccess) return GGMS_OK;
-  if (e == cudaErrorMemoryAllocation) return GGMS_E_OOM;
-  return GGMS_E_CUDA;
-}
-
-#define GGMS_CU(x)                                  \
-  do {                                              \
-    cudaError_t e_ = (x);                           \
-    if (e_ != cudaSuccess) return cuda_status(e_);  \
-  } while (0)
-
-static int ensure_arena(Context* c, size_t bytes) {
-  if (c->arena_bytes >= bytes) return GGMS_OK;
-  if (c->arena) {
-    GGMS_CU(cudaDeviceSynchronize());
-    cudaFree(c->arena);
-    c->arena = nullptr;
-    c->arena_bytes = 0;
-  }
-  size_t want = bytes + bytes / 8;
-  GGMS_CU(cudaMalloc(&c->arena, want));
-  c->arena_bytes = want;
-  return GGMS_OK;
-}
-
-static int ensure_pinned(Context* c, size_t bytes) {
-  if (c->pinned_bytes >= bytes) return GGMS_OK;
-  if (c->pinned) {
-    GGMS_CU(cudaDeviceSynchronize());
-    cudaFreeHost(c->pinned);
-    c->pinned = nullptr;
-    c->pinned_bytes = 0;
-  }
-  size_t want = std::max<size_t>(bytes, 1 << 16);
-  GGMS_CU(cudaMallocHost(&c->pinned, want));
-  c->pinned_bytes = want;
-  return GGMS_OK;
-}
-
-static int create_context(Context** out, int device) {
-  Context* c = new (std::nothrow) Context();
-  if (!c) return GGMS_E_OOM;
-  c->device = device;
-  cudaError_t e = cudaSetDevice(device);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
-  if (e != cudaSuccess) {
-    delete c;
-    return cuda_status(e);
-  }
-  *out = c;
-  return GGMS_OK;
-}
-
-static void destroy_context(Context* c) {
-  if (!c) return;
-  int prev = 0;
-  cudaGetDevice(&prev);
-  cudaSetDevice(c->device);
-  cudaDeviceSynchronize();
-  if (c->arena) cudaFree(c->arena);
-  if (c->pinned) cudaFreeHost(c->pinned);
-  for (int i = 0; i < Context::RING; ++i)
-    for (int j = 0; j < 6; ++j)
-      if (c->ev[i][j]) cudaEventDestroy(c->ev[i][j]);
-  for (auto& g : c->graphs)
-    if (g.exec) cudaGraphExecDestroy(g.exec);
-  if (c->capture) cudaStreamDestroy(c->capture);
-  if (c->pin_busy) cudaEventDestroy(c->pin_busy);
-  if (c->body) cudaStreamDestroy(c->body);
-  if (c->side) cudaStreamDestroy(c->side);
-  if (c->fork) cudaEventDestroy(c->fork);
-  if (c->join) cudaEventDestroy(c->join);
-  cudaSetDevice(prev);
-  delete c;
-}
-
-// default contexts of the drop-in entry points, one per device
-static std::mutex g_default_mu;
-static Context* g_default[64];
-
-static int default_context(Context** out) {
-  int dev = 0;
-  GGMS_CU(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) return GGMS_E_UNSUPPORTED;
-  std::lock_guard<std::mutex> lk(g_default_mu);
-  if (!g_default[dev]) {
-    int rc = create_context(&g_default[dev], dev);
-    if (rc != GGMS_OK) return rc;
-  }
-  *out = g_default[dev];
-  return GGMS_OK;
-}
-
-// ------------------------------------------------------------------ workspace layout
-struct Bump {
-  size_t off = 0;
-  size_t take(size_t bytes) {
-    size_t o = (off + 255) & ~(size_t)255;
-    off = o + bytes;
-    return o;
-  }
-};
+GGMS_BEGIN
 
 template <typename K>
 struct Workspace {
@@ -202,21 +59,6 @@ struct Workspace {
   size_t bytes;
 };
 
-struct Plan {
-  uint64_t n;
-  uint32_t nk;
-  uint32_t B;        // level-0 buckets
-  uint32_t S;        // sample size
-  uint32_t cap_seg;
-  uint32_t cap_tiles;
-  uint32_t ncta;     // CTAs of the two passes (identical grids)
-  int assigner;
-  int train_steps;
-  float bound;
-  float window_z;    // < 0: no PASS 1 windows
-  uint64_t seed;
-  uint32_t cap_q;    // batched path: caller segments with quantile bins (0: single path)
-};
 
 template <typename K>
 static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) {
@@ -301,115 +143,7 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
   return w;
 }
 
-static uint32_t pow2_floor(uint64_t v) {
-  uint32_t r = 1;
-  while ((uint64_t)r * 2 <= v && r < (1u << 30)) r <<= 1;
-  return r;
-}
 
-static int make_plan(Plan* p, uint64_t n, uint32_t nk, const ggms_opts& o) {
-  p->n = n;
-  p->nk = nk;
-  uint32_t B = (uint32_t)o.num_buckets;
-  if (B == 0) {
-    // about 2^11 elements per bucket, between 2^10 and 2^13 buckets
-    B = pow2_floor(std::max<uint64_t>(n >> 11, 1));
-    B = std::min<uint32_t>(std::max<uint32_t>(B, 1u << 10), 1u << 13);
-  }
-  if (B < (1u << 10) || B > (1u << 15) || (B & (B - 1))) return GGMS_E_INVALID_ARG;
-  p->B = B;
-  int asg = o.assigner;
-  if (asg < GGMS_ASSIGNER_AUTO || asg > GGMS_ASSIGNER_LEARNED_MLP) return GGMS_E_INVALID_ARG;
-  p->assigner = asg;
-  uint32_t S = (uint32_t)o.sample_size;
-  if (S == 0) S = (asg == GGMS_ASSIGNER_SAMPLED) ? 1024u : (1u << 16);
-  if (S < 1024u || S > 65536u || (S & (S - 1))) return GGMS_E_INVALID_ARG;
-  p->S = S;
-  p->ncta = 0;
-  p->cap_seg = nk + 1;
-  p->cap_tiles = (uint32_t)((n + TILE - 1) / TILE) + p->cap_seg;
-  p->train_steps = o.train_steps > 0 ? o.train_steps : 0;
-  p->bound = o.imbalance_bound > 0.0f ? o.imbalance_bound : 3.0f;
-  p->window_z = o.window_z == 0.0f ? 8.0f : o.window_z;
-  p->seed = o.seed;
-  p->cap_q = 0;
-  return GGMS_OK;
-}
-
-static inline uint32_t float_bits(float f) {
-  uint32_t u;
-  memcpy(&u, &f, 4);
-  return u;
-}
-
-// ------------------------------------------------------------------ CUDA graphs
-// A call whose kernel sequence and arguments repeat (same pointers, sizes,
-// options and workspace) is captured into a CUDA graph the second time it is
-// seen and replayed from then on: one graph launch instead of ~30 kernel
-// launches.  `enqueue(stream)` must issue only stream-ordered work (no host
-// sync, no allocation).  The first call of a key runs directly, which also
-// sets the kernels' attributes before any capture.  A failed capture falls
-// back to running directly.
-template <typename F>
-static int run_graphed(Context* c, const uint64_t* key, int nkey, cudaStream_t st, F&& enqueue) {
-  auto same = [&](const Context::Graph& g) {
-    for (int i = 0; i < 16; ++i)
-      if (g.key[i] != (i < nkey ? key[i] : 0ull)) return false;
-    return true;
-  };
-  Context::Graph* hit = nullptr;
-  for (auto& g : c->graphs)
-    if (same(g)) hit = &g;
-  if (hit && hit->exec) {
-    hit->used = ++c->clock;
-    GGMS_CU(cudaGraphLaunch(hit->exec, st));
-    c->launches += hit->launches;
-    ++c->graph_launches;
-    return GGMS_OK;
-  }
-  if (!hit) {  // first sighting: remember the key (evicting the least recently used), run directly
-    if (c->graphs.size() >= Context::GRAPHS) {
-      auto lru = std::min_element(c->graphs.begin(), c->graphs.end(),
-                                  [](const Context::Graph& a, const Context::Graph& b) { return a.used < b.used; });
-      if (lru->exec) cudaGraphExecDestroy(lru->exec);
-      c->graphs.erase(lru);
-    }
-    Context::Graph g;
-    for (int i = 0; i < 16; ++i) g.key[i] = i < nkey ? key[i] : 0ull;
-    g.used = ++c->clock;
-    c->graphs.push_back(g);
-    return enqueue(st);
-  }
-  // second sighting: capture, then launch
-  if (!c->capture) GGMS_CU(cudaStreamCreateWithFlags(&c->capture, cudaStreamNonBlocking));
-  const long long before = c->launches;
-  if (cudaStreamBeginCapture(c->capture, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return enqueue(st);
-  const int rc = enqueue(c->capture);
-  cudaGraph_t graph = nullptr;
-  const cudaError_t e = cudaStreamEndCapture(c->capture, &graph);
-  cudaGraphExec_t exec = nullptr;
-  const bool ok = rc == GGMS_OK && e == cudaSuccess && graph &&
-                  cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
-  if (graph) cudaGraphDestroy(graph);
-  const long long captured = c->launches - before;  // kernels the graph holds
-  c->launches = before;
-  if (!ok) {
-    cudaGetLastError();
-    return enqueue(st);
-  }
-  hit->exec = exec;
-  hit->launches = captured;
-  hit->used = ++c->clock;
-  GGMS_CU(cudaGraphLaunch(exec, st));
-  c->launches += captured;
-  ++c->graph_launches;
-  return GGMS_OK;
-}
-
-// One refinement level.  Captured into a graph, it becomes an IF node whose
-// condition lvl_gate sets on the device: once a level finds no segment, it
-// and every later level cost nothing.  Run directly, the level's kernels are
-// launched as they are (each returns at once when there is no work).
 template <typename F>
 static int enqueue_level(Context* c, cudaStream_t s, Counters* C, int p, F&& body) {
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -469,7 +203,7 @@ template <typename T>
 struct PassVariant {
   using K = typename KeyOf<T>::K;
   int nt, unroll;
-  void (*count)(const T*, uint64_t, const Grid<K>*, const Counters*, const Windows<K>*, uint32_t*, uint32_t*);
+  void (*count)(const T*, uint64_t, const Grid<K>*, Counters*, const Windows<K>*, uint32_t*, uint32_t*);
   void (*compact)(const T*, uint64_t, const Grid<K>*, Counters*, const Windows<K>*, const uint32_t*,
                   const uint32_t*, K*, uint64_t);
   void (*coarse)(const T*, uint64_t, const Grid<K>*, Counters*, const uint32_t*, const uint32_t*, K*, uint64_t);
@@ -552,20 +286,6 @@ static int launch_small_select(Context* ctx, const InT* src, const Seg<K>* segs_
 }
 
 // Profiling slot of the current call (or null when profiling is off).
-static cudaEvent_t* prof_slot(Context* c) {
-  if (!c->profile) return nullptr;
-  if (c->ring_count == Context::RING) return nullptr;  // ring full: drop
-  int idx = (c->ring_head + c->ring_count) % Context::RING;
-  if (!c->ev[idx][0])
-    for (int j = 0; j < 6; ++j) cudaEventCreate(&c->ev[idx][j]);
-  c->ring_count++;
-  return c->ev[idx];
-}
-static inline void prof_rec(cudaEvent_t* slot, int j, cudaStream_t st) {
-  if (slot) cudaEventRecord(slot[j], st);
-}
-
-static inline unsigned cdiv(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }
 
 // ------------------------------------------------------------------ the single-vector path
 template <typename T>
@@ -649,6 +369,7 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
       ++ctx->launches;
       asg_merge_rank<K><<<cdiv(S, 256), 256, 0, s>>>(w.samp_tmp, w.samp_sorted, S, 4096u);
     }
+    prof_rec(prof, 6, s);
     rc = setup_attrs<K>();
     if (rc) return rc;
     if (p.assigner == GGMS_ASSIGNER_SAMPLED) {
@@ -669,11 +390,12 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
       GGMS_CU(cudaEventRecord(ctx->join, ctx->side));
       rc = learn_and_choose<K>(p.assigner, w.samp_sorted, S, p.B, p.train_steps, p.bound, w.asg,
                                w.grid, w.learn, &w.C->asg_choice, w.krank, nk, n, p.window_z, s,
-                               &ctx->launches, ctx->join);
+                               &ctx->launches, ctx->join, p.pl_knots);
       if (rc) return rc;
     }
 
     // ---- PASS 1 windows
+    prof_rec(prof, 7, s);
     if (p.window_z >= 0.0f) {
       ++ctx->launches;
       l0_window<K><<<1, WIN_NT, l0_window_smem<K>(p.B), s>>>(w.samp_sorted, S, w.krank, nk, n, w.grid,
@@ -761,6 +483,7 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     }
 
     // ---- answers
+    prof_rec(prof, 8, s);
     T* d_out = host_out ? (T*)w.out_dev : out;
     ++ctx->launches;
     write_out<T><<<cdiv(nk, 256), 256, 0, s>>>(w.kkey, w.kseg, nk, d_out, w.C);
@@ -781,9 +504,11 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
                             p.seed, (uint64_t)(uint32_t)p.train_steps | ((uint64_t)pv->nt << 32),
                             (uint64_t)pv->unroll | ((uint64_t)float_bits(p.bound) << 8),
                             (uint64_t)float_bits(p.window_z), (uint64_t)(uintptr_t)ctx->arena,
-                            (uint64_t)(uintptr_t)ctx->pinned};
+                            (uint64_t)(uintptr_t)ctx->pinned, (uint64_t)p.pl_knots};
     rc = run_graphed(ctx, key, (int)(sizeof(key) / sizeof(key[0])), st, enqueue);
   }
+  if (rc) return rc;
+  rc = mark_done(ctx, st);
   if (rc) return rc;
   if (host_k && !topk) {
     if (!ctx->pin_busy) GGMS_CU(cudaEventCreateWithFlags(&ctx->pin_busy, cudaEventDisableTiming));
@@ -801,7 +526,7 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     GGMS_CU(cudaMemcpy(&ls, w.learn, sizeof(LearnState), cudaMemcpyDeviceToHost));
     s->assigner_used = (int32_t)a_used.kind;
     s->num_buckets = (int32_t)p.B;
-    s->full_passes = 2;
+    s->full_passes = (int32_t)pin_C->passes;
     s->levels = (int32_t)pin_C->levels_run;
     s->candidates = (int64_t)pin_C->cand0;
     s->refine_elements = (int64_t)pin_C->refine_elems;
@@ -813,47 +538,13 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     s->model_imbalance = (p.assigner == GGMS_ASSIGNER_SAMPLED) ? 0.0f : ls.imbalance;
     s->model_loss = (p.assigner == GGMS_ASSIGNER_SAMPLED) ? 0.0f : ls.loss;
     s->window_runs = (int32_t)pin_C->win_runs;
+    if (!o.pad0) s->model_segments = (p.assigner == GGMS_ASSIGNER_SAMPLED || a_used.kind == GGMS_ASSIGNER_SAMPLED)
+                                         ? 0 : (int32_t)ls.M;
   }
   if (pin_C->status) return (int)pin_C->status;
   return GGMS_OK;
 }
 
-// ------------------------------------------------------------------ autotuner
-// With opts->autotune set and the bucket count and pass shape left to the
-// library, the first call of a shape class (type, log2 n, log2 K, assigner,
-// where ks and answers live) times every candidate on the caller's own data --
-// each candidate a full, correct call: 1 warm-up + 2 timed with CUDA events on
-// the caller's stream -- and keeps the fastest in the context; later calls of
-// the class use it.  The batched path tunes the CTAs per SM of its level
-// kernels the same way (class: type, log2 n, log2 K, log2 segments).
-static const Context::Tuned* tuned_find(Context* c, const uint64_t* key) {
-  for (const auto& t : c->tuned)
-    if (!memcmp(t.key, key, sizeof(t.key))) return &t;
-  return nullptr;
-}
-
-static int bitlen64(uint64_t v) {
-  int b = 0;
-  while (v) { ++b; v >>= 1; }
-  return b;
-}
-
-template <typename F>
-static int time_calls(cudaStream_t st, F&& call, float* ms) {
-  int rc = call();  // warm-up (and graph capture of repeated calls)
-  if (rc) return rc;
-  cudaEvent_t e0, e1;
-  GGMS_CU(cudaEventCreate(&e0));
-  GGMS_CU(cudaEventCreate(&e1));
-  GGMS_CU(cudaEventRecord(e0, st));
-  for (int i = 0; i < 2 && !rc; ++i) rc = call();
-  GGMS_CU(cudaEventRecord(e1, st));
-  GGMS_CU(cudaEventSynchronize(e1));
-  cudaEventElapsedTime(ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  return rc;
-}
 
 template <typename T>
 static int run_single_tuned(Context* c, const T* d_in, uint64_t n, const uint32_t* ks, uint64_t nk, T* out,
@@ -918,11 +609,7 @@ static int topk_call(ggms_context* cx, const T* d_in, int64_t n, int64_t K, T* o
                      const ggms_opts* opts, void* stream) {
   if (n <= 0 || K <= 0) return GGMS_E_INVALID_ARG;
   ggms_opts o;
-  ggms_default_opts(&o);
-  if (opts) {
-    if (opts->struct_size != (int32_t)sizeof(ggms_opts)) return GGMS_E_INVALID_ARG;
-    o = *opts;
-  }
+  if (read_opts(opts, &o) != GGMS_OK) return GGMS_E_INVALID_ARG;
   Context* c = (Context*)cx;
   if (!c) {
     int rc = default_context(&c);
@@ -937,11 +624,7 @@ static int ex(ggms_context* cx, const T* d_in, int64_t n, const uint32_t* ks, in
               const ggms_opts* opts, void* stream) {
   if (n <= 0 || nk < 0) return GGMS_E_INVALID_ARG;
   ggms_opts o;
-  ggms_default_opts(&o);
-  if (opts) {
-    if (opts->struct_size != (int32_t)sizeof(ggms_opts)) return GGMS_E_INVALID_ARG;
-    o = *opts;
-  }
+  if (read_opts(opts, &o) != GGMS_OK) return GGMS_E_INVALID_ARG;
   Context* c = (Context*)cx;
   if (!c) {
     int rc = default_context(&c);
@@ -1077,6 +760,8 @@ static int run_segmented(Context* ctx, const T* d_in, const int64_t* seg_off, in
     rc = run_graphed(ctx, key, (int)(sizeof(key) / sizeof(key[0])), st, enqueue);
   }
   if (rc) return rc;
+  rc = mark_done(ctx, st);
+  if (rc) return rc;
   if (o.stats) {
     Counters hc;
     GGMS_CU(cudaMemcpyAsync(&hc, w.C, sizeof(Counters), cudaMemcpyDeviceToHost, st));
@@ -1084,7 +769,7 @@ static int run_segmented(Context* ctx, const T* d_in, const int64_t* seg_off, in
     memset(o.stats, 0, sizeof(ggms_stats));
     o.stats->levels = (int32_t)hc.levels_run;
     o.stats->refine_elements = (int64_t)hc.refine_elems;
-    o.stats->full_passes = 2;
+    o.stats->full_passes = (int32_t)hc.passes;
     if (hc.status) return (int)hc.status;
   }
   return GGMS_OK;
@@ -1131,11 +816,7 @@ static int segmented(ggms_context* cx, const T* d_in, const int64_t* seg_off, in
                      const uint32_t* ks, const int64_t* k_off, T* out, const ggms_opts* opts,
                      void* stream) {
   ggms_opts o;
-  ggms_default_opts(&o);
-  if (opts) {
-    if (opts->struct_size != (int32_t)sizeof(ggms_opts)) return GGMS_E_INVALID_ARG;
-    o = *opts;
-  }
+  if (read_opts(opts, &o) != GGMS_OK) return GGMS_E_INVALID_ARG;
   Context* c = (Context*)cx;
   if (!c) {
     int rc = default_context(&c);
@@ -1146,274 +827,5 @@ static int segmented(ggms_context* cx, const T* d_in, const int64_t* seg_off, in
 }
 
 
-// ------------------------------------------------------------------ diagnostics
-namespace diag {
 
-struct DevBuf {
-  void* p = nullptr;
-  ~DevBuf() { if (p) cudaFree(p); }
-};
-
-static int pl_gradient(const uint32_t* keys, int S, const float* theta, float* loss, float* grad,
-                       uint32_t* knots, int* Mout) {
-  if (!keys || S < 2 || S > 65536 || !theta || !loss || !grad) return GGMS_E_INVALID_ARG;
-  DevBuf dk, da, dt, dout, dl;
-  GGMS_CU(cudaMalloc(&dk.p, 4ull * S));
-  GGMS_CU(cudaMalloc(&da.p, sizeof(Assigner<uint32_t>)));
-  GGMS_CU(cudaMalloc(&dl.p, sizeof(LearnState)));
-  GGMS_CU(cudaMalloc(&dt.p, 4ull * PL_M));
-  GGMS_CU(cudaMalloc(&dout.p, 4ull * (PL_M + 1)));
-  GGMS_CU(cudaMemcpy(dk.p, keys, 4ull * S, cudaMemcpyHostToDevice));
-  GGMS_CU(cudaMemcpy(dt.p, theta, 4ull * PL_M, cudaMemcpyHostToDevice));
-  auto* A = (Assigner<uint32_t>*)da.p;
-  float* dloss = (float*)dout.p;
-  float* dgrad = dloss + 1;
-  auto* L = (LearnState*)dl.p;
-  GGMS_CU(cudaFuncSetAttribute(pl_grad_probe<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)sizeof(LearnSmem<uint32_t>)));
-  GGMS_CU(cudaFuncSetAttribute(setup_pl_knots<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)sizeof(LearnSmem<uint32_t>)));
-  // the same three kernels as training: knots, statistics, forward/backward
-  setup_pl_knots<uint32_t><<<1, SETUP_NT, sizeof(LearnSmem<uint32_t>)>>>((const uint32_t*)dk.p,
-                                                                          (uint32_t)S, 1u << 14, A);
-  pl_stats_grid<uint32_t><<<(PL_M + 31) / 32, 1024>>>((const uint32_t*)dk.p, (uint32_t)S, A, L);
-  pl_grad_probe<uint32_t><<<1, SETUP_NT, sizeof(LearnSmem<uint32_t>)>>>(A, (uint32_t)S, L,
-                                                                         (const float*)dt.p, dloss, dgrad);
-  GGMS_CU(cudaDeviceSynchronize());
-  Assigner<uint32_t> h;
-  GGMS_CU(cudaMemcpy(&h, A, sizeof(h), cudaMemcpyDeviceToHost));
-  GGMS_CU(cudaMemcpy(loss, dloss, 4, cudaMemcpyDeviceToHost));
-  GGMS_CU(cudaMemcpy(grad, dgrad, 4ull * h.M, cudaMemcpyDeviceToHost));
-  if (knots) memcpy(knots, h.x, 4ull * (h.M + 1));
-  if (Mout) *Mout = (int)h.M;
-  return GGMS_OK;
-}
-
-static int mlp_gradient(const float* x, const float* t, const float* params, float* loss, float* grad) {
-  if (!x || !t || !params || !loss || !grad) return GGMS_E_INVALID_ARG;
-  DevBuf dx, dt, dp, dprobe;
-  GGMS_CU(cudaMalloc(&dx.p, 4ull * MLP_Q));
-  GGMS_CU(cudaMalloc(&dt.p, 4ull * MLP_Q));
-  GGMS_CU(cudaMalloc(&dp.p, 4ull * MLP_NP));
-  GGMS_CU(cudaMalloc(&dprobe.p, 4ull * (MLP_NP + 1)));
-  GGMS_CU(cudaMemcpy(dx.p, x, 4ull * MLP_Q, cudaMemcpyHostToDevice));
-  GGMS_CU(cudaMemcpy(dt.p, t, 4ull * MLP_Q, cudaMemcpyHostToDevice));
-  GGMS_CU(cudaMemcpy(dp.p, params, 4ull * MLP_NP, cudaMemcpyHostToDevice));
-  GGMS_CU(cudaFuncSetAttribute(mlp_train<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)sizeof(MlpSmem)));
-  mlp_train<uint32_t><<<MLP_CTAS, MLP_NT, sizeof(MlpSmem)>>>(
-      nullptr, 0u, nullptr, nullptr, (float*)dp.p, 0u, 0.0f, (const float*)dx.p, (const float*)dt.p,
-      (float*)dprobe.p);
-  GGMS_CU(cudaDeviceSynchronize());
-  float* hp = (float*)malloc(4ull * (MLP_NP + 1));
-  if (!hp) return GGMS_E_OOM;
-  cudaError_t e = cudaMemcpy(hp, dprobe.p, 4ull * (MLP_NP + 1), cudaMemcpyDeviceToHost);
-  if (e == cudaSuccess) {
-    memcpy(grad, hp, 4ull * MLP_NP);
-    *loss = hp[MLP_NP];
-  }
-  free(hp);
-  return cuda_status(e);
-}
-
-static int fit(const uint32_t* keys, int S, int kind, int steps, float* l0, float* l1, float* imb_m,
-               float* imb_s) {
-  if (!keys || S < 1024 || (kind != GGMS_ASSIGNER_LEARNED_PL && kind != GGMS_ASSIGNER_LEARNED_MLP))
-    return GGMS_E_INVALID_ARG;
-  DevBuf dk, da, dg, dl, dc;
-  GGMS_CU(cudaMalloc(&dk.p, 4ull * S));
-  GGMS_CU(cudaMalloc(&da.p, 2 * sizeof(Assigner<uint32_t>)));
-  GGMS_CU(cudaMalloc(&dg.p, 2 * sizeof(Grid<uint32_t>)));
-  GGMS_CU(cudaMalloc(&dl.p, sizeof(LearnState)));
-  GGMS_CU(cudaMalloc(&dc.p, 4));
-  GGMS_CU(cudaMemcpy(dk.p, keys, 4ull * S, cudaMemcpyHostToDevice));
-  auto* As = (Assigner<uint32_t>*)da.p;
-  auto* Gs = (Grid<uint32_t>*)dg.p;
-  auto* L = (LearnState*)dl.p;
-  const uint32_t* k = (const uint32_t*)dk.p;
-  const uint32_t B = 1u << 14;
-  int rc = setup_attrs<uint32_t>();
-  if (rc) return rc;
-  setup_sampled<uint32_t><<<1, SETUP_NT, sizeof(SetupSmem<uint32_t>)>>>(k, (uint32_t)S, B, &As[0], &Gs[0]);
-  long long launches = 0;
-  rc = learn_and_choose<uint32_t>(kind, k, (uint32_t)S, B, steps, 1e30f, As, Gs, L, (uint32_t*)dc.p,
-                                  nullptr, 0u, 0ull, -1.0f, 0, &launches);
-  if (rc) return rc;
-  GGMS_CU(cudaDeviceSynchronize());
-  LearnState hl;
-  Grid<uint32_t> a0, a1;
-  GGMS_CU(cudaMemcpy(&hl, L, sizeof(hl), cudaMemcpyDeviceToHost));
-  GGMS_CU(cudaMemcpy(&a0, &Gs[0], sizeof(a0), cudaMemcpyDeviceToHost));
-  GGMS_CU(cudaMemcpy(&a1, &Gs[1], sizeof(a1), cudaMemcpyDeviceToHost));
-  if (l0) *l0 = (kind == GGMS_ASSIGNER_LEARNED_PL) ? hl.loss_init : -1.0f;
-  if (l1) *l1 = (kind == GGMS_ASSIGNER_LEARNED_PL) ? hl.loss : hl.mlp_loss;
-  if (imb_m) *imb_m = a1.quality;
-  if (imb_s) *imb_s = a0.quality;
-  return GGMS_OK;
-}
-
-}  // namespace diag
-
-}  // namespace ggms
-
-// ====================================================================== C ABI
-using namespace ggms;
-
-extern "C" {
-
-void ggms_default_opts(ggms_opts* o) {
-  if (!o) return;
-  memset(o, 0, sizeof(*o));
-  o->struct_size = (int32_t)sizeof(ggms_opts);
-  o->assigner = GGMS_ASSIGNER_AUTO;
-  o->seed = 0x5EEDull;
-  o->imbalance_bound = 3.0f;
-}
-
-const char* ggms_status_string(int s) {
-  switch (s) {
-    case GGMS_OK: return "ok";
-    case GGMS_E_INVALID_ARG: return "invalid argument";
-    case GGMS_E_OOM: return "out of memory";
-    case GGMS_E_NOT_CONVERGED: return "not converged";
-    case GGMS_E_CUDA: return "CUDA error";
-    case GGMS_E_UNSUPPORTED: return "unsupported";
-    case GGMS_E_INTERNAL: return "internal error";
-    default: return "unknown status";
-  }
-}
-
-int ggms_version(void) { return 100; }
-
-int ggms_create(ggms_context** ctx, int device) {
-  if (!ctx) return GGMS_E_INVALID_ARG;
-  Context* c = nullptr;
-  int rc = create_context(&c, device);
-  if (rc) return rc;
-  *ctx = (ggms_context*)c;
-  return GGMS_OK;
-}
-
-int ggms_destroy(ggms_context* ctx) {
-  destroy_context((Context*)ctx);
-  return GGMS_OK;
-}
-
-int ggms_get_default_context(ggms_context** ctx) {
-  if (!ctx) return GGMS_E_INVALID_ARG;
-  Context* c = nullptr;
-  int rc = default_context(&c);
-  if (rc) return rc;
-  *ctx = (ggms_context*)c;
-  return GGMS_OK;
-}
-
-int ggms_context_profile(ggms_context* ctx, int enable) {
-  Context* c = (Context*)ctx;
-  if (!c) return GGMS_E_INVALID_ARG;
-  std::lock_guard<std::mutex> lk(c->mu);
-  c->profile = enable != 0;
-  return GGMS_OK;
-}
-
-int ggms_context_pass_times(ggms_context* ctx, float* p1, float* p2, float* call, int max) {
-  Context* c = (Context*)ctx;
-  if (!c || max < 0) return -GGMS_E_INVALID_ARG;
-  std::lock_guard<std::mutex> lk(c->mu);
-  int got = 0;
-  while (c->ring_count > 0 && got < max) {
-    cudaEvent_t* e = c->ev[c->ring_head];
-    if (cudaEventSynchronize(e[5]) != cudaSuccess) return -GGMS_E_CUDA;
-    float a = 0, b = 0, t = 0;
-    cudaEventElapsedTime(&a, e[1], e[2]);
-    cudaEventElapsedTime(&b, e[3], e[4]);
-    cudaEventElapsedTime(&t, e[0], e[5]);
-    if (p1) p1[got] = a;
-    if (p2) p2[got] = b;
-    if (call) call[got] = t;
-    ++got;
-    c->ring_head = (c->ring_head + 1) % Context::RING;
-    c->ring_count--;
-  }
-  return got;
-}
-
-int64_t ggms_context_launches(ggms_context* ctx) {
-  Context* c = (Context*)ctx;
-  if (!c) return -1;
-  return (int64_t)c->launches;
-}
-
-int64_t ggms_context_graph_launches(ggms_context* ctx) {
-  Context* c = (Context*)ctx;
-  if (!c) return -1;
-  std::lock_guard<std::mutex> lk(c->mu);
-  return c->graph_launches;
-}
-
-#define GGMS_DROPIN(NAME, T)                                                                 \
-  int NAME(const T* d_vector, int length, const uint32_t* kVals, int numKs, T* outputs,     \
-           int blocks, int threads) {                                                        \
-    (void)blocks;                                                                            \
-    (void)threads;                                                                           \
-    return dropin<T>(d_vector, length, kVals, numKs, outputs);                               \
-  }
-
-GGMS_DROPIN(ggms_bucket_multiselect_f32, float)
-GGMS_DROPIN(ggms_bucket_multiselect_f64, double)
-GGMS_DROPIN(ggms_bucket_multiselect_u32, uint32_t)
-GGMS_DROPIN(ggms_bucket_multiselect_i32, int32_t)
-GGMS_DROPIN(ggms_iterative_smos_f32, float)
-GGMS_DROPIN(ggms_iterative_smos_f64, double)
-GGMS_DROPIN(ggms_iterative_smos_u32, uint32_t)
-GGMS_DROPIN(ggms_iterative_smos_i32, int32_t)
-
-#define GGMS_EX(NAME, T)                                                                      \
-  int NAME(ggms_context* ctx, const T* d_in, int64_t n, const uint32_t* ks, int64_t nk,      \
-           T* out, const ggms_opts* opts, void* stream) {                                     \
-    return ex<T>(ctx, d_in, n, ks, nk, out, opts, stream);                                    \
-  }
-
-GGMS_EX(ggms_multiselect_f32_ex, float)
-GGMS_EX(ggms_multiselect_f64_ex, double)
-GGMS_EX(ggms_multiselect_u32_ex, uint32_t)
-GGMS_EX(ggms_multiselect_i32_ex, int32_t)
-
-#define GGMS_TOPK(NAME, T)                                                                   \
-  int NAME(ggms_context* ctx, const T* d_in, int64_t n, int64_t K, T* out,                  \
-           const ggms_opts* opts, void* stream) {                                            \
-    return topk_call<T>(ctx, d_in, n, K, out, opts, stream);                                 \
-  }
-
-GGMS_TOPK(ggms_topk_f32, float)
-GGMS_TOPK(ggms_topk_f64, double)
-GGMS_TOPK(ggms_topk_u32, uint32_t)
-GGMS_TOPK(ggms_topk_i32, int32_t)
-
-int ggms_multiselect_segmented_f32(ggms_context* ctx, const float* d_in, const int64_t* seg_off,
-                                   int64_t nseg, const uint32_t* ks, const int64_t* k_off,
-                                   float* out, const ggms_opts* opts, void* stream) {
-  return segmented<float>(ctx, d_in, seg_off, nseg, ks, k_off, out, opts, stream);
-}
-int ggms_multiselect_segmented_u32(ggms_context* ctx, const uint32_t* d_in, const int64_t* seg_off,
-                                   int64_t nseg, const uint32_t* ks, const int64_t* k_off,
-                                   uint32_t* out, const ggms_opts* opts, void* stream) {
-  return segmented<uint32_t>(ctx, d_in, seg_off, nseg, ks, k_off, out, opts, stream);
-}
-
-int ggms_diag_pl_gradient(const uint32_t* keys, int S, const float* theta, float* loss, float* grad,
-                          uint32_t* knots, int* M) {
-  return diag::pl_gradient(keys, S, theta, loss, grad, knots, M);
-}
-
-int ggms_diag_mlp_gradient(const float* x, const float* t, const float* params, float* loss,
-                           float* grad) {
-  return diag::mlp_gradient(x, t, params, loss, grad);
-}
-
-int ggms_diag_fit(const uint32_t* keys, int S, int kind, int steps, float* l0, float* l1,
-                  float* imb_m, float* imb_s) {
-  return diag::fit(keys, S, kind, steps, l0, l1, imb_m, imb_s);
-}
-
-}  // extern "C"
+GGMS_END

@@ -14,6 +14,16 @@
 #include <type_traits>
 #include <cuda_runtime.h>
 
+// Kernels and the host code that launches them are compiled once per value
+// type, each translation unit in its own inline namespace ggms::GGMS_TU, so
+// no two units share a kernel (or the flag that records that its launch
+// attributes were set).  The types and inline helpers below are shared.
+#ifndef GGMS_TU
+#define GGMS_TU tu_default
+#endif
+#define GGMS_BEGIN namespace ggms { inline namespace GGMS_TU {
+#define GGMS_END } }
+
 namespace ggms {
 
 // ------------------------------------------------------------------ key traits
@@ -275,7 +285,7 @@ struct Counters {
   uint32_t ntiny;             // tiny segments created by the current level (batched path)
   uint32_t nbig[2];           // segments of pool p that a level refines (listed in bigs[p])
   uint32_t coarse;            // level 0 copies NGRP groups of buckets (most buckets hold a k)
-  uint32_t pad1[1];
+  uint32_t passes;            // launches that read the whole input (counted by the kernels themselves)
 };
 
 // PASS 1 windows (l0_window).  From the sample, every requested k gets a

@@ -31,7 +31,7 @@
 #include "ggms_internal.cuh"
 #include "../../include/ggms.h"
 
-namespace ggms {
+GGMS_BEGIN
 
 constexpr unsigned FULL = 0xFFFFFFFFu;
 
@@ -387,7 +387,7 @@ __device__ __forceinline__ void count_runs(const Windows<typename KeyOf<T>::K>& 
 template <typename T, int NT, int UNROLL>
 __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_count(const T* __restrict__ in, uint64_t n,
                                               const Grid<typename KeyOf<T>::K>* __restrict__ Gs,
-                                              const Counters* __restrict__ C,
+                                              Counters* C,
                                               const Windows<typename KeyOf<T>::K>* __restrict__ Wg,
                                               uint32_t* __restrict__ hist0, uint32_t* __restrict__ crow) {
   using K = typename KeyOf<T>::K;
@@ -403,6 +403,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_count(const T* __res
   const uint32_t B = gv.B;
   K* wq = reinterpret_cast<K*>(hs + B) + (threadIdx.x >> 5) * WQ_DEPTH;
   if (threadIdx.x == 0) W = *Wg;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&C->passes, 1u);
   for (uint32_t i = threadIdx.x; i < B; i += NT) hs[i] = 0u;
   __syncthreads();
   const uint32_t lane = threadIdx.x & 31;
@@ -788,6 +789,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
   extern __shared__ __align__(16) uint8_t smem[];
   __shared__ Windows<K> W;
   if (threadIdx.x == 0) W = *Wg;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&C->passes, 1u);
   const Grid<K>* G = Gs + C->asg_choice;
   uint2* s1 = (uint2*)smem;
   uint2* s2 = s1 + GRID_T1;
@@ -1062,6 +1064,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact_coarse(const
   constexpr uint32_t NONE = 0xFFFFFFFFu;
   static_assert(CH <= 65536u, "chunk ranks are 16-bit");
   if (!C->coarse) return;  // l0_compact copies this call's buckets
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&C->passes, 1u);
   extern __shared__ __align__(16) uint8_t smem[];
   __shared__ uint32_t gbase[NGRP], hist[NGRP], off[NGRP], cflag[NGRP / 32];
   __shared__ uint32_t total_s;
@@ -1343,6 +1346,7 @@ __global__ __launch_bounds__(NT) void lvl_count(const InT* __restrict__ src,
   __shared__ __align__(16) uint16_t qd[Q ? QDS : 8];
   const uint32_t nt = min(C->ntiles[p], caps.tiles);
   const uint32_t ns = min(C->nsegs[p], caps.segs);
+  if (Q && nt && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&C->passes, 1u);  // level 0 reads the input
   uint32_t loaded = 0xFFFFFFFFu;  // quantile table in shared memory
   for (uint32_t t = blockIdx.x; t < nt; t += gridDim.x) {
     const TileRef tr = tiles[t];
@@ -1492,6 +1496,8 @@ __global__ __launch_bounds__(NT) void lvl_compact(const InT* __restrict__ src,
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t nt = min(C->ntiles[p], caps.tiles);
   const uint32_t ns = min(C->nsegs[p], caps.segs);
+  if (Q && nt && blockIdx.x == 0 && threadIdx.x == 0)  // level 0 reads the input
+    atomicAdd(&const_cast<Counters*>(C)->passes, 1u);
   uint32_t loaded = 0xFFFFFFFFu;  // segment whose child map (and table) is in shared memory
   for (uint32_t t = blockIdx.x; t < nt; t += gridDim.x) {
     const TileRef tr = tiles[t];
@@ -2017,4 +2023,4 @@ __global__ void write_out(const typename KeyOf<T>::K* __restrict__ k_key,
   out[i] = KeyOf<T>::from(k_key[i]);
 }
 
-}  // namespace ggms
+GGMS_END

@@ -22,7 +22,7 @@
 #pragma once
 #include "ggms_setup.cuh"
 
-namespace ggms {
+GGMS_BEGIN
 
 constexpr int PL_M = 1024;       // segments of the learned PL model
 constexpr int MLP_H = 32;        // hidden width of the MLP model
@@ -267,8 +267,8 @@ __host__ __device__ constexpr uint32_t pl_knots_for(uint32_t B) {
 // Quantile knots: q_j = round(j * (S - 1) / M), initial CDF j / M.
 template <typename K>
 __device__ void pl_knots(const K* sorted, uint32_t S, uint32_t B, uint32_t kind, Assigner<K>* A,
-                         LearnSmem<K>& sm) {
-  const uint32_t Mq = pl_knots_for(B);
+                         LearnSmem<K>& sm, uint32_t mreq = 0) {
+  const uint32_t Mq = mreq ? min(pl_knots_for(B), mreq) : pl_knots_for(B);
   for (uint32_t j = threadIdx.x; j <= Mq; j += blockDim.x) {
     sm.q[j] = (uint32_t)(((uint64_t)j * (S - 1u) + Mq / 2) / Mq);
     sm.qcdf[j] = (float)j / (float)Mq;
@@ -302,13 +302,14 @@ __device__ void learned_finish(const K* sorted, uint32_t S, uint32_t B, uint32_t
 // The whole learned-PL setup in one CTA: knots -> statistics -> training ->
 // bases -> grid -> occupancy -> choice (grid 1 if within the bound, else the
 // sampled grid 0 stays in use).
-// Knots of the learned PL model (one CTA): quantile knots, deduplicated.
+// Knots of the learned PL model (one CTA): quantile knots, deduplicated;
+// mreq segments requested (0: the default, min(PL_M, B / 4)).
 template <typename K>
 __global__ __launch_bounds__(SETUP_NT) void setup_pl_knots(const K* __restrict__ sorted, uint32_t S,
-                                                          uint32_t B, Assigner<K>* A) {
+                                                          uint32_t B, Assigner<K>* A, uint32_t mreq) {
   extern __shared__ __align__(16) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
-  pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, A, sm);
+  pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, A, sm, mreq);
 }
 
 // Training and compilation of the learned PL model (one CTA), after
@@ -373,18 +374,18 @@ __global__ __launch_bounds__(SETUP_NT) void pl_grad_probe(const Assigner<K>* __r
   }
 }
 
-}  // namespace ggms
+GGMS_END
 
 #include "ggms_mlp.cuh"
 
-namespace ggms {
+GGMS_BEGIN
 
 template <typename K>
 static int learn_and_choose(int kind, const K* sorted, uint32_t S, uint32_t B, int steps_opt,
                             float bound, Assigner<K>* As, Grid<K>* Gs, LearnState* L,
                             uint32_t* choice, const uint32_t* krank, uint32_t nk, uint64_t n,
                             float window_z, cudaStream_t st, long long* launches,
-                            cudaEvent_t sampled_done = nullptr) {
+                            cudaEvent_t sampled_done = nullptr, uint32_t pl_knots = 0) {
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(setup_learned_pl<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -396,11 +397,11 @@ static int learn_and_choose(int kind, const K* sorted, uint32_t S, uint32_t B, i
   }
   if (kind == GGMS_ASSIGNER_LEARNED_MLP) {
     int rc = mlp_fit_and_compile<K>(sorted, S, B, steps_opt, bound, As, Gs, L, choice, st, launches,
-                                    sampled_done);
+                                    sampled_done, pl_knots);
     if (rc) return rc;
   } else {
     const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 4u;
-    setup_pl_knots<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, &As[1]);
+    setup_pl_knots<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, &As[1], pl_knots);
     pl_stats_grid<K><<<(PL_M + 31) / 32, 1024, 0, st>>>(sorted, S, &As[1], L);
     // the choice compares with the sampled grid: wait for it (it may be built
     // on another stream, concurrently with the knots and the statistics)
@@ -413,4 +414,4 @@ static int learn_and_choose(int kind, const K* sorted, uint32_t S, uint32_t B, i
   return cudaGetLastError() == cudaSuccess ? GGMS_OK : GGMS_E_CUDA;
 }
 
-}  // namespace ggms
+GGMS_END

@@ -19,7 +19,7 @@
 #include <cooperative_groups.h>
 
 
-namespace ggms {
+GGMS_BEGIN
 
 namespace cg = cooperative_groups;
 
@@ -293,10 +293,11 @@ __device__ void mlp_eval_knots(const float* __restrict__ P, const Assigner<K>* _
 
 template <typename K>
 __global__ __launch_bounds__(SETUP_NT) void setup_mlp_begin(const K* __restrict__ sorted, uint32_t S,
-                                                           uint32_t B, Assigner<K>* A, float* P) {
+                                                           uint32_t B, Assigner<K>* A, float* P,
+                                                           uint32_t mreq) {
   extern __shared__ __align__(16) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
-  pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_MLP, A, sm);
+  pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_MLP, A, sm, mreq);
   mlp_init<K>(sorted, S, A, P);
 }
 
@@ -309,6 +310,7 @@ __global__ __launch_bounds__(SETUP_NT) void setup_mlp_finish(const K* __restrict
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
   mlp_eval_knots<K>(P, A, (float*)sm.Bs, sm.cdf);
   for (uint32_t j = threadIdx.x; j <= A->M; j += blockDim.x) L->cdf[j] = sm.cdf[j];
+  if (threadIdx.x == 0) L->M = A->M;  // segments of the compiled piecewise-linear form
   pl_set_bases<K>(sm.cdf, A, sm.Bs, GGMS_ASSIGNER_LEARNED_MLP);
   // G is the learned slot of the grid pair: G - 1 is the sampled grid
   learned_finish<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_MLP, bound, A, G, G - 1, L, choice, sm);
@@ -317,7 +319,8 @@ __global__ __launch_bounds__(SETUP_NT) void setup_mlp_finish(const K* __restrict
 template <typename K>
 static int mlp_fit_and_compile(const K* sorted, uint32_t S, uint32_t B, int steps_opt, float bound,
                                Assigner<K>* As, Grid<K>* Gs, LearnState* L, uint32_t* choice,
-                               cudaStream_t st, long long* launches, cudaEvent_t sampled_done) {
+                               cudaStream_t st, long long* launches, cudaEvent_t sampled_done,
+                               uint32_t pl_knots) {
   static bool attr_set = false;
   if (!attr_set) {
     if (cudaFuncSetAttribute(mlp_train<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -331,7 +334,7 @@ static int mlp_fit_and_compile(const K* sorted, uint32_t S, uint32_t B, int step
   }
   const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 150u;
   float* P = L->mlp_params;
-  setup_mlp_begin<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, &As[1], P);
+  setup_mlp_begin<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, &As[1], P, pl_knots);
   mlp_train<K><<<MLP_CTAS, MLP_NT, sizeof(MlpSmem), st>>>(sorted, S, &As[1], L, P, steps, 0.05f,
                                                           nullptr, nullptr, nullptr);
   if (sampled_done && cudaStreamWaitEvent(st, sampled_done, 0) != cudaSuccess) return GGMS_E_CUDA;
@@ -341,4 +344,4 @@ static int mlp_fit_and_compile(const K* sorted, uint32_t S, uint32_t B, int step
   return cudaGetLastError() == cudaSuccess ? GGMS_OK : GGMS_E_CUDA;
 }
 
-}  // namespace ggms
+GGMS_END

@@ -272,25 +272,28 @@ struct DevState {
   int sms;
 };
 static std::mutex g_mu;
-static DevState g_dev[MAX_DEVICES];
+static int g_sms[MAX_DEVICES];
 
-// Once per device, with that device current: the address of its scratch
-// region and its SM count.
+// With the caller's device current: the address of its scratch region and its
+// SM count.  The address is looked up on every call (a table lookup once the
+// module is loaded; it allocates nothing), so it is never stale -- after a
+// cudaDeviceReset the module is reloaded and the region may move.  The SM
+// count is kept per device.
 static int device_state(DevState* out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return GGMS_E_CUDA;
   if (dev < 0 || dev >= MAX_DEVICES) return GGMS_E_UNSUPPORTED;
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess || !p) return GGMS_E_CUDA;
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_dev[dev].scratch) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess || !p) return GGMS_E_CUDA;
+  if (g_sms[dev] <= 0) {
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
       return GGMS_E_CUDA;
-    g_dev[dev].sms = sms;
-    g_dev[dev].scratch = static_cast<uint32_t*>(p);
+    g_sms[dev] = sms;
   }
-  *out = g_dev[dev];
+  out->scratch = static_cast<uint32_t*>(p);
+  out->sms = g_sms[dev];
   return GGMS_OK;
 }
 
@@ -309,6 +312,9 @@ extern "C" int ggms_multiselect_noalloc_f32(const float* d_in, int64_t n, const 
     if (ks[i] < 1u || (int64_t)ks[i] > n) return GGMS_E_INVALID_ARG;
     kl.k[i] = ks[i];
   }
+  // An error that earlier work left in the runtime belongs to that work: do
+  // not launch on top of it, and do not clear it.
+  if (cudaPeekAtLastError() != cudaSuccess) return GGMS_E_CUDA;
   DevState ds;
   const int rc = device_state(&ds);
   if (rc != GGMS_OK) return rc;

@@ -9,7 +9,7 @@
 #pragma once
 #include "ggms_kernels.cuh"
 
-namespace ggms {
+GGMS_BEGIN
 
 constexpr int SETUP_NT = 1024;
 
@@ -732,4 +732,4 @@ __global__ __launch_bounds__(SETUP_NT) void setup_sampled(const K* __restrict__ 
   if (threadIdx.x == 0) G->quality = qv;
 }
 
-}  // namespace ggms
+GGMS_END

@@ -16,7 +16,7 @@
 #pragma once
 #include "ggms_setup.cuh"
 
-namespace ggms {
+GGMS_BEGIN
 
 constexpr uint32_t WIN_MAXRAW = 64;    // runs before merging; more: no windows
 constexpr uint32_t WIN_NT = 1024;
@@ -165,4 +165,4 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
   }
 }
 
-}  // namespace ggms
+GGMS_END

@@ -40,7 +40,8 @@ ASSIGNER_SAMPLED = 1
 ASSIGNER_LEARNED_PL = 2
 ASSIGNER_LEARNED_MLP = 3
 ASSIGNER_NAMES = {0: "auto", 1: "sampled", 2: "learned_pl", 3: "learned_mlp"}
-PL_KNOTS = 1024   # segments of the learned piecewise-linear CDF
+PL_KNOTS = 1024   # most segments of the learned piecewise-linear CDF (opts.pl_knots picks fewer)
+PHASES = ("sample_sort", "assigner", "windows", "pass1", "between", "pass2", "finish", "answers")
 
 SUFFIX = {np.dtype(np.float32): "f32", np.dtype(np.float64): "f64",
           np.dtype(np.uint32): "u32", np.dtype(np.int32): "i32"}
@@ -68,6 +69,7 @@ class Stats(ctypes.Structure):
         ("model_imbalance", ctypes.c_float),
         ("model_loss", ctypes.c_float),
         ("window_runs", ctypes.c_int32),
+        ("model_segments", ctypes.c_int32),
     ]
 
     def as_dict(self):
@@ -92,6 +94,8 @@ class Opts(ctypes.Structure):
         ("window_z", ctypes.c_float),
         ("autotune", ctypes.c_int32),
         ("stats", ctypes.POINTER(Stats)),
+        ("pl_knots", ctypes.c_int32),
+        ("pad0", ctypes.c_int32),
     ]
 
 
@@ -134,6 +138,10 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ggms_get_default_context.argtypes = [ctypes.POINTER(vp)]
     lib.ggms_context_profile.argtypes = [vp, i32]
     lib.ggms_context_pass_times.argtypes = [vp, vp, vp, vp, i32]
+    lib.ggms_context_phase_times.restype = i32
+    lib.ggms_context_phase_times.argtypes = [vp, vp, i32]
+    lib.ggms_context_status.restype = i32
+    lib.ggms_context_status.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_int)]
     lib.ggms_context_launches.restype = i64
     lib.ggms_context_launches.argtypes = [vp]
     lib.ggms_context_graph_launches.restype = i64
@@ -188,6 +196,22 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def status(self, stream: int = 0) -> int:
+        """Device-side status of the last call this context enqueued (waits for it)."""
+        st = ctypes.c_int(0)
+        rc = load().ggms_context_status(self.ptr, ctypes.c_void_p(stream), ctypes.byref(st))
+        if rc:
+            raise GGMSError(rc, "ggms_context_status")
+        return st.value
+
+    def phase_times(self, max_calls: int = 256):
+        """Per-phase device times (ms) of the profiled calls: a list of dicts keyed by PHASES."""
+        buf = (ctypes.c_float * (len(PHASES) * max_calls))()
+        got = load().ggms_context_phase_times(self.ptr, buf, max_calls)
+        if got < 0:
+            raise GGMSError(-got, "ggms_context_phase_times")
+        return [dict(zip(PHASES, buf[i * len(PHASES):(i + 1) * len(PHASES)])) for i in range(got)]
 
 
 def _suffix(dtype) -> str:

@@ -59,7 +59,9 @@ enum {
 typedef struct ggms_stats {
   int32_t assigner_used;        /* GGMS_ASSIGNER_* that produced the level-0 buckets */
   int32_t num_buckets;          /* level-0 buckets */
-  int32_t full_passes;          /* passes that read the whole input (2 in every case) */
+  int32_t full_passes;          /* launches that read the whole input, counted by those kernels on the
+                                   device: 2 on the single-vector path (PASS 1 and PASS 2); on the
+                                   batched path the level-0 count and copy when a segment needs them */
   int32_t levels;               /* refinement levels that ran over candidates */
   int64_t candidates;           /* elements the level-0 compaction copied */
   int64_t refine_elements;      /* elements read by all refinement levels together */
@@ -71,6 +73,8 @@ typedef struct ggms_stats {
   float model_imbalance;        /* max/mean of the model's buckets on its own sample (learned) */
   float model_loss;             /* final training loss of the learned model */
   int32_t window_runs;          /* PASS 1 windows: bucket runs PASS 1 bucketed (0: every key bucketed) */
+  int32_t model_segments;       /* segments of the learned model's piecewise-linear form (0: sampled);
+                                   written only for callers whose opts carry pl_knots */
 } ggms_stats;
 
 typedef struct ggms_opts {
@@ -91,6 +95,11 @@ typedef struct ggms_opts {
                                    shape class times the candidates on the caller's data and the context
                                    keeps the fastest (the batched path tunes its level kernels' CTAs) */
   ggms_stats* stats;            /* optional host pointer */
+  int32_t pl_knots;             /* segments of the learned piecewise-linear CDF model: 16..1024;
+                                   0 = auto (min(1024, num_buckets / 4)).  Appended last: a caller
+                                   built against the layout without it (struct_size = its offset)
+                                   is still accepted and gets the default */
+  int32_t pad0;
 } ggms_opts;
 
 GGMS_API void ggms_default_opts(ggms_opts* opts);
@@ -117,6 +126,28 @@ GGMS_API int ggms_get_default_context(ggms_context** ctx);
 GGMS_API int ggms_context_profile(ggms_context* ctx, int enable);
 GGMS_API int ggms_context_pass_times(ggms_context* ctx, float* pass1_ms, float* pass2_ms,
                                      float* call_ms, int max);
+/* Per-phase device times of profiled single-vector calls (drains the same ring
+ * as ggms_context_pass_times): for each call GGMS_PHASES floats, in order
+ *   0 k set-up, sample and sample sort   1 assigner (sampled and learned)
+ *   2 PASS 1 windows                     3 PASS 1 (count)
+ *   4 between the passes (scan, locate, children, write cursors)
+ *   5 PASS 2 (copy)                      6 finishing (in-shared-memory select,
+ *                                          refinement levels)
+ *   7 answers (write-out, copies)
+ * Returns the number of calls written (at most `max`), or -status. */
+#define GGMS_PHASES 8
+GGMS_API int ggms_context_phase_times(ggms_context* ctx, float* ms, int max);
+
+/* Device-side status of the last call this context enqueued (no reference
+ * counterpart: the reference is synchronous and prints).  Calls whose ks and
+ * answers both live in device memory return GGMS_OK without a host sync, so a
+ * problem only the device can see -- a device-resident k outside [1, n], a
+ * decreasing segment offset, a failed internal check -- is recorded in the
+ * call's device counters instead.  This waits for that call (and, if `stream`
+ * is not NULL, for the work enqueued on `stream` before it) and stores its
+ * GGMS_* status in *status.  Host-synchronous calls already return it.  The
+ * next call of the context overwrites it. */
+GGMS_API int ggms_context_status(ggms_context* ctx, void* stream, int* status);
 GGMS_API int64_t ggms_context_launches(ggms_context* ctx);
 /* Calls of this context that ran as a replay of a captured CUDA graph: a call
  * whose arguments, options and workspace repeat is captured the second time
@@ -156,7 +187,8 @@ GGMS_API int ggms_iterative_smos_i32(const int32_t* d_vector, int length, const 
  * Same semantics; the k and output arrays may be host or device memory
  * (opts->ks_on_device / out_on_device), work is enqueued on `stream`.
  * With both arrays on the device the call is asynchronous (no host sync)
- * unless opts->stats is set.  1 <= n <= 2^32 - 1. */
+ * unless opts->stats is set; a device-resident k outside [1, n] is then
+ * reported by ggms_context_status, not by the return value.  1 <= n <= 2^32 - 1. */
 GGMS_API int ggms_multiselect_f32_ex(ggms_context* ctx, const float* d_in, int64_t n,
                             const uint32_t* ks, int64_t nk, float* out,
                             const ggms_opts* opts, void* stream);
@@ -189,7 +221,13 @@ GGMS_API int ggms_topk_i32(ggms_context* ctx, const int32_t* d_in, int64_t n, in
  * Segment s is d_in[seg_off[s] .. seg_off[s+1]); its ks are
  * ks[k_off[s] .. k_off[s+1]) (1-based k-th largest within the segment) and its
  * answers go to out[k_off[s] .. k_off[s+1]).  seg_off and k_off hold nseg+1
- * entries; all five arrays are DEVICE memory.  Asynchronous on `stream`. */
+ * entries; all five arrays are DEVICE memory.  Work is enqueued on `stream`,
+ * but the call first reads seg_off[0], seg_off[nseg], k_off[0] and k_off[nseg]
+ * back to the host (the totals size the workspace): one host sync on `stream`
+ * per call, so the call cannot itself be captured into the caller's CUDA graph
+ * (repeated calls replay the library's own graph).  Errors that only the
+ * device sees (a k outside its segment, seg_off decreasing) are reported by
+ * ggms_context_status. */
 GGMS_API int ggms_multiselect_segmented_f32(ggms_context* ctx, const float* d_in, const int64_t* seg_off,
                                    int64_t nseg, const uint32_t* ks, const int64_t* k_off,
                                    float* out, const ggms_opts* opts, void* stream);

@@ -50,15 +50,17 @@ extern "C" {
  *
  * Status: GGMS_OK; GGMS_E_INVALID_ARG for a null or misaligned pointer, n
  * outside [1, 2^32 - 1], num_ks < 0 or a k outside [1, n]; GGMS_E_UNSUPPORTED
- * for num_ks > GGMS_NOALLOC_MAX_KS; GGMS_E_CUDA when set-up or a launch fails.
+ * for num_ks > GGMS_NOALLOC_MAX_KS; GGMS_E_CUDA when set-up or a launch fails,
+ * or when the CUDA runtime already holds an error from earlier work on this
+ * thread (the call then launches nothing and leaves that error for its owner).
  * Every argument is checked on the host before any CUDA call.  num_ks == 0
  * returns GGMS_OK and launches nothing.
  *
- * Set-up: the first call on a device (the device current on the calling
- * thread) looks up the address of that device's scratch region once, with
- * cudaGetSymbolAddress, which makes the driver load the library's kernels on
- * that device if it has not yet.  Make that first call before any stream
- * capture begins.
+ * Set-up: every call looks up the address of the current device's scratch
+ * region with cudaGetSymbolAddress (after the first call on a device this is a
+ * lookup that allocates nothing; the first one makes the driver load the
+ * library's kernels on that device if it has not yet).  Make the first call on
+ * a device before any stream capture begins.
  *
  * Zero state: nothing in the scratch region needs to be zero on entry.  The
  * call's first kernel writes the per-k state and clears the level-0 histogram;

@@ -58,6 +58,12 @@ int ggms_cpu_multiselect_f64(const double* in, int64_t n, const uint32_t* ks, in
                              double* out, int threads, int method);
 int ggms_cpu_multiselect_u32(const uint32_t* in, int64_t n, const uint32_t* ks, int64_t nk,
                              uint32_t* out, int threads, int method);
+/* Segmented (the oracle's segmented layout): each segment by method 1, the
+ * segments spread over the threads.  Returns 0 or -1. */
+int ggms_cpu_multiselect_segmented_f32(const float* in, const int64_t* seg_off, int64_t nseg,
+                                       const uint32_t* ks, const int64_t* k_off, float* out, int threads);
+int ggms_cpu_multiselect_segmented_u32(const uint32_t* in, const int64_t* seg_off, int64_t nseg,
+                                       const uint32_t* ks, const int64_t* k_off, uint32_t* out, int threads);
 int ggms_cpu_max_threads(void);
 
 #ifdef __cplusplus

@@ -54,6 +54,10 @@ def lib() -> ctypes.CDLL:
             f = getattr(l, f"ggms_cpu_multiselect_{suf}")
             f.restype = ctypes.c_int
             f.argtypes = [vp, i64, vp, i64, vp, ctypes.c_int, ctypes.c_int]
+        for suf in ("f32", "u32"):
+            f = getattr(l, f"ggms_cpu_multiselect_segmented_{suf}")
+            f.restype = ctypes.c_int
+            f.argtypes = [vp, vp, i64, vp, vp, vp, ctypes.c_int]
         l.ggms_cpu_max_threads.restype = ctypes.c_int
         l.ggms_oracle_key_f32.restype = ctypes.c_uint32
         l.ggms_oracle_key_f32.argtypes = [ctypes.c_float]
@@ -98,6 +102,20 @@ def cpu_multiselect(values, ks, threads: int = 0, method: int = 1) -> np.ndarray
     out = np.empty(len(ks), dtype=values.dtype)
     rc = getattr(lib(), f"ggms_cpu_multiselect_{_SUF[values.dtype]}")(
         _p(values), len(values), _p(ks), len(ks), _p(out), threads, method)
+    if rc:
+        raise ValueError("cpu baseline rejected the arguments")
+    return out
+
+
+def cpu_multiselect_segmented(values, seg_off, ks, k_off, threads: int = 0) -> np.ndarray:
+    """OpenMP per-segment multi-select (checked against select_segmented by the CPU tests)."""
+    values = np.ascontiguousarray(values)
+    seg_off = np.ascontiguousarray(seg_off, dtype=np.int64)
+    k_off = np.ascontiguousarray(k_off, dtype=np.int64)
+    ks = np.ascontiguousarray(ks, dtype=np.uint32)
+    out = np.empty(len(ks), dtype=values.dtype)
+    rc = getattr(lib(), f"ggms_cpu_multiselect_segmented_{_SUF[values.dtype]}")(
+        _p(values), _p(seg_off), len(seg_off) - 1, _p(ks), _p(k_off), _p(out), threads)
     if rc:
         raise ValueError("cpu baseline rejected the arguments")
     return out

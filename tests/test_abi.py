@@ -39,6 +39,26 @@ def test_default_opts_layout():
     o = ggms_b200.default_opts()
     assert o.struct_size == ctypes.sizeof(ggms_b200.Opts)
     assert o.assigner == ggms_b200.ASSIGNER_AUTO
+    assert o.pl_knots == 0
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """The binding's ctypes structs have the C header's sizes and offsets
+    (compiled here with gcc against include/ggms.h)."""
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    src = tmp_path / "layout.c"
+    src.write_text(
+        '#include <stddef.h>\n#include <stdio.h>\n#include "ggms.h"\n'
+        'int main(void) { printf("%zu %zu %zu %zu %zu\\n", sizeof(ggms_opts), offsetof(ggms_opts, stats),'
+        ' offsetof(ggms_opts, pl_knots), sizeof(ggms_stats), offsetof(ggms_stats, window_runs));'
+        ' return 0; }\n')
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", inc, str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True,
+                                          check=True).stdout.split()]
+    O, S = ggms_b200.Opts, ggms_b200.Stats
+    assert got == [ctypes.sizeof(O), O.stats.offset, O.pl_knots.offset, ctypes.sizeof(S),
+                   S.window_runs.offset]
 
 
 

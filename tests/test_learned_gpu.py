@@ -143,13 +143,15 @@ def test_training_improves_balance(gen, kind):
     r = G.diag_fit(keys, kind)
     if kind == G.ASSIGNER_LEARNED_PL:
         # training never ends worse than its quantile init (keep-best), and the
-        # 256-knot model's buckets are more even than the 17 sampled pivots'
+        # learned model's buckets are more even than the 17 sampled pivots'
         assert r["loss_after"] <= r["loss_before"]
         assert r["imbalance_model"] < r["imbalance_sampled"], r
     else:
-        # the MLP reaches a small CDF error (mean squared, CDF units)
+        # the MLP reaches a small CDF error (mean squared, CDF units), and its
+        # buckets, measured on the same sample, are more even than the 17
+        # sampled pivots'
         assert r["loss_after"] < 1e-3, r
-        assert r["imbalance_model"] < 64.0, r
+        assert r["imbalance_model"] < r["imbalance_sampled"], r
 
 
 @pytest.mark.parametrize("gen,seed", [("mixture8_f32", 31), ("lognormal_f32", 32)])
@@ -164,7 +166,12 @@ def test_learned_needs_less_refinement(ctx, gen, seed):
         out, st = G.select(ctx, d.data_ptr(), n, ks, np.float32, assigner=a, stats=True)
         np.testing.assert_array_equal(out.view(np.uint32), exp.view(np.uint32))
         res[a] = st
-    samp, pl = res[G.ASSIGNER_SAMPLED], res[G.ASSIGNER_LEARNED_PL]
+    samp, pl, mlp = res[G.ASSIGNER_SAMPLED], res[G.ASSIGNER_LEARNED_PL], res[G.ASSIGNER_LEARNED_MLP]
     assert pl["assigner_used"] == "learned_pl"
     assert pl["bucket_max_over_mean"] < samp["bucket_max_over_mean"]
     assert pl["candidates"] <= samp["candidates"]
+    # the MLP, when its fit is accepted, also beats the sampled pivots on the
+    # whole input: more even level-0 buckets and no more candidates
+    if mlp["assigner_used"] == "learned_mlp":
+        assert mlp["bucket_max_over_mean"] < samp["bucket_max_over_mean"], (mlp, samp)
+        assert mlp["candidates"] <= samp["candidates"], (mlp, samp)

@@ -96,3 +96,14 @@ def test_segmented_oracle():
         a, b = koff[s], koff[s + 1]
         if b > a:
             np.testing.assert_array_equal(out[a:b], orc.select(v[off[s]:off[s + 1]], ks[a:b]))
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.uint32])
+def test_cpu_segmented_matches_oracle(dtype):
+    """The OpenMP per-segment checker used at the batched benchmark's full shape
+    gives the oracle's answers on the same kind of batch."""
+    from ggms_b200 import datagen as D
+    vals, seg_off, ks, k_off = D.segmented_batch(96, 7, 4, 16, kmax=64, dtype=dtype)
+    vals[::101] = vals[3]  # duplicates across segments
+    got = orc.cpu_multiselect_segmented(vals, seg_off, ks, k_off, threads=4)
+    np.testing.assert_array_equal(orc.bits(got), orc.bits(orc.select_segmented(vals, seg_off, ks, k_off)))

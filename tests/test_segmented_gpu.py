@@ -58,6 +58,22 @@ def test_segmented_config5_shape(ctx, dtype):
     np.testing.assert_array_equal(orc.bits(got), orc.bits(exp))
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.uint32])
+def test_segmented_config5_full(ctx, dtype):
+    """The batched benchmark at its stated shape: 4096 segments, lengths
+    log-uniform in [2^10, 2^24] scaled to 2^30 keys in all (the stated length
+    law alone would give ~7*2^30), 1-512 random ks each; float32 segments
+    alternate uniform and normal values, the second batch is uint32.  Checked
+    per segment against the OpenMP per-segment multi-select, which the CPU
+    tests check against the oracle."""
+    vals, seg_off, ks, k_off = D.segmented_batch(4096, 41, 10, 24, kmax=512, dtype=dtype,
+                                                 total_cap=1 << 30)
+    assert len(seg_off) == 4097 and (1 << 30) - 4096 <= seg_off[-1] <= (1 << 30)
+    got = run_segmented(ctx, vals, seg_off, ks, k_off)
+    exp = orc.cpu_multiselect_segmented(vals, seg_off, ks, k_off)
+    np.testing.assert_array_equal(orc.bits(got), orc.bits(exp))
+
+
 @pytest.mark.parametrize("dtype", [np.float32, np.float64, np.uint32, np.int32])
 @pytest.mark.parametrize("n,K", [(1, 1), (1000, 1000), (100_000, 17), (1 << 20, 4096), (1 << 22, 100)])
 def test_topk(ctx, dtype, n, K):
