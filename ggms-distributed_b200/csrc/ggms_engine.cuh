@@ -30,7 +30,6 @@ struct Workspace {
   K* kkey;
   K* samp_raw;
   K* samp_sorted;
-  K* samp_tmp;
   Assigner<K>* asg;       // [0] sampled, [1] learned (the PL models)
   Grid<K>* grid;          // [0] sampled, [1] learned (what the passes evaluate)
   LearnState* learn;
@@ -72,7 +71,6 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
   size_t o_kkey = b.take(sizeof(K) * p.nk);
   size_t o_sr = b.take(sizeof(K) * p.S);
   size_t o_ss = b.take(sizeof(K) * p.S);
-  size_t o_st = b.take(sizeof(K) * p.S);
   size_t o_asg = b.take(sizeof(Assigner<K>) * 2);
   size_t o_grid = b.take(sizeof(Grid<K>) * 2);
   size_t o_learn = b.take(sizeof(LearnState));
@@ -112,7 +110,6 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
   w.kkey = (K*)(base + o_kkey);
   w.samp_raw = (K*)(base + o_sr);
   w.samp_sorted = (K*)(base + o_ss);
-  w.samp_tmp = (K*)(base + o_st);
   w.asg = (Assigner<K>*)(base + o_asg);
   w.grid = (Grid<K>*)(base + o_grid);
   w.learn = (LearnState*)(base + o_learn);
@@ -183,30 +180,37 @@ constexpr int MAX_LEVELS_32 = 3;
 constexpr int MAX_LEVELS_64 = 6;
 
 template <typename T>
-static size_t l0_count_smem(uint32_t B, int nt) {
-  return GRID_SMEM + (size_t)B * 4u + wq_bytes((uint32_t)nt, sizeof(typename KeyOf<T>::K));
+static size_t l0_count_smem(uint32_t B, int nt, int unroll, uint32_t nst) {
+  const size_t base = GRID_SMEM + (size_t)B * 4u + wq_bytes((uint32_t)nt, sizeof(typename KeyOf<T>::K));
+  return unroll < 0 ? ((base + 127) & ~(size_t)127) + ring_bytes(0, nst) : base;
 }
 template <typename T>
-static size_t l0_coarse_smem(int nt, int unroll) {
-  const size_t ch = (size_t)nt * (unroll < 4 ? unroll : 4) * (16 / sizeof(T));
-  return GRID_SMEM + ch * (sizeof(typename KeyOf<T>::K) + 1);
+static size_t l0_coarse_smem(int nt, int unroll, uint32_t nst) {
+  const size_t ch = (size_t)nt * coarse_du(unroll < 0 ? 0 : unroll) * (16 / sizeof(T));
+  const size_t base = GRID_SMEM + ch * (sizeof(typename KeyOf<T>::K) + 1);
+  return unroll < 0 ? ((base + 127) & ~(size_t)127) + ring_bytes(0, nst) : base;
 }
 template <typename T>
-static size_t l0_compact_smem(uint32_t B, int nt) {
-  return GRID_SMEM + (MAX_B0 / 32 + l0_compact_qwords((uint32_t)nt, sizeof(typename KeyOf<T>::K)) + HOT_WORDS) * 4u +
-         (size_t)B * 4u;
+static size_t l0_compact_smem(uint32_t B, int nt, int unroll, uint32_t nst) {
+  const size_t base = GRID_SMEM +
+                      (MAX_B0 / 32 + l0_compact_qwords((uint32_t)nt, sizeof(typename KeyOf<T>::K)) + HOT_WORDS) * 4u +
+                      (size_t)B * 4u;
+  return unroll < 0 ? ((base + 127) & ~(size_t)127) + ring_bytes(0, nst) : base;
 }
 
-// Launch shapes of the two passes (CTA size x 16-byte loads in flight per
-// thread); the default and the autotuner pick among these instantiations.
+// Launch shapes of the two passes: CTA size x 16-byte loads in flight per
+// thread (unroll 2, 4 or 8, register streams), or unroll -1: the TMA ring
+// (bulk copies into shared-memory stages); the default and the autotuner pick
+// among these instantiations.
 template <typename T>
 struct PassVariant {
   using K = typename KeyOf<T>::K;
   int nt, unroll;
-  void (*count)(const T*, uint64_t, const Grid<K>*, Counters*, const Windows<K>*, uint32_t*, uint32_t*);
+  void (*count)(const T*, uint64_t, const Grid<K>*, Counters*, const Windows<K>*, uint32_t*, uint32_t*, uint32_t);
   void (*compact)(const T*, uint64_t, const Grid<K>*, Counters*, const Windows<K>*, const uint32_t*,
-                  const uint32_t*, K*, uint64_t);
-  void (*coarse)(const T*, uint64_t, const Grid<K>*, Counters*, const uint32_t*, const uint32_t*, K*, uint64_t);
+                  const uint32_t*, K*, uint64_t, uint32_t);
+  void (*coarse)(const T*, uint64_t, const Grid<K>*, Counters*, const uint32_t*, const uint32_t*, K*, uint64_t,
+                 uint32_t);
 };
 
 template <typename T>
@@ -219,6 +223,7 @@ static const PassVariant<T>* pass_variant(int nt, int unroll) {
       {512, 8, l0_count<T, 512, 8>, l0_compact<T, 512, 8>, l0_compact_coarse<T, 512, 8>},
       {1024, 2, l0_count<T, 1024, 2>, l0_compact<T, 1024, 2>, l0_compact_coarse<T, 1024, 2>},
       {1024, 4, l0_count<T, 1024, 4>, l0_compact<T, 1024, 4>, l0_compact_coarse<T, 1024, 4>},
+      {1024, -1, l0_count<T, 1024, 0>, l0_compact<T, 1024, 0>, l0_compact_coarse<T, 1024, 0>},
   };
   for (const auto& x : v)
     if (x.nt == nt && x.unroll == unroll) return &x;
@@ -226,15 +231,31 @@ static const PassVariant<T>* pass_variant(int nt, int unroll) {
 }
 
 constexpr int DEFAULT_PASS_NT = 1024;
-constexpr int DEFAULT_PASS_UNROLL = 4;
+constexpr int DEFAULT_PASS_UNROLL = -1;  // the TMA ring
+
+// Stages of the TMA ring: as many 16 KB stages (2..6) as fit in the shared
+// memory a CTA may use next to the larger of the three pass kernels' other
+// needs (static shared memory included, with margin).
+template <typename T>
+static uint32_t ring_stages(Context* c, uint32_t B, int nt) {
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device) != cudaSuccess)
+    optin = 227 * 1024;
+  const size_t base = std::max(std::max(l0_count_smem<T>(B, nt, 0, 0), l0_compact_smem<T>(B, nt, 0, 0)),
+                               l0_coarse_smem<T>(nt, 0, 0));
+  const size_t margin = 8192 + 128;  // static shared memory of the pass kernels, alignment
+  const size_t room = (size_t)optin > base + margin ? (size_t)optin - base - margin : 0;
+  return (uint32_t)std::min<size_t>(6, std::max<size_t>(2, room / RING_BYTES));
+}
 
 // The two passes must split the input among CTAs identically (PASS 2 writes
 // into per-CTA ranges sized by PASS 1), so both get the same grid: as many
 // CTAs as fit on every SM at once for the larger of the two.
 template <typename T>
-static int l0_ncta(Context* c, const PassVariant<T>* pv, uint32_t B, uint32_t* ncta) {
-  const size_t s1 = l0_count_smem<T>(B, pv->nt), s2 = l0_compact_smem<T>(B, pv->nt);
-  const size_t s3 = l0_coarse_smem<T>(pv->nt, pv->unroll);
+static int l0_ncta(Context* c, const PassVariant<T>* pv, uint32_t B, uint32_t nst, uint32_t* ncta) {
+  const size_t s1 = l0_count_smem<T>(B, pv->nt, pv->unroll, nst);
+  const size_t s2 = l0_compact_smem<T>(B, pv->nt, pv->unroll, nst);
+  const size_t s3 = l0_coarse_smem<T>(pv->nt, pv->unroll, nst);
   GGMS_CU(cudaFuncSetAttribute((const void*)pv->count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
   GGMS_CU(cudaFuncSetAttribute((const void*)pv->compact, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
   GGMS_CU(cudaFuncSetAttribute((const void*)pv->coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s3));
@@ -311,7 +332,8 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   const PassVariant<T>* pv = pass_variant<T>(o.pass_threads ? o.pass_threads : DEFAULT_PASS_NT,
                                               o.pass_unroll ? o.pass_unroll : DEFAULT_PASS_UNROLL);
   if (!pv) return GGMS_E_INVALID_ARG;
-  rc = l0_ncta<T>(ctx, pv, p.B, &p.ncta);
+  p.ring_st = pv->unroll < 0 ? ring_stages<T>(ctx, p.B, pv->nt) : 0u;
+  rc = l0_ncta<T>(ctx, pv, p.B, p.ring_st, &p.ncta);
   if (rc) return rc;
   Workspace<K> w0 = layout<K>(p, sizeof(T), nullptr);
   rc = ensure_arena(ctx, w0.bytes);
@@ -352,22 +374,25 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
 
     // ---- level-0 assigner
     const uint32_t S = p.S;
-    ++ctx->launches;
-    asg_sample<T><<<cdiv(S, 256), 256, 0, s>>>(d_in, n, S, p.seed, w.samp_raw);
-    if (S <= 1024) {
+    if (S >= CS_MIN_S) {  // sample and sort in one cluster launch
+      static bool cs_attr = false;
+      if (!cs_attr) {
+        GGMS_CU(cudaFuncSetAttribute(asg_sample_sort_cluster<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(ClusterSortSmem<K>)));
+        cs_attr = true;
+      }
       ++ctx->launches;
-      asg_sort_chunks<K, 1024, 1024><<<1, 1024, 0, s>>>(w.samp_raw, w.samp_sorted, S);
-    } else if (S <= 2048) {
-      ++ctx->launches;
-      asg_sort_chunks<K, 2048, 1024><<<1, 1024, 0, s>>>(w.samp_raw, w.samp_sorted, S);
-    } else if (S <= 4096) {
-      ++ctx->launches;
-      asg_sort_chunks<K, 4096, 1024><<<1, 1024, 0, s>>>(w.samp_raw, w.samp_sorted, S);
-    } else {
-      ++ctx->launches;
-      asg_sort_chunks<K, 4096, 1024><<<S / 4096, 1024, 0, s>>>(w.samp_raw, w.samp_tmp, S);
-      ++ctx->launches;
-      asg_merge_rank<K><<<cdiv(S, 256), 256, 0, s>>>(w.samp_tmp, w.samp_sorted, S, 4096u);
+      asg_sample_sort_cluster<T><<<CS_CTAS, CS_NT, sizeof(ClusterSortSmem<K>), s>>>(d_in, n, S, p.seed,
+                                                                                 w.samp_sorted);
+    } else {  // up to 4096 keys: draw them, then one CTA sorts them
+      ctx->launches += 2;
+      asg_sample<T><<<cdiv(S, 256), 256, 0, s>>>(d_in, n, S, p.seed, w.samp_raw);
+      if (S <= 1024)
+        asg_sort_chunks<K, 1024, 1024><<<1, 1024, 0, s>>>(w.samp_raw, w.samp_sorted, S);
+      else if (S <= 2048)
+        asg_sort_chunks<K, 2048, 1024><<<1, 1024, 0, s>>>(w.samp_raw, w.samp_sorted, S);
+      else
+        asg_sort_chunks<K, 4096, 1024><<<1, 1024, 0, s>>>(w.samp_raw, w.samp_sorted, S);
     }
     prof_rec(prof, 6, s);
     rc = setup_attrs<K>();
@@ -410,8 +435,8 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     GGMS_CU(cudaMemsetAsync(w.aflag0, 0, 4ull * (p.B / 32), s));
     prof_rec(prof, 1, s);
     ++ctx->launches;
-    pv->count<<<grid_c, pv->nt, l0_count_smem<T>(p.B, pv->nt), s>>>(d_in, n, w.grid, w.C, w.win, w.hist0,
-                                                                      w.crow);
+    pv->count<<<grid_c, pv->nt, l0_count_smem<T>(p.B, pv->nt, pv->unroll, p.ring_st), s>>>(
+        d_in, n, w.grid, w.C, w.win, w.hist0, w.crow, p.ring_st);
     prof_rec(prof, 2, s);
     ++ctx->launches;
     l0_scan<K><<<1, 1024, 4u * p.B, s>>>(w.hist0, p.B, w.C, w.win, w.aflagc);
@@ -434,11 +459,11 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     // ---- PASS 2: compact the buckets that still need refinement
     prof_rec(prof, 3, s);
     ++ctx->launches;
-    pv->compact<<<grid_c, pv->nt, l0_compact_smem<T>(p.B, pv->nt), s>>>(d_in, n, w.grid, w.C, w.win, w.cmap0,
-                                                                        w.crow, w.cand[0], (uint64_t)n);
+    pv->compact<<<grid_c, pv->nt, l0_compact_smem<T>(p.B, pv->nt, pv->unroll, p.ring_st), s>>>(
+        d_in, n, w.grid, w.C, w.win, w.cmap0, w.crow, w.cand[0], (uint64_t)n, p.ring_st);
     ++ctx->launches;  // one of the two PASS-2 kernels returns at once
-    pv->coarse<<<grid_c, pv->nt, l0_coarse_smem<T>(pv->nt, pv->unroll), s>>>(d_in, n, w.grid, w.C, w.cmap0,
-                                                                              w.crow, w.cand[0], (uint64_t)n);
+    pv->coarse<<<grid_c, pv->nt, l0_coarse_smem<T>(pv->nt, pv->unroll, p.ring_st), s>>>(
+        d_in, n, w.grid, w.C, w.cmap0, w.crow, w.cand[0], (uint64_t)n, p.ring_st);
     prof_rec(prof, 4, s);
     rc = launch_small_select<K>(ctx, w.cand[0], w.segs[1], w.khead[1], w, caps, s);
     if (rc) return rc;
@@ -565,9 +590,9 @@ static int run_single_tuned(Context* c, const T* d_in, uint64_t n, const uint32_
     return run_single<T>(c, d_in, n, ks, nk, out, b, st, topk);
   }
   static const int Bs[] = {4096, 8192, 16384};
-  static const int shapes[][2] = {{1024, 4}, {512, 4}, {512, 8}};
+  static const int shapes[][2] = {{1024, -1}, {1024, 4}, {512, 4}, {512, 8}};
   float best = 3.4e38f;
-  Context::Tuned pick{{key[0], key[1], key[2], key[3]}, 8192, 1024, 4, 8};
+  Context::Tuned pick{{key[0], key[1], key[2], key[3]}, 8192, DEFAULT_PASS_NT, DEFAULT_PASS_UNROLL, 8};
   for (int B : Bs) {
     for (const auto& sh : shapes) {
       ggms_opts t = b;

@@ -186,6 +186,7 @@ struct Plan {
   uint64_t seed;
   uint32_t cap_q;    // batched path: caller segments with quantile bins (0: single path)
   uint32_t pl_knots; // learned PL model: requested segments (0: the default)
+  uint32_t ring_st;  // stages of the passes' TMA ring (0: register streams)
 };
 
 
@@ -223,6 +224,7 @@ static int make_plan(Plan* p, uint64_t n, uint32_t nk, const ggms_opts& o) {
   p->cap_q = 0;
   if (o.pl_knots != 0 && (o.pl_knots < 16 || o.pl_knots > 1024)) return GGMS_E_INVALID_ARG;
   p->pl_knots = (uint32_t)o.pl_knots;
+  p->ring_st = 0;
   return GGMS_OK;
 }
 

@@ -28,6 +28,8 @@
 // refined with exact radix bins of the known key range, which ends in a bounded
 // number of levels (3 for 32-bit keys, 6 for 64-bit) with every k exact.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "ggms_internal.cuh"
 #include "../../include/ggms.h"
 
@@ -39,6 +41,15 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
   return m;
+}
+
+__device__ __forceinline__ uint32_t warp_incl_scan_u32(uint32_t v, uint32_t lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, v, o);
+    if ((int)lane >= o) v += t;
+  }
+  return v;
 }
 
 __device__ __forceinline__ void set_status(Counters* C, uint32_t code) {
@@ -182,43 +193,136 @@ __global__ __launch_bounds__(NT) void asg_sort_chunks(const K* __restrict__ in, 
   for (uint32_t i = threadIdx.x; i < cnt; i += NT) out[base + i] = s[i];
 }
 
-// Stable merge of G sorted chunks by ranking: each key counts the keys before
-// it in every other chunk (ties go to the lower chunk).  Every CTA first keeps
-// every MR_IDX-th key of every chunk in shared memory, so each count is a
-// search over those (shared memory) and then over MR_IDX keys (global).
-constexpr uint32_t MR_IDX = 64;
+// Sample and sort in one launch of one thread-block cluster (S >= 8192 keys).
+// CTA c of the cluster draws sample keys [c * S/8, (c + 1) * S/8) straight from
+// the input (the positions asg_sample draws) into its shared memory; then an
+// LSD radix sort with 8-bit digits runs over the whole cluster: per digit
+// pass, every warp ranks its keys stably (32 keys at a time; the lanes that
+// share a digit are found with 8 ballots, no atomics), the CTAs exchange their
+// 256 digit counts through distributed shared memory, and every key is stored
+// straight into the shared memory of the CTA that owns its new position.  A
+// pass in which every key has the same digit is skipped (the permutation is
+// the identity).  4 passes for 32-bit keys, 8 for 64-bit ones; the sorted
+// sample is written out with coalesced stores.
+namespace cgx = cooperative_groups;
+constexpr int CS_CTAS = 8;
+constexpr int CS_NT = 1024;
+constexpr uint32_t CS_MIN_S = CS_CTAS * CS_NT;         // 8192: one key per thread
+constexpr uint32_t CS_MAX_PER = 65536u / CS_CTAS;      // keys per CTA at S = 65536
 
 template <typename K>
-__global__ __launch_bounds__(256) void asg_merge_rank(const K* __restrict__ chunks, K* sorted, uint32_t S,
-                                                     uint32_t CH) {
-  __shared__ K idx[65536u / MR_IDX];  // S <= 65536
-  const uint32_t G = (S + CH - 1) / CH;
-  const uint32_t per = CH / MR_IDX;  // index entries per chunk (CH is a multiple of MR_IDX)
-  for (uint32_t j = threadIdx.x; j < G * per; j += blockDim.x) {
-    const uint32_t pos = j * MR_IDX;
-    idx[j] = pos < S ? chunks[pos] : key_max<K>();
+struct ClusterSortSmem {
+  K a[CS_MAX_PER];                 // keys in the current order (this CTA's share)
+  K b[CS_MAX_PER];                 // the next pass's order, written by every CTA
+  uint32_t hist[CS_NT / 32][256];  // per warp: digit counts, then their prefixes over the warps
+  uint32_t ccnt[256];              // this CTA's digit counts (read by the cluster)
+  uint32_t gbase[256];             // first position of (digit, this CTA) in the next order
+  uint32_t red[33];
+  uint32_t skip;
+};
+
+template <typename T>
+__global__ void __cluster_dims__(CS_CTAS, 1, 1) __launch_bounds__(CS_NT)
+asg_sample_sort_cluster(const T* __restrict__ in, uint64_t n, uint32_t S, uint64_t seed,
+                        typename KeyOf<T>::K* sorted) {
+  using K = typename KeyOf<T>::K;
+  constexpr int KB = (int)sizeof(K) * 8;
+  constexpr int KPT_MAX = CS_MAX_PER / CS_NT;          // 8
+  extern __shared__ __align__(128) uint8_t smem_raw[];
+  ClusterSortSmem<K>& sm = *reinterpret_cast<ClusterSortSmem<K>*>(smem_raw);
+  cgx::cluster_group cluster = cgx::this_cluster();
+  const uint32_t me = cluster.block_rank();
+  const uint32_t per = S / CS_CTAS;                    // keys per CTA
+  const uint32_t kpt = per / CS_NT;                    // keys per thread, 1..8
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // warp w owns positions [w * 32 * kpt, (w + 1) * 32 * kpt) of this CTA's
+  // share; in round r its lane l holds position w * 32 * kpt + r * 32 + l
+  const uint32_t wbase = warp * 32u * kpt;
+  K* A = sm.a;
+  K* Bv = sm.b;
+  for (uint32_t r = 0; r < kpt; ++r) {
+    const uint32_t i = me * per + wbase + r * 32u + lane;   // sample index
+    const uint64_t h = mix64(seed ^ mix64((uint64_t)i + 0x632BE59BD9B4E019ull));
+    A[wbase + r * 32u + lane] = KeyOf<T>::to(in[__umul64hi(h, n)]);
   }
-  __syncthreads();
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= S) return;
-  const uint32_t c = i / CH, p = i % CH;
-  const K key = chunks[i];
-  uint32_t rank = p;
-  for (uint32_t c2 = 0; c2 < G; ++c2) {
-    if (c2 == c) continue;
-    const K* a = chunks + (size_t)c2 * CH;
-    const K* ai = idx + c2 * per;
-    const uint32_t len = min(CH, S - c2 * CH);
-    const bool upper = c2 < c;  // keys <= key (upper bound) or < key (lower bound) come before
-    auto before = [&](K v) { return upper ? v <= key : v < key; };
-    uint32_t lo = 0, hi = (len + MR_IDX - 1u) / MR_IDX;  // first index entry not before key
-    while (lo < hi) { const uint32_t m = (lo + hi) >> 1; if (before(ai[m])) lo = m + 1; else hi = m; }
-    hi = min(lo * MR_IDX, len);
-    lo = lo ? (lo - 1u) * MR_IDX + 1u : 0u;
-    while (lo < hi) { const uint32_t m = (lo + hi) >> 1; if (before(a[m])) lo = m + 1; else hi = m; }
-    rank += lo;
+  const uint32_t lt = lanemask_lt();
+  for (int sh = 0; sh < KB; sh += 8) {
+    for (uint32_t d = lane; d < 256u; d += 32u) sm.hist[warp][d] = 0u;
+    __syncwarp();
+    uint32_t dg[KPT_MAX], off[KPT_MAX];
+#pragma unroll
+    for (int r = 0; r < KPT_MAX; ++r) {
+      if ((uint32_t)r >= kpt) break;
+      const uint32_t d = (uint32_t)(A[wbase + r * 32u + lane] >> sh) & 255u;
+      uint32_t peers = FULL;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        const uint32_t m = __ballot_sync(FULL, (d >> b) & 1u);
+        peers &= ((d >> b) & 1u) ? m : ~m;
+      }
+      const uint32_t base = sm.hist[warp][d];
+      __syncwarp();
+      if ((peers & lt) == 0u) sm.hist[warp][d] = base + __popc(peers);  // the lowest lane of the group
+      __syncwarp();
+      dg[r] = d;
+      off[r] = base + __popc(peers & lt);
+    }
+    __syncthreads();
+    // per digit: exclusive prefix over the warps (in place) and this CTA's total
+    {
+      const uint32_t d = tid >> 2, q = tid & 3u;       // 4 threads per digit, 8 warps each
+      uint32_t c[8], sum = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) { c[j] = sm.hist[q * 8 + j][d]; sum += c[j]; }
+      uint32_t inc = sum;
+#pragma unroll
+      for (int o = 1; o < 4; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(FULL, inc, o);
+        if ((int)q >= o) inc += t;
+      }
+      uint32_t run = inc - sum;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) { sm.hist[q * 8 + j][d] = run; run += c[j]; }
+      if (q == 3u) sm.ccnt[d] = inc;
+    }
+    cluster.sync();  // every CTA's digit counts are visible
+    if (tid < 256u) {
+      uint32_t tot = 0, before = 0;
+#pragma unroll
+      for (int c = 0; c < CS_CTAS; ++c) {
+        const uint32_t v = *cluster.map_shared_rank(&sm.ccnt[tid], (unsigned)c);
+        tot += v;
+        before += ((uint32_t)c < me) ? v : 0u;
+      }
+      // exclusive scan of the totals over the 256 digits (8 warps)
+      const uint32_t inc = warp_incl_scan_u32(tot, lane);
+      if (lane == 31) sm.red[warp] = inc;
+      if (tid == 0) sm.skip = 0u;
+      asm volatile("bar.sync 1, 256;" ::: "memory");
+      uint32_t pre = inc - tot;
+      for (uint32_t w = 0; w < warp; ++w) pre += sm.red[w];
+      sm.gbase[tid] = pre + before;
+      if (tot == S) sm.skip = 1u;  // every key has this digit: nothing moves
+    }
+    __syncthreads();
+    if (!sm.skip) {
+#pragma unroll
+      for (int r = 0; r < KPT_MAX; ++r) {
+        if ((uint32_t)r >= kpt) break;
+        const uint32_t pos = sm.gbase[dg[r]] + sm.hist[warp][dg[r]] + off[r];
+        const K key = A[wbase + r * 32u + lane];
+        *cluster.map_shared_rank(&Bv[pos % per], pos / per) = key;
+      }
+    }
+    cluster.sync();  // the next order is complete; the counts have been read
+    if (!sm.skip) {
+      K* t = A;
+      A = Bv;
+      Bv = t;
+    }
   }
-  sorted[rank] = key;
+  K* out = sorted + (size_t)me * per;
+  for (uint32_t i = tid; i < per; i += CS_NT) out[i] = A[i];
 }
 
 template <typename K>
@@ -315,50 +419,288 @@ struct RunTest {
   }
 };
 
-// The uniform main loop of both passes: `rounds` rounds of UNROLL 16-byte
-// loads per thread, the same number on every lane, so a warp stays converged.
-// Keys that pass test(key) go through the per-warp queue to take(key), 32 at
-// a time; the queue's leftovers (qn < 32) stay for the caller.
-template <typename T, int UNROLL, typename Test, typename Take>
-__device__ __forceinline__ void stream_keys(const uint4* vp, uint64_t rounds, uint64_t step,
-                                            typename KeyOf<T>::K* wq, uint32_t& qn, uint32_t lane,
-                                            Test& test, Take&& take) {
-  using K = typename KeyOf<T>::K;
-  constexpr int EPV = Vec16<T>::N;
-  for (uint64_t r = 0; r < rounds; ++r, vp += step * UNROLL) {
-    uint4 q[UNROLL];
-#pragma unroll
-    for (int u = 0; u < UNROLL; ++u) q[u] = ld_stream16(vp + u * step);
-#pragma unroll
-    for (int u = 0; u < UNROLL; ++u) {
-      T e[EPV];
-      unpack16<T>(q[u], e);
-      K kk[EPV];
-      bool hh[EPV];
-      bool any = false;
-#pragma unroll
-      for (int t = 0; t < EPV; ++t) {
-        kk[t] = KeyOf<T>::to(e[t]);
-        hh[t] = test(kk[t]);
-        any = any || hh[t];
+// ------------------------------------------------------------------ input streams of the passes
+// The body of the input (16-byte vectors from its first 16-byte boundary) is
+// split between the CTAs the same way in PASS 1 and PASS 2, so that PASS 2's
+// per-CTA write ranges (sized by PASS 1) fit.  Two ways to stream it:
+//   UNROLL > 0:  grid-strided rounds of UNROLL non-allocating vector loads per
+//                thread, into registers;
+//   UNROLL == 0: chunks of RING_VECS vectors (16 KB) dealt round-robin to the
+//                CTAs and staged in a ring of shared-memory stages: thread 0
+//                fills a stage with one bulk copy (cp.async.bulk, the TMA
+//                engine) that completes on the stage's "full" mbarrier; every
+//                thread reads its V vectors back and each warp then arrives on
+//                the stage's "empty" mbarrier, after which thread 0 refills it.
+//                Several chunks stay in flight per SM all the time, with no
+//                registers held for them.
+// Every thread of a CTA handles the same number of vectors either way, so the
+// warps stay converged.  The vectors past the main loop (main_end .. nvec) are
+// left to the caller, one per thread, grid-strided.
+constexpr uint32_t RING_BYTES = 16384;
+constexpr uint32_t RING_VECS = RING_BYTES / 16;
+constexpr uint32_t RING_MAX_ST = 8;
+
+struct RingBars {
+  unsigned long long full[RING_MAX_ST];
+  unsigned long long empty[RING_MAX_ST];
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t a, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t a) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return ok != 0u;
+}
+// Waits until the phase of parity `parity` of barrier `a` has completed; gives
+// up (false) after about a second, so that a broken pipeline cannot hang the GPU.
+__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity) {
+  if (mbar_try(a, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try(a, parity))
+    if (clock64() - t0 > (2ll << 30)) return false;
+  return true;
+}
+// One bulk copy global -> this CTA's shared memory, completing on mbarrier `bar`
+// (both addresses 16-byte aligned, bytes a multiple of 16).
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+// The TMA ring of one CTA.  All threads call start() and next(); next() is
+// CTA-uniform (every thread sees the same chunk count).
+template <int NT>
+struct Ring {
+  static constexpr int V = (int)(RING_VECS / NT);  // vectors per thread per chunk
+  const uint4* body;
+  uint4* stage0;
+  uint32_t bars, nst, nmine, j, issued, G, b;
+  bool ok;
+
+  __device__ __forceinline__ uint32_t full(uint32_t s) const { return bars + 8u * s; }
+  __device__ __forceinline__ uint32_t empty(uint32_t s) const { return bars + 8u * (RING_MAX_ST + s); }
+  // thread 0: this CTA's chunk jj into stage jj % nst
+  __device__ __forceinline__ void issue(uint32_t jj) {
+    const uint32_t s = jj % nst;
+    const uint64_t c = (uint64_t)b + (uint64_t)jj * G;
+    mbar_expect_tx(full(s), RING_BYTES);
+    bulk_g2s(smem_u32(stage0 + (size_t)s * RING_VECS), body + c * RING_VECS, RING_BYTES, full(s));
+  }
+  __device__ __forceinline__ void start(const uint4* body_, uint64_t nch, uint4* ring, RingBars* rb,
+                                        uint32_t nst_) {
+    body = body_;
+    stage0 = ring;
+    bars = smem_u32(rb);
+    nst = min(max(nst_, 2u), RING_MAX_ST);
+    G = gridDim.x;
+    b = blockIdx.x;
+    nmine = nch > b ? (uint32_t)((nch - b + G - 1) / G) : 0u;
+    j = 0;
+    issued = 0;
+    ok = true;
+    if (threadIdx.x == 0) {
+      for (uint32_t s = 0; s < nst; ++s) {
+        mbar_init(full(s), 1u);
+        mbar_init(empty(s), NT / 32);
       }
-      if (!__any_sync(FULL, any)) continue;
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (; issued < min(nst, nmine); ++issued) issue(issued);
+  }
+  // This thread's V vectors of the CTA's next chunk; false when the CTA has
+  // none left, or (warp-uniformly) after a wait gave up.
+  __device__ __forceinline__ bool next(uint4 (&q)[V]) {
+    if (j >= nmine || !ok) return false;
+    const uint32_t s = j % nst;
+    bool good = mbar_wait(full(s), (j / nst) & 1u);
+    if (__all_sync(FULL, good)) {
+      const uint4* st = stage0 + (size_t)s * RING_VECS;
 #pragma unroll
-      for (int t = 0; t < EPV; ++t) {
-        K k0;
-        if (wq_push(wq, qn, hh[t], kk[t], lane, &k0)) take(k0);
+      for (int v = 0; v < V; ++v) q[v] = st[threadIdx.x + v * NT];
+      __syncwarp();
+      if ((threadIdx.x & 31u) == 0u) mbar_arrive(empty(s));
+      if (threadIdx.x == 0 && j >= 1 && issued < nmine) {  // refill the stage chunk j - 1 used
+        const uint32_t jp = issued - nst;                    // == j - 1
+        if (mbar_wait(empty(jp % nst), (jp / nst) & 1u)) {
+          issue(issued);
+          ++issued;
+        } else {
+          good = false;
+        }
+      }
+    } else {
+      good = false;
+    }
+    ok = __all_sync(FULL, good);
+    ++j;
+    return ok;
+  }
+  // After the main loop (all threads): with a wait that gave up anywhere, the
+  // status is set and thread 0 waits (bounded) for the copies it issued that
+  // were not consumed, so none is still writing when the CTA exits.
+  __device__ __forceinline__ void finish(Counters* C) {
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        atomicCAS(&C->status, 0u, (uint32_t)GGMS_E_INTERNAL);
+        for (uint32_t jj = 0; jj < issued; ++jj)
+          if (jj + nst >= issued) mbar_wait(full(jj % nst), (jj / nst) & 1u);
       }
     }
   }
+};
+
+// The main loop's driver for one pass kernel: run(f) calls f(vector) for each
+// of this thread's vectors of the main part.  run() is called at most once,
+// by all threads (the kernels branch on CTA-uniform values only); the ring is
+// started inside it, so a kernel that skips the main part has no copy in flight.
+template <int NT, int UNROLL>
+struct PassStream {
+  const uint4* body;
+  uint4* ring_smem;
+  RingBars* rb;
+  uint64_t nvec, nch, gtid, gstride, main_end, rounds;
+  uint32_t nst;
+  bool started;
+  Ring<NT> ring;
+  __device__ __forceinline__ void start(const uint4* body_, uint64_t nvec_, uint4* ring_smem_, RingBars* rb_,
+                                        uint32_t nst_) {
+    body = body_;
+    nvec = nvec_;
+    ring_smem = ring_smem_;
+    rb = rb_;
+    nst = nst_;
+    started = false;
+    gtid = (uint64_t)blockIdx.x * NT + threadIdx.x;
+    gstride = (uint64_t)gridDim.x * NT;
+    if (UNROLL > 0) {
+      rounds = nvec / (gstride * (UNROLL > 0 ? UNROLL : 1));
+      main_end = rounds * gstride * (UNROLL > 0 ? UNROLL : 1);
+    } else {
+      nch = nvec / RING_VECS;
+      main_end = nch * RING_VECS;
+    }
+  }
+  template <typename F>
+  __device__ __forceinline__ void run(F&& f) {
+    if constexpr (UNROLL > 0) {
+      const uint4* vp = body + gtid;
+      for (uint64_t r = 0; r < rounds; ++r, vp += gstride * UNROLL) {
+        uint4 q[UNROLL];
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) q[u] = ld_stream16(vp + u * gstride);
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) f(q[u]);
+      }
+    } else {
+      ring.start(body, nch, ring_smem, rb, nst);
+      started = true;
+      uint4 q[Ring<NT>::V];
+      while (ring.next(q)) {
+#pragma unroll
+        for (int v = 0; v < Ring<NT>::V; ++v) f(q[v]);
+      }
+    }
+  }
+  // The TMA ring only: this thread's vectors of the CTA's next DU / V chunks
+  // into q; returns how many it wrote (CTA-uniform; 0 at the end).
+  template <int DU>
+  __device__ __forceinline__ int next_batch(uint4 (&q)[DU]) {
+    constexpr int V = Ring<NT>::V;
+    static_assert(DU % V == 0, "a batch holds whole chunks");
+    if (!started) {
+      ring.start(body, nch, ring_smem, rb, nst);
+      started = true;
+    }
+    int got = 0;
+#pragma unroll
+    for (int c = 0; c < DU / V; ++c) {
+      uint4 t[V];
+      if (!ring.next(t)) break;
+#pragma unroll
+      for (int v = 0; v < V; ++v) q[c * V + v] = t[v];
+      got += V;
+    }
+    return got;
+  }
+  // All threads, after the main part (a no-op when the ring never started).
+  __device__ __forceinline__ void finish(Counters* C) {
+    if constexpr (UNROLL == 0) {
+      if (started) ring.finish(C);
+    }
+  }
+  // vectors of the main part this thread handles
+  __device__ __forceinline__ uint64_t my_vecs() const {
+    if constexpr (UNROLL > 0) {
+      return rounds * UNROLL;
+    } else {
+      const uint64_t G = gridDim.x, b = blockIdx.x;
+      return (nch > b ? (nch - b + G - 1) / G : 0) * (uint64_t)Ring<NT>::V;
+    }
+  }
+};
+
+// Shared-memory bytes of a pass kernel's ring (0 for the register streams).
+__host__ __device__ constexpr size_t ring_bytes(int unroll, uint32_t nst) {
+  return unroll > 0 ? 0 : (size_t)nst * RING_BYTES + 128;
+}
+// The ring's place: the end of the kernel's dynamic shared memory, 128-byte aligned.
+__device__ __forceinline__ uint4* ring_at(uint8_t* smem, size_t used) {
+  return reinterpret_cast<uint4*>(smem + ((used + 127) & ~(size_t)127));
+}
+
+// The uniform main loop's per-vector step: keys that pass test(key) go through
+// the per-warp queue to take(key), 32 at a time; the queue's leftovers (qn < 32)
+// stay for the caller.
+template <typename T, typename Src, typename Test, typename Take>
+__device__ __forceinline__ void stream_keys(Src& src, typename KeyOf<T>::K* wq, uint32_t& qn, uint32_t lane,
+                                            Test& test, Take&& take) {
+  using K = typename KeyOf<T>::K;
+  constexpr int EPV = Vec16<T>::N;
+  src.run([&](const uint4& qv) {
+    T e[EPV];
+    unpack16<T>(qv, e);
+    K kk[EPV];
+    bool hh[EPV];
+    bool any = false;
+#pragma unroll
+    for (int t = 0; t < EPV; ++t) {
+      kk[t] = KeyOf<T>::to(e[t]);
+      hh[t] = test(kk[t]);
+      any = any || hh[t];
+    }
+    if (!__any_sync(FULL, any)) return;
+#pragma unroll
+    for (int t = 0; t < EPV; ++t) {
+      K k0;
+      if (wq_push(wq, qn, hh[t], kk[t], lane, &k0)) take(k0);
+    }
+  });
 }
 
 // PASS 1 over windows with R runs (compile-time): the run tests, the per-run
 // counts (CNT) into below[0..R), the keys inside a run to take().
-template <typename T, int UNROLL, uint32_t R, bool CNT, typename Take>
-__device__ __forceinline__ void count_runs(const Windows<typename KeyOf<T>::K>& W, const uint4* vp,
-                                           uint64_t rounds, uint64_t step, typename KeyOf<T>::K* wq,
-                                           uint32_t& qn, uint32_t lane, uint32_t (&below)[L0_WIN],
-                                           Take&& take) {
+template <typename T, uint32_t R, bool CNT, typename Src, typename Take>
+__device__ __forceinline__ void count_runs(const Windows<typename KeyOf<T>::K>& W, Src& src,
+                                           typename KeyOf<T>::K* wq, uint32_t& qn, uint32_t lane,
+                                           uint32_t (&below)[L0_WIN], Take&& take) {
   using K = typename KeyOf<T>::K;
   RunTest<K, R, CNT> t;
 #pragma unroll
@@ -367,7 +709,7 @@ __device__ __forceinline__ void count_runs(const Windows<typename KeyOf<T>::K>& 
     t.sp[r] = (K)(W.hi[r] - W.lo[r]);
     t.bl[r] = 0u;
   }
-  stream_keys<T, UNROLL>(vp, rounds, step, wq, qn, lane, t, take);
+  stream_keys<T>(src, wq, qn, lane, t, take);
 #pragma unroll
   for (uint32_t r = 0; r < R; ++r) below[r] = t.bl[r];
 }
@@ -389,12 +731,14 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_count(const T* __res
                                               const Grid<typename KeyOf<T>::K>* __restrict__ Gs,
                                               Counters* C,
                                               const Windows<typename KeyOf<T>::K>* __restrict__ Wg,
-                                              uint32_t* __restrict__ hist0, uint32_t* __restrict__ crow) {
+                                              uint32_t* __restrict__ hist0, uint32_t* __restrict__ crow,
+                                              uint32_t ring_st) {
   using K = typename KeyOf<T>::K;
   constexpr int EPV = Vec16<T>::N;
-  extern __shared__ __align__(16) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem[];
   __shared__ Windows<K> W;
   __shared__ uint32_t red[NT / 32][2 * L0_WIN + 1];
+  __shared__ RingBars rbars;
   const Grid<K>* G = Gs + C->asg_choice;
   uint2* s1 = (uint2*)smem;
   uint2* s2 = s1 + GRID_T1;
@@ -413,8 +757,9 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_count(const T* __res
   uint64_t head = ((16u - (uint32_t)((uintptr_t)in & 15u)) & 15u) / sizeof(T);
   if (head > n) head = n;
   const uint64_t nvec = (n - head) / EPV;
-  const uint4* vp = reinterpret_cast<const uint4*>(in + head) + gtid;
-  const uint64_t rounds = nvec / (gstride * UNROLL);
+  PassStream<NT, UNROLL> src;
+  src.start(reinterpret_cast<const uint4*>(in + head), nvec,
+            ring_at(smem, GRID_SMEM + (size_t)B * 4u + wq_bytes((uint32_t)NT, sizeof(K))), &rbars, ring_st);
 
   auto bucket = [&](K key) { return min(grid_eval<K>(gv, key), B - 1u); };
   // windows: this thread's count of keys below each run's first key (only
@@ -423,47 +768,42 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_count(const T* __res
   uint32_t seen = 0;  // keys this thread counted (windows only)
 
   if (!W.on) {
-    for (uint64_t r = 0; r < rounds; ++r, vp += gstride * UNROLL) {
-      uint4 q[UNROLL];
+    src.run([&](const uint4& qv) {
+      T e[EPV];
+      unpack16<T>(qv, e);
+      uint32_t b[EPV];
 #pragma unroll
-      for (int u = 0; u < UNROLL; ++u) q[u] = ld_stream16(vp + u * gstride);
+      for (int t = 0; t < EPV; ++t) b[t] = bucket(KeyOf<T>::to(e[t]));
+      bool same = true;
 #pragma unroll
-      for (int u = 0; u < UNROLL; ++u) {
-        T e[EPV];
-        unpack16<T>(q[u], e);
-        uint32_t b[EPV];
+      for (int t = 1; t < EPV; ++t) same = same && (b[t] == b[0]);
+      if (same) {
+        atomicAdd(&hs[b[0]], (uint32_t)EPV);
+      } else {
 #pragma unroll
-        for (int t = 0; t < EPV; ++t) b[t] = bucket(KeyOf<T>::to(e[t]));
-        bool same = true;
-#pragma unroll
-        for (int t = 1; t < EPV; ++t) same = same && (b[t] == b[0]);
-        if (same) {
-          atomicAdd(&hs[b[0]], (uint32_t)EPV);
-        } else {
-#pragma unroll
-          for (int t = 0; t < EPV; ++t) atomicAdd(&hs[b[t]], 1u);
-        }
+        for (int t = 0; t < EPV; ++t) atomicAdd(&hs[b[t]], 1u);
       }
-    }
+    });
   } else {
     // R runs and (CNT) the per-run counts are compile-time, so that the bounds
     // and counts stay in registers
     uint32_t qn = 0;  // warp-uniform queue fill
     auto take = [&](K k) { atomicAdd(&hs[bucket(k)], 1u); };
     switch (W.R * 2u + (W.cnt ? 1u : 0u)) {
-      case 2: count_runs<T, UNROLL, 1, false>(W, vp, rounds, gstride, wq, qn, lane, below, take); break;
-      case 3: count_runs<T, UNROLL, 1, true>(W, vp, rounds, gstride, wq, qn, lane, below, take); break;
-      case 4: count_runs<T, UNROLL, 2, false>(W, vp, rounds, gstride, wq, qn, lane, below, take); break;
-      case 5: count_runs<T, UNROLL, 2, true>(W, vp, rounds, gstride, wq, qn, lane, below, take); break;
-      case 6: count_runs<T, UNROLL, 3, false>(W, vp, rounds, gstride, wq, qn, lane, below, take); break;
-      case 7: count_runs<T, UNROLL, 3, true>(W, vp, rounds, gstride, wq, qn, lane, below, take); break;
-      case 8: count_runs<T, UNROLL, 4, false>(W, vp, rounds, gstride, wq, qn, lane, below, take); break;
-      default: count_runs<T, UNROLL, 4, true>(W, vp, rounds, gstride, wq, qn, lane, below, take); break;
+      case 2: count_runs<T, 1, false>(W, src, wq, qn, lane, below, take); break;
+      case 3: count_runs<T, 1, true>(W, src, wq, qn, lane, below, take); break;
+      case 4: count_runs<T, 2, false>(W, src, wq, qn, lane, below, take); break;
+      case 5: count_runs<T, 2, true>(W, src, wq, qn, lane, below, take); break;
+      case 6: count_runs<T, 3, false>(W, src, wq, qn, lane, below, take); break;
+      case 7: count_runs<T, 3, true>(W, src, wq, qn, lane, below, take); break;
+      case 8: count_runs<T, 4, false>(W, src, wq, qn, lane, below, take); break;
+      default: count_runs<T, 4, true>(W, src, wq, qn, lane, below, take); break;
     }
-    seen += (uint32_t)(rounds * UNROLL * EPV);
+    seen += (uint32_t)(src.my_vecs() * EPV);
     __syncwarp();
     if (lane < qn) atomicAdd(&hs[bucket(wq[lane])], 1u);
   }
+  src.finish(C);
   // the partial last round, then the unaligned head and the tail that does not fill a vector
   auto tally = [&](K key) {
     if (!W.on) {
@@ -482,7 +822,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_count(const T* __res
     if (h) atomicAdd(&hs[bucket(key)], 1u);
   };
   const T* vbase = in + head;
-  for (uint64_t i = rounds * gstride * UNROLL + gtid; i < nvec; i += gstride) {
+  for (uint64_t i = src.main_end + gtid; i < nvec; i += gstride) {
     T e[EPV];
     unpack16<T>(ld_stream16(vbase + i * EPV), e);
 #pragma unroll
@@ -782,12 +1122,14 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
                                                 const Windows<typename KeyOf<T>::K>* __restrict__ Wg,
                                                 const uint32_t* __restrict__ cmap0,
                                                 const uint32_t* __restrict__ crow,
-                                                typename KeyOf<T>::K* dst, uint64_t dst_cap) {
+                                                typename KeyOf<T>::K* dst, uint64_t dst_cap,
+                                                uint32_t ring_st) {
   using K = typename KeyOf<T>::K;
   constexpr int EPV = Vec16<T>::N;
   if (C->coarse) return;  // l0_compact_coarse copies this call's groups
-  extern __shared__ __align__(16) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem[];
   __shared__ Windows<K> W;
+  __shared__ RingBars rbars;
   if (threadIdx.x == 0) W = *Wg;
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&C->passes, 1u);
   const Grid<K>* G = Gs + C->asg_choice;
@@ -891,8 +1233,9 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
   uint64_t head = ((16u - (uint32_t)((uintptr_t)in & 15u)) & 15u) / sizeof(T);
   if (head > n) head = n;
   const uint64_t nvec = (n - head) / EPV;
-  const uint4* vp = reinterpret_cast<const uint4*>(in + head) + gtid;
-  const uint64_t rounds = nvec / (gstride * UNROLL);
+  PassStream<NT, UNROLL> src;
+  src.start(reinterpret_cast<const uint4*>(in + head), nvec,
+            ring_at(smem, GRID_SMEM + (size_t)(MAX_B0 / 32 + QW + HOT_WORDS + B) * 4u), &rbars, ring_st);
   bool overflow = false;
   auto put = [&](uint32_t b, K key) {
     const uint32_t slot = atomicAdd(&cur[b], 1u);
@@ -929,37 +1272,26 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
       t.lo[r] = win ? W.lo[r] : run_lo[r];
       t.sp[r] = win ? (K)(W.hi[r] - W.lo[r]) : run_span[r];
     }
-    stream_keys<T, UNROLL>(vp, rounds, gstride, wq, qn, lane, t, bucket_and_put);
+    stream_keys<T>(src, wq, qn, lane, t, bucket_and_put);
   };
   // Most buckets copied: every key takes the long path anyway, so the queue
   // only serialises it; each lane buckets its keys directly, all EPV of a
   // vector at once (independent lookups in flight).
   auto dense = [&]() {
-    constexpr int DU = UNROLL < 4 ? UNROLL : 4;  // vectors in flight (the same elements as PASS 1)
-    const uint4* dp = vp;
-    for (uint64_t r = 0; r < rounds; ++r, dp += gstride * UNROLL) {
+    src.run([&](const uint4& qv) {
+      T e[EPV];
+      unpack16<T>(qv, e);
+      K kk[EPV];
+      uint32_t b[EPV];
 #pragma unroll
-      for (int u0 = 0; u0 < UNROLL; u0 += DU) {
-      uint4 q[DU];
-#pragma unroll
-      for (int u = 0; u < DU; ++u) q[u] = ld_stream16(dp + (u0 + u) * gstride);
-#pragma unroll
-      for (int u = 0; u < DU; ++u) {
-        T e[EPV];
-        unpack16<T>(q[u], e);
-        K kk[EPV];
-        uint32_t b[EPV];
-#pragma unroll
-        for (int t = 0; t < EPV; ++t) {
-          kk[t] = KeyOf<T>::to(e[t]);
-          b[t] = bmap(min(grid_eval<K>(gv, kk[t]), B - 1u));
-        }
-#pragma unroll
-        for (int t = 0; t < EPV; ++t)
-          if ((amask[b[t] >> 5] >> (b[t] & 31)) & 1u) put(b[t], kk[t]);
+      for (int t = 0; t < EPV; ++t) {
+        kk[t] = KeyOf<T>::to(e[t]);
+        b[t] = bmap(min(grid_eval<K>(gv, kk[t]), B - 1u));
       }
-      }
-    }
+#pragma unroll
+      for (int t = 0; t < EPV; ++t)
+        if ((amask[b[t] >> 5] >> (b[t] & 31)) & 1u) put(b[t], kk[t]);
+    });
   };
   if (!use_win && nruns > L0_RUNS && ncopied * 2u >= B) {
     dense();
@@ -976,12 +1308,13 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
     case 2: runs(std::integral_constant<uint32_t, 2>{}, false); break;
     case 3: runs(std::integral_constant<uint32_t, 3>{}, false); break;
     case 4: runs(std::integral_constant<uint32_t, 4>{}, false); break;
-    default: stream_keys<T, UNROLL>(vp, rounds, gstride, wq, qn, lane, in_hot, bucket_and_put); break;
+    default: stream_keys<T>(src, wq, qn, lane, in_hot, bucket_and_put); break;
   }
+  src.finish(C);
   __syncwarp();
   if (lane < qn) bucket_and_put(wq[lane]);
   const T* vbase = in + head;
-  for (uint64_t i = rounds * gstride * UNROLL + gtid; i < nvec; i += gstride) {
+  for (uint64_t i = src.main_end + gtid; i < nvec; i += gstride) {
     T e[EPV];
     unpack16<T>(ld_stream16(vbase + i * EPV), e);
 #pragma unroll
@@ -1040,9 +1373,11 @@ __global__ void l0_mode_ks(const uint32_t* __restrict__ I, const uint32_t* __res
 }
 
 // Keys of one PASS-2 chunk of the coarse mode: up to 4 vectors per thread.
+// vectors per thread per staged chunk: up to 4 (the TMA ring: 4)
+__host__ __device__ constexpr int coarse_du(int unroll) { return unroll == 0 ? 4 : (unroll < 4 ? unroll : 4); }
 template <typename T, int NT, int UNROLL>
 __host__ __device__ constexpr uint32_t coarse_chunk() {
-  return (uint32_t)NT * (UNROLL < 4 ? UNROLL : 4) * Vec16<T>::N;
+  return (uint32_t)NT * coarse_du(UNROLL) * Vec16<T>::N;
 }
 
 // PASS 2 of the coarse mode.  Same element -> CTA assignment as PASS 1; CTA
@@ -1056,18 +1391,20 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact_coarse(const
                                                        const Grid<typename KeyOf<T>::K>* __restrict__ Gs,
                                                        Counters* C, const uint32_t* __restrict__ cmap0,
                                                        const uint32_t* __restrict__ crow,
-                                                       typename KeyOf<T>::K* dst, uint64_t dst_cap) {
+                                                       typename KeyOf<T>::K* dst, uint64_t dst_cap,
+                                                       uint32_t ring_st) {
   using K = typename KeyOf<T>::K;
   constexpr int EPV = Vec16<T>::N;
-  constexpr int DU = UNROLL < 4 ? UNROLL : 4;
+  constexpr int DU = coarse_du(UNROLL);
   constexpr uint32_t CH = coarse_chunk<T, NT, UNROLL>();
   constexpr uint32_t NONE = 0xFFFFFFFFu;
   static_assert(CH <= 65536u, "chunk ranks are 16-bit");
   if (!C->coarse) return;  // l0_compact copies this call's buckets
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&C->passes, 1u);
-  extern __shared__ __align__(16) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem[];
   __shared__ uint32_t gbase[NGRP], hist[NGRP], off[NGRP], cflag[NGRP / 32];
   __shared__ uint32_t total_s;
+  __shared__ RingBars rbars;
   const Grid<K>* G = Gs + C->asg_choice;
   uint2* s1 = (uint2*)smem;
   uint2* s2 = s1 + GRID_T1;
@@ -1095,91 +1432,104 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact_coarse(const
   uint64_t head = ((16u - (uint32_t)((uintptr_t)in & 15u)) & 15u) / sizeof(T);
   if (head > n) head = n;
   const uint64_t nvec = (n - head) / EPV;
-  const uint4* vp = reinterpret_cast<const uint4*>(in + head) + gtid;
-  const uint64_t rounds = nvec / (gstride * UNROLL);
+  PassStream<NT, UNROLL> src;
+  src.start(reinterpret_cast<const uint4*>(in + head), nvec,
+            ring_at(smem, GRID_SMEM + (size_t)CH * (sizeof(K) + 1)), &rbars, ring_st);
   bool overflow = false;
-  // chunk c: DU vectors of round c / CPR; the next chunk's loads are issued
-  // before this chunk's barriers, so they are in flight while it is staged
-  constexpr int CPR = UNROLL / DU;
-  const uint64_t nch = rounds * CPR;
-  auto chunk_ptr = [&](uint64_t c) {
-    return vp + (c / CPR) * gstride * UNROLL + (uint64_t)((int)(c % CPR) * DU) * gstride;
-  };
-  uint4 q[DU];
-  if (nch) {
-    const uint4* p0 = chunk_ptr(0);
+  // One chunk: the first `got` of this thread's DU vectors (got is CTA-uniform).
+  // The group of every key (bucket >> gsh), its rank among the chunk's keys of
+  // that group (a shared atomic), a scan of the NGRP counts, the keys into
+  // shared memory in group order, then thread i stores staged key i.
+  auto stage = [&](const uint4 (&q)[DU], int got) {
+    uint32_t pk[DU * EPV];  // (group << 16) | rank inside the chunk's group, or NONE
 #pragma unroll
-    for (int u = 0; u < DU; ++u) q[u] = ld_stream16(p0 + u * gstride);
-  }
-  for (uint64_t c = 0; c < nch; ++c) {
-    {
-      uint32_t pk[DU * EPV];  // (group << 16) | rank inside the chunk's group, or NONE
+    for (int u = 0; u < DU; ++u) {
+      T e[EPV];
+      unpack16<T>(q[u], e);
+      uint32_t g[EPV];
 #pragma unroll
-      for (int u = 0; u < DU; ++u) {
-        T e[EPV];
-        unpack16<T>(q[u], e);
-        uint32_t g[EPV];
+      for (int t = 0; t < EPV; ++t) g[t] = u < got ? group(KeyOf<T>::to(e[t])) : NONE;
 #pragma unroll
-        for (int t = 0; t < EPV; ++t) g[t] = group(KeyOf<T>::to(e[t]));
+      for (int t = 0; t < EPV; ++t)
+        pk[u * EPV + t] = g[t] == NONE ? NONE : (g[t] << 16) | atomicAdd(&hist[g[t]], 1u);
+    }
+    __syncthreads();
+    if (tid < 32) {  // exclusive scan of the NGRP counts, 8 per lane
+      uint32_t c8[NGRP / 32], sum = 0;
 #pragma unroll
-        for (int t = 0; t < EPV; ++t)
-          pk[u * EPV + t] = g[t] == NONE ? NONE : (g[t] << 16) | atomicAdd(&hist[g[t]], 1u);
+      for (int j = 0; j < (int)(NGRP / 32); ++j) { c8[j] = hist[lane * (NGRP / 32) + j]; sum += c8[j]; }
+      uint32_t inc = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(FULL, inc, o);
+        if ((int)lane >= o) inc += t;
       }
+      uint32_t run = inc - sum;
+#pragma unroll
+      for (int j = 0; j < (int)(NGRP / 32); ++j) { off[lane * (NGRP / 32) + j] = run; run += c8[j]; }
+      if (lane == 31) total_s = inc;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < DU; ++u) {
+      T e[EPV];
+      unpack16<T>(q[u], e);
+#pragma unroll
+      for (int t = 0; t < EPV; ++t) {
+        const uint32_t x = pk[u * EPV + t];
+        if (x != NONE) {
+          const uint32_t g = x >> 16, pos = off[g] + (x & 0xFFFFu);
+          stg[pos] = KeyOf<T>::to(e[t]);
+          sg[pos] = (uint8_t)g;
+        }
+      }
+    }
+    __syncthreads();
+    const uint32_t tot = total_s;
+    for (uint32_t i = tid; i < tot; i += NT) {
+      const uint32_t g = sg[i];
+      const uint64_t slot = (uint64_t)gbase[g] + (i - off[g]);
+      if (slot < dst_cap) dst[slot] = stg[i]; else overflow = true;
+    }
+    __syncthreads();
+    for (uint32_t g = tid; g < NGRP; g += NT) {
+      gbase[g] += hist[g];
+      hist[g] = 0u;
+    }
+    __syncthreads();
+  };
+  if constexpr (UNROLL > 0) {
+    // chunk c: DU vectors of round c / CPR; the next chunk's loads are issued
+    // before this chunk's barriers, so they are in flight while it is staged
+    constexpr int CPR = UNROLL / DU;
+    const uint4* vp = reinterpret_cast<const uint4*>(in + head) + gtid;
+    const uint64_t nch = src.rounds * CPR;
+    auto chunk_ptr = [&](uint64_t c) {
+      return vp + (c / CPR) * gstride * UNROLL + (uint64_t)((int)(c % CPR) * DU) * gstride;
+    };
+    uint4 q[DU];
+    if (nch) {
+      const uint4* p0 = chunk_ptr(0);
+#pragma unroll
+      for (int u = 0; u < DU; ++u) q[u] = ld_stream16(p0 + u * gstride);
+    }
+    for (uint64_t c = 0; c < nch; ++c) {
       uint4 qn[DU];
       if (c + 1 < nch) {
         const uint4* pn = chunk_ptr(c + 1);
 #pragma unroll
         for (int u = 0; u < DU; ++u) qn[u] = ld_stream16(pn + u * gstride);
       }
-      __syncthreads();
-      if (tid < 32) {  // exclusive scan of the NGRP counts, 8 per lane
-        uint32_t c8[NGRP / 32], sum = 0;
-#pragma unroll
-        for (int j = 0; j < (int)(NGRP / 32); ++j) { c8[j] = hist[lane * (NGRP / 32) + j]; sum += c8[j]; }
-        uint32_t inc = sum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const uint32_t t = __shfl_up_sync(FULL, inc, o);
-          if ((int)lane >= o) inc += t;
-        }
-        uint32_t run = inc - sum;
-#pragma unroll
-        for (int j = 0; j < (int)(NGRP / 32); ++j) { off[lane * (NGRP / 32) + j] = run; run += c8[j]; }
-        if (lane == 31) total_s = inc;
-      }
-      __syncthreads();
-#pragma unroll
-      for (int u = 0; u < DU; ++u) {
-        T e[EPV];
-        unpack16<T>(q[u], e);
-#pragma unroll
-        for (int t = 0; t < EPV; ++t) {
-          const uint32_t x = pk[u * EPV + t];
-          if (x != NONE) {
-            const uint32_t g = x >> 16, pos = off[g] + (x & 0xFFFFu);
-            stg[pos] = KeyOf<T>::to(e[t]);
-            sg[pos] = (uint8_t)g;
-          }
-        }
-      }
-      __syncthreads();
-      const uint32_t tot = total_s;
-      for (uint32_t i = tid; i < tot; i += NT) {
-        const uint32_t g = sg[i];
-        const uint64_t slot = (uint64_t)gbase[g] + (i - off[g]);
-        if (slot < dst_cap) dst[slot] = stg[i]; else overflow = true;
-      }
-      __syncthreads();
-      for (uint32_t g = tid; g < NGRP; g += NT) {
-        gbase[g] += hist[g];
-        hist[g] = 0u;
-      }
-      __syncthreads();
+      stage(q, DU);
 #pragma unroll
       for (int u = 0; u < DU; ++u) q[u] = qn[u];
     }
+  } else {
+    uint4 q[DU];
+    for (int got; (got = src.template next_batch<DU>(q)) > 0;) stage(q, got);
   }
-  // the partial last round, the unaligned head and the tail: one key at a time
+  src.finish(C);
+  // the vectors past the main part, the unaligned head and the tail: one key at a time
   auto put = [&](K key) {
     const uint32_t g = group(key);
     if (g == NONE) return;
@@ -1187,7 +1537,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact_coarse(const
     if (slot < dst_cap) dst[slot] = key; else overflow = true;
   };
   const T* vbase = in + head;
-  for (uint64_t i = rounds * gstride * UNROLL + gtid; i < nvec; i += gstride) {
+  for (uint64_t i = src.main_end + gtid; i < nvec; i += gstride) {
     T e[EPV];
     unpack16<T>(ld_stream16(vbase + i * EPV), e);
 #pragma unroll
@@ -1577,7 +1927,7 @@ __global__ __launch_bounds__(NT) void small_select(const InT* __restrict__ src,
                                                   Caps caps) {
   using K = typename KeyOf<InT>::K;
   Counters* C = const_cast<Counters*>(C_);
-  extern __shared__ __align__(16) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem[];
   K* vals = (K*)smem;
   uint32_t* hist = (uint32_t*)(smem + SMALL_SMEM);           // [SS_GROUP][256]
   __shared__ uint32_t kid[SS_MAXK];

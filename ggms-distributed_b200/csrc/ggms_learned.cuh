@@ -307,7 +307,7 @@ __device__ void learned_finish(const K* sorted, uint32_t S, uint32_t B, uint32_t
 template <typename K>
 __global__ __launch_bounds__(SETUP_NT) void setup_pl_knots(const K* __restrict__ sorted, uint32_t S,
                                                           uint32_t B, Assigner<K>* A, uint32_t mreq) {
-  extern __shared__ __align__(16) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
   pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, A, sm, mreq);
 }
@@ -324,7 +324,7 @@ __global__ __launch_bounds__(SETUP_NT) void setup_learned_pl(const K* __restrict
                                                             uint32_t* choice,
                                                             const uint32_t* __restrict__ krank,
                                                             uint32_t nk, uint64_t n, float window_z) {
-  extern __shared__ __align__(16) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
   __shared__ Warp wsh;
   __shared__ uint32_t wred[33];
@@ -361,7 +361,7 @@ __global__ __launch_bounds__(SETUP_NT) void pl_grad_probe(const Assigner<K>* __r
                                                          const LearnState* L,
                                                          const float* __restrict__ theta_in,
                                                          float* loss_out, float* grad_out) {
-  extern __shared__ __align__(16) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
   const uint32_t M = A->M;
   pl_stats_load(L, M, sm.st);

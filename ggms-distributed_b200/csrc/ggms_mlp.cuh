@@ -150,7 +150,7 @@ __global__ void __cluster_dims__(MLP_CTAS, 1, 1) __launch_bounds__(MLP_NT)
 mlp_train(const K* __restrict__ sorted, uint32_t S_n, const Assigner<K>* __restrict__ A,
           LearnState* L, float* Pglob, uint32_t steps, float lr, const float* px, const float* pt,
           float* probe) {
-  extern __shared__ __align__(16) uint8_t smem_raw[];
+  extern __shared__ __align__(128) uint8_t smem_raw[];
   MlpSmem& S = *reinterpret_cast<MlpSmem*>(smem_raw);
   cg::cluster_group cluster = cg::this_cluster();
   const unsigned rank = cluster.block_rank();
@@ -295,7 +295,7 @@ template <typename K>
 __global__ __launch_bounds__(SETUP_NT) void setup_mlp_begin(const K* __restrict__ sorted, uint32_t S,
                                                            uint32_t B, Assigner<K>* A, float* P,
                                                            uint32_t mreq) {
-  extern __shared__ __align__(16) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
   pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_MLP, A, sm, mreq);
   mlp_init<K>(sorted, S, A, P);
@@ -306,7 +306,7 @@ __global__ __launch_bounds__(SETUP_NT) void setup_mlp_finish(const K* __restrict
                                                             uint32_t B, float bound, const float* P,
                                                             Assigner<K>* A, Grid<K>* G, LearnState* L,
                                                             uint32_t* choice) {
-  extern __shared__ __align__(16) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
   mlp_eval_knots<K>(P, A, (float*)sm.Bs, sm.cdf);
   for (uint32_t j = threadIdx.x; j <= A->M; j += blockDim.x) L->cdf[j] = sm.cdf[j];

@@ -709,7 +709,7 @@ struct SetupSmem {
 template <typename K>
 __global__ __launch_bounds__(SETUP_NT) void setup_sampled(const K* __restrict__ sorted, uint32_t S,
                                                          uint32_t B, Assigner<K>* A, Grid<K>* G) {
-  extern __shared__ __align__(16) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem[];
   SetupSmem<K>& sm = *reinterpret_cast<SetupSmem<K>*>(smem);
   __shared__ uint32_t q[17];
   __shared__ float cdf[17];

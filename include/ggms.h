@@ -88,7 +88,10 @@ typedef struct ggms_opts {
   int32_t ks_on_device;         /* 1: the k array is device memory */
   int32_t out_on_device;        /* 1: the output array is device memory */
   int32_t pass_threads;         /* CTA size of the two passes: 256, 512 or 1024; 0 = tuned default */
-  int32_t pass_unroll;          /* 16-byte loads in flight per thread: 2, 4 or 8; 0 = tuned default */
+  int32_t pass_unroll;          /* how the passes stream the input: 2, 4 or 8 16-byte loads in flight
+                                   per thread (registers), or -1 = 16 KB chunks staged by bulk copies
+                                   (TMA) in a ring of shared-memory stages (pass_threads 1024 only);
+                                   0 = the default (-1) */
   float window_z;               /* PASS 1 windows: safety margin of the predicted k positions in
                                    binomial standard deviations; 0 = 8; < 0 = no windows */
   int32_t autotune;             /* 1: when num_buckets and the pass shape are left at 0, the first call of a
