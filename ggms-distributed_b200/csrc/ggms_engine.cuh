@@ -36,6 +36,7 @@ struct Workspace {
   Windows<K>* win;        // PASS 1 windows
   uint32_t* hist0;
   uint32_t* aflag0;
+  uint32_t* kcnt0;        // per level-0 bucket: ks it holds (right after aflag0: one memset clears both)
   uint32_t* cmap0;
   uint32_t* crow;         // per-CTA bucket counts of PASS 1 -> per-CTA cursors of PASS 2
   uint32_t* ic;           // coarse mode: inclusive counts of the NGRP groups
@@ -76,7 +77,7 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
   size_t o_learn = b.take(sizeof(LearnState));
   size_t o_win = b.take(sizeof(Windows<K>));
   size_t o_h0 = b.take(4ull * p.B);
-  size_t o_a0 = b.take(4ull * (p.B / 32));
+  size_t o_a0 = b.take(4ull * (p.B / 32) + 4ull * p.B);
   size_t o_c0 = b.take(4ull * p.B);
   size_t o_crow = b.take(4ull * p.B * (p.ncta ? p.ncta : 1));
   size_t o_ic = b.take(4ull * NGRP);
@@ -116,6 +117,7 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
   w.win = (Windows<K>*)(base + o_win);
   w.hist0 = (uint32_t*)(base + o_h0);
   w.aflag0 = (uint32_t*)(base + o_a0);
+  w.kcnt0 = w.aflag0 + p.B / 32;
   w.cmap0 = (uint32_t*)(base + o_c0);
   w.crow = (uint32_t*)(base + o_crow);
   w.ic = (uint32_t*)(base + o_ic);
@@ -141,19 +143,47 @@ static Workspace<K> layout(const Plan& p, size_t out_elem_bytes, uint8_t* base) 
 }
 
 
-template <typename F>
-static int enqueue_level(Context* c, cudaStream_t s, Counters* C, int p, F&& body) {
+// The refinement levels first..maxlev (1-based) of the single-vector path.
+// Captured into a graph, level l becomes an IF node and level l + 1 is nested
+// inside its body, so a level without segments skips every later level at
+// the cost of one conditional node.  The condition of the first level is set
+// by an earlier kernel (handle `first`, created by level_handle()); the later
+// ones by lvl_gate at the end of the enclosing level.  Run directly, the
+// levels' kernels are launched as they are (each returns at once when there
+// is no work).  body(stream, l) enqueues level l's kernels.
+static int level_handle(cudaStream_t s, cudaGraphConditionalHandle* h) {
+  *h = 0;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   GGMS_CU(cudaStreamIsCapturing(s, &cs));
-  if (cs != cudaStreamCaptureStatusActive) return body(s);
+  if (cs != cudaStreamCaptureStatusActive) return GGMS_OK;
+  cudaGraph_t g = nullptr;
+  GGMS_CU(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, nullptr, nullptr));
+  GGMS_CU(cudaGraphConditionalHandleCreate(h, g, 0u, cudaGraphCondAssignDefault));
+  return GGMS_OK;
+}
+
+template <typename F>
+static int enqueue_levels(Context* c, cudaStream_t s, Counters* C, int l, int maxlev,
+                          cudaGraphConditionalHandle first, F&& body) {
+  if (l > maxlev) return GGMS_OK;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  GGMS_CU(cudaStreamIsCapturing(s, &cs));
+  if (cs != cudaStreamCaptureStatusActive) {
+    const int rc = body(s, l);
+    if (rc) return rc;
+    return enqueue_levels(c, s, C, l + 1, maxlev, 0, body);
+  }
+  if (l > Context::MAX_NEST) return GGMS_E_INTERNAL;
   cudaGraph_t g = nullptr;
   const cudaGraphNode_t* deps = nullptr;
   size_t nd = 0;
-  GGMS_CU(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
-  cudaGraphConditionalHandle h;
-  GGMS_CU(cudaGraphConditionalHandleCreate(&h, g, 0u, cudaGraphCondAssignDefault));
-  ++c->launches;
-  lvl_gate<<<1, 1, 0, s>>>(C, p, h);
+  cudaGraphConditionalHandle h = first;
+  if (!h) {
+    GGMS_CU(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+    GGMS_CU(cudaGraphConditionalHandleCreate(&h, g, 0u, cudaGraphCondAssignDefault));
+    ++c->launches;
+    lvl_gate<<<1, 1, 0, s>>>(C, l & 1, h);
+  }
   GGMS_CU(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
   cudaGraphNodeParams np = {};
   np.type = cudaGraphNodeTypeConditional;
@@ -162,12 +192,14 @@ static int enqueue_level(Context* c, cudaStream_t s, Counters* C, int p, F&& bod
   np.conditional.size = 1;
   cudaGraphNode_t cn;
   GGMS_CU(cudaGraphAddNode(&cn, g, deps, nd, &np));
-  if (!c->body) GGMS_CU(cudaStreamCreateWithFlags(&c->body, cudaStreamNonBlocking));
-  GGMS_CU(cudaStreamBeginCaptureToGraph(c->body, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+  cudaStream_t& bs = c->bodies[l - 1];
+  if (!bs) GGMS_CU(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking));
+  GGMS_CU(cudaStreamBeginCaptureToGraph(bs, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                         cudaStreamCaptureModeThreadLocal));
-  const int rc = body(c->body);
+  int rc = body(bs, l);
+  if (!rc) rc = enqueue_levels(c, bs, C, l + 1, maxlev, 0, body);
   cudaGraph_t out = nullptr;
-  const cudaError_t e = cudaStreamEndCapture(c->body, &out);
+  const cudaError_t e = cudaStreamEndCapture(bs, &out);
   if (rc) return rc;
   GGMS_CU(e);
   GGMS_CU(cudaStreamUpdateCaptureDependencies(s, &cn, 1, cudaStreamSetCaptureDependencies));
@@ -182,33 +214,33 @@ constexpr int MAX_LEVELS_64 = 6;
 template <typename T>
 static size_t l0_count_smem(uint32_t B, int nt, int unroll, uint32_t nst) {
   const size_t base = GRID_SMEM + (size_t)B * 4u + wq_bytes((uint32_t)nt, sizeof(typename KeyOf<T>::K));
-  return unroll < 0 ? ((base + 127) & ~(size_t)127) + ring_bytes(0, nst) : base;
+  return unroll < 0 ? ((base + 127) & ~(size_t)127) + ring_bytes(unroll, nst) : base;
 }
 template <typename T>
 static size_t l0_coarse_smem(int nt, int unroll, uint32_t nst) {
   const size_t ch = (size_t)nt * coarse_du(unroll < 0 ? 0 : unroll) * (16 / sizeof(T));
   const size_t base = GRID_SMEM + ch * (sizeof(typename KeyOf<T>::K) + 1);
-  return unroll < 0 ? ((base + 127) & ~(size_t)127) + ring_bytes(0, nst) : base;
+  return unroll < 0 ? ((base + 127) & ~(size_t)127) + ring_bytes(unroll, nst) : base;
 }
 template <typename T>
 static size_t l0_compact_smem(uint32_t B, int nt, int unroll, uint32_t nst) {
   const size_t base = GRID_SMEM +
                       (MAX_B0 / 32 + l0_compact_qwords((uint32_t)nt, sizeof(typename KeyOf<T>::K)) + HOT_WORDS) * 4u +
                       (size_t)B * 4u;
-  return unroll < 0 ? ((base + 127) & ~(size_t)127) + ring_bytes(0, nst) : base;
+  return unroll < 0 ? ((base + 127) & ~(size_t)127) + ring_bytes(unroll, nst) : base;
 }
 
 // Launch shapes of the two passes: CTA size x 16-byte loads in flight per
-// thread (unroll 2, 4 or 8, register streams), or unroll -1: the TMA ring
-// (bulk copies into shared-memory stages); the default and the autotuner pick
-// among these instantiations.
+// thread (unroll 2, 4 or 8, register streams), unroll -1: the TMA ring (bulk
+// copies into shared-memory stages), unroll -2: per-thread async copies into
+// shared memory; the default and the autotuner pick among these instantiations.
 template <typename T>
 struct PassVariant {
   using K = typename KeyOf<T>::K;
   int nt, unroll;
   void (*count)(const T*, uint64_t, const Grid<K>*, Counters*, const Windows<K>*, uint32_t*, uint32_t*, uint32_t);
   void (*compact)(const T*, uint64_t, const Grid<K>*, Counters*, const Windows<K>*, const uint32_t*,
-                  const uint32_t*, K*, uint64_t, uint32_t);
+                  const uint32_t*, K*, uint64_t, uint32_t, const uint32_t*);
   void (*coarse)(const T*, uint64_t, const Grid<K>*, Counters*, const uint32_t*, const uint32_t*, K*, uint64_t,
                  uint32_t);
 };
@@ -223,7 +255,8 @@ static const PassVariant<T>* pass_variant(int nt, int unroll) {
       {512, 8, l0_count<T, 512, 8>, l0_compact<T, 512, 8>, l0_compact_coarse<T, 512, 8>},
       {1024, 2, l0_count<T, 1024, 2>, l0_compact<T, 1024, 2>, l0_compact_coarse<T, 1024, 2>},
       {1024, 4, l0_count<T, 1024, 4>, l0_compact<T, 1024, 4>, l0_compact_coarse<T, 1024, 4>},
-      {1024, -1, l0_count<T, 1024, 0>, l0_compact<T, 1024, 0>, l0_compact_coarse<T, 1024, 0>},
+      {1024, -1, l0_count<T, 1024, -1>, l0_compact<T, 1024, -1>, l0_compact_coarse<T, 1024, -1>},
+      {1024, -2, l0_count<T, 1024, -2>, l0_compact<T, 1024, -2>, l0_compact_coarse<T, 1024, -2>},
   };
   for (const auto& x : v)
     if (x.nt == nt && x.unroll == unroll) return &x;
@@ -231,31 +264,39 @@ static const PassVariant<T>* pass_variant(int nt, int unroll) {
 }
 
 constexpr int DEFAULT_PASS_NT = 1024;
-constexpr int DEFAULT_PASS_UNROLL = -1;  // the TMA ring
+constexpr int DEFAULT_PASS_UNROLL = 4;  // register streams (the staged ones measure no faster here)
 
-// Stages of the TMA ring: as many 16 KB stages (2..6) as fit in the shared
-// memory a CTA may use next to the larger of the three pass kernels' other
-// needs (static shared memory included, with margin).
-template <typename T>
-static uint32_t ring_stages(Context* c, uint32_t B, int nt) {
+// Stages of the TMA ring of one pass kernel whose other shared memory is
+// `base` bytes: as many 32 KB stages (2..4) as fit next to it in what a CTA
+// may use (its static shared memory included, with margin).
+static uint32_t ring_stages(Context* c, size_t base) {
   int optin = 0;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device) != cudaSuccess)
     optin = 227 * 1024;
-  const size_t base = std::max(std::max(l0_count_smem<T>(B, nt, 0, 0), l0_compact_smem<T>(B, nt, 0, 0)),
-                               l0_coarse_smem<T>(nt, 0, 0));
   const size_t margin = 8192 + 128;  // static shared memory of the pass kernels, alignment
   const size_t room = (size_t)optin > base + margin ? (size_t)optin - base - margin : 0;
-  return (uint32_t)std::min<size_t>(6, std::max<size_t>(2, room / RING_BYTES));
+  return (uint32_t)std::min<size_t>(4, std::max<size_t>(2, room / RING_BYTES));
+}
+
+// Stages of the three pass kernels' rings: [0] count, [1] compact, [2] coarse
+// (0 for the other streams).
+template <typename T>
+static void pass_stages(Context* c, const PassVariant<T>* pv, uint32_t B, uint32_t* st) {
+  for (int i = 0; i < 3; ++i) st[i] = 0u;
+  if (pv->unroll != -1) return;
+  st[0] = ring_stages(c, l0_count_smem<T>(B, pv->nt, -1, 0));
+  st[1] = ring_stages(c, l0_compact_smem<T>(B, pv->nt, -1, 0));
+  st[2] = ring_stages(c, l0_coarse_smem<T>(pv->nt, -1, 0));
 }
 
 // The two passes must split the input among CTAs identically (PASS 2 writes
 // into per-CTA ranges sized by PASS 1), so both get the same grid: as many
 // CTAs as fit on every SM at once for the larger of the two.
 template <typename T>
-static int l0_ncta(Context* c, const PassVariant<T>* pv, uint32_t B, uint32_t nst, uint32_t* ncta) {
-  const size_t s1 = l0_count_smem<T>(B, pv->nt, pv->unroll, nst);
-  const size_t s2 = l0_compact_smem<T>(B, pv->nt, pv->unroll, nst);
-  const size_t s3 = l0_coarse_smem<T>(pv->nt, pv->unroll, nst);
+static int l0_ncta(Context* c, const PassVariant<T>* pv, uint32_t B, const uint32_t* nst, uint32_t* ncta) {
+  const size_t s1 = l0_count_smem<T>(B, pv->nt, pv->unroll, nst[0]);
+  const size_t s2 = l0_compact_smem<T>(B, pv->nt, pv->unroll, nst[1]);
+  const size_t s3 = l0_coarse_smem<T>(pv->nt, pv->unroll, nst[2]);
   GGMS_CU(cudaFuncSetAttribute((const void*)pv->count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
   GGMS_CU(cudaFuncSetAttribute((const void*)pv->compact, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
   GGMS_CU(cudaFuncSetAttribute((const void*)pv->coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s3));
@@ -267,10 +308,15 @@ static int l0_ncta(Context* c, const PassVariant<T>* pv, uint32_t B, uint32_t ns
   return GGMS_OK;
 }
 
+// Up to this many ks, the steps between the passes run in one CTA (l0_between).
+constexpr uint32_t L0_FUSED_MAX_KS = 65536;
+
 template <typename K>
 static int setup_attrs() {
   static bool done = false;
   if (done) return GGMS_OK;
+  GGMS_CU(cudaFuncSetAttribute(l0_between<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)l0_between_smem(MAX_B0)));
   GGMS_CU(cudaFuncSetAttribute(l0_scan<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)(4u * MAX_B0)));
   GGMS_CU(cudaFuncSetAttribute(setup_sampled<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -294,15 +340,22 @@ static int launch_small_select(Context* ctx, const InT* src, const Seg<K>* segs_
                                  (int)sm));
     attr = true;
   }
+  // the warp finisher (its own list of segments) runs on the side stream,
+  // next to the CTA finisher
+  if (caps.tiny_keys) {
+    if (const int r_ = ensure_side(ctx)) return r_;
+    GGMS_CU(cudaEventRecord(ctx->fork2, st));
+    GGMS_CU(cudaStreamWaitEvent(ctx->side, ctx->fork2, 0));
+    ++ctx->launches;
+    tiny_select<InT, TS_NT><<<ctx->sms * 8, TS_NT, 0, ctx->side>>>(src, segs_q, w.tinies, w.C, khead_q, w.knext,
+                                                                   k_off, w.krank, w.kseg, w.kkey, caps);
+    GGMS_CU(cudaEventRecord(ctx->join2, ctx->side));
+  }
   ++ctx->launches;
   small_select<InT, SS_NT><<<ctx->sms * 2, SS_NT, sm, st>>>(src, segs_q, w.smalls, w.C, khead_q, w.knext,
                                                             k_off, w.krank, w.kseg, w.kkey, caps.small_keys,
                                                             caps);
-  if (caps.tiny_keys) {
-    ++ctx->launches;
-    tiny_select<InT, TS_NT><<<ctx->sms * 8, TS_NT, 0, st>>>(src, segs_q, w.tinies, w.C, khead_q, w.knext,
-                                                            k_off, w.krank, w.kseg, w.kkey, caps);
-  }
+  if (caps.tiny_keys) GGMS_CU(cudaStreamWaitEvent(st, ctx->join2, 0));
   return GGMS_OK;
 }
 
@@ -332,7 +385,7 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
   const PassVariant<T>* pv = pass_variant<T>(o.pass_threads ? o.pass_threads : DEFAULT_PASS_NT,
                                               o.pass_unroll ? o.pass_unroll : DEFAULT_PASS_UNROLL);
   if (!pv) return GGMS_E_INVALID_ARG;
-  p.ring_st = pv->unroll < 0 ? ring_stages<T>(ctx, p.B, pv->nt) : 0u;
+  pass_stages<T>(ctx, pv, p.B, p.ring_st);
   rc = l0_ncta<T>(ctx, pv, p.B, p.ring_st, &p.ncta);
   if (rc) return rc;
   Workspace<K> w0 = layout<K>(p, sizeof(T), nullptr);
@@ -404,9 +457,7 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     } else {
       // the sampled grid (fallback and judge) is built on a side stream while
       // the learned model's knots and statistics are computed: fork and join
-      if (!ctx->side) GGMS_CU(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
-      if (!ctx->fork) GGMS_CU(cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming));
-      if (!ctx->join) GGMS_CU(cudaEventCreateWithFlags(&ctx->join, cudaEventDisableTiming));
+      if (const int r_ = ensure_side(ctx)) return r_;
       GGMS_CU(cudaEventRecord(ctx->fork, s));
       GGMS_CU(cudaStreamWaitEvent(ctx->side, ctx->fork, 0));
       ++ctx->launches;
@@ -432,51 +483,68 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     // ---- PASS 1: count
     const int grid_c = (int)p.ncta;
     GGMS_CU(cudaMemsetAsync(w.hist0, 0, 4ull * p.B, s));
-    GGMS_CU(cudaMemsetAsync(w.aflag0, 0, 4ull * (p.B / 32), s));
+    GGMS_CU(cudaMemsetAsync(w.aflag0, 0, 4ull * (p.B / 32) + 4ull * p.B, s));  // flags and k counts
     prof_rec(prof, 1, s);
     ++ctx->launches;
-    pv->count<<<grid_c, pv->nt, l0_count_smem<T>(p.B, pv->nt, pv->unroll, p.ring_st), s>>>(
-        d_in, n, w.grid, w.C, w.win, w.hist0, w.crow, p.ring_st);
+    pv->count<<<grid_c, pv->nt, l0_count_smem<T>(p.B, pv->nt, pv->unroll, p.ring_st[0]), s>>>(
+        d_in, n, w.grid, w.C, w.win, w.hist0, w.crow, p.ring_st[0]);
     prof_rec(prof, 2, s);
-    ++ctx->launches;
-    l0_scan<K><<<1, 1024, 4u * p.B, s>>>(w.hist0, p.B, w.C, w.win, w.aflagc);
-    ++ctx->launches;
-    lvl_locate_rows<<<cdiv(nk, 256), 256, 0, s>>>(w.hist0, p.B, nk, w.krank, w.kseg, w.kbin,
-                                                     w.aflag0, p.B / 32, w.C);
-    // most buckets hold a k: copy groups of buckets instead (coarse mode)
-    ++ctx->launches;
-    l0_mode_ks<K><<<cdiv(nk, 256), 256, 0, s>>>(w.hist0, w.aflag0, p.B, w.win, w.C, w.ic, w.aflagc, nk, w.krank,
-                                                 w.kseg, w.kbin);
+    if (nk <= L0_FUSED_MAX_KS) {
+      // scan, locate and the coarse-mode decision in one CTA
+      ++ctx->launches;
+      l0_between<K><<<1, 1024, l0_between_smem(p.B), s>>>(w.hist0, p.B, w.C, w.win, nk, w.krank, w.kseg, w.kbin,
+                                                           w.kcnt0, w.aflag0, w.ic, w.aflagc);
+    } else {
+      ++ctx->launches;
+      l0_scan<K><<<1, 1024, 4u * p.B, s>>>(w.hist0, p.B, w.C, w.win, w.aflagc);
+      ++ctx->launches;
+      lvl_locate_rows<<<cdiv(nk, 256), 256, 0, s>>>(w.hist0, p.B, nk, w.krank, w.kseg, w.kbin,
+                                                       w.aflag0, p.B / 32, w.C, w.kcnt0);
+      // most buckets hold a k: copy groups of buckets instead (coarse mode)
+      ++ctx->launches;
+      l0_mode_ks<K><<<cdiv(nk, 256), 256, 0, s>>>(w.hist0, w.aflag0, p.B, w.win, w.C, w.ic, w.aflagc, nk, w.krank,
+                                                   w.kseg, w.kbin);
+    }
     ++ctx->launches;
     l0_children<K><<<cdiv(p.B, 256), 256, 0, s>>>(w.hist0, w.aflag0, p.B, w.grid, w.C, w.win, w.cmap0,
                                                      w.segs[1], w.cursor[1], w.tiles[1], w.points,
-                                                     w.khead[1], w.smalls, w.bigs[1], caps, w.ic, w.aflagc);
+                                                     w.khead[1], w.smalls, w.bigs[1], caps, w.ic, w.aflagc,
+                                                     w.kcnt0, tiny_keys<K>(), w.tinies);
+    // the first refinement level runs only when a level-0 child needs it: the
+    // kernel that relabels the ks after l0_children sets that condition
+    cudaGraphConditionalHandle lev1 = 0;
+    rc = level_handle(s, &lev1);
+    if (rc) return rc;
     ++ctx->launches;
-    lvl_relabel<K><<<cdiv(nk, 256), 256, 0, s>>>(w.cmap0, p.B, nk, w.kbin, w.kseg, w.kkey,
-                                                    w.points, w.C, w.segs[1], w.khead[1], w.knext);
-    ++ctx->launches;
-    l0_bases<K><<<ctx->sms * 4, 256, 0, s>>>(w.crow, p.B, p.ncta, w.segs[1], w.C, caps);
+    l0_relabel_bases<K><<<ctx->sms * 4, 256, 0, s>>>(w.cmap0, nk, w.kbin, w.kseg, w.kkey, w.points, w.C,
+                                                      w.segs[1], w.khead[1], w.knext, w.crow, p.B, p.ncta,
+                                                      caps, lev1);
     // ---- PASS 2: compact the buckets that still need refinement
     prof_rec(prof, 3, s);
     ++ctx->launches;
-    pv->compact<<<grid_c, pv->nt, l0_compact_smem<T>(p.B, pv->nt, pv->unroll, p.ring_st), s>>>(
-        d_in, n, w.grid, w.C, w.win, w.cmap0, w.crow, w.cand[0], (uint64_t)n, p.ring_st);
+    pv->compact<<<grid_c, pv->nt, l0_compact_smem<T>(p.B, pv->nt, pv->unroll, p.ring_st[1]), s>>>(
+        d_in, n, w.grid, w.C, w.win, w.cmap0, w.crow, w.cand[0], (uint64_t)n, p.ring_st[1], w.hist0);
     ++ctx->launches;  // one of the two PASS-2 kernels returns at once
-    pv->coarse<<<grid_c, pv->nt, l0_coarse_smem<T>(pv->nt, pv->unroll, p.ring_st), s>>>(
-        d_in, n, w.grid, w.C, w.cmap0, w.crow, w.cand[0], (uint64_t)n, p.ring_st);
+    pv->coarse<<<grid_c, pv->nt, l0_coarse_smem<T>(pv->nt, pv->unroll, p.ring_st[2]), s>>>(
+        d_in, n, w.grid, w.C, w.cmap0, w.crow, w.cand[0], (uint64_t)n, p.ring_st[2]);
     prof_rec(prof, 4, s);
-    rc = launch_small_select<K>(ctx, w.cand[0], w.segs[1], w.khead[1], w, caps, s);
+    {
+      // level 0 also has warp-sized children (l0_children); the refinement
+      // levels of this path do not
+      Caps c0 = caps;
+      c0.tiny_keys = tiny_keys<K>();
+      rc = launch_small_select<K>(ctx, w.cand[0], w.segs[1], w.khead[1], w, c0, s);
+    }
     if (rc) return rc;
 
     // ---- refinement levels over candidates
     const int maxlev = (sizeof(K) == 4) ? MAX_LEVELS_32 : MAX_LEVELS_64;
     const int lv_grid = ctx->sms * 8;
     const int seg_grid = std::min<int>((int)p.cap_seg, ctx->sms * 2);
-    for (int l = 1; l <= maxlev; ++l) {
+    rc = enqueue_levels(ctx, s, w.C, 1, maxlev, lev1, [&](cudaStream_t s, int l) -> int {
       const int pp = l & 1, q = pp ^ 1;
       const K* src = w.cand[(l - 1) & 1];
       K* dst = w.cand[l & 1];
-      rc = enqueue_level(ctx, s, w.C, pp, [&](cudaStream_t s) -> int {
       ++ctx->launches;
       lvl_prep<<<ctx->sms * 2, 256, 0, s>>>(w.rows[pp], w.aflag[pp], w.bigs[pp], w.C, pp, caps);
       ++ctx->launches;
@@ -503,9 +571,8 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
         return launch_small_select<K>(ctx, dst, w.segs[q], w.khead[q], w, caps, s);
       }
       return GGMS_OK;
-      });
-      if (rc) return rc;
-    }
+    });
+    if (rc) return rc;
 
     // ---- answers
     prof_rec(prof, 8, s);
@@ -590,7 +657,7 @@ static int run_single_tuned(Context* c, const T* d_in, uint64_t n, const uint32_
     return run_single<T>(c, d_in, n, ks, nk, out, b, st, topk);
   }
   static const int Bs[] = {4096, 8192, 16384};
-  static const int shapes[][2] = {{1024, -1}, {1024, 4}, {512, 4}, {512, 8}};
+  static const int shapes[][2] = {{1024, 4}, {1024, -2}, {512, 4}, {512, 8}};
   float best = 3.4e38f;
   Context::Tuned pick{{key[0], key[1], key[2], key[3]}, 8192, DEFAULT_PASS_NT, DEFAULT_PASS_UNROLL, 8};
   for (int B : Bs) {

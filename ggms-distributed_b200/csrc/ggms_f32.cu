@@ -37,4 +37,10 @@ int ggms_multiselect_segmented_f32(ggms_context* ctx, const float* d_in, const i
   return segmented<float>(ctx, d_in, seg_off, nseg, ks, k_off, out, opts, stream);
 }
 
+#ifdef GGMS_SETUP_TRACE
+GGMS_API int ggms_trace_read_f32(unsigned long long* out) {
+  return cudaMemcpyFromSymbol(out, ggms_trace_buf, sizeof(ggms_trace_buf)) == cudaSuccess ? 0 : 4;
+}
+#endif
+
 }  // extern "C"

@@ -53,9 +53,10 @@ struct Context {
   uint64_t clock = 0;
   cudaStream_t capture = nullptr;  // private stream the graphs are captured on
   cudaEvent_t pin_busy = nullptr;  // recorded after the last call's uploads from the pinned buffer
-  cudaStream_t body = nullptr;     // private stream the conditional level bodies are captured on
-  cudaStream_t side = nullptr;     // the sampled assigner's build, next to the learned one
-  cudaEvent_t fork = nullptr, join = nullptr;
+  static constexpr int MAX_NEST = 8;
+  cudaStream_t bodies[MAX_NEST] = {};  // private streams the nested level bodies are captured on
+  cudaStream_t side = nullptr;     // the sampled assigner's build next to the learned one; the warp finisher
+  cudaEvent_t fork = nullptr, join = nullptr, fork2 = nullptr, join2 = nullptr;
   // autotuner: launch shapes and bucket counts picked per shape class
   struct Tuned {
     uint64_t key[4];
@@ -135,12 +136,21 @@ static void destroy_context(Context* c) {
     if (g.exec) cudaGraphExecDestroy(g.exec);
   if (c->capture) cudaStreamDestroy(c->capture);
   if (c->pin_busy) cudaEventDestroy(c->pin_busy);
-  if (c->body) cudaStreamDestroy(c->body);
+  for (auto& b : c->bodies)
+    if (b) cudaStreamDestroy(b);
   if (c->side) cudaStreamDestroy(c->side);
-  if (c->fork) cudaEventDestroy(c->fork);
-  if (c->join) cudaEventDestroy(c->join);
+  for (cudaEvent_t e : {c->fork, c->join, c->fork2, c->join2})
+    if (e) cudaEventDestroy(e);
   cudaSetDevice(prev);
   delete c;
+}
+
+// The side stream and its fork / join events (created on first use).
+static int ensure_side(Context* c) {
+  if (!c->side) GGMS_CU(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+  for (cudaEvent_t* e : {&c->fork, &c->join, &c->fork2, &c->join2})
+    if (!*e) GGMS_CU(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  return GGMS_OK;
 }
 
 // default contexts of the drop-in entry points, one per device
@@ -186,7 +196,7 @@ struct Plan {
   uint64_t seed;
   uint32_t cap_q;    // batched path: caller segments with quantile bins (0: single path)
   uint32_t pl_knots; // learned PL model: requested segments (0: the default)
-  uint32_t ring_st;  // stages of the passes' TMA ring (0: register streams)
+  uint32_t ring_st[3];  // stages of the passes' TMA rings: count, compact, coarse (0: other streams)
 };
 
 
@@ -224,7 +234,7 @@ static int make_plan(Plan* p, uint64_t n, uint32_t nk, const ggms_opts& o) {
   p->cap_q = 0;
   if (o.pl_knots != 0 && (o.pl_knots < 16 || o.pl_knots > 1024)) return GGMS_E_INVALID_ARG;
   p->pl_knots = (uint32_t)o.pl_knots;
-  p->ring_st = 0;
+  p->ring_st[0] = p->ring_st[1] = p->ring_st[2] = 0;
   return GGMS_OK;
 }
 
@@ -317,11 +327,7 @@ static int run_graphed(Context* c, const uint64_t* key, int nkey, cudaStream_t s
   return GGMS_OK;
 }
 
-// One refinement level.  Captured into a graph, it becomes an IF node whose
-// condition lvl_gate sets on the device: once a level finds no segment, it
-// and every later level cost nothing.  Run directly, the level's kernels are
-// launched as they are (each returns at once when there is no work).
-
+// Profiling slot of the current call (or null when profiling is off).
 static cudaEvent_t* prof_slot(Context* c) {
   if (!c->profile) return nullptr;
   if (c->ring_count == Context::RING) return nullptr;  // ring full: drop

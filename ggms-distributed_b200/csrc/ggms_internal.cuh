@@ -24,6 +24,26 @@
 #define GGMS_BEGIN namespace ggms { inline namespace GGMS_TU {
 #define GGMS_END } }
 
+// Set-up tracing for development builds only (-DGGMS_SETUP_TRACE): thread 0
+// of block 0 stores %globaltimer at numbered points of the kernels into this
+// unit's ggms_trace_buf (ggms_f32.cu exports a reader in such builds).
+// Compiled out otherwise.
+#ifdef GGMS_SETUP_TRACE
+static __device__ unsigned long long ggms_trace_buf[64];
+#define GGMS_TRACE(i)                                                  \
+  do {                                                                 \
+    if (threadIdx.x == 0 && blockIdx.x == 0) {                         \
+      unsigned long long t_;                                           \
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_));           \
+      ggms_trace_buf[(i)] = t_;                                        \
+    }                                                                  \
+  } while (0)
+#else
+#define GGMS_TRACE(i) \
+  do {                \
+  } while (0)
+#endif
+
 namespace ggms {
 
 // ------------------------------------------------------------------ key traits

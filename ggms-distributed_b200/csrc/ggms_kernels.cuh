@@ -130,6 +130,7 @@ __device__ void block_inclusive_scan_global(uint32_t* data, uint32_t cnt, uint32
 // wrappers compute length - k + 1, 1-based smallest: bucketMultiselect.cu:860-861).
 __global__ void k_init_single(const uint32_t* __restrict__ ks, uint32_t nk, uint64_t n,
                               uint32_t* k_rank, uint32_t* k_seg, Counters* C) {
+  GGMS_TRACE(0);
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nk) return;
   uint32_t k = ks[i];
@@ -238,6 +239,7 @@ asg_sample_sort_cluster(const T* __restrict__ in, uint64_t n, uint32_t S, uint64
   // warp w owns positions [w * 32 * kpt, (w + 1) * 32 * kpt) of this CTA's
   // share; in round r its lane l holds position w * 32 * kpt + r * 32 + l
   const uint32_t wbase = warp * 32u * kpt;
+  GGMS_TRACE(1);
   K* A = sm.a;
   K* Bv = sm.b;
   for (uint32_t r = 0; r < kpt; ++r) {
@@ -323,6 +325,7 @@ asg_sample_sort_cluster(const T* __restrict__ in, uint64_t n, uint32_t S, uint64
   }
   K* out = sorted + (size_t)me * per;
   for (uint32_t i = tid; i < per; i += CS_NT) out[i] = A[i];
+  GGMS_TRACE(2);
 }
 
 template <typename K>
@@ -422,23 +425,31 @@ struct RunTest {
 // ------------------------------------------------------------------ input streams of the passes
 // The body of the input (16-byte vectors from its first 16-byte boundary) is
 // split between the CTAs the same way in PASS 1 and PASS 2, so that PASS 2's
-// per-CTA write ranges (sized by PASS 1) fit.  Two ways to stream it:
+// per-CTA write ranges (sized by PASS 1) fit.  Three ways to stream it (the
+// template parameter UNROLL of the pass kernels):
 //   UNROLL > 0:  grid-strided rounds of UNROLL non-allocating vector loads per
 //                thread, into registers;
-//   UNROLL == 0: chunks of RING_VECS vectors (16 KB) dealt round-robin to the
-//                CTAs and staged in a ring of shared-memory stages: thread 0
-//                fills a stage with one bulk copy (cp.async.bulk, the TMA
-//                engine) that completes on the stage's "full" mbarrier; every
-//                thread reads its V vectors back and each warp then arrives on
-//                the stage's "empty" mbarrier, after which thread 0 refills it.
-//                Several chunks stay in flight per SM all the time, with no
-//                registers held for them.
-// Every thread of a CTA handles the same number of vectors either way, so the
-// warps stay converged.  The vectors past the main loop (main_end .. nvec) are
-// left to the caller, one per thread, grid-strided.
-constexpr uint32_t RING_BYTES = 16384;
+//   UNROLL == -1 (TMA ring): chunks of RING_VECS vectors (32 KB) dealt
+//                round-robin to the CTAs and staged in a ring of shared-memory
+//                stages: thread 0 fills a stage with one bulk copy
+//                (cp.async.bulk, the TMA engine) that completes on the stage's
+//                "full" mbarrier; every thread reads its V vectors back and
+//                each warp then arrives on the stage's "empty" mbarrier.
+//                Thread 0 refills every released stage as it passes by and
+//                blocks only when the chunk it needs itself is not issued yet;
+//   UNROLL == -2 (async copies): chunks of 1024 vectors (16 KB) dealt
+//                round-robin to the CTAs; every thread copies its own vectors
+//                of the next ASYNC_D - 1 chunks into its private shared-memory
+//                slots with cp.async and waits only for its own oldest group:
+//                no barrier between threads at all.
+// Every thread of a CTA handles the same number of vectors in all three, so
+// the warps stay converged.  The vectors past the main part (main_end ..
+// nvec) are left to the caller, one per thread, grid-strided.
+constexpr uint32_t RING_BYTES = 32768;
 constexpr uint32_t RING_VECS = RING_BYTES / 16;
 constexpr uint32_t RING_MAX_ST = 8;
+constexpr uint32_t ASYNC_VECS = 1024;   // vectors of one async-copy chunk (16 KB)
+constexpr int ASYNC_D = 4;              // async-copy chunks per thread in shared memory
 
 struct RingBars {
   unsigned long long full[RING_MAX_ST];
@@ -466,6 +477,16 @@ __device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
       : "memory");
   return ok != 0u;
 }
+// Non-blocking test of the same.
+__device__ __forceinline__ bool mbar_test(uint32_t a, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return ok != 0u;
+}
 // Waits until the phase of parity `parity` of barrier `a` has completed; gives
 // up (false) after about a second, so that a broken pipeline cannot hang the GPU.
 __device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity) {
@@ -482,6 +503,13 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
                "l"(src), "r"(bytes), "r"(bar)
                : "memory");
 }
+// One 16-byte asynchronous copy global -> shared (L2 only), in the thread's current group.
+__device__ __forceinline__ void async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // The TMA ring of one CTA.  All threads call start() and next(); next() is
 // CTA-uniform (every thread sees the same chunk count).
@@ -529,23 +557,29 @@ struct Ring {
   // none left, or (warp-uniformly) after a wait gave up.
   __device__ __forceinline__ bool next(uint4 (&q)[V]) {
     if (j >= nmine || !ok) return false;
+    bool good = true;
+    if (threadIdx.x == 0) {
+      // refill every stage the warps have released (without waiting), and
+      // block only when the chunk needed now has not been issued
+      while (issued < nmine) {
+        const uint32_t jp = issued - nst;  // the chunk the stage held before
+        if (issued > j && !mbar_test(empty(jp % nst), (jp / nst) & 1u)) break;
+        if (!mbar_wait(empty(jp % nst), (jp / nst) & 1u)) {
+          good = false;
+          break;
+        }
+        issue(issued);
+        ++issued;
+      }
+    }
     const uint32_t s = j % nst;
-    bool good = mbar_wait(full(s), (j / nst) & 1u);
+    if (good) good = mbar_wait(full(s), (j / nst) & 1u);
     if (__all_sync(FULL, good)) {
       const uint4* st = stage0 + (size_t)s * RING_VECS;
 #pragma unroll
       for (int v = 0; v < V; ++v) q[v] = st[threadIdx.x + v * NT];
       __syncwarp();
       if ((threadIdx.x & 31u) == 0u) mbar_arrive(empty(s));
-      if (threadIdx.x == 0 && j >= 1 && issued < nmine) {  // refill the stage chunk j - 1 used
-        const uint32_t jp = issued - nst;                    // == j - 1
-        if (mbar_wait(empty(jp % nst), (jp / nst) & 1u)) {
-          issue(issued);
-          ++issued;
-        } else {
-          good = false;
-        }
-      }
     } else {
       good = false;
     }
@@ -567,12 +601,65 @@ struct Ring {
   }
 };
 
+// The async-copy pipeline of one thread (UNROLL == -2).
+template <int NT>
+struct AsyncPipe {
+  static constexpr int V = (int)(ASYNC_VECS / NT);  // vectors per thread per chunk
+  const uint4* body;
+  uint4* slots;  // [ASYNC_D][ASYNC_VECS] vectors, this thread's at tid + v * NT
+  uint32_t nmine, j, G, b;
+  __device__ __forceinline__ void load(uint32_t jj) {
+    const uint64_t c = (uint64_t)b + (uint64_t)jj * G;
+    const uint32_t sl = jj % ASYNC_D;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const uint32_t x = threadIdx.x + v * NT;
+      async16(smem_u32(slots + (size_t)sl * ASYNC_VECS + x), body + c * ASYNC_VECS + x);
+    }
+  }
+  __device__ __forceinline__ void start(const uint4* body_, uint64_t nch, uint4* slots_) {
+    body = body_;
+    slots = slots_;
+    G = gridDim.x;
+    b = blockIdx.x;
+    nmine = nch > b ? (uint32_t)((nch - b + G - 1) / G) : 0u;
+    j = 0;
+    for (uint32_t jj = 0; jj + 1 < (uint32_t)ASYNC_D; ++jj) {
+      if (jj < nmine) load(jj);
+      async_commit();
+    }
+  }
+  __device__ __forceinline__ bool next(uint4 (&q)[V]) {
+    if (j >= nmine) {
+      async_wait<0>();
+      return false;
+    }
+    // the slot chunk j + D - 1 goes to was read in the previous call
+    if (j + ASYNC_D - 1 < nmine) load(j + ASYNC_D - 1);
+    async_commit();
+    async_wait<ASYNC_D - 1>();  // this thread's copies of chunk j have landed
+    const uint4* sl = slots + (size_t)(j % ASYNC_D) * ASYNC_VECS;
+#pragma unroll
+    for (int v = 0; v < V; ++v) q[v] = sl[threadIdx.x + v * NT];
+    ++j;
+    return true;
+  }
+};
+
+// vectors of one chunk of a staged stream
+__host__ __device__ constexpr uint32_t stream_chunk_vecs(int unroll) {
+  return unroll == -1 ? RING_VECS : ASYNC_VECS;
+}
+
 // The main loop's driver for one pass kernel: run(f) calls f(vector) for each
-// of this thread's vectors of the main part.  run() is called at most once,
-// by all threads (the kernels branch on CTA-uniform values only); the ring is
-// started inside it, so a kernel that skips the main part has no copy in flight.
+// of this thread's vectors of the main part.  run() (or next_batch()) is used
+// by all threads or none (the kernels branch on CTA-uniform values only); the
+// staging starts inside it, so a kernel that skips the main part has no copy
+// in flight.
 template <int NT, int UNROLL>
 struct PassStream {
+  static constexpr bool RING = UNROLL == -1, ASYNC = UNROLL == -2;
+  static constexpr int V = RING ? Ring<NT>::V : AsyncPipe<NT>::V;
   const uint4* body;
   uint4* ring_smem;
   RingBars* rb;
@@ -580,6 +667,7 @@ struct PassStream {
   uint32_t nst;
   bool started;
   Ring<NT> ring;
+  AsyncPipe<NT> pipe;
   __device__ __forceinline__ void start(const uint4* body_, uint64_t nvec_, uint4* ring_smem_, RingBars* rb_,
                                         uint32_t nst_) {
     body = body_;
@@ -590,13 +678,22 @@ struct PassStream {
     started = false;
     gtid = (uint64_t)blockIdx.x * NT + threadIdx.x;
     gstride = (uint64_t)gridDim.x * NT;
-    if (UNROLL > 0) {
-      rounds = nvec / (gstride * (UNROLL > 0 ? UNROLL : 1));
-      main_end = rounds * gstride * (UNROLL > 0 ? UNROLL : 1);
+    if constexpr (UNROLL > 0) {
+      rounds = nvec / (gstride * UNROLL);
+      main_end = rounds * gstride * UNROLL;
     } else {
-      nch = nvec / RING_VECS;
-      main_end = nch * RING_VECS;
+      nch = nvec / stream_chunk_vecs(UNROLL);
+      main_end = nch * stream_chunk_vecs(UNROLL);
     }
+  }
+  __device__ __forceinline__ void begin() {
+    if constexpr (RING) ring.start(body, nch, ring_smem, rb, nst);
+    if constexpr (ASYNC) pipe.start(body, nch, ring_smem);
+    started = true;
+  }
+  __device__ __forceinline__ bool next(uint4 (&q)[V]) {
+    if constexpr (RING) return ring.next(q);
+    else return pipe.next(q);
   }
   template <typename F>
   __device__ __forceinline__ void run(F&& f) {
@@ -610,41 +707,37 @@ struct PassStream {
         for (int u = 0; u < UNROLL; ++u) f(q[u]);
       }
     } else {
-      ring.start(body, nch, ring_smem, rb, nst);
-      started = true;
-      uint4 q[Ring<NT>::V];
-      while (ring.next(q)) {
+      begin();
+      uint4 q[V];
+      while (next(q)) {
 #pragma unroll
-        for (int v = 0; v < Ring<NT>::V; ++v) f(q[v]);
+        for (int v = 0; v < V; ++v) f(q[v]);
       }
     }
   }
-  // The TMA ring only: this thread's vectors of the CTA's next DU / V chunks
+  // Staged streams only: this thread's vectors of the CTA's next DU / V chunks
   // into q; returns how many it wrote (CTA-uniform; 0 at the end).
   template <int DU>
   __device__ __forceinline__ int next_batch(uint4 (&q)[DU]) {
-    constexpr int V = Ring<NT>::V;
     static_assert(DU % V == 0, "a batch holds whole chunks");
-    if (!started) {
-      ring.start(body, nch, ring_smem, rb, nst);
-      started = true;
-    }
+    if (!started) begin();
     int got = 0;
 #pragma unroll
     for (int c = 0; c < DU / V; ++c) {
       uint4 t[V];
-      if (!ring.next(t)) break;
+      if (!next(t)) break;
 #pragma unroll
       for (int v = 0; v < V; ++v) q[c * V + v] = t[v];
       got += V;
     }
     return got;
   }
-  // All threads, after the main part (a no-op when the ring never started).
+  // All threads, after the main part (a no-op when the staging never started).
   __device__ __forceinline__ void finish(Counters* C) {
-    if constexpr (UNROLL == 0) {
+    if constexpr (RING) {
       if (started) ring.finish(C);
     }
+    if constexpr (ASYNC) async_wait<0>();
   }
   // vectors of the main part this thread handles
   __device__ __forceinline__ uint64_t my_vecs() const {
@@ -652,14 +745,16 @@ struct PassStream {
       return rounds * UNROLL;
     } else {
       const uint64_t G = gridDim.x, b = blockIdx.x;
-      return (nch > b ? (nch - b + G - 1) / G : 0) * (uint64_t)Ring<NT>::V;
+      return (nch > b ? (nch - b + G - 1) / G : 0) * (uint64_t)V;
     }
   }
 };
 
-// Shared-memory bytes of a pass kernel's ring (0 for the register streams).
+// Shared-memory bytes of a pass kernel's staging (0 for the register streams;
+// nst: stages of the TMA ring).
 __host__ __device__ constexpr size_t ring_bytes(int unroll, uint32_t nst) {
-  return unroll > 0 ? 0 : (size_t)nst * RING_BYTES + 128;
+  return unroll == -1 ? (size_t)nst * RING_BYTES + 128
+                      : unroll == -2 ? (size_t)ASYNC_D * ASYNC_VECS * 16 + 128 : 0;
 }
 // The ring's place: the end of the kernel's dynamic shared memory, 128-byte aligned.
 __device__ __forceinline__ uint4* ring_at(uint8_t* smem, size_t used) {
@@ -743,6 +838,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_count(const T* __res
   uint2* s1 = (uint2*)smem;
   uint2* s2 = s1 + GRID_T1;
   uint32_t* hs = (uint32_t*)(smem + GRID_SMEM);
+  GGMS_TRACE(24);
   const GridView<K> gv = grid_to_smem<K>(G, s1, s2);
   const uint32_t B = gv.B;
   K* wq = reinterpret_cast<K*>(hs + B) + (threadIdx.x >> 5) * WQ_DEPTH;
@@ -892,6 +988,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_count(const T* __res
     row[i] = v;
     if (v) atomicAdd(&hist0[i], v);
   }
+  GGMS_TRACE(25);
 }
 
 // Inclusive scan of the level-0 counts (one CTA) + the largest bucket.  The
@@ -905,6 +1002,7 @@ __global__ __launch_bounds__(1024) void l0_scan(uint32_t* hist0, uint32_t B, Cou
   __shared__ uint32_t w[72];
   __shared__ uint32_t mx;
   __shared__ Windows<K> W;
+  GGMS_TRACE(26);
   if (threadIdx.x == 0) {
     W = *Wg;
     mx = 0;
@@ -928,59 +1026,62 @@ __global__ __launch_bounds__(1024) void l0_scan(uint32_t* hist0, uint32_t B, Cou
   block_inclusive_scan_global<1024>(sh_counts, B, w, &C->max_bucket0);
   for (uint32_t i = threadIdx.x; i < B; i += 1024) hist0[i] = sh_counts[i];
   if (on && threadIdx.x == 0) C->max_bucket0 = mx;
+  GGMS_TRACE(27);
 }
 
-// Each k finds the bucket holding its rank: the smallest b with I[b] > r.
+// Each k finds the bucket holding its rank: the smallest b with I[b] > r
+// (I: the inclusive counts of its segment's row).  Returns the bucket, or
+// K_NIL when the rank lies beyond the row (cannot happen; status set).
+__device__ __forceinline__ uint32_t locate_one(const uint32_t* I, uint32_t row_len, uint32_t& r, Counters* C) {
+  if (r >= I[row_len - 1]) {  // cannot happen: rank beyond the segment
+    set_status(C, GGMS_E_INTERNAL);
+    return K_NIL;
+  }
+  uint32_t lo = 0, hi = row_len - 1;
+  while (lo < hi) {
+    const uint32_t m = (lo + hi) >> 1;
+    if (I[m] > r) hi = m; else lo = m + 1;
+  }
+  r -= lo ? I[lo - 1] : 0u;
+  return lo;
+}
+
+// With kcnt (level 0 of one vector), the ks of each bucket are also counted.
 __global__ void lvl_locate_rows(const uint32_t* __restrict__ rows, uint32_t row_len, uint32_t nk,
                                 uint32_t* k_rank, const uint32_t* __restrict__ k_seg,
                                 uint32_t* k_bin, uint32_t* aflag, uint32_t flag_words,
-                                Counters* C) {
+                                Counters* C, uint32_t* kcnt = nullptr) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nk) return;
   const uint32_t s = k_seg[i];
   if (s == K_DONE) return;
-  const uint32_t* I = rows + (size_t)s * row_len;
-  const uint32_t r = k_rank[i];
-  if (r >= I[row_len - 1]) {  // cannot happen: rank beyond the segment
-    set_status(C, GGMS_E_INTERNAL);
-    return;
-  }
-  uint32_t lo = 0, hi = row_len - 1;
-  while (lo < hi) {
-    uint32_t m = (lo + hi) >> 1;
-    if (I[m] > r) hi = m; else lo = m + 1;
-  }
+  uint32_t r = k_rank[i];
+  const uint32_t lo = locate_one(rows + (size_t)s * row_len, row_len, r, C);
+  if (lo == K_NIL) return;
   k_bin[i] = lo;
-  k_rank[i] = r - (lo ? I[lo - 1] : 0u);
+  k_rank[i] = r;
   atomicOr(&aflag[(size_t)s * flag_words + (lo >> 5)], 1u << (lo & 31));
+  if (kcnt) atomicAdd(&kcnt[lo], 1u);
 }
 
-// Active level-0 buckets -> refinement segments (or points).  One thread per bucket.
-// In the coarse mode (C->coarse) the children are the NGRP groups of 2^gsh
-// consecutive buckets instead (counts from ic, flags from aflagc).
+// Active level-0 buckets -> refinement segments (or points).  In the coarse
+// mode (C->coarse) the children are the NGRP groups of 2^gsh consecutive
+// buckets instead (counts from ic, flags from aflagc).  A child of at most
+// tiny_keys keys that holds at most TS_SORT_ABOVE ks (kcnt0) is finished by
+// one warp (tiny_select), a larger small one by one CTA.
+constexpr uint32_t TS_SORT_ABOVE = 8;
+
+// Level-0 child of bucket (or group) b, which holds a k; I: inclusive counts of
+// the buckets (or, coarse, of the groups).
 template <typename K>
-__global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __restrict__ aflag,
-                            uint32_t B, const Grid<K>* __restrict__ Gs, Counters* C,
-                            const Windows<K>* __restrict__ Wg,
-                            uint32_t* cmap0, Seg<K>* segs1, uint32_t* cursor1, TileRef* tiles1,
-                            K* points, uint32_t* khead1, uint32_t* smalls, uint32_t* bigs1, Caps caps,
-                            const uint32_t* __restrict__ ic, const uint32_t* __restrict__ aflagc) {
-  // the key-range searches below evaluate the grid ~64 times per bucket: keep
-  // it in shared memory (every thread helps load it before any returns)
-  __shared__ uint2 s1[GRID_T1];
-  __shared__ uint2 s2[GRID_SUBCAP];
-  const GridView<K> gv = grid_to_smem<K>(Gs + C->asg_choice, s1, s2);
-  __syncthreads();
-  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool coarse = C->coarse != 0u;
-  const uint32_t gsh = coarse_shift(B);
-  if (b >= (coarse ? NGRP : B)) return;
-  if (!(((coarse ? aflagc : aflag)[b >> 5] >> (b & 31)) & 1u)) {
-    cmap0[b] = CM_NONE;
-    return;
-  }
-  const uint32_t start = b ? (coarse ? ic : I)[b - 1] : 0u;
-  const uint32_t cnt = (coarse ? ic : I)[b] - start;
+__device__ __forceinline__ void l0_child_make(uint32_t b, bool coarse, uint32_t gsh, uint32_t B,
+                                              const uint32_t* I, const GridView<K>& gv, const Windows<K>& W,
+                                              Counters* C, uint32_t* cmap0, Seg<K>* segs1, uint32_t* cursor1,
+                                              TileRef* tiles1, K* points, uint32_t* khead1, uint32_t* smalls,
+                                              uint32_t* bigs1, const Caps& caps, const uint32_t* kcnt0,
+                                              uint32_t tiny_keys, uint32_t* tinies) {
+  const uint32_t start = b ? I[b - 1] : 0u;
+  const uint32_t cnt = I[b] - start;
   // key range of bucket b: [L(b), L(b+1) - 1], L(x) = smallest key with eval >= x
   auto L = [&](uint32_t target) -> K {
     K lo = 0, hi = key_max<K>();
@@ -993,7 +1094,7 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
   // a gap bucket (windows) stands for its whole gap: up to the gap's last bucket;
   // a group, for its buckets [b << gsh, (b + 1) << gsh)
   const uint32_t b0 = coarse ? b << gsh : b;
-  const uint32_t e = coarse ? ((b + 1u) << gsh) - 1u : win_end<K>(*Wg, b);
+  const uint32_t e = coarse ? ((b + 1u) << gsh) - 1u : win_end<K>(W, b);
   const K lo = (b0 == 0) ? (K)0 : L(b0);
   const K hi = (e >= B - 1) ? key_max<K>() : (K)(L(e + 1) - 1);
   atomicAdd(&C->active0, 1u);
@@ -1021,8 +1122,9 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
   cmap0[b] = id;
   atomicAdd(&C->cand0, (unsigned long long)cnt);
   if (s.small) {
-    const uint32_t si = atomicAdd(&C->nsmall, 1u);
-    if (si < caps.segs) smalls[si] = id; else set_status(C, GGMS_E_INTERNAL);
+    const bool tiny = !coarse && cnt <= tiny_keys && kcnt0[b] <= TS_SORT_ABOVE;
+    const uint32_t si = atomicAdd(tiny ? &C->ntiny : &C->nsmall, 1u);
+    if (si < caps.segs) (tiny ? tinies : smalls)[si] = id; else set_status(C, GGMS_E_INTERNAL);
     return;
   }
   const uint32_t bi = atomicAdd(&C->nbig[1], 1u);
@@ -1033,17 +1135,41 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
   for (uint32_t t = 0; t < nt; ++t) tiles1[t0 + t] = TileRef{id, t};
 }
 
+// One thread per bucket (or group).
+template <typename K>
+__global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __restrict__ aflag,
+                            uint32_t B, const Grid<K>* __restrict__ Gs, Counters* C,
+                            const Windows<K>* __restrict__ Wg,
+                            uint32_t* cmap0, Seg<K>* segs1, uint32_t* cursor1, TileRef* tiles1,
+                            K* points, uint32_t* khead1, uint32_t* smalls, uint32_t* bigs1, Caps caps,
+                            const uint32_t* __restrict__ ic, const uint32_t* __restrict__ aflagc,
+                            const uint32_t* __restrict__ kcnt0, uint32_t tiny_keys, uint32_t* tinies) {
+  // the key-range searches evaluate the grid ~64 times per bucket: keep it in
+  // shared memory (every thread helps load it before any returns)
+  __shared__ uint2 s1[GRID_T1];
+  __shared__ uint2 s2[GRID_SUBCAP];
+  GGMS_TRACE(28);
+  const GridView<K> gv = grid_to_smem<K>(Gs + C->asg_choice, s1, s2);
+  __syncthreads();
+  GGMS_TRACE(29);
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool coarse = C->coarse != 0u;
+  const uint32_t gsh = coarse_shift(B);
+  if (b >= (coarse ? NGRP : B)) return;
+  if (!(((coarse ? aflagc : aflag)[b >> 5] >> (b & 31)) & 1u)) {
+    cmap0[b] = CM_NONE;
+    return;
+  }
+  l0_child_make<K>(b, coarse, gsh, B, coarse ? ic : I, gv, *Wg, C, cmap0, segs1, cursor1, tiles1, points, khead1,
+                   smalls, bigs1, caps, kcnt0, tiny_keys, tinies);
+}
+
 // ks follow their bin: resolved (single key) or the id of the next segment.
 template <typename K>
-__global__ void lvl_relabel(const uint32_t* __restrict__ cmap, uint32_t row_len, uint32_t nk,
-                            const uint32_t* __restrict__ k_bin, uint32_t* k_seg, K* k_key,
-                            const K* __restrict__ points, Counters* C,
-                            const Seg<K>* __restrict__ segs_q, uint32_t* khead_q, uint32_t* knext) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nk) return;
-  const uint32_t s = k_seg[i];
-  if (s == K_DONE) return;
-  const uint32_t e = cmap[(size_t)s * row_len + k_bin[i]];
+__device__ __forceinline__ void relabel_one(uint32_t i, uint32_t e, uint32_t* k_seg, K* k_key,
+                                            const K* __restrict__ points, Counters* C,
+                                            const Seg<K>* __restrict__ segs_q, uint32_t* khead_q,
+                                            uint32_t* knext) {
   if (e == CM_NONE) {
     set_status(C, GGMS_E_INTERNAL);
     k_seg[i] = K_DONE;
@@ -1058,14 +1184,119 @@ __global__ void lvl_relabel(const uint32_t* __restrict__ cmap, uint32_t row_len,
   }
 }
 
+template <typename K>
+__global__ void lvl_relabel(const uint32_t* __restrict__ cmap, uint32_t row_len, uint32_t nk,
+                            const uint32_t* __restrict__ k_bin, uint32_t* k_seg, K* k_key,
+                            const K* __restrict__ points, Counters* C,
+                            const Seg<K>* __restrict__ segs_q, uint32_t* khead_q, uint32_t* knext) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nk) return;
+  const uint32_t s = k_seg[i];
+  if (s == K_DONE) return;
+  relabel_one<K>(i, cmap[(size_t)s * row_len + k_bin[i]], k_seg, k_key, points, C, segs_q, khead_q, knext);
+}
+
+// The first steps between PASS 1 and PASS 2 of one vector in ONE CTA (1024
+// threads), through shared memory: the scan of the bucket counts, every k's
+// bucket and rank in it, and the coarse-mode decision with the groups' counts
+// and flags -- what l0_scan, lvl_locate_rows and l0_mode_ks do in three
+// launches.  l0_children and l0_relabel_bases follow.  Dynamic shared memory:
+// l0_between_smem(B).
+__host__ __device__ constexpr size_t l0_between_smem(uint32_t B) {
+  return 4u * (size_t)B + 4u * ((size_t)B / 32u);
+}
+
+template <typename K>
+__global__ __launch_bounds__(1024) void l0_between(uint32_t* hist0, uint32_t B, Counters* C,
+                                                   const Windows<K>* __restrict__ Wg, uint32_t nk,
+                                                   uint32_t* k_rank, const uint32_t* __restrict__ k_seg,
+                                                   uint32_t* k_bin, uint32_t* kcnt0, uint32_t* aflag0,
+                                                   uint32_t* ic, uint32_t* aflagc) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ Windows<K> W;
+  __shared__ uint32_t red[72];
+  __shared__ uint32_t mx, ntot;
+  __shared__ uint32_t afc[NGRP / 32];
+  GGMS_TRACE(26);
+  uint32_t* I = reinterpret_cast<uint32_t*>(smem);  // [B] counts, then inclusive counts
+  uint32_t* af = I + B;                             // [B / 32] buckets holding a k
+  const uint32_t tid = threadIdx.x;
+  if (tid == 0) {
+    W = *Wg;
+    mx = 0;
+    ntot = 0;
+  }
+  if (tid < NGRP / 32) afc[tid] = 0u;
+  for (uint32_t w = tid; w < B / 32; w += 1024) af[w] = 0u;
+  __syncthreads();
+  // 1. inclusive scan of the counts (and the largest bucket outside the gap buckets)
+  const bool on = W.on != 0u;
+  uint32_t m = 0;
+  for (uint32_t i = tid; i < B; i += 1024) {
+    const uint32_t v = hist0[i];
+    I[i] = v;
+    if (on) {
+      bool gap = false;
+#pragma unroll
+      for (uint32_t g = 0; g <= L0_WIN; ++g) gap = gap || (g <= W.R && i == W.gb0[g]);
+      if (!gap) m = max(m, v);
+    }
+  }
+  __syncthreads();
+  if (on) atomicMax(&mx, m);
+  block_inclusive_scan_global<1024>(I, B, red, &C->max_bucket0);
+  for (uint32_t i = tid; i < B; i += 1024) hist0[i] = I[i];
+  if (on && tid == 0) C->max_bucket0 = mx;
+  GGMS_TRACE(43);
+  // 2. every k: its bucket and its rank inside it
+  for (uint32_t i = tid; i < nk; i += 1024) {
+    if (k_seg[i] == K_DONE) continue;
+    uint32_t r = k_rank[i];
+    const uint32_t b = locate_one(I, B, r, C);
+    if (b == K_NIL) continue;
+    k_bin[i] = b;
+    k_rank[i] = r;
+    atomicOr(&af[b >> 5], 1u << (b & 31));
+    atomicAdd(&kcnt0[b], 1u);
+  }
+  __syncthreads();
+  GGMS_TRACE(44);
+  // 3. coarse mode: most buckets hold a k (and no windows): groups of buckets
+  uint32_t a = 0;
+  for (uint32_t w = tid; w < B / 32; w += 1024) {
+    const uint32_t f = af[w];
+    aflag0[w] = f;
+    a += __popc(f);
+  }
+  atomicAdd(&ntot, a);
+  const uint32_t gsh = coarse_shift(B);
+  for (uint32_t g = tid; g < NGRP; g += 1024) ic[g] = I[((g + 1u) << gsh) - 1u];
+  __syncthreads();
+  const bool coarse = !on && ntot * 2u >= B;
+  if (tid == 0) C->coarse = coarse ? 1u : 0u;
+  if (coarse) {
+    for (uint32_t i = tid; i < nk; i += 1024) {
+      if (k_seg[i] == K_DONE) continue;
+      const uint32_t b = k_bin[i], g = b >> gsh, g0 = g << gsh;
+      k_rank[i] += (b ? I[b - 1] : 0u) - (g0 ? I[g0 - 1] : 0u);
+      k_bin[i] = g;
+      atomicOr(&afc[g >> 5], 1u << (g & 31));
+    }
+  }
+  __syncthreads();
+  if (tid < NGRP / 32) aflagc[tid] = afc[tid];
+  GGMS_TRACE(45);
+}
+
 // Per-CTA write cursors for PASS 2: for every level-0 child (a copied bucket
 // b), one warp turns column b of the per-CTA count rows into exclusive
 // prefixes plus the child's offset, in place.  CTA g of PASS 2 then owns the
 // slots [crow[g][b], crow[g][b] + its count) of bucket b.
 template <typename K>
-__global__ void l0_bases(uint32_t* crow, uint32_t B, uint32_t ncta, const Seg<K>* __restrict__ segs1,
-                         const Counters* __restrict__ C, Caps caps) {
+__device__ __forceinline__ void bases_body(uint32_t* crow, uint32_t B, uint32_t ncta, const Seg<K>* __restrict__ segs1,
+                                           const Counters* __restrict__ C, const Caps& caps) {
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  GGMS_TRACE(30);
   const uint32_t ns = min(C->nsegs[1], caps.segs);
   const bool coarse = C->coarse != 0u;
   const uint32_t gsh = coarse_shift(B);
@@ -1096,6 +1327,32 @@ __global__ void l0_bases(uint32_t* crow, uint32_t B, uint32_t ncta, const Seg<K>
   }
 }
 
+template <typename K>
+__global__ void l0_bases(uint32_t* crow, uint32_t B, uint32_t ncta, const Seg<K>* __restrict__ segs1,
+                         const Counters* __restrict__ C, Caps caps) {
+  bases_body<K>(crow, B, ncta, segs1, C, caps);
+}
+
+// After l0_children: the ks follow their level-0 child (lvl_relabel) and the
+// per-CTA write cursors of PASS 2 are formed (l0_bases), in one launch --
+// threads [0, nk) relabel, all warps then take children for the cursors.
+// In a captured graph it also sets the condition of the first refinement
+// level (lev1, nonzero): whether some level-0 child needs one.
+template <typename K>
+__global__ void l0_relabel_bases(const uint32_t* __restrict__ cmap0, uint32_t nk,
+                                 const uint32_t* __restrict__ k_bin, uint32_t* k_seg, K* k_key,
+                                 const K* __restrict__ points, Counters* C, const Seg<K>* __restrict__ segs1,
+                                 uint32_t* khead1, uint32_t* knext, uint32_t* crow, uint32_t B, uint32_t ncta,
+                                 Caps caps, cudaGraphConditionalHandle lev1) {
+  if (lev1 && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(lev1, C->nbig[1] ? 1u : 0u);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nk; i += gridDim.x * blockDim.x) {
+    const uint32_t s = k_seg[i];
+    if (s == K_DONE) continue;
+    relabel_one<K>(i, cmap0[k_bin[i]], k_seg, k_key, points, C, segs1, khead1, knext);
+  }
+  bases_body<K>(crow, B, ncta, segs1, C, caps);
+}
+
 // PASS 2.  Re-reads the input with the same element -> CTA assignment as
 // PASS 1; a key whose bucket is copied goes to slot atomicAdd(&cur[b], 1) of
 // this CTA's private range (a shared-memory atomic: no global round trip).
@@ -1123,10 +1380,11 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
                                                 const uint32_t* __restrict__ cmap0,
                                                 const uint32_t* __restrict__ crow,
                                                 typename KeyOf<T>::K* dst, uint64_t dst_cap,
-                                                uint32_t ring_st) {
+                                                uint32_t ring_st, const uint32_t* __restrict__ I0) {
   using K = typename KeyOf<T>::K;
   constexpr int EPV = Vec16<T>::N;
   if (C->coarse) return;  // l0_compact_coarse copies this call's groups
+  GGMS_TRACE(32);
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ Windows<K> W;
   __shared__ RingBars rbars;
@@ -1154,7 +1412,9 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
       wpre[w] = __popc(bits);
     }
   }
+  __shared__ unsigned long long hot_mass_s;
   for (uint32_t w = threadIdx.x; w < HOT_WORDS; w += NT) hot[w] = 0u;
+  if (threadIdx.x == 0) hot_mass_s = 0ull;
   __syncthreads();
   if (warp == 0) {  // exclusive prefix of the per-word counts (B / 32 <= 1024 words)
     uint32_t run = 0;
@@ -1183,13 +1443,20 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
       return (b & 31) ? wpre[w] + __popc(amask[w] & ((1u << (b & 31)) - 1u)) : wpre[w];
     };
     const K dmax = (K)(gv.gmax - gv.origin);
+    unsigned long long mass = 0;  // keys of this thread's hot cells (the buckets they span, from PASS 1)
     for (uint32_t c = threadIdx.x; c < ncell; c += NT) {
       const K d0 = (K)c << gv.sh1;
       const K d1 = (c + 1u < ncell) ? (K)(((K)(c + 1u) << gv.sh1) - 1u) : dmax;
       const uint32_t lo = bmap(min(grid_eval<K>(gv, (K)(gv.origin + d0)), B - 1u));
       const uint32_t hi = bmap(min(grid_eval<K>(gv, (K)(gv.origin + min(d1, dmax))), B - 1u));
-      if (rank(hi + 1u) != rank(lo)) atomicOr(&hot[c >> 5], 1u << (c & 31));
+      if (rank(hi + 1u) != rank(lo)) {
+        atomicOr(&hot[c >> 5], 1u << (c & 31));
+        mass += I0[hi] - (lo ? I0[lo - 1] : 0u);
+      }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mass += __shfl_xor_sync(FULL, mass, o);
+    if (lane == 0 && mass) atomicAdd(&hot_mass_s, mass);  // buckets shared by two cells count twice
   }
   __syncthreads();
   // Maximal runs of hot cells as key intervals [lo, lo + span]; with at most
@@ -1259,6 +1526,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
   // With windows and no gap bucket to copy, every copied bucket lies inside a
   // window run: when the runs are narrow (tight), their key ranges (few, known
   // exactly) are the test.
+  GGMS_TRACE(33);
   bool use_win = W.on != 0u && W.tight != 0u;
   for (uint32_t g = 0; g <= L0_WIN && use_win; ++g)
     if (g <= W.R && W.gb0[g] <= W.gb1[g] && ((amask[W.gb0[g] >> 5] >> (W.gb0[g] & 31)) & 1u))
@@ -1293,7 +1561,9 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
         if ((amask[b[t] >> 5] >> (b[t] & 31)) & 1u) put(b[t], kk[t]);
     });
   };
-  if (!use_win && nruns > L0_RUNS && ncopied * 2u >= B) {
+  // hot cells that hold most of the keys (ks spread over all ranks): every key
+  // takes the long path anyway, so it goes there directly
+  if (!use_win && nruns > L0_RUNS && (ncopied * 2u >= B || hot_mass_s * 2u > n)) {
     dense();
   } else if (use_win) {
     switch (W.R) {
@@ -1311,6 +1581,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
     default: stream_keys<T>(src, wq, qn, lane, in_hot, bucket_and_put); break;
   }
   src.finish(C);
+  GGMS_TRACE(34);
   __syncwarp();
   if (lane < qn) bucket_and_put(wq[lane]);
   const T* vbase = in + head;
@@ -1352,6 +1623,7 @@ __global__ void l0_mode_ks(const uint32_t* __restrict__ I, const uint32_t* __res
                            const Windows<K>* __restrict__ Wg, Counters* C, uint32_t* ic, uint32_t* aflagc,
                            uint32_t nk, uint32_t* k_rank, const uint32_t* __restrict__ k_seg, uint32_t* k_bin) {
   __shared__ uint32_t tot;
+  GGMS_TRACE(38);
   if (threadIdx.x == 0) tot = 0u;
   __syncthreads();
   uint32_t a = 0;
@@ -1373,8 +1645,8 @@ __global__ void l0_mode_ks(const uint32_t* __restrict__ I, const uint32_t* __res
 }
 
 // Keys of one PASS-2 chunk of the coarse mode: up to 4 vectors per thread.
-// vectors per thread per staged chunk: up to 4 (the TMA ring: 4)
-__host__ __device__ constexpr int coarse_du(int unroll) { return unroll == 0 ? 4 : (unroll < 4 ? unroll : 4); }
+// vectors per thread per staged chunk: up to 4 (the staged streams: 4)
+__host__ __device__ constexpr int coarse_du(int unroll) { return unroll <= 0 ? 4 : (unroll < 4 ? unroll : 4); }
 template <typename T, int NT, int UNROLL>
 __host__ __device__ constexpr uint32_t coarse_chunk() {
   return (uint32_t)NT * coarse_du(UNROLL) * Vec16<T>::N;
@@ -1561,6 +1833,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact_coarse(const
 // Gate of a refinement level inside a captured CUDA graph: the level (an IF
 // node) runs only while every level so far had segments to refine.
 __global__ void lvl_gate(Counters* C, int p, cudaGraphConditionalHandle h) {
+  GGMS_TRACE(41 + p);
   if (C->nbig[p] == 0u) C->done = 1u;
   cudaGraphSetConditional(h, C->done ? 0u : 1u);
 }
@@ -1937,6 +2210,7 @@ __global__ __launch_bounds__(NT) void small_select(const InT* __restrict__ src,
   __shared__ K upk[SS_GROUP];       // distinct prefixes of the current round
   __shared__ uint32_t hmap[SS_GROUP];  // k -> its prefix's histogram
   __shared__ uint32_t nuniq;
+  GGMS_TRACE(35);
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t ns = min(C->nsmall, caps.segs);
   for (uint32_t t = blockIdx.x; t < ns; t += gridDim.x) {
@@ -2096,6 +2370,7 @@ __global__ __launch_bounds__(NT) void small_select(const InT* __restrict__ src,
     if (tid == 0) atomicAdd(&C->small_segs, 1u);
     __syncthreads();
   }
+  GGMS_TRACE(36);
 }
 
 // One warp finishes a whole tiny segment (at most tiny_keys<K>() keys, as
@@ -2106,7 +2381,6 @@ __global__ __launch_bounds__(NT) void small_select(const InT* __restrict__ src,
 // the lanes read their ks' answers from it.  The ks come from the segment's
 // list, or (k_off given: the segments are the caller's) from its k range.
 constexpr int TS_NT = 128;
-constexpr uint32_t TS_SORT_ABOVE = 8;
 
 template <typename K>
 __device__ __forceinline__ K warp_radix_select(const K* v, uint32_t cnt, int bits, uint32_t r, uint32_t* h,
@@ -2187,6 +2461,7 @@ __global__ __launch_bounds__(NT) void tiny_select(const InT* __restrict__ src,
   // so that every warp gets work): lane j loads entry j's descriptor and k-list
   // head -- the chain of dependent loads is paid once per batch -- then the warp
   // finishes the segments one by one
+  GGMS_TRACE(39);
   const uint32_t nwarps = gridDim.x * NW;
   const uint32_t batch = max(1u, min(32u, nt / nwarps));
   for (uint32_t t0 = (blockIdx.x * NW + wid) * batch; t0 < nt; t0 += nwarps * batch) {
@@ -2279,6 +2554,7 @@ __global__ __launch_bounds__(NT) void tiny_select(const InT* __restrict__ src,
     }
     if (lane == 0) atomicAdd(&C->small_segs, nb);
   }
+  GGMS_TRACE(40);
 }
 
 // ------------------------------------------------------------------ batched segments
@@ -2368,6 +2644,7 @@ template <typename T>
 __global__ void write_out(const typename KeyOf<T>::K* __restrict__ k_key,
                           const uint32_t* __restrict__ k_seg, uint32_t nk, T* out, Counters* C) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  GGMS_TRACE(37);
   if (i >= nk) return;
   if (k_seg[i] != K_DONE) set_status(C, GGMS_E_NOT_CONVERGED);
   out[i] = KeyOf<T>::from(k_key[i]);

@@ -69,6 +69,7 @@ template <typename K>
 __global__ __launch_bounds__(1024) void pl_stats_grid(const K* __restrict__ sorted, uint32_t S,
                                                      const Assigner<K>* __restrict__ A, LearnState* L) {
   __shared__ K sidx[65536u / PL_IDX];
+  GGMS_TRACE(7);
   const uint32_t M = A->M;
   const uint32_t nidx = (S + PL_IDX - 1u) / PL_IDX;  // S <= 65536
   for (uint32_t j = threadIdx.x; j < nidx; j += blockDim.x) sidx[j] = sorted[j * PL_IDX];
@@ -104,6 +105,7 @@ __global__ __launch_bounds__(1024) void pl_stats_grid(const K* __restrict__ sort
     sy2 += __shfl_xor_sync(FULL, sy2, o);
   }
   if (lane == 0) L->st[j] = PLStats{n, su, su2, sy, syu, sy2};
+  GGMS_TRACE(8);
 }
 
 // The statistics into shared memory for training (all threads call it).
@@ -120,29 +122,42 @@ __device__ __forceinline__ void pl_stats_load(const LearnState* L, uint32_t M, P
 constexpr int PL_NT = PL_M;
 __device__ __forceinline__ void bar_pl() { asm volatile("bar.sync 1, %0;" ::"n"(PL_NT) : "memory"); }
 
+// Cross-warp partials of pl_fb and their combinations (made by warp 0).
 struct PLRed {
-  double a[PL_NT / 32], b[PL_NT / 32], c[PL_NT / 32];
+  double a[PL_NT / 32], b[PL_NT / 32], c[PL_NT / 32], e[PL_NT / 32];
+  double pa[PL_NT / 32], pb[PL_NT / 32];  // exclusive prefixes over the warps
+  double ta, tb, tc, te;                  // totals
 };
 
+// Warp 0: exclusive prefix of x[0..32) into pre[], the total into *tot.
+__device__ __forceinline__ void warp0_prefix(const double* x, double* pre, double* tot, uint32_t lane) {
+  const double v = x[lane];
+  const double inc = warp_incl_scan(v, lane);
+  pre[lane] = inc - v;
+  if (lane == 31) *tot = inc;
+}
+__device__ __forceinline__ void warp0_sum(const double* x, double* tot, uint32_t lane) {
+  double v = x[lane];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  if (lane == 0) *tot = v;
+}
+
 // Returns the loss; *g = d loss / d theta_j; cdf_out (if given) gets P_j / D and 1 at M.
+// Four named barriers: each cross-warp sum or prefix is formed once, by warp 0.
 __device__ float pl_fb(float theta, const PLStats* st, uint32_t M, double S, PLRed& red, float* g,
                        float* cdf_out) {
+  static_assert(PL_NT == 1024, "warp 0 combines exactly 32 warp partials");
   const uint32_t j = threadIdx.x, lane = j & 31, warp = j >> 5;
-  constexpr int NW = PL_NT / 32;
   const bool act = j < M;
   const double d = act ? (double)softplusf(theta) : 0.0;
   // P_j = sum_{t<j} d_t, D = sum d
-  double inc = warp_incl_scan(d, lane);
+  const double inc = warp_incl_scan(d, lane);
   if (lane == 31) red.a[warp] = inc;
   bar_pl();
-  double P = inc - d, D = 0.0;
-#pragma unroll
-  for (int w = 0; w < NW; ++w) {
-    const double t = red.a[w];
-    if (w < (int)warp) P += t;
-    D += t;
-  }
+  if (warp == 0) warp0_prefix(red.a, red.pa, &red.ta, lane);
   bar_pl();
+  const double P = inc - d + red.pa[warp], D = red.ta;
   const double invD = 1.0 / D;
   double R = 0, U = 0, Qc = 0, Lc = 0;
   if (act) {
@@ -158,26 +173,23 @@ __device__ float pl_fb(float theta, const PLStats* st, uint32_t M, double S, PLR
     if (cdf_out) cdf_out[j] = (float)p;
   }
   // suffix of R and totals of Qc, Lc
-  double rin = warp_incl_scan(R, lane);
+  const double rin = warp_incl_scan(R, lane);
   double q = Qc, l = Lc;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     q += __shfl_xor_sync(FULL, q, o);
     l += __shfl_xor_sync(FULL, l, o);
   }
-  if (lane == 31) red.a[warp] = rin;
-  if (lane == 0) { red.b[warp] = q; red.c[warp] = l; }
+  if (lane == 31) red.b[warp] = rin;
+  if (lane == 0) { red.c[warp] = q; red.e[warp] = l; }
   bar_pl();
-  double before = rin, Rt = 0, Q = 0, L = 0;
-#pragma unroll
-  for (int w = 0; w < NW; ++w) {
-    const double t = red.a[w];
-    if (w < (int)warp) before += t;
-    Rt += t;
-    Q += red.b[w];
-    L += red.c[w];
+  if (warp == 0) {
+    warp0_prefix(red.b, red.pb, &red.tb, lane);
+    warp0_sum(red.c, &red.tc, lane);
+    warp0_sum(red.e, &red.te, lane);
   }
   bar_pl();
+  const double before = rin + red.pb[warp], Rt = red.tb, Q = red.tc, L = red.te;
   // dF_i/d delta_t = (1{t < j_i} + u_i 1{t = j_i} - F_i) / D
   const double after = Rt - before;
   if (act) *g = (float)((2.0 / (S * D)) * (after + U - Q) * (double)sigmoidf_(theta));
@@ -288,8 +300,11 @@ __device__ void learned_finish(const K* sorted, uint32_t S, uint32_t B, uint32_t
                                Assigner<K>* A, Grid<K>* G, const Grid<K>* G0, LearnState* L,
                                uint32_t* choice, LearnSmem<K>& sm, const Warp* wp = nullptr) {
   const AsgView<K> av = asg_copy<K>(A, sm.su.asg);
+  GGMS_TRACE(14);
   const GridView<K> gv = grid_compile<K>(av, B, kind, G, sm.su.s1, sm.su.s2, sm.su.cs);
+  GGMS_TRACE(15);
   const float qv = grid_measure<K>(gv, sorted, S, sm.su.hist256, wp);
+  GGMS_TRACE(16);
   if (threadIdx.x == 0) {
     G->quality = qv;
     const uint32_t c = (qv <= bound || qv < G0->quality) ? 1u : 0u;
@@ -309,7 +324,9 @@ __global__ __launch_bounds__(SETUP_NT) void setup_pl_knots(const K* __restrict__
                                                           uint32_t B, Assigner<K>* A, uint32_t mreq) {
   extern __shared__ __align__(128) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
+  GGMS_TRACE(5);
   pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, A, sm, mreq);
+  GGMS_TRACE(6);
 }
 
 // Training and compilation of the learned PL model (one CTA), after
@@ -329,7 +346,9 @@ __global__ __launch_bounds__(SETUP_NT) void setup_learned_pl(const K* __restrict
   __shared__ Warp wsh;
   __shared__ uint32_t wred[33];
   const uint32_t M = A->M;  // knots: setup_pl_knots; statistics: pl_stats_grid
+  GGMS_TRACE(9);
   pl_stats_load(L, M, sm.st);
+  GGMS_TRACE(10);
   if (threadIdx.x < PL_NT) {
     const float loss = pl_train_block(sm.st, M, S, steps, lr, sm.red, sm.cdf, &L->loss_init,
                                       L->theta, L->grad);
@@ -340,6 +359,7 @@ __global__ __launch_bounds__(SETUP_NT) void setup_learned_pl(const K* __restrict
     }
   }
   __syncthreads();
+  GGMS_TRACE(11);
   if (window_z >= 0.0f) {
     // the statistics are dead after training: their space holds the bins
     build_warp(krank, nk, n, S, window_z, L0_WIN, reinterpret_cast<uint32_t*>(sm.st), wred, &wsh);
@@ -349,8 +369,10 @@ __global__ __launch_bounds__(SETUP_NT) void setup_learned_pl(const K* __restrict
     wsh.p[1] = wsh.w[1] = 1.0f;
   }
   __syncthreads();
+  GGMS_TRACE(12);
   if (threadIdx.x == 0) L->focus_points = wsh.n;
   pl_set_bases<K>(sm.cdf, A, sm.Bs, GGMS_ASSIGNER_LEARNED_PL, &wsh);
+  GGMS_TRACE(13);
   learned_finish<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, bound, A, G, G0, L, choice, sm, &wsh);
 }
 

@@ -1,12 +1,17 @@
 // ggms_mlp.cuh -- monotone 1-32-32-1 MLP CDF model, trained on the GPU.
 //
-//   x = (key - x_0) / (x_M - x_0)                    (key space, in [0, 1])
+//   x = F0(key)                      the sampled pivots' piecewise-linear CDF
+//                                    (the reference's bucket map), in [0, 1]
 //   h1 = tanh(w1 * x + c1)           w1 = softplus(V1) > 0     (32)
 //   h2 = tanh(W2 h1 + c2)            W2 = softplus(V2) > 0     (32 x 32)
 //   y  = sigmoid(w3 . h2 + c3)       w3 = softplus(V3) > 0
-// Positive weights and increasing activations make y non-decreasing in x, so
-// the compiled assigner is monotone.  Loss: mean (y_i - t_i)^2 over Q = 1024
-// training points at the quantiles of the self-drawn sample (t_i = rank / S).
+// Positive weights and increasing activations make y non-decreasing in x, and
+// F0 is non-decreasing, so y(F0(key)) is monotone in the key and so is the
+// compiled assigner.  The network thus learns a monotone correction of the
+// sampled model: where the data's density changes inside a pivot interval
+// (mixtures, heavy tails) F0 is off and the network bends it back.  Loss:
+// mean (y_i - t_i)^2 over Q = 1024 training points at the quantiles of the
+// self-drawn sample (t_i = rank / S).
 //
 // Training runs in ONE launch of one thread-block cluster (8 CTAs x 128
 // threads, one training point per thread): every step each CTA computes its
@@ -123,10 +128,24 @@ __device__ void mlp_cta_grad(MlpSmem& S, float inv_q) {
   __syncthreads();
 }
 
-// Training points: Q sample quantiles, x normalized over the knot range of A,
-// target t = (rank + 0.5) / S.
+// The network's input: the sampled model A0's CDF at `key`, the position of the
+// key on A0's piecewise-linear bucket map divided by the bucket count
+// (continuous, not rounded to a bucket), clamped to [0, 1].
 template <typename K>
-__device__ void mlp_load_points(MlpSmem& S, const K* sorted, uint32_t S_n, const Assigner<K>* A,
+__device__ __forceinline__ float mlp_input(const Assigner<K>* __restrict__ A0, K key) {
+  const uint32_t M = A0->M;
+  const K x0 = A0->x[0];
+  if (M == 0u || key <= x0) return 0.0f;
+  if (key >= A0->x[M]) return 1.0f;
+  uint32_t j = A0->idx[(uint32_t)((K)(key - x0) >> A0->csh)];
+  while (j + 1u < M && key >= A0->x[j + 1u]) ++j;
+  const float b = (float)A0->base[j] + __fmul_rn(key_to_float_rn((K)(key - A0->x[j])), A0->slope[j]);
+  return fminf(fmaxf(__fdiv_rn(b, (float)A0->B), 0.0f), 1.0f);
+}
+
+// Training points: Q sample quantiles, x = F0 of the key, target t = (rank + 0.5) / S.
+template <typename K>
+__device__ void mlp_load_points(MlpSmem& S, const K* sorted, uint32_t S_n, const Assigner<K>* A0,
                                 const float* px, const float* pt) {
   const int tid = threadIdx.x;
   const uint32_t gi = blockIdx.x * MLP_NT + tid;
@@ -136,9 +155,7 @@ __device__ void mlp_load_points(MlpSmem& S, const K* sorted, uint32_t S_n, const
     return;
   }
   const uint32_t si = (uint32_t)(((uint64_t)(2 * gi + 1) * S_n) / (2 * MLP_Q));
-  const K x0 = A->x[0], xM = A->x[A->M];
-  const float span = key_to_float_rn((K)(xM - x0));
-  S.x[tid] = span > 0.0f ? fminf(__fdiv_rn(key_to_float_rn((K)(sorted[si] - x0)), span), 1.0f) : 0.0f;
+  S.x[tid] = mlp_input<K>(A0, sorted[si]);
   S.t[tid] = ((float)si + 0.5f) / (float)S_n;
 }
 
@@ -147,7 +164,7 @@ __device__ void mlp_load_points(MlpSmem& S, const K* sorted, uint32_t S_n, const
 // probe[0..MLP_NP) and probe[MLP_NP] (used by the gradient check).
 template <typename K>
 __global__ void __cluster_dims__(MLP_CTAS, 1, 1) __launch_bounds__(MLP_NT)
-mlp_train(const K* __restrict__ sorted, uint32_t S_n, const Assigner<K>* __restrict__ A,
+mlp_train(const K* __restrict__ sorted, uint32_t S_n, const Assigner<K>* __restrict__ A0,
           LearnState* L, float* Pglob, uint32_t steps, float lr, const float* px, const float* pt,
           float* probe) {
   extern __shared__ __align__(128) uint8_t smem_raw[];
@@ -160,7 +177,7 @@ mlp_train(const K* __restrict__ sorted, uint32_t S_n, const Assigner<K>* __restr
     S.m1[p] = 0.0f;
     S.m2[p] = 0.0f;
   }
-  mlp_load_points<K>(S, sorted, S_n, A, px, pt);
+  mlp_load_points<K>(S, sorted, S_n, A0, px, pt);
   __syncthreads();
   MlpSmem* S0 = cluster.map_shared_rank(&S, 0);
   const float inv_q = 1.0f / (float)MLP_Q;
@@ -228,16 +245,14 @@ mlp_train(const K* __restrict__ sorted, uint32_t S_n, const Assigner<K>* __restr
 // unit k steps where that approximation crosses (k + 0.5)/32.  Layer 3: the
 // mean of the layer-2 steps through the near-linear part of the sigmoid.
 template <typename K>
-__device__ void mlp_init(const K* __restrict__ sorted, uint32_t S_n, const Assigner<K>* __restrict__ A,
+__device__ void mlp_init(const K* __restrict__ sorted, uint32_t S_n, const Assigner<K>* __restrict__ A0,
                          float* P) {
   const int tid = threadIdx.x;
-  const K x0 = A->x[0], xM = A->x[A->M];
-  const float span = key_to_float_rn((K)(xM - x0));
-  auto qx = [&](int j) -> float {  // normalized key of quantile (2j+1)/64; -1 -> 0, 32 -> 1
+  auto qx = [&](int j) -> float {  // the input at quantile (2j+1)/64; -1 -> 0, 32 -> 1
     if (j < 0) return 0.0f;
     if (j > 31) return 1.0f;
     const uint32_t si = (uint32_t)(((uint64_t)(2 * j + 1) * S_n) / 64u);
-    return span > 0.0f ? __fdiv_rn(key_to_float_rn((K)(sorted[si] - x0)), span) : 0.0f;
+    return mlp_input<K>(A0, sorted[si]);
   };
   for (int p = tid; p < MLP_NP; p += blockDim.x) {
     float v = 0.0f;
@@ -263,15 +278,14 @@ __device__ void mlp_init(const K* __restrict__ sorted, uint32_t S_n, const Assig
   }
 }
 
-// Evaluate the trained MLP at the knots of A and write the normalized CDF.
+// Evaluate the trained MLP at the knots of A (input F0 of each knot) and write
+// the normalized CDF.
 template <typename K>
 __device__ void mlp_eval_knots(const float* __restrict__ P, const Assigner<K>* __restrict__ A,
-                               float* y, float* cdf) {
+                               const Assigner<K>* __restrict__ A0, float* y, float* cdf) {
   const uint32_t M = A->M;
-  const K x0 = A->x[0];
-  const float span = key_to_float_rn((K)(A->x[M] - x0));
   for (uint32_t j = threadIdx.x; j <= M; j += blockDim.x) {
-    const float x = span > 0.0f ? fminf(__fdiv_rn(key_to_float_rn((K)(A->x[j] - x0)), span), 1.0f) : 0.0f;
+    const float x = mlp_input<K>(A0, A->x[j]);
     float h1[32];
 #pragma unroll
     for (int i = 0; i < 32; ++i) h1[i] = tanhf(fmaf(softplusf(P[P_V1 + i]), x, P[P_C1 + i]));
@@ -293,12 +307,12 @@ __device__ void mlp_eval_knots(const float* __restrict__ P, const Assigner<K>* _
 
 template <typename K>
 __global__ __launch_bounds__(SETUP_NT) void setup_mlp_begin(const K* __restrict__ sorted, uint32_t S,
-                                                           uint32_t B, Assigner<K>* A, float* P,
-                                                           uint32_t mreq) {
+                                                           uint32_t B, Assigner<K>* A, const Assigner<K>* A0,
+                                                           float* P, uint32_t mreq) {
   extern __shared__ __align__(128) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
   pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_MLP, A, sm, mreq);
-  mlp_init<K>(sorted, S, A, P);
+  mlp_init<K>(sorted, S, A0, P);
 }
 
 template <typename K>
@@ -308,7 +322,7 @@ __global__ __launch_bounds__(SETUP_NT) void setup_mlp_finish(const K* __restrict
                                                             uint32_t* choice) {
   extern __shared__ __align__(128) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
-  mlp_eval_knots<K>(P, A, (float*)sm.Bs, sm.cdf);
+  mlp_eval_knots<K>(P, A, A - 1, (float*)sm.Bs, sm.cdf);  // A - 1: the sampled assigner of the pair
   for (uint32_t j = threadIdx.x; j <= A->M; j += blockDim.x) L->cdf[j] = sm.cdf[j];
   if (threadIdx.x == 0) L->M = A->M;  // segments of the compiled piecewise-linear form
   pl_set_bases<K>(sm.cdf, A, sm.Bs, GGMS_ASSIGNER_LEARNED_MLP);
@@ -334,10 +348,12 @@ static int mlp_fit_and_compile(const K* sorted, uint32_t S, uint32_t B, int step
   }
   const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 150u;
   float* P = L->mlp_params;
-  setup_mlp_begin<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, &As[1], P, pl_knots);
-  mlp_train<K><<<MLP_CTAS, MLP_NT, sizeof(MlpSmem), st>>>(sorted, S, &As[1], L, P, steps, 0.05f,
-                                                          nullptr, nullptr, nullptr);
+  // the network's input is the sampled model: wait for it (it may be built on
+  // another stream)
   if (sampled_done && cudaStreamWaitEvent(st, sampled_done, 0) != cudaSuccess) return GGMS_E_CUDA;
+  setup_mlp_begin<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, &As[1], &As[0], P, pl_knots);
+  mlp_train<K><<<MLP_CTAS, MLP_NT, sizeof(MlpSmem), st>>>(sorted, S, &As[0], L, P, steps, 0.05f,
+                                                          nullptr, nullptr, nullptr);
   setup_mlp_finish<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, bound, P, &As[1],
                                                                   &Gs[1], L, choice);
   *launches += 3;

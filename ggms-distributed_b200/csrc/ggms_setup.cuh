@@ -659,8 +659,18 @@ __device__ float grid_measure(const GridView<K>& g, const K* sorted_all, uint32_
     }
   }
   __syncthreads();
+  // the largest group: 8 warps reduce 32 counts each, then every thread reads the 8
+  __shared__ uint32_t wmax[8];
+  if (threadIdx.x < 256) {
+    uint32_t m = hist256[threadIdx.x];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(FULL, m, o));
+    if (lane == 0) wmax[threadIdx.x >> 5] = m;
+  }
+  __syncthreads();
   uint32_t mx = 0;
-  for (uint32_t i = 0; i < 256; ++i) mx = max(mx, hist256[i]);
+#pragma unroll
+  for (int w = 0; w < 8; ++w) mx = max(mx, wmax[w]);
   __syncthreads();
   return (float)mx / ((float)S / 256.0f);
 }
@@ -713,6 +723,7 @@ __global__ __launch_bounds__(SETUP_NT) void setup_sampled(const K* __restrict__ 
   SetupSmem<K>& sm = *reinterpret_cast<SetupSmem<K>*>(smem);
   __shared__ uint32_t q[17];
   __shared__ float cdf[17];
+  GGMS_TRACE(3);
   if (threadIdx.x == 0) {
     const uint32_t end_off = max(1u, (22u * S) / 1024u);
     const uint32_t piv_off = (S - 2u * end_off) / 14u;
@@ -730,6 +741,7 @@ __global__ __launch_bounds__(SETUP_NT) void setup_sampled(const K* __restrict__ 
   const GridView<K> gv = grid_compile<K>(av, B, GGMS_ASSIGNER_SAMPLED, G, sm.s1, sm.s2, sm.cs);
   const float qv = grid_measure<K>(gv, sorted, S, sm.hist256);
   if (threadIdx.x == 0) G->quality = qv;
+  GGMS_TRACE(4);
 }
 
 GGMS_END

@@ -45,6 +45,7 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
   __shared__ uint32_t rs[WIN_MAXRAW], re[WIN_MAXRAW], ss[WIN_MAXRAW], se[WIN_MAXRAW];
   __shared__ Windows<K> sw;
   const uint32_t tid = threadIdx.x;
+  GGMS_TRACE(17);
   const GridView<K> gv = grid_to_smem<K>(Gs + C->asg_choice, s1, s2);
   const uint32_t B = gv.B;
   int32_t* cnt = reinterpret_cast<int32_t*>(bm + B / 32u);  // difference array [B + 1]
@@ -52,6 +53,7 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
   for (uint32_t j = tid; j < nidx; j += WIN_NT) sidx[j] = sorted[j * WIN_IDX];
   for (uint32_t b = tid; b <= B; b += WIN_NT) cnt[b] = 0;
   __syncthreads();
+  GGMS_TRACE(18);
   // 1. bucket range of every k, as +1 / -1 in the difference array
   for (uint32_t i = tid; i < nk; i += WIN_NT) {
     const double q = ((double)krank[i] + 0.5) / (double)n;
@@ -66,10 +68,12 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
     atomicAdd(&cnt[b1 + 1u], -1);
   }
   __syncthreads();
+  GGMS_TRACE(19);
   // 2. buckets some k may hold, then their runs in bucket order (B / 32 <= 1024 words)
   coverage_bitmap(cnt, B, bm, red);
   const uint32_t nraw = bitmap_runs(bm, B / 32u, rs, re, WIN_MAXRAW, red);
   const uint32_t nraw2 = nraw;
+  GGMS_TRACE(20);
   // 3. sample positions of the raw runs: [ss, se) = the sample keys whose
   //    bucket lies in the run (binary search over the sorted sample)
   if (tid < 2u * min(nraw, WIN_MAXRAW)) {
@@ -91,6 +95,7 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
     if (tid & 1u) se[j] = lo; else ss[j] = lo;
   }
   __syncthreads();
+  GGMS_TRACE(21);
   // 4. merge runs across gaps that hold under 1/256 of the sample; decide:
   //    at most L0_WIN runs holding at most a quarter of the sample
   if (tid == 0) {
@@ -138,6 +143,7 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
     }
   }
   __syncthreads();
+  GGMS_TRACE(22);
   // 5. key range of each run: [L(rb0), L(rb1 + 1) - 1], L(x) = smallest key with bucket >= x
   if (sw.on && tid < 2u * sw.R) {
     const uint32_t r = tid >> 1;
@@ -163,6 +169,7 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
     *W = sw;
     C->win_runs = sw.on ? sw.R : 0u;
   }
+  GGMS_TRACE(23);
 }
 
 GGMS_END

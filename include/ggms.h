@@ -89,9 +89,10 @@ typedef struct ggms_opts {
   int32_t out_on_device;        /* 1: the output array is device memory */
   int32_t pass_threads;         /* CTA size of the two passes: 256, 512 or 1024; 0 = tuned default */
   int32_t pass_unroll;          /* how the passes stream the input: 2, 4 or 8 16-byte loads in flight
-                                   per thread (registers), or -1 = 16 KB chunks staged by bulk copies
-                                   (TMA) in a ring of shared-memory stages (pass_threads 1024 only);
-                                   0 = the default (-1) */
+                                   per thread (registers); -1 = 32 KB chunks staged by bulk copies (TMA)
+                                   in a ring of shared-memory stages; -2 = 16 KB chunks copied by every
+                                   thread with cp.async into its own shared-memory slots, three chunks
+                                   ahead (-1 and -2: pass_threads 1024 only); 0 = the default (4) */
   float window_z;               /* PASS 1 windows: safety margin of the predicted k positions in
                                    binomial standard deviations; 0 = 8; < 0 = no windows */
   int32_t autotune;             /* 1: when num_buckets and the pass shape are left at 0, the first call of a

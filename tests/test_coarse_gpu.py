@@ -33,7 +33,7 @@ def test_coarse_exact(ctx, gen, assigner):
         assert st["active_buckets"] <= 256, st
 
 
-@pytest.mark.parametrize("shape", [(256, 8), (512, 2), (1024, 2), (1024, 4), (1024, -1)])
+@pytest.mark.parametrize("shape", [(256, 8), (512, 2), (1024, 2), (1024, 4), (1024, -1), (1024, -2)])
 def test_coarse_pass_shapes(ctx, shape):
     v = D.VALUE_GENERATORS["lognormal_f32"](N, 5)
     ks = D.ks_uniform(N, 6000, 6)

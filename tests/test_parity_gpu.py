@@ -247,3 +247,14 @@ def test_config4_learned(ctx, gen, seed):
     for a, kw in ((G.ASSIGNER_SAMPLED, {}), (G.ASSIGNER_LEARNED_PL, {"pl_knots": 256}),
                   (G.ASSIGNER_LEARNED_PL, {}), (G.ASSIGNER_LEARNED_MLP, {}), (G.ASSIGNER_AUTO, {})):
         assert_bits(run(ctx, v, ks, assigner=a, **kw), exp)
+
+
+def test_many_ks_unfused_between_steps(ctx):
+    """More than 65536 ks: the steps between the passes run as separate
+    launches (scan, locate, mode, children, relabel) instead of one CTA."""
+    n = 1 << 22
+    v = D.normal_f32(n, 71)
+    ks = D.ks_uniform(n, 70_000, 72)
+    ks[:3] = [1, n, n // 2]
+    for a in (G.ASSIGNER_SAMPLED, G.ASSIGNER_AUTO):
+        assert_bits(run(ctx, v, ks, assigner=a), orc.select(v, ks))
