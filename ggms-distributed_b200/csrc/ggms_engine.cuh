@@ -352,9 +352,8 @@ static int launch_small_select(Context* ctx, const InT* src, const Seg<K>* segs_
     GGMS_CU(cudaEventRecord(ctx->join2, ctx->side));
   }
   ++ctx->launches;
-  small_select<InT, SS_NT><<<ctx->sms * 2, SS_NT, sm, st>>>(src, segs_q, w.smalls, w.C, khead_q, w.knext,
-                                                            k_off, w.krank, w.kseg, w.kkey, caps.small_keys,
-                                                            caps);
+  GGMS_CU(launch_pdl(small_select<InT, SS_NT>, ctx->sms * 2, SS_NT, sm, st, src, segs_q, w.smalls, w.C, khead_q,
+                     w.knext, k_off, w.krank, w.kseg, w.kkey, caps.small_keys, caps));
   if (caps.tiny_keys) GGMS_CU(cudaStreamWaitEvent(st, ctx->join2, 0));
   return GGMS_OK;
 }
@@ -427,16 +426,17 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
 
     // ---- level-0 assigner
     const uint32_t S = p.S;
-    if (S >= CS_MIN_S) {  // sample and sort in one cluster launch
+    if (S >= CS_MIN_S) {  // draw the sample over the whole GPU, sort it in one cluster
       static bool cs_attr = false;
       if (!cs_attr) {
-        GGMS_CU(cudaFuncSetAttribute(asg_sample_sort_cluster<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        GGMS_CU(cudaFuncSetAttribute(asg_sort_cluster<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sizeof(ClusterSortSmem<K>)));
         cs_attr = true;
       }
-      ++ctx->launches;
-      asg_sample_sort_cluster<T><<<CS_CTAS, CS_NT, sizeof(ClusterSortSmem<K>), s>>>(d_in, n, S, p.seed,
-                                                                                 w.samp_sorted);
+      ctx->launches += 2;
+      GGMS_CU(launch_pdl(asg_sample<T>, cdiv(S, 256), 256, 0, s, d_in, n, S, p.seed, w.samp_raw));
+      GGMS_CU(launch_pdl(asg_sort_cluster<K>, CS_CTAS, CS_NT, sizeof(ClusterSortSmem<K>), s,
+                         (const K*)w.samp_raw, S, w.samp_sorted));
     } else {  // up to 4096 keys: draw them, then one CTA sorts them
       ctx->launches += 2;
       asg_sample<T><<<cdiv(S, 256), 256, 0, s>>>(d_in, n, S, p.seed, w.samp_raw);
@@ -452,8 +452,8 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     if (rc) return rc;
     if (p.assigner == GGMS_ASSIGNER_SAMPLED) {
       ++ctx->launches;
-      setup_sampled<K><<<1, SETUP_NT, sizeof(SetupSmem<K>), s>>>(w.samp_sorted, S, p.B, &w.asg[0],
-                                                                   &w.grid[0]);
+      GGMS_CU(launch_pdl(setup_sampled<K>, 1, SETUP_NT, sizeof(SetupSmem<K>), s, w.samp_sorted, S, p.B, &w.asg[0],
+                         &w.grid[0]));
     } else {
       // the sampled grid (fallback and judge) is built on a side stream while
       // the learned model's knots and statistics are computed: fork and join
@@ -472,28 +472,30 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
 
     // ---- PASS 1 windows
     prof_rec(prof, 7, s);
-    if (p.window_z >= 0.0f) {
+    const bool windows = p.window_z >= 0.0f;
+    if (windows) {
       ++ctx->launches;
-      l0_window<K><<<1, WIN_NT, l0_window_smem<K>(p.B), s>>>(w.samp_sorted, S, w.krank, nk, n, w.grid,
-                                                               w.C, p.window_z, w.win);
-    } else {
-      GGMS_CU(cudaMemsetAsync(w.win, 0, sizeof(Windows<K>), s));
+      GGMS_CU(launch_pdl(l0_window<K>, 1, WIN_NT, l0_window_smem<K>(p.B), s, w.samp_sorted, S, w.krank, nk, n,
+                         w.grid, w.C, p.window_z, w.win));
     }
 
     // ---- PASS 1: count
     const int grid_c = (int)p.ncta;
-    GGMS_CU(cudaMemsetAsync(w.hist0, 0, 4ull * p.B, s));
-    GGMS_CU(cudaMemsetAsync(w.aflag0, 0, 4ull * (p.B / 32) + 4ull * p.B, s));  // flags and k counts
+    // the histogram, the flags and k counts (and, without windows, the windows)
+    static_assert(sizeof(Windows<K>) % 4 == 0, "zeroed as words");
+    ++ctx->launches;
+    GGMS_CU(launch_pdl(zero_words, 8, 1024, 0, s, w.hist0, p.B, w.aflag0, p.B / 32 + p.B,
+                       windows ? (uint32_t*)nullptr : (uint32_t*)w.win, (uint32_t)(sizeof(Windows<K>) / 4)));
     prof_rec(prof, 1, s);
     ++ctx->launches;
-    pv->count<<<grid_c, pv->nt, l0_count_smem<T>(p.B, pv->nt, pv->unroll, p.ring_st[0]), s>>>(
-        d_in, n, w.grid, w.C, w.win, w.hist0, w.crow, p.ring_st[0]);
+    GGMS_CU(launch_pdl(pv->count, grid_c, pv->nt, l0_count_smem<T>(p.B, pv->nt, pv->unroll, p.ring_st[0]), s, d_in,
+                       n, w.grid, w.C, w.win, w.hist0, w.crow, p.ring_st[0]));
     prof_rec(prof, 2, s);
     if (nk <= L0_FUSED_MAX_KS) {
       // scan, locate and the coarse-mode decision in one CTA
       ++ctx->launches;
-      l0_between<K><<<1, 1024, l0_between_smem(p.B), s>>>(w.hist0, p.B, w.C, w.win, nk, w.krank, w.kseg, w.kbin,
-                                                           w.kcnt0, w.aflag0, w.ic, w.aflagc);
+      GGMS_CU(launch_pdl(l0_between<K>, 1, 1024, l0_between_smem(p.B), s, w.hist0, p.B, w.C, w.win, nk, w.krank,
+                         w.kseg, w.kbin, w.kcnt0, w.aflag0, w.ic, w.aflagc));
     } else {
       ++ctx->launches;
       l0_scan<K><<<1, 1024, 4u * p.B, s>>>(w.hist0, p.B, w.C, w.win, w.aflagc);
@@ -506,27 +508,26 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
                                                    w.kseg, w.kbin);
     }
     ++ctx->launches;
-    l0_children<K><<<cdiv(p.B, 256), 256, 0, s>>>(w.hist0, w.aflag0, p.B, w.grid, w.C, w.win, w.cmap0,
-                                                     w.segs[1], w.cursor[1], w.tiles[1], w.points,
-                                                     w.khead[1], w.smalls, w.bigs[1], caps, w.ic, w.aflagc,
-                                                     w.kcnt0, tiny_keys<K>(), w.tinies);
+    GGMS_CU(launch_pdl(l0_children<K>, cdiv(p.B, 256), 256, 0, s, w.hist0, w.aflag0, p.B, w.grid, w.C, w.win,
+                       w.cmap0, w.segs[1], w.cursor[1], w.tiles[1], w.points, w.khead[1], w.smalls, w.bigs[1], caps,
+                       w.ic, w.aflagc, w.kcnt0, tiny_keys<K>(), w.tinies));
     // the first refinement level runs only when a level-0 child needs it: the
     // kernel that relabels the ks after l0_children sets that condition
     cudaGraphConditionalHandle lev1 = 0;
     rc = level_handle(s, &lev1);
     if (rc) return rc;
     ++ctx->launches;
-    l0_relabel_bases<K><<<ctx->sms * 4, 256, 0, s>>>(w.cmap0, nk, w.kbin, w.kseg, w.kkey, w.points, w.C,
-                                                      w.segs[1], w.khead[1], w.knext, w.crow, p.B, p.ncta,
-                                                      caps, lev1);
+    GGMS_CU(launch_pdl(l0_relabel_bases<K>, ctx->sms * 4, 256, 0, s, w.cmap0, nk, w.kbin, w.kseg, w.kkey, w.points,
+                       w.C, w.segs[1], w.khead[1], w.knext, w.crow, p.B, p.ncta, caps, lev1));
     // ---- PASS 2: compact the buckets that still need refinement
     prof_rec(prof, 3, s);
     ++ctx->launches;
-    pv->compact<<<grid_c, pv->nt, l0_compact_smem<T>(p.B, pv->nt, pv->unroll, p.ring_st[1]), s>>>(
-        d_in, n, w.grid, w.C, w.win, w.cmap0, w.crow, w.cand[0], (uint64_t)n, p.ring_st[1], w.hist0);
+    GGMS_CU(launch_pdl(pv->compact, grid_c, pv->nt, l0_compact_smem<T>(p.B, pv->nt, pv->unroll, p.ring_st[1]), s,
+                       d_in, n, w.grid, w.C, w.win, w.cmap0, w.crow, w.cand[0], (uint64_t)n, p.ring_st[1],
+                       w.hist0));
     ++ctx->launches;  // one of the two PASS-2 kernels returns at once
-    pv->coarse<<<grid_c, pv->nt, l0_coarse_smem<T>(pv->nt, pv->unroll, p.ring_st[2]), s>>>(
-        d_in, n, w.grid, w.C, w.cmap0, w.crow, w.cand[0], (uint64_t)n, p.ring_st[2]);
+    GGMS_CU(launch_pdl(pv->coarse, grid_c, pv->nt, l0_coarse_smem<T>(pv->nt, pv->unroll, p.ring_st[2]), s, d_in,
+                       n, w.grid, w.C, w.cmap0, w.crow, w.cand[0], (uint64_t)n, p.ring_st[2]));
     prof_rec(prof, 4, s);
     {
       // level 0 also has warp-sized children (l0_children); the refinement
@@ -628,7 +629,9 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
     s->sample_size = (int32_t)p.S;
     s->bucket_max_over_mean = (float)pin_C->max_bucket0 / ((float)n / (float)p.B);
     s->model_imbalance = (p.assigner == GGMS_ASSIGNER_SAMPLED) ? 0.0f : ls.imbalance;
-    s->model_loss = (p.assigner == GGMS_ASSIGNER_SAMPLED) ? 0.0f : ls.loss;
+    s->model_loss = p.assigner == GGMS_ASSIGNER_SAMPLED        ? 0.0f
+                    : p.assigner == GGMS_ASSIGNER_LEARNED_MLP ? ls.mlp_loss
+                                                              : ls.loss;
     s->window_runs = (int32_t)pin_C->win_runs;
     if (!o.pad0) s->model_segments = (p.assigner == GGMS_ASSIGNER_SAMPLED || a_used.kind == GGMS_ASSIGNER_SAMPLED)
                                          ? 0 : (int32_t)ls.M;

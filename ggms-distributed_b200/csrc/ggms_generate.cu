@@ -9,9 +9,12 @@
 // only write (4 or 8 bytes per element, coalesced): HBM-write bound.
 //
 // The reference's tables (DistributedSMOS/generateProblems.cu:75-79, 438-446,
-// 509-513) give the kind numbering; the two generators that sort a cuRAND sample
-// (KILLER FLOATS / KILLER DOUBLES) are not restated here.
+// 509-513) give the kind numbering.  The two KILLER kinds sort their masked sample
+// (DistributedSMOS/generateProblems.cu:422-436, 493-507): that sort is CUB's device
+// radix sort over the bits the mask leaves, on the caller's stream, into
+// stream-ordered scratch (cudaMallocAsync / cudaFreeAsync).
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -106,6 +109,31 @@ __global__ void __launch_bounds__(256) gen_u32(uint32_t* __restrict__ out, Param
   }
 }
 
+// KILLER FLOATS / DOUBLES, step 1: the uniform draw of kind 0 with its exponent
+// masked away, as bit patterns (generateBucketKillerFloats masks with 0x80EFFFFF,
+// generateBucketKillerDoubles with 0x800FFFFFFFFFFFFF): subnormals and, for floats,
+// the lowest normal binade.
+__global__ void __launch_bounds__(256) killer_draw_f32(uint32_t* __restrict__ out, Params p) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += stride)
+    out[i] = __float_as_uint(unit24(draw(p.key0, i))) & 0x80EFFFFFu;
+}
+
+__global__ void __launch_bounds__(256) killer_draw_f64(unsigned long long* __restrict__ out, Params p) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += stride)
+    out[i] = (unsigned long long)__double_as_longlong((double)(draw(p.key0, i) >> 11) * 0x1p-53) &
+             0x800FFFFFFFFFFFFFull;
+}
+
+// Step 3: the first slots take the powers of two 2^lo .. 2^(lo + count - 1), built
+// from their exponent fields (bias: 127 for float, 1023 for double).
+template <typename U, int MANT, int BIAS>
+__global__ void __launch_bounds__(256) killer_powers(U* __restrict__ out, int lo, int count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) out[i] = (U)(lo + i + BIAS) << MANT;
+}
+
 uint64_t gcd64(uint64_t a, uint64_t b) {
   while (b) {
     const uint64_t t = a % b;
@@ -145,21 +173,59 @@ int grid_for(int64_t n) {
 
 constexpr int64_t kPermMaxN = (int64_t)1 << 32;
 
+// draw (kernel) -> sort the pattern's low `bits` bits (the others are zero) ->
+// powers of two at the front; the scratch holds the draw and CUB's temporaries.
+template <typename U, int MANT, int BIAS>
+int killer(U* d_out, int64_t n, uint64_t seed, cudaStream_t st, int bits, int lo, int npow) {
+  size_t tmp_bytes = 0;
+  if (cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, (const U*)nullptr, (U*)nullptr, (int)n, 0, bits,
+                                     st) != cudaSuccess)
+    return GGMS_E_CUDA;
+  const size_t keys_bytes = ((size_t)n * sizeof(U) + 255) & ~(size_t)255;
+  void* scratch = nullptr;
+  if (cudaMallocAsync(&scratch, keys_bytes + tmp_bytes, st) != cudaSuccess) return GGMS_E_CUDA;
+  U* keys = (U*)scratch;
+  if constexpr (sizeof(U) == 4)
+    killer_draw_f32<<<grid_for(n), kThreads, 0, st>>>(keys, make_params(n, 0, seed));
+  else
+    killer_draw_f64<<<grid_for(n), kThreads, 0, st>>>(keys, make_params(n, 0, seed));
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cub::DeviceRadixSort::SortKeys((uint8_t*)scratch + keys_bytes, tmp_bytes, keys, d_out, (int)n, 0, bits,
+                                       st);
+  const int count = n < npow ? (int)n : npow;  // the reference writes all npow slots
+  if (e == cudaSuccess) {
+    killer_powers<U, MANT, BIAS><<<(count + 255) / 256, 256, 0, st>>>(d_out, lo, count);
+    e = cudaGetLastError();
+  }
+  const cudaError_t f = cudaFreeAsync(scratch, st);
+  return e == cudaSuccess && f == cudaSuccess ? GGMS_OK : GGMS_E_CUDA;
+}
+
+constexpr int64_t kKillerMaxN = ((int64_t)1 << 31) - 1;  // CUB's item count is an int here
+
 }  // namespace ggms_gen
 
 using namespace ggms_gen;
 
 extern "C" GGMS_API int ggms_generate_f32(float* d_out, int64_t n, int kind, uint64_t seed, void* stream) {
   if (!d_out || n <= 0 || kind < 0 || kind > 9) return GGMS_E_INVALID_ARG;
-  if (kind == 2) return GGMS_E_UNSUPPORTED;
   if ((kind == 6 || kind == 8) && n > kPermMaxN) return GGMS_E_UNSUPPORTED;
+  if (kind == 2) {  // KILLER FLOATS: 2^-126 .. 2^126 in the first 253 slots
+    if (n > kKillerMaxN) return GGMS_E_UNSUPPORTED;
+    return killer<uint32_t, 23, 127>((uint32_t*)d_out, n, seed, (cudaStream_t)stream, 24, -126, 253);
+  }
   gen_f32<<<grid_for(n), kThreads, 0, (cudaStream_t)stream>>>(d_out, make_params(n, kind, seed));
   return launch_status();
 }
 
 extern "C" GGMS_API int ggms_generate_f64(double* d_out, int64_t n, int kind, uint64_t seed, void* stream) {
   if (!d_out || n <= 0 || kind < 0 || kind > 2) return GGMS_E_INVALID_ARG;
-  if (kind == 2) return GGMS_E_UNSUPPORTED;
+  if (kind == 2) {  // KILLER DOUBLES: 2^-1022 .. 2^1022 in the first 2045 slots
+    if (n > kKillerMaxN) return GGMS_E_UNSUPPORTED;
+    return killer<unsigned long long, 52, 1023>((unsigned long long*)d_out, n, seed, (cudaStream_t)stream, 52,
+                                                -1022, 2045);
+  }
   gen_f64<<<grid_for(n), kThreads, 0, (cudaStream_t)stream>>>(d_out, make_params(n, kind, seed));
   return launch_status();
 }

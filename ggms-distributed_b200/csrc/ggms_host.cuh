@@ -11,6 +11,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <utility>
 #include <vector>
 
 #include "ggms_internal.cuh"
@@ -143,6 +144,25 @@ static void destroy_context(Context* c) {
     if (e) cudaEventDestroy(e);
   cudaSetDevice(prev);
   delete c;
+}
+
+// Launch on stream s with programmatic stream serialization: the kernel may be
+// scheduled while the kernel before it on the stream is finishing (every
+// kernel of this library waits for its predecessor first, pdl_entry).
+template <typename... P, typename... A>
+static cudaError_t launch_pdl(void (*k)(P...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                              A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
 }
 
 // The side stream and its fork / join events (created on first use).

@@ -46,6 +46,18 @@ static __device__ unsigned long long ggms_trace_buf[64];
 
 namespace ggms {
 
+// ------------------------------------------------------------------ programmatic dependent launch
+// The host launches the kernels of one call with programmatic stream
+// serialization, so that a kernel can be scheduled while the one before it on
+// the stream is still finishing.  Every kernel therefore begins here: it waits
+// for the grids it depends on to complete (their memory visible) before it
+// reads or writes anything, then lets the next kernel begin launching.  For a
+// kernel launched without that attribute both instructions are no-ops.
+__device__ __forceinline__ void pdl_entry() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ------------------------------------------------------------------ key traits
 template <typename T> struct KeyOf;
 template <> struct KeyOf<float> {

@@ -125,11 +125,25 @@ __device__ void block_inclusive_scan_global(uint32_t* data, uint32_t cnt, uint32
   __syncthreads();
 }
 
+// Zeroes up to three ranges of 32-bit words (a null range is skipped): the
+// level-0 histogram, flags and k counts, and the windows when there are none.
+// In the kernel chain instead of memset nodes, which would end the chain's
+// programmatic launches.
+__global__ void zero_words(uint32_t* a, uint32_t na, uint32_t* b, uint32_t nb, uint32_t* c, uint32_t nc) {
+  pdl_entry();
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
+  for (uint32_t i = t; i < na; i += st) a[i] = 0u;
+  for (uint32_t i = t; i < nb; i += st) b[i] = 0u;
+  if (c)
+    for (uint32_t i = t; i < nc; i += st) c[i] = 0u;
+}
+
 // ------------------------------------------------------------------ ks
 // 1-based k-th largest -> 0-based rank in ascending order (the reference's
 // wrappers compute length - k + 1, 1-based smallest: bucketMultiselect.cu:860-861).
 __global__ void k_init_single(const uint32_t* __restrict__ ks, uint32_t nk, uint64_t n,
                               uint32_t* k_rank, uint32_t* k_seg, Counters* C) {
+  pdl_entry();
   GGMS_TRACE(0);
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nk) return;
@@ -146,6 +160,7 @@ __global__ void k_init_single(const uint32_t* __restrict__ ks, uint32_t nk, uint
 
 // top-k: k_i = i + 1 (the (i+1)-th largest), i.e. ascending rank n - 1 - i
 __global__ void k_init_topk(uint32_t nk, uint64_t n, uint32_t* k_rank, uint32_t* k_seg) {
+  pdl_entry();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nk) return;
   k_rank[i] = (uint32_t)(n - 1u - i);
@@ -156,6 +171,7 @@ __global__ void k_init_topk(uint32_t nk, uint64_t n, uint32_t* k_rank, uint32_t*
 template <typename T>
 __global__ void asg_sample(const T* __restrict__ in, uint64_t n, uint32_t S, uint64_t seed,
                            typename KeyOf<T>::K* out) {
+  pdl_entry();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= S) return;
   uint64_t h = mix64(seed ^ mix64((uint64_t)i + 0x632BE59BD9B4E019ull));
@@ -166,6 +182,7 @@ __global__ void asg_sample(const T* __restrict__ in, uint64_t n, uint32_t S, uin
 // Bitonic sort of one chunk of CH keys per CTA in shared memory.
 template <typename K, int CH, int NT>
 __global__ __launch_bounds__(NT) void asg_sort_chunks(const K* __restrict__ in, K* out, uint32_t S) {
+  pdl_entry();
   __shared__ K s[CH];
   const uint32_t base = blockIdx.x * CH;
   const uint32_t cnt = min((uint32_t)CH, S - base);
@@ -194,15 +211,25 @@ __global__ __launch_bounds__(NT) void asg_sort_chunks(const K* __restrict__ in, 
   for (uint32_t i = threadIdx.x; i < cnt; i += NT) out[base + i] = s[i];
 }
 
-// Sample and sort in one launch of one thread-block cluster (S >= 8192 keys).
-// CTA c of the cluster draws sample keys [c * S/8, (c + 1) * S/8) straight from
-// the input (the positions asg_sample draws) into its shared memory; then an
-// LSD radix sort with 8-bit digits runs over the whole cluster: per digit
-// pass, every warp ranks its keys stably (32 keys at a time; the lanes that
-// share a digit are found with 8 ballots, no atomics), the CTAs exchange their
-// 256 digit counts through distributed shared memory, and every key is stored
-// straight into the shared memory of the CTA that owns its new position.  A
-// pass in which every key has the same digit is skipped (the permutation is
+// Sort of a drawn sample (S >= 8192 keys, asg_sample drew it: a wide grid
+// reaches the random positions far faster than 8 SMs would) in one launch of
+// one thread-block cluster.  CTA c loads sample keys [c * S/8, (c + 1) * S/8)
+// into its shared memory; then an LSD radix sort with 8-bit digits runs over
+// the whole cluster.  Per digit pass:
+//   1. every warp ranks its keys stably (32 keys at a time; the lanes that
+//      share a digit are found with 8 ballots, no atomics);
+//   2. the CTAs read each other's 256 digit counts through distributed shared
+//      memory: every CTA learns where its keys of each digit start, both in its
+//      own digit-grouped order and in the cluster's next order;
+//   3. each CTA groups its keys by digit in its own shared memory (random
+//      stores stay on the SM);
+//   4. each CTA copies its grouped keys to their owners: thread i moves key i,
+//      so a warp's 32 stores go to consecutive positions of one or two digit
+//      runs -- whole lines over the SM-to-SM network instead of one 4- or
+//      8-byte transaction per key.
+// Two cluster barriers per pass: counts visible (before 2) and the next order
+// complete (after 4); every key is read out of the current order in step 1,
+// before the first barrier, so step 4 may overwrite it.  A pass in which every key has the same digit is skipped (the permutation is
 // the identity).  4 passes for 32-bit keys, 8 for 64-bit ones; the sorted
 // sample is written out with coalesced stores.
 namespace cgx = cooperative_groups;
@@ -213,27 +240,28 @@ constexpr uint32_t CS_MAX_PER = 65536u / CS_CTAS;      // keys per CTA at S = 65
 
 template <typename K>
 struct ClusterSortSmem {
-  K a[CS_MAX_PER];                 // keys in the current order (this CTA's share)
-  K b[CS_MAX_PER];                 // the next pass's order, written by every CTA
+  K a[CS_MAX_PER];                 // this CTA's share of the current order
+  K b[CS_MAX_PER];                 // this CTA's keys grouped by the pass's digit
   uint32_t hist[CS_NT / 32][256];  // per warp: digit counts, then their prefixes over the warps
   uint32_t ccnt[256];              // this CTA's digit counts (read by the cluster)
   uint32_t gbase[256];             // first position of (digit, this CTA) in the next order
-  uint32_t red[33];
+  uint32_t lbase[256];             // first position of the digit in b
+  uint32_t red[2][8];
   uint32_t skip;
 };
 
-template <typename T>
+template <typename K>
 __global__ void __cluster_dims__(CS_CTAS, 1, 1) __launch_bounds__(CS_NT)
-asg_sample_sort_cluster(const T* __restrict__ in, uint64_t n, uint32_t S, uint64_t seed,
-                        typename KeyOf<T>::K* sorted) {
-  using K = typename KeyOf<T>::K;
+asg_sort_cluster(const K* __restrict__ drawn, uint32_t S, K* sorted) {
+  pdl_entry();
   constexpr int KB = (int)sizeof(K) * 8;
   constexpr int KPT_MAX = CS_MAX_PER / CS_NT;          // 8
   extern __shared__ __align__(128) uint8_t smem_raw[];
   ClusterSortSmem<K>& sm = *reinterpret_cast<ClusterSortSmem<K>*>(smem_raw);
   cgx::cluster_group cluster = cgx::this_cluster();
   const uint32_t me = cluster.block_rank();
-  const uint32_t per = S / CS_CTAS;                    // keys per CTA
+  const uint32_t per = S / CS_CTAS;                    // keys per CTA: a power of two
+  const uint32_t per_sh = (uint32_t)__ffs((int)per) - 1u;
   const uint32_t kpt = per / CS_NT;                    // keys per thread, 1..8
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   // warp w owns positions [w * 32 * kpt, (w + 1) * 32 * kpt) of this CTA's
@@ -241,21 +269,19 @@ asg_sample_sort_cluster(const T* __restrict__ in, uint64_t n, uint32_t S, uint64
   const uint32_t wbase = warp * 32u * kpt;
   GGMS_TRACE(1);
   K* A = sm.a;
-  K* Bv = sm.b;
-  for (uint32_t r = 0; r < kpt; ++r) {
-    const uint32_t i = me * per + wbase + r * 32u + lane;   // sample index
-    const uint64_t h = mix64(seed ^ mix64((uint64_t)i + 0x632BE59BD9B4E019ull));
-    A[wbase + r * 32u + lane] = KeyOf<T>::to(in[__umul64hi(h, n)]);
-  }
+  for (uint32_t i = tid; i < per; i += CS_NT) A[i] = drawn[(size_t)me * per + i];
+  __syncthreads();
   const uint32_t lt = lanemask_lt();
   for (int sh = 0; sh < KB; sh += 8) {
     for (uint32_t d = lane; d < 256u; d += 32u) sm.hist[warp][d] = 0u;
     __syncwarp();
+    K key[KPT_MAX];
     uint32_t dg[KPT_MAX], off[KPT_MAX];
 #pragma unroll
     for (int r = 0; r < KPT_MAX; ++r) {
       if ((uint32_t)r >= kpt) break;
-      const uint32_t d = (uint32_t)(A[wbase + r * 32u + lane] >> sh) & 255u;
+      key[r] = A[wbase + r * 32u + lane];
+      const uint32_t d = (uint32_t)(key[r] >> sh) & 255u;
       uint32_t peers = FULL;
 #pragma unroll
       for (int b = 0; b < 8; ++b) {
@@ -287,7 +313,7 @@ asg_sample_sort_cluster(const T* __restrict__ in, uint64_t n, uint32_t S, uint64
       for (int j = 0; j < 8; ++j) { sm.hist[q * 8 + j][d] = run; run += c[j]; }
       if (q == 3u) sm.ccnt[d] = inc;
     }
-    cluster.sync();  // every CTA's digit counts are visible
+    cluster.sync();  // (1) every CTA's digit counts are visible
     if (tid < 256u) {
       uint32_t tot = 0, before = 0;
 #pragma unroll
@@ -296,32 +322,44 @@ asg_sample_sort_cluster(const T* __restrict__ in, uint64_t n, uint32_t S, uint64
         tot += v;
         before += ((uint32_t)c < me) ? v : 0u;
       }
-      // exclusive scan of the totals over the 256 digits (8 warps)
-      const uint32_t inc = warp_incl_scan_u32(tot, lane);
-      if (lane == 31) sm.red[warp] = inc;
+      const uint32_t mine = sm.ccnt[tid];
+      // exclusive scans over the 256 digits (8 warps): the totals and this CTA's counts
+      const uint32_t inc_t = warp_incl_scan_u32(tot, lane);
+      const uint32_t inc_m = warp_incl_scan_u32(mine, lane);
+      if (lane == 31) {
+        sm.red[0][warp] = inc_t;
+        sm.red[1][warp] = inc_m;
+      }
       if (tid == 0) sm.skip = 0u;
       asm volatile("bar.sync 1, 256;" ::: "memory");
-      uint32_t pre = inc - tot;
-      for (uint32_t w = 0; w < warp; ++w) pre += sm.red[w];
-      sm.gbase[tid] = pre + before;
+      uint32_t pre_t = inc_t - tot, pre_m = inc_m - mine;
+      for (uint32_t w = 0; w < warp; ++w) {
+        pre_t += sm.red[0][w];
+        pre_m += sm.red[1][w];
+      }
+      sm.gbase[tid] = pre_t + before;
+      sm.lbase[tid] = pre_m;
       if (tot == S) sm.skip = 1u;  // every key has this digit: nothing moves
     }
     __syncthreads();
-    if (!sm.skip) {
+    const bool skip = sm.skip != 0u;
+    if (!skip) {
 #pragma unroll
       for (int r = 0; r < KPT_MAX; ++r) {
         if ((uint32_t)r >= kpt) break;
-        const uint32_t pos = sm.gbase[dg[r]] + sm.hist[warp][dg[r]] + off[r];
-        const K key = A[wbase + r * 32u + lane];
-        *cluster.map_shared_rank(&Bv[pos % per], pos / per) = key;
+        sm.b[sm.lbase[dg[r]] + sm.hist[warp][dg[r]] + off[r]] = key[r];
       }
     }
-    cluster.sync();  // the next order is complete; the counts have been read
-    if (!sm.skip) {
-      K* t = A;
-      A = Bv;
-      Bv = t;
+    __syncthreads();  // b is complete (the cluster's a was read into registers before (1))
+    if (!skip) {
+      for (uint32_t i = tid; i < per; i += CS_NT) {
+        const K k = sm.b[i];
+        const uint32_t d = (uint32_t)(k >> sh) & 255u;
+        const uint32_t pos = sm.gbase[d] + (i - sm.lbase[d]);
+        *cluster.map_shared_rank(&A[pos & (per - 1u)], pos >> per_sh) = k;
+      }
     }
+    cluster.sync();  // (2) the next order is complete; the counts have been read
   }
   K* out = sorted + (size_t)me * per;
   for (uint32_t i = tid; i < per; i += CS_NT) out[i] = A[i];
@@ -828,6 +866,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_count(const T* __res
                                               const Windows<typename KeyOf<T>::K>* __restrict__ Wg,
                                               uint32_t* __restrict__ hist0, uint32_t* __restrict__ crow,
                                               uint32_t ring_st) {
+  pdl_entry();
   using K = typename KeyOf<T>::K;
   constexpr int EPV = Vec16<T>::N;
   extern __shared__ __align__(128) uint8_t smem[];
@@ -998,6 +1037,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_count(const T* __res
 template <typename K>
 __global__ __launch_bounds__(1024) void l0_scan(uint32_t* hist0, uint32_t B, Counters* C,
                                                 const Windows<K>* __restrict__ Wg, uint32_t* aflagc) {
+  pdl_entry();
   extern __shared__ uint32_t sh_counts[];
   __shared__ uint32_t w[72];
   __shared__ uint32_t mx;
@@ -1051,6 +1091,7 @@ __global__ void lvl_locate_rows(const uint32_t* __restrict__ rows, uint32_t row_
                                 uint32_t* k_rank, const uint32_t* __restrict__ k_seg,
                                 uint32_t* k_bin, uint32_t* aflag, uint32_t flag_words,
                                 Counters* C, uint32_t* kcnt = nullptr) {
+  pdl_entry();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nk) return;
   const uint32_t s = k_seg[i];
@@ -1144,6 +1185,7 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
                             K* points, uint32_t* khead1, uint32_t* smalls, uint32_t* bigs1, Caps caps,
                             const uint32_t* __restrict__ ic, const uint32_t* __restrict__ aflagc,
                             const uint32_t* __restrict__ kcnt0, uint32_t tiny_keys, uint32_t* tinies) {
+  pdl_entry();
   // the key-range searches evaluate the grid ~64 times per bucket: keep it in
   // shared memory (every thread helps load it before any returns)
   __shared__ uint2 s1[GRID_T1];
@@ -1189,6 +1231,7 @@ __global__ void lvl_relabel(const uint32_t* __restrict__ cmap, uint32_t row_len,
                             const uint32_t* __restrict__ k_bin, uint32_t* k_seg, K* k_key,
                             const K* __restrict__ points, Counters* C,
                             const Seg<K>* __restrict__ segs_q, uint32_t* khead_q, uint32_t* knext) {
+  pdl_entry();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nk) return;
   const uint32_t s = k_seg[i];
@@ -1212,6 +1255,7 @@ __global__ __launch_bounds__(1024) void l0_between(uint32_t* hist0, uint32_t B, 
                                                    uint32_t* k_rank, const uint32_t* __restrict__ k_seg,
                                                    uint32_t* k_bin, uint32_t* kcnt0, uint32_t* aflag0,
                                                    uint32_t* ic, uint32_t* aflagc) {
+  pdl_entry();
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ Windows<K> W;
   __shared__ uint32_t red[72];
@@ -1330,6 +1374,7 @@ __device__ __forceinline__ void bases_body(uint32_t* crow, uint32_t B, uint32_t 
 template <typename K>
 __global__ void l0_bases(uint32_t* crow, uint32_t B, uint32_t ncta, const Seg<K>* __restrict__ segs1,
                          const Counters* __restrict__ C, Caps caps) {
+  pdl_entry();
   bases_body<K>(crow, B, ncta, segs1, C, caps);
 }
 
@@ -1344,6 +1389,7 @@ __global__ void l0_relabel_bases(const uint32_t* __restrict__ cmap0, uint32_t nk
                                  const K* __restrict__ points, Counters* C, const Seg<K>* __restrict__ segs1,
                                  uint32_t* khead1, uint32_t* knext, uint32_t* crow, uint32_t B, uint32_t ncta,
                                  Caps caps, cudaGraphConditionalHandle lev1) {
+  pdl_entry();
   if (lev1 && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(lev1, C->nbig[1] ? 1u : 0u);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nk; i += gridDim.x * blockDim.x) {
     const uint32_t s = k_seg[i];
@@ -1381,6 +1427,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
                                                 const uint32_t* __restrict__ crow,
                                                 typename KeyOf<T>::K* dst, uint64_t dst_cap,
                                                 uint32_t ring_st, const uint32_t* __restrict__ I0) {
+  pdl_entry();
   using K = typename KeyOf<T>::K;
   constexpr int EPV = Vec16<T>::N;
   if (C->coarse) return;  // l0_compact_coarse copies this call's groups
@@ -1413,87 +1460,108 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
     }
   }
   __shared__ unsigned long long hot_mass_s;
-  for (uint32_t w = threadIdx.x; w < HOT_WORDS; w += NT) hot[w] = 0u;
-  if (threadIdx.x == 0) hot_mass_s = 0ull;
-  __syncthreads();
-  if (warp == 0) {  // exclusive prefix of the per-word counts (B / 32 <= 1024 words)
-    uint32_t run = 0;
-    for (uint32_t w0 = 0; w0 < B / 32; w0 += 32) {
-      const uint32_t v = wpre[w0 + lane];
-      uint32_t inc = v;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(FULL, inc, o);
-        if ((int)lane >= o) inc += t;
-      }
-      wpre[w0 + lane] = run + inc - v;
-      run += __shfl_sync(FULL, inc, 31);
-    }
-    if (lane == 0) wpre[B / 32] = run;
+  __shared__ K run_lo[L0_RUNS], run_span[L0_RUNS];
+  __shared__ uint32_t nruns_s, ncopied_s;
+  if (threadIdx.x == 0) {
+    hot_mass_s = 0ull;
+    nruns_s = 0u;
+    ncopied_s = 0u;
   }
   __syncthreads();
-  const uint32_t ncopied = wpre[B / 32];  // read before the queues reuse the table
+  // With windows and no gap bucket to copy, every copied bucket lies inside a
+  // window run: when the runs are narrow (tight), their key ranges (few, known
+  // exactly) are the key test, and the hot cells below are not needed (every
+  // thread decides the same from W and the mask).
+  bool use_win = W.on != 0u && W.tight != 0u;
+  for (uint32_t g = 0; g <= L0_WIN && use_win; ++g)
+    if (g <= W.R && W.gb0[g] <= W.gb1[g] && ((amask[W.gb0[g] >> 5] >> (W.gb0[g] & 31)) & 1u))
+      use_win = false;
   // with windows, a key outside every run belongs to its gap's bucket
   auto bmap = [&](uint32_t b) { return W.on ? win_map(W, b) : b; };
-  {
-    // a cell is hot when a copied bucket lies in [bucket of its first key,
-    // bucket of its last key] (the grid and bmap are monotone in the key)
-    auto rank = [&](uint32_t b) {  // copied buckets below b, b <= B
-      const uint32_t w = b >> 5;
-      return (b & 31) ? wpre[w] + __popc(amask[w] & ((1u << (b & 31)) - 1u)) : wpre[w];
-    };
-    const K dmax = (K)(gv.gmax - gv.origin);
-    unsigned long long mass = 0;  // keys of this thread's hot cells (the buckets they span, from PASS 1)
-    for (uint32_t c = threadIdx.x; c < ncell; c += NT) {
-      const K d0 = (K)c << gv.sh1;
-      const K d1 = (c + 1u < ncell) ? (K)(((K)(c + 1u) << gv.sh1) - 1u) : dmax;
-      const uint32_t lo = bmap(min(grid_eval<K>(gv, (K)(gv.origin + d0)), B - 1u));
-      const uint32_t hi = bmap(min(grid_eval<K>(gv, (K)(gv.origin + min(d1, dmax))), B - 1u));
-      if (rank(hi + 1u) != rank(lo)) {
-        atomicOr(&hot[c >> 5], 1u << (c & 31));
-        mass += I0[hi] - (lo ? I0[lo - 1] : 0u);
+  if (use_win) {
+    // the keys past the main part are tested by their bucket alone
+    for (uint32_t w = threadIdx.x; w < HOT_WORDS; w += NT) hot[w] = FULL;
+  } else {
+    for (uint32_t w = threadIdx.x; w < HOT_WORDS; w += NT) hot[w] = 0u;
+    if (warp == 0) {  // exclusive prefix of the per-word counts (B / 32 <= 1024 words)
+      uint32_t run = 0;
+      for (uint32_t w0 = 0; w0 < B / 32; w0 += 32) {
+        const uint32_t v = wpre[w0 + lane];
+        uint32_t inc = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t t = __shfl_up_sync(FULL, inc, o);
+          if ((int)lane >= o) inc += t;
+        }
+        wpre[w0 + lane] = run + inc - v;
+        run += __shfl_sync(FULL, inc, 31);
+      }
+      if (lane == 0) {
+        wpre[B / 32] = run;
+        ncopied_s = run;
       }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mass += __shfl_xor_sync(FULL, mass, o);
-    if (lane == 0 && mass) atomicAdd(&hot_mass_s, mass);  // buckets shared by two cells count twice
-  }
-  __syncthreads();
-  // Maximal runs of hot cells as key intervals [lo, lo + span]; with at most
-  // L0_RUNS of them the cell test becomes a few compares in registers.
-  __shared__ K run_lo[L0_RUNS], run_span[L0_RUNS];
-  __shared__ uint32_t nruns_s;
-  if (threadIdx.x == 0) {
-    uint32_t nr = 0, start = 0;
-    bool in_run = false;
-    auto record = [&](uint32_t c0, uint32_t c1) {
-      if (nr < L0_RUNS) {
-        const K lo = (c0 == 0) ? (K)0 : (K)(gv.origin + ((K)c0 << gv.sh1));
-        const K hi = (c1 + 1u >= ncell) ? key_max<K>() : (K)(gv.origin + ((K)(c1 + 1u) << gv.sh1) - 1u);
-        run_lo[nr] = lo;
-        run_span[nr] = (K)(hi - lo);
-      }
-      ++nr;
-    };
-    for (uint32_t w = 0; w < HOT_WORDS && nr <= L0_RUNS; ++w) {
-      const uint32_t bits = hot[w];
-      if ((!in_run && bits == 0u) || (in_run && bits == FULL)) continue;
-      for (uint32_t b = 0; b < 32; ++b) {
-        const uint32_t c = w * 32 + b;
-        const bool hb = c < ncell && ((bits >> b) & 1u);
-        if (hb && !in_run) {
-          in_run = true;
-          start = c;
-        } else if (!hb && in_run) {
-          in_run = false;
-          record(start, c - 1u);
+    __syncthreads();
+    {
+      // a cell is hot when a copied bucket lies in [bucket of its first key,
+      // bucket of its last key] (the grid and bmap are monotone in the key)
+      auto rank = [&](uint32_t b) {  // copied buckets below b, b <= B
+        const uint32_t w = b >> 5;
+        return (b & 31) ? wpre[w] + __popc(amask[w] & ((1u << (b & 31)) - 1u)) : wpre[w];
+      };
+      const K dmax = (K)(gv.gmax - gv.origin);
+      unsigned long long mass = 0;  // keys of this thread's hot cells (the buckets they span, from PASS 1)
+      for (uint32_t c = threadIdx.x; c < ncell; c += NT) {
+        const K d0 = (K)c << gv.sh1;
+        const K d1 = (c + 1u < ncell) ? (K)(((K)(c + 1u) << gv.sh1) - 1u) : dmax;
+        const uint32_t lo = bmap(min(grid_eval<K>(gv, (K)(gv.origin + d0)), B - 1u));
+        const uint32_t hi = bmap(min(grid_eval<K>(gv, (K)(gv.origin + min(d1, dmax))), B - 1u));
+        if (rank(hi + 1u) != rank(lo)) {
+          atomicOr(&hot[c >> 5], 1u << (c & 31));
+          mass += I0[hi] - (lo ? I0[lo - 1] : 0u);
         }
       }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) mass += __shfl_xor_sync(FULL, mass, o);
+      if (lane == 0 && mass) atomicAdd(&hot_mass_s, mass);  // buckets shared by two cells count twice
     }
-    if (in_run) record(start, ncell - 1u);
-    nruns_s = nr;
+    __syncthreads();
+    // Maximal runs of hot cells as key intervals [lo, lo + span]; with at most
+    // L0_RUNS of them the cell test becomes a few compares in registers.
+    if (threadIdx.x == 0) {
+      uint32_t nr = 0, start = 0;
+      bool in_run = false;
+      auto record = [&](uint32_t c0, uint32_t c1) {
+        if (nr < L0_RUNS) {
+          const K lo = (c0 == 0) ? (K)0 : (K)(gv.origin + ((K)c0 << gv.sh1));
+          const K hi = (c1 + 1u >= ncell) ? key_max<K>() : (K)(gv.origin + ((K)(c1 + 1u) << gv.sh1) - 1u);
+          run_lo[nr] = lo;
+          run_span[nr] = (K)(hi - lo);
+        }
+        ++nr;
+      };
+      for (uint32_t w = 0; w < HOT_WORDS && nr <= L0_RUNS; ++w) {
+        const uint32_t bits = hot[w];
+        if ((!in_run && bits == 0u) || (in_run && bits == FULL)) continue;
+        for (uint32_t b = 0; b < 32; ++b) {
+          const uint32_t c = w * 32 + b;
+          const bool hb = c < ncell && ((bits >> b) & 1u);
+          if (hb && !in_run) {
+            in_run = true;
+            start = c;
+          } else if (!hb && in_run) {
+            in_run = false;
+            record(start, c - 1u);
+          }
+        }
+      }
+      if (in_run) record(start, ncell - 1u);
+      nruns_s = nr;
+    }
   }
   __syncthreads();
+  const uint32_t ncopied = ncopied_s;
+  GGMS_TRACE(33);
 
   const uint64_t gtid = (uint64_t)blockIdx.x * NT + threadIdx.x;
   const uint64_t gstride = (uint64_t)gridDim.x * NT;
@@ -1522,15 +1590,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
   K* wq = reinterpret_cast<K*>(wpre) + (threadIdx.x >> 5) * WQ_DEPTH;
   uint32_t qn = 0;  // warp-uniform
 
-  // every lane runs the same number of rounds, so the warp stays converged.
-  // With windows and no gap bucket to copy, every copied bucket lies inside a
-  // window run: when the runs are narrow (tight), their key ranges (few, known
-  // exactly) are the test.
-  GGMS_TRACE(33);
-  bool use_win = W.on != 0u && W.tight != 0u;
-  for (uint32_t g = 0; g <= L0_WIN && use_win; ++g)
-    if (g <= W.R && W.gb0[g] <= W.gb1[g] && ((amask[W.gb0[g] >> 5] >> (W.gb0[g] & 31)) & 1u))
-      use_win = false;
+  // every lane runs the same number of rounds, so the warp stays converged
   const uint32_t nruns = nruns_s;
   auto runs = [&](auto rc, bool win) {
     constexpr uint32_t R = decltype(rc)::value;
@@ -1622,6 +1682,7 @@ template <typename K>
 __global__ void l0_mode_ks(const uint32_t* __restrict__ I, const uint32_t* __restrict__ aflag0, uint32_t B,
                            const Windows<K>* __restrict__ Wg, Counters* C, uint32_t* ic, uint32_t* aflagc,
                            uint32_t nk, uint32_t* k_rank, const uint32_t* __restrict__ k_seg, uint32_t* k_bin) {
+  pdl_entry();
   __shared__ uint32_t tot;
   GGMS_TRACE(38);
   if (threadIdx.x == 0) tot = 0u;
@@ -1665,6 +1726,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact_coarse(const
                                                        const uint32_t* __restrict__ crow,
                                                        typename KeyOf<T>::K* dst, uint64_t dst_cap,
                                                        uint32_t ring_st) {
+  pdl_entry();
   using K = typename KeyOf<T>::K;
   constexpr int EPV = Vec16<T>::N;
   constexpr int DU = coarse_du(UNROLL);
@@ -1833,6 +1895,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact_coarse(const
 // Gate of a refinement level inside a captured CUDA graph: the level (an IF
 // node) runs only while every level so far had segments to refine.
 __global__ void lvl_gate(Counters* C, int p, cudaGraphConditionalHandle h) {
+  pdl_entry();
   GGMS_TRACE(41 + p);
   if (C->nbig[p] == 0u) C->done = 1u;
   cudaGraphSetConditional(h, C->done ? 0u : 1u);
@@ -1842,6 +1905,7 @@ __global__ void lvl_gate(Counters* C, int p, cudaGraphConditionalHandle h) {
 // tiny_select finished have none); reset the child pool's counters
 __global__ void lvl_prep(uint32_t* rows, uint32_t* aflag, const uint32_t* __restrict__ bigs, Counters* C,
                          int p, Caps caps) {
+  pdl_entry();
   const uint32_t nb = min(C->nbig[p], caps.segs);
   for (uint32_t j = blockIdx.x; j < nb; j += gridDim.x) {
     const uint32_t sid = bigs[j];
@@ -1896,6 +1960,7 @@ __global__ __launch_bounds__(1024) void seg_sample(const T* __restrict__ in, Seg
                                                    const uint32_t* __restrict__ qsegs,
                                                    const Counters* __restrict__ C, uint32_t cap_q,
                                                    typename KeyOf<T>::K* qtab, uint16_t* qdir, uint64_t seed) {
+  pdl_entry();
   using K = typename KeyOf<T>::K;
   __shared__ K sv[QSAMP];
   const uint32_t tid = threadIdx.x;
@@ -1963,6 +2028,7 @@ __global__ __launch_bounds__(NT) void lvl_count(const InT* __restrict__ src,
                                                Counters* C, int p, uint32_t* rows, Caps caps,
                                                const typename KeyOf<InT>::K* __restrict__ qtab,
                                                const uint16_t* __restrict__ qdir) {
+  pdl_entry();
   using K = typename KeyOf<InT>::K;
   __shared__ uint32_t h[NBIN];
   __shared__ __align__(16) K qb[Q ? QB : 1];
@@ -2013,6 +2079,7 @@ __global__ __launch_bounds__(NT) void lvl_count(const InT* __restrict__ src,
 
 __global__ __launch_bounds__(1024) void lvl_scan(uint32_t* rows, const uint32_t* __restrict__ bigs,
                                                   const Counters* __restrict__ C, int p, Caps caps) {
+  pdl_entry();
   __shared__ uint32_t w[72];
   const uint32_t nb = min(C->nbig[p], caps.segs);
   for (uint32_t j = blockIdx.x; j < nb; j += gridDim.x)
@@ -2029,6 +2096,7 @@ __global__ __launch_bounds__(NT) void lvl_children(uint32_t* rows, const uint32_
                                                   K* points, uint32_t* khead_q, uint32_t* smalls,
                                                   uint32_t* tinies, const uint32_t* __restrict__ bigs,
                                                   uint32_t* bigs_q, Caps caps, const K* __restrict__ qtab) {
+  pdl_entry();
   constexpr int PER = NBIN / NT;
   const uint32_t nb = min(C->nbig[p], caps.segs);
   for (uint32_t j = blockIdx.x; j < nb; j += gridDim.x) {
@@ -2112,6 +2180,7 @@ __global__ __launch_bounds__(NT) void lvl_compact(const InT* __restrict__ src,
                                                  uint32_t* cursor_q, typename KeyOf<InT>::K* dst,
                                                  Caps caps, const typename KeyOf<InT>::K* __restrict__ qtab,
                                                  const uint16_t* __restrict__ qdir) {
+  pdl_entry();
   using K = typename KeyOf<InT>::K;
   __shared__ uint32_t cm[NBIN];
   __shared__ __align__(16) K qb[Q ? QB : 1];
@@ -2198,6 +2267,7 @@ __global__ __launch_bounds__(NT) void small_select(const InT* __restrict__ src,
                                                   const uint32_t* __restrict__ k_rank, uint32_t* k_seg,
                                                   typename KeyOf<InT>::K* k_key, uint32_t small_keys,
                                                   Caps caps) {
+  pdl_entry();
   using K = typename KeyOf<InT>::K;
   Counters* C = const_cast<Counters*>(C_);
   extern __shared__ __align__(128) uint8_t smem[];
@@ -2447,6 +2517,7 @@ __global__ __launch_bounds__(NT) void tiny_select(const InT* __restrict__ src,
                                                  const int64_t* __restrict__ k_off,
                                                  const uint32_t* __restrict__ k_rank, uint32_t* k_seg,
                                                  typename KeyOf<InT>::K* k_key, Caps caps) {
+  pdl_entry();
   using K = typename KeyOf<InT>::K;
   constexpr uint32_t TK = tiny_keys<K>();
   constexpr int NW = NT / 32;
@@ -2568,6 +2639,7 @@ __global__ void seg_init(const int64_t* __restrict__ seg_off, uint32_t nseg,
                          const int64_t* __restrict__ k_off, Seg<K>* segs0, TileRef* tiles0,
                          uint32_t* khead0, uint32_t* smalls, uint32_t* tinies, uint32_t* bigs0,
                          uint32_t cap_q, Counters* C, Caps caps) {
+  pdl_entry();
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nseg) return;
   const int64_t a = seg_off[s], b = seg_off[s + 1];
@@ -2610,7 +2682,8 @@ __global__ void seg_init(const int64_t* __restrict__ seg_off, uint32_t nseg,
   for (uint32_t t = 0; t < nt; ++t) tiles0[t0 + t] = TileRef{s, t};
 }
 
-__global__ void seg_set_count(Counters* C, uint32_t nseg) { C->nsegs[0] = nseg; }
+__global__ void seg_set_count(Counters* C, uint32_t nseg) {
+  pdl_entry(); C->nsegs[0] = nseg; }
 
 // k i belongs to the segment s with k_off[s] <= i < k_off[s+1]; the ks of a
 // segment that is finished directly go on its list.
@@ -2619,6 +2692,7 @@ __global__ void k_init_seg(const uint32_t* __restrict__ ks, uint32_t nk,
                            const int64_t* __restrict__ seg_off, const int64_t* __restrict__ k_off,
                            uint32_t nseg, const Seg<K>* __restrict__ segs0, uint32_t* khead0,
                            uint32_t* knext, uint32_t* k_rank, uint32_t* k_seg, Counters* C) {
+  pdl_entry();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nk) return;
   uint32_t lo = 0, hi = nseg - 1;  // largest s with k_off[s] <= i
@@ -2643,6 +2717,7 @@ __global__ void k_init_seg(const uint32_t* __restrict__ ks, uint32_t nk,
 template <typename T>
 __global__ void write_out(const typename KeyOf<T>::K* __restrict__ k_key,
                           const uint32_t* __restrict__ k_seg, uint32_t nk, T* out, Counters* C) {
+  pdl_entry();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   GGMS_TRACE(37);
   if (i >= nk) return;

@@ -44,6 +44,7 @@ struct LearnState {
   uint32_t choice;               // 1 learned accepted, 0 fell back to sampled
   uint32_t focus_points;         // breakpoints of the bucket focus (2: none)
   uint32_t pad[1];
+  Warp warp;                     // the bucket focus (setup_pl_knots builds it, the bases use it)
   PLStats st[PL_M];              // per-segment statistics (pl_stats_grid -> training)
   // MLP parameters (see ggms_mlp.cuh)
   float mlp_params[MLP_NPARAM + 3];
@@ -68,6 +69,7 @@ constexpr uint32_t PL_IDX = 64;
 template <typename K>
 __global__ __launch_bounds__(1024) void pl_stats_grid(const K* __restrict__ sorted, uint32_t S,
                                                      const Assigner<K>* __restrict__ A, LearnState* L) {
+  pdl_entry();
   __shared__ K sidx[65536u / PL_IDX];
   GGMS_TRACE(7);
   const uint32_t M = A->M;
@@ -202,7 +204,14 @@ __device__ float pl_fb(float theta, const PLStats* st, uint32_t M, double S, PLR
 __device__ float pl_train_block(const PLStats* st, uint32_t M, uint32_t S, uint32_t steps, float lr,
                                 PLRed& red, float* cdf_out, float* loss0_out, float* theta_out,
                                 float* grad_out) {
-  float theta = 0.5413248546f;  // softplus^-1(1): uniform increments = the quantile init
+  // start from the sample's own CDF: increments proportional to each segment's
+  // sample count (for knots at uniform quantiles, all 1: softplus^-1(1))
+  float theta;
+  {
+    const float c = threadIdx.x < M ? (float)st[threadIdx.x].n : 0.0f;
+    const float delta = fmaxf(c * (float)M / (float)S, 1.0e-4f);
+    theta = delta > 20.0f ? delta : logf(expm1f(delta));
+  }
   float m1 = 0.0f, m2 = 0.0f, g = 0.0f;
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
   float b1t = 1.0f, b2t = 1.0f;
@@ -317,14 +326,31 @@ __device__ void learned_finish(const K* sorted, uint32_t S, uint32_t B, uint32_t
 // The whole learned-PL setup in one CTA: knots -> statistics -> training ->
 // bases -> grid -> occupancy -> choice (grid 1 if within the bound, else the
 // sampled grid 0 stays in use).
-// Knots of the learned PL model (one CTA): quantile knots, deduplicated;
-// mreq segments requested (0: the default, min(PL_M, B / 4)).
+// Knots of the learned PL model (one CTA): mreq segments requested (0: the
+// default, min(PL_M, B / 4)).  With window_z >= 0 the bucket focus is built
+// here too, from the ks (krank: their ascending ranks among n keys), and
+// stored in L for setup_learned_pl; L == null: no focus.
 template <typename K>
 __global__ __launch_bounds__(SETUP_NT) void setup_pl_knots(const K* __restrict__ sorted, uint32_t S,
-                                                          uint32_t B, Assigner<K>* A, uint32_t mreq) {
+                                                          uint32_t B, Assigner<K>* A, uint32_t mreq,
+                                                          const uint32_t* __restrict__ krank, uint32_t nk,
+                                                          uint64_t n, float window_z, LearnState* L) {
+  pdl_entry();
   extern __shared__ __align__(128) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
+  __shared__ Warp wsh;
+  __shared__ uint32_t wred[33];
   GGMS_TRACE(5);
+  if (L && window_z >= 0.0f) {
+    // the statistics' space is unused here: it holds the focus bins
+    build_warp(krank, nk, n, S, window_z, L0_WIN, reinterpret_cast<uint32_t*>(sm.st), wred, &wsh);
+  } else if (threadIdx.x == 0) {
+    wsh.n = 2;
+    wsh.p[0] = wsh.w[0] = 0.0f;
+    wsh.p[1] = wsh.w[1] = 1.0f;
+  }
+  __syncthreads();
+  if (L && threadIdx.x == 0) L->warp = wsh;
   pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, A, sm, mreq);
   GGMS_TRACE(6);
 }
@@ -341,10 +367,10 @@ __global__ __launch_bounds__(SETUP_NT) void setup_learned_pl(const K* __restrict
                                                             uint32_t* choice,
                                                             const uint32_t* __restrict__ krank,
                                                             uint32_t nk, uint64_t n, float window_z) {
+  pdl_entry();
   extern __shared__ __align__(128) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
   __shared__ Warp wsh;
-  __shared__ uint32_t wred[33];
   const uint32_t M = A->M;  // knots: setup_pl_knots; statistics: pl_stats_grid
   GGMS_TRACE(9);
   pl_stats_load(L, M, sm.st);
@@ -360,14 +386,7 @@ __global__ __launch_bounds__(SETUP_NT) void setup_learned_pl(const K* __restrict
   }
   __syncthreads();
   GGMS_TRACE(11);
-  if (window_z >= 0.0f) {
-    // the statistics are dead after training: their space holds the bins
-    build_warp(krank, nk, n, S, window_z, L0_WIN, reinterpret_cast<uint32_t*>(sm.st), wred, &wsh);
-  } else if (threadIdx.x == 0) {
-    wsh.n = 2;
-    wsh.p[0] = wsh.w[0] = 0.0f;
-    wsh.p[1] = wsh.w[1] = 1.0f;
-  }
+  if (threadIdx.x == 0) wsh = L->warp;  // built with the knots (setup_pl_knots)
   __syncthreads();
   GGMS_TRACE(12);
   if (threadIdx.x == 0) L->focus_points = wsh.n;
@@ -383,6 +402,7 @@ __global__ __launch_bounds__(SETUP_NT) void pl_grad_probe(const Assigner<K>* __r
                                                          const LearnState* L,
                                                          const float* __restrict__ theta_in,
                                                          float* loss_out, float* grad_out) {
+  pdl_entry();
   extern __shared__ __align__(128) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
   const uint32_t M = A->M;
@@ -423,14 +443,17 @@ static int learn_and_choose(int kind, const K* sorted, uint32_t S, uint32_t B, i
     if (rc) return rc;
   } else {
     const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 4u;
-    setup_pl_knots<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, &As[1], pl_knots);
-    pl_stats_grid<K><<<(PL_M + 31) / 32, 1024, 0, st>>>(sorted, S, &As[1], L);
+    if (launch_pdl(setup_pl_knots<K>, 1, SETUP_NT, sizeof(LearnSmem<K>), st, sorted, S, B, &As[1], pl_knots, krank,
+                   nk, n, window_z, L) != cudaSuccess ||
+        launch_pdl(pl_stats_grid<K>, (PL_M + 31) / 32, 1024, 0, st, sorted, S, (const Assigner<K>*)&As[1], L) !=
+            cudaSuccess)
+      return GGMS_E_CUDA;
     // the choice compares with the sampled grid: wait for it (it may be built
     // on another stream, concurrently with the knots and the statistics)
     if (sampled_done && cudaStreamWaitEvent(st, sampled_done, 0) != cudaSuccess) return GGMS_E_CUDA;
-    setup_learned_pl<K><<<1, SETUP_NT, sizeof(LearnSmem<K>), st>>>(sorted, S, B, steps, 0.02f, bound,
-                                                                    &As[1], &Gs[1], &Gs[0], L, choice,
-                                                                    krank, nk, n, window_z);
+    if (launch_pdl(setup_learned_pl<K>, 1, SETUP_NT, sizeof(LearnSmem<K>), st, sorted, S, B, steps, 0.02f, bound,
+                   &As[1], &Gs[1], (const Grid<K>*)&Gs[0], L, choice, krank, nk, n, window_z) != cudaSuccess)
+      return GGMS_E_CUDA;
     *launches += 3;
   }
   return cudaGetLastError() == cudaSuccess ? GGMS_OK : GGMS_E_CUDA;

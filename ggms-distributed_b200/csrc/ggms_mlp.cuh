@@ -10,8 +10,12 @@
 // compiled assigner.  The network thus learns a monotone correction of the
 // sampled model: where the data's density changes inside a pivot interval
 // (mixtures, heavy tails) F0 is off and the network bends it back.  Loss:
-// mean (y_i - t_i)^2 over Q = 1024 training points at the quantiles of the
-// self-drawn sample (t_i = rank / S).
+// mean (z_i - logit t_i)^2 over Q = 1024 training points at the quantiles of
+// the self-drawn sample (t_i = (rank + 1/2) / S), i.e. the error of the
+// sigmoid's argument.  In logit units the tails weigh as much as the middle:
+// a CDF-space error would let the network squeeze the top and bottom percent
+// of the keys into a few buckets where the sigmoid saturates (on a lognormal
+// sample that made one of 256 bucket groups hold 8x its share).
 //
 // Training runs in ONE launch of one thread-block cluster (8 CTAs x 128
 // threads, one training point per thread): every step each CTA computes its
@@ -74,10 +78,9 @@ __device__ void mlp_cta_grad(MlpSmem& S, float inv_q) {
       h2[k] = tanh_(a);
       z = fmaf(S.w3[k], h2[k], z);
     }
-    const float y = sigmoidf_(z);
-    const float e = y - S.t[tid];
+    const float e = z - S.t[tid];  // S.t holds logit targets
     S.err[tid] = e * e;
-    const float dz = 2.0f * e * inv_q * y * (1.0f - y);
+    const float dz = 2.0f * e * inv_q;
     S.dz[tid] = dz;
     float dh1[32];
 #pragma unroll
@@ -143,7 +146,10 @@ __device__ __forceinline__ float mlp_input(const Assigner<K>* __restrict__ A0, K
   return fminf(fmaxf(__fdiv_rn(b, (float)A0->B), 0.0f), 1.0f);
 }
 
-// Training points: Q sample quantiles, x = F0 of the key, target t = (rank + 0.5) / S.
+__device__ __forceinline__ float logitf_(float t) { return logf(t) - log1pf(-t); }
+
+// Training points: Q sample quantiles, x = F0 of the key, target
+// logit((rank + 0.5) / S); explicit points carry CDF targets in (0, 1).
 template <typename K>
 __device__ void mlp_load_points(MlpSmem& S, const K* sorted, uint32_t S_n, const Assigner<K>* A0,
                                 const float* px, const float* pt) {
@@ -151,12 +157,12 @@ __device__ void mlp_load_points(MlpSmem& S, const K* sorted, uint32_t S_n, const
   const uint32_t gi = blockIdx.x * MLP_NT + tid;
   if (px) {  // explicit points (gradient probe)
     S.x[tid] = px[gi];
-    S.t[tid] = pt[gi];
+    S.t[tid] = logitf_(pt[gi]);
     return;
   }
   const uint32_t si = (uint32_t)(((uint64_t)(2 * gi + 1) * S_n) / (2 * MLP_Q));
   S.x[tid] = mlp_input<K>(A0, sorted[si]);
-  S.t[tid] = ((float)si + 0.5f) / (float)S_n;
+  S.t[tid] = logitf_(((float)si + 0.5f) / (float)S_n);
 }
 
 // The cluster training kernel.  steps == 0 with probe != null: one forward /
@@ -167,6 +173,7 @@ __global__ void __cluster_dims__(MLP_CTAS, 1, 1) __launch_bounds__(MLP_NT)
 mlp_train(const K* __restrict__ sorted, uint32_t S_n, const Assigner<K>* __restrict__ A0,
           LearnState* L, float* Pglob, uint32_t steps, float lr, const float* px, const float* pt,
           float* probe) {
+  pdl_entry();
   extern __shared__ __align__(128) uint8_t smem_raw[];
   MlpSmem& S = *reinterpret_cast<MlpSmem*>(smem_raw);
   cg::cluster_group cluster = cg::this_cluster();
@@ -309,6 +316,7 @@ template <typename K>
 __global__ __launch_bounds__(SETUP_NT) void setup_mlp_begin(const K* __restrict__ sorted, uint32_t S,
                                                            uint32_t B, Assigner<K>* A, const Assigner<K>* A0,
                                                            float* P, uint32_t mreq) {
+  pdl_entry();
   extern __shared__ __align__(128) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
   pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_MLP, A, sm, mreq);
@@ -320,6 +328,7 @@ __global__ __launch_bounds__(SETUP_NT) void setup_mlp_finish(const K* __restrict
                                                             uint32_t B, float bound, const float* P,
                                                             Assigner<K>* A, Grid<K>* G, LearnState* L,
                                                             uint32_t* choice) {
+  pdl_entry();
   extern __shared__ __align__(128) uint8_t smem[];
   LearnSmem<K>& sm = *reinterpret_cast<LearnSmem<K>*>(smem);
   mlp_eval_knots<K>(P, A, A - 1, (float*)sm.Bs, sm.cdf);  // A - 1: the sampled assigner of the pair

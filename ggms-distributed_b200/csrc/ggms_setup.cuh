@@ -614,8 +614,10 @@ __device__ void build_warp(const uint32_t* __restrict__ krank, uint32_t nk, uint
 // Occupancy of the grid's buckets on the (sorted) sample, over 256 groups of
 // buckets: max / mean.
 // At most GRID_MEASURE_N samples are used (a strided subsample of the sorted
-// sample, still sorted): 64 per group on average, enough to see imbalance.
-constexpr uint32_t GRID_MEASURE_N = 16384;
+// sample, still sorted): 32 per group on average, enough to see imbalance
+// against the bound (3.0: a group holding three times its share), and all of
+// a thread's samples are loaded at once.
+constexpr uint32_t GRID_MEASURE_N = 8192;
 
 template <typename K>
 __device__ float grid_measure(const GridView<K>& g, const K* sorted_all, uint32_t S_all, uint32_t* hist256,
@@ -624,19 +626,19 @@ __device__ float grid_measure(const GridView<K>& g, const K* sorted_all, uint32_
   const uint32_t S = S_all / stride;
   for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) hist256[i] = 0;
   __syncthreads();
-  // coalesced loads, four in flight per thread; the sample is sorted, so the
+  // coalesced loads, eight in flight per thread; the sample is sorted, so the
   // 32 lanes of a warp usually share a group: one add per warp then
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t NTh = blockDim.x;
-  for (uint32_t base = 0; base < S; base += 4 * NTh) {
-    K v[4];
+  for (uint32_t base = 0; base < S; base += 8 * NTh) {
+    K v[8];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < 8; ++u) {
       const uint32_t i = base + u * NTh + threadIdx.x;
       v[u] = i < S ? sorted_all[(size_t)i * stride] : (K)0;
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < 8; ++u) {
       const uint32_t i = base + u * NTh + threadIdx.x;
       const bool ok = i < S;
       uint32_t grp = 0xFFFFFFFFu;
@@ -719,6 +721,7 @@ struct SetupSmem {
 template <typename K>
 __global__ __launch_bounds__(SETUP_NT) void setup_sampled(const K* __restrict__ sorted, uint32_t S,
                                                          uint32_t B, Assigner<K>* A, Grid<K>* G) {
+  pdl_entry();
   extern __shared__ __align__(128) uint8_t smem[];
   SetupSmem<K>& sm = *reinterpret_cast<SetupSmem<K>*>(smem);
   __shared__ uint32_t q[17];

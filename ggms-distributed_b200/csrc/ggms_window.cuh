@@ -36,6 +36,7 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
                                                    const uint32_t* __restrict__ krank, uint32_t nk,
                                                    uint64_t n, const Grid<K>* __restrict__ Gs,
                                                    Counters* C, float z, Windows<K>* W) {
+  pdl_entry();
   extern __shared__ __align__(128) uint8_t smem[];
   uint2* s1 = reinterpret_cast<uint2*>(smem);
   uint2* s2 = s1 + GRID_T1;

@@ -71,7 +71,8 @@ typedef struct ggms_stats {
   int32_t sample_size;          /* keys drawn for the assigner */
   float bucket_max_over_mean;   /* level-0 occupancy: max bucket / (n / num_buckets) */
   float model_imbalance;        /* max/mean of the model's buckets on its own sample (learned) */
-  float model_loss;             /* final training loss of the learned model */
+  float model_loss;             /* final training loss of the learned model (PL: squared CDF error over
+                                   its sample; MLP: mean squared logit error at its training points) */
   int32_t window_runs;          /* PASS 1 windows: bucket runs PASS 1 bucketed (0: every key bucketed) */
   int32_t model_segments;       /* segments of the learned model's piecewise-linear form (0: sampled);
                                    written only for callers whose opts carry pl_knots */

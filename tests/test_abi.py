@@ -73,8 +73,8 @@ def test_generate_rejects_before_launch():
         assert fn(fake, 0, 0, 1, None) == 1
         assert fn(fake, 16, -1, 1, None) == 1
         assert fn(fake, 16, kinds, 1, None) == 1
-    assert lib.ggms_generate_f32(fake, 16, 2, 1, None) == 5      # KILLER FLOATS
-    assert lib.ggms_generate_f64(fake, 16, 2, 1, None) == 5      # KILLER DOUBLES
+    assert lib.ggms_generate_f32(fake, 1 << 31, 2, 1, None) == 5    # KILLER FLOATS: CUB's int count
+    assert lib.ggms_generate_f64(fake, 1 << 31, 2, 1, None) == 5    # KILLER DOUBLES
     assert lib.ggms_generate_f32(fake, (1 << 32) + 1, 8, 1, None) == 5
     assert lib.ggms_generate_u32(fake, (1 << 32) + 1, 1, 1, None) == 5
 

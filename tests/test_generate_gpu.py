@@ -14,7 +14,7 @@ import ggms_oracle as orc
 pytestmark = pytest.mark.gpu
 
 N = 1 << 20
-FLOAT_KINDS = [0, 1, 3, 4, 5, 6, 7, 8, 9]
+FLOAT_KINDS = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9]
 
 
 def _gen(dtype, kind, seed, n=N):
@@ -27,7 +27,8 @@ def _gen(dtype, kind, seed, n=N):
 
 
 @pytest.mark.parametrize("dtype,kind", [(np.float32, k) for k in FLOAT_KINDS]
-                         + [(np.float64, 0), (np.float64, 1), (np.uint32, 0), (np.uint32, 1), (np.uint32, 2)])
+                         + [(np.float64, 0), (np.float64, 1), (np.float64, 2), (np.uint32, 0), (np.uint32, 1),
+                            (np.uint32, 2)])
 def test_deterministic_per_seed(dtype, kind):
     _, a = _gen(dtype, kind, 7)
     _, b = _gen(dtype, kind, 7)
@@ -80,6 +81,27 @@ def test_double_and_uint_distributions():
     assert np.array_equal(r, (np.arange(n) % 100).astype(np.uint32))
 
 
+@pytest.mark.parametrize("dtype,npow,mant,bias,mask", [
+    (np.float32, 253, 23, 127, 0x80EFFFFF), (np.float64, 2045, 52, 1023, 0x800FFFFFFFFFFFFF)])
+@pytest.mark.parametrize("n", [N, 300_001, 2045, 100, 1])
+def test_killer_kinds(dtype, npow, mant, bias, mask, n):
+    """KILLER FLOATS / DOUBLES (DistributedSMOS/generateProblems.cu:422-436,
+    493-507): kind 0's draw for the same seed with the exponent masked away, sorted
+    as bit patterns, then 2^(1-bias), 2^(2-bias), ... in the first slots."""
+    ib = np.uint32 if dtype == np.float32 else np.uint64
+    _, k = _gen(dtype, 2, 31, n)
+    _, u = _gen(dtype, 0, 31, n)
+    kb, ub = k.view(ib), u.view(ib)
+    head = min(n, npow)
+    powers = ((np.arange(head) + 1).astype(ib) << ib(mant))   # exponent fields 1 .. npow
+    assert np.array_equal(kb[:head], powers)
+    assert np.array_equal(k[:head], np.ldexp(np.ones(head, dtype), np.arange(head) + 1 - bias))
+    want = np.sort(ub & ib(mask))[head:]
+    assert np.array_equal(kb[head:], want)
+    if n == N:
+        assert (kb[head:] >> ib(mant) <= 1).all() and (kb[head:] >> ib(mant) == 0).any()
+
+
 @pytest.mark.parametrize("n", [1, 2, 5, 1000, 65537])
 def test_two_valued_counts_small_n(n):
     _, ot = _gen(np.float32, 8, 11, n)
@@ -89,7 +111,8 @@ def test_two_valued_counts_small_n(n):
 
 
 @pytest.mark.parametrize("dtype,kind", [(np.float32, k) for k in FLOAT_KINDS]
-                         + [(np.float64, 0), (np.float64, 1), (np.uint32, 0), (np.uint32, 1), (np.uint32, 2)])
+                         + [(np.float64, 0), (np.float64, 1), (np.float64, 2), (np.uint32, 0), (np.uint32, 1),
+                            (np.uint32, 2)])
 def test_multiselect_on_generated(dtype, kind):
     t, v = _gen(dtype, kind, 100 + kind)
     g = np.random.default_rng(kind)

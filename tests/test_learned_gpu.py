@@ -98,10 +98,11 @@ def mlp_forward_backward_cpu(x, t, p):
     h1 = np.tanh(np.outer(x, w1) + c1)            # Q x 32
     h2 = np.tanh(h1 @ W2.T + c2)                  # Q x 32
     z = h2 @ w3 + c3
-    y = sigmoid(z)
+    # the loss is taken on the sigmoid's argument: targets in logit units
+    tl = np.log(t) - np.log1p(-t)
     Q = len(x)
-    loss = np.mean((y - t) ** 2)
-    dz = 2 * (y - t) / Q * y * (1 - y)
+    loss = np.mean((z - tl) ** 2)
+    dz = 2 * (z - tl) / Q
     gw3 = h2.T @ dz
     gc3 = dz.sum()
     da2 = np.outer(dz, w3) * (1 - h2 ** 2)
@@ -118,7 +119,7 @@ def mlp_forward_backward_cpu(x, t, p):
 def test_mlp_gradient_matches_cpu():
     g = np.random.default_rng(3)
     x = np.sort(g.random(1024)).astype(np.float32)
-    t = ((np.arange(1024) + 0.5) / 1024 + 0.05 * np.sin(7 * x)).astype(np.float32)
+    t = np.clip((np.arange(1024) + 0.5) / 1024 + 0.05 * np.sin(7 * x), 1e-3, 1 - 1e-3).astype(np.float32)
     p = (0.3 * g.standard_normal(1153)).astype(np.float32)
     p[P_V2:P_C2] -= 3.0
     loss, grad = G.diag_mlp_gradient(x, t, p)
@@ -147,10 +148,10 @@ def test_training_improves_balance(gen, kind):
         assert r["loss_after"] <= r["loss_before"]
         assert r["imbalance_model"] < r["imbalance_sampled"], r
     else:
-        # the MLP reaches a small CDF error (mean squared, CDF units), and its
+        # the MLP reaches a small error (mean squared, logit units), and its
         # buckets, measured on the same sample, are more even than the 17
         # sampled pivots'
-        assert r["loss_after"] < 1e-3, r
+        assert r["loss_after"] < 1e-2, r
         assert r["imbalance_model"] < r["imbalance_sampled"], r
 
 
