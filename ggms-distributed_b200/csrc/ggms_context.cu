@@ -36,7 +36,7 @@ static int pl_gradient(const uint32_t* keys, int S, const float* theta, float* l
   GGMS_CU(cudaFuncSetAttribute(setup_pl_knots<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(LearnSmem<uint32_t>)));
   // the same three kernels as training: knots, statistics, forward/backward
-  setup_pl_knots<uint32_t><<<1, SETUP_NT, sizeof(LearnSmem<uint32_t>)>>>(
+  setup_pl_knots<uint32_t><<<2, SETUP_NT, sizeof(LearnSmem<uint32_t>)>>>(
       (const uint32_t*)dk.p, (uint32_t)S, 1u << 14, A, 0u, nullptr, 0u, 0ull, -1.0f, L);
   pl_stats_grid<uint32_t><<<(PL_M + 31) / 32, 1024>>>((const uint32_t*)dk.p, (uint32_t)S, A, L);
   pl_grad_probe<uint32_t><<<1, SETUP_NT, sizeof(LearnSmem<uint32_t>)>>>(A, (uint32_t)S, L,

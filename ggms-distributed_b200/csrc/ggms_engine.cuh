@@ -361,6 +361,64 @@ static int launch_small_select(Context* ctx, const InT* src, const Seg<K>* segs_
 // Profiling slot of the current call (or null when profiling is off).
 
 // ------------------------------------------------------------------ the single-vector path
+
+// The sample sort's cluster: attributes set once per key type; 16 CTAs when the
+// sample has at least one key per thread of 16 CTAs and the device can place a
+// 16-CTA cluster of this kernel, else 8; 0: too small for a cluster (S < 8192);
+// -1: the attributes could not be set.
+template <typename K, int CTAS>
+static cudaError_t launch_sort_cluster(cudaStream_t s, const K* drawn, uint32_t S, K* sorted) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(CTAS);
+  cfg.blockDim = dim3(CS_NT);
+  cfg.dynamicSmemBytes = sizeof(ClusterSortSmem<K, CTAS>);
+  cfg.stream = s;
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = CTAS;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 2;
+  return cudaLaunchKernelEx(&cfg, asg_sort_cluster<K, CTAS>, drawn, S, sorted);
+}
+
+template <typename K>
+static int sort_cluster_ctas(uint32_t S) {
+  static int have16 = -1;  // -1: not probed yet
+  if (have16 < 0) {
+    have16 = 0;
+    if (cudaFuncSetAttribute(asg_sort_cluster<K, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(ClusterSortSmem<K, 8>)) != cudaSuccess ||
+        cudaFuncSetAttribute(asg_sort_cluster<K, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(ClusterSortSmem<K, 16>)) != cudaSuccess)
+      return -1;
+    if (cudaFuncSetAttribute(asg_sort_cluster<K, 16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+        cudaSuccess) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(16);
+      cfg.blockDim = dim3(CS_NT);
+      cfg.dynamicSmemBytes = sizeof(ClusterSortSmem<K, 16>);
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = 16;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      int nclusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&nclusters, asg_sort_cluster<K, 16>, &cfg) == cudaSuccess &&
+          nclusters >= 1)
+        have16 = 1;
+    }
+    cudaGetLastError();  // a refused probe leaves no error behind
+  }
+  if (S >= cs_min_s(16) && have16) return 16;
+  return S >= cs_min_s(8) ? 8 : 0;
+}
+
 template <typename T>
 static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* ks, uint64_t nk64,
                       T* out, const ggms_opts& o_in, cudaStream_t st, bool topk = false) {
@@ -426,17 +484,14 @@ static int run_single(Context* ctx, const T* d_in, uint64_t n, const uint32_t* k
 
     // ---- level-0 assigner
     const uint32_t S = p.S;
-    if (S >= CS_MIN_S) {  // draw the sample over the whole GPU, sort it in one cluster
-      static bool cs_attr = false;
-      if (!cs_attr) {
-        GGMS_CU(cudaFuncSetAttribute(asg_sort_cluster<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(ClusterSortSmem<K>)));
-        cs_attr = true;
-      }
+    const int cs_ctas = sort_cluster_ctas<K>(S);
+    if (cs_ctas < 0) return GGMS_E_CUDA;
+    if (cs_ctas) {  // draw the sample over the whole GPU, sort it in one cluster
       ctx->launches += 2;
       GGMS_CU(launch_pdl(asg_sample<T>, cdiv(S, 256), 256, 0, s, d_in, n, S, p.seed, w.samp_raw));
-      GGMS_CU(launch_pdl(asg_sort_cluster<K>, CS_CTAS, CS_NT, sizeof(ClusterSortSmem<K>), s,
-                         (const K*)w.samp_raw, S, w.samp_sorted));
+      const cudaError_t e_sort = cs_ctas == 16 ? launch_sort_cluster<K, 16>(s, w.samp_raw, S, w.samp_sorted)
+                                               : launch_sort_cluster<K, 8>(s, w.samp_raw, S, w.samp_sorted);
+      GGMS_CU(e_sort);
     } else {  // up to 4096 keys: draw them, then one CTA sorts them
       ctx->launches += 2;
       asg_sample<T><<<cdiv(S, 256), 256, 0, s>>>(d_in, n, S, p.seed, w.samp_raw);

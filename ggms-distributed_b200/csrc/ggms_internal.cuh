@@ -275,6 +275,62 @@ __device__ __forceinline__ uint32_t grid_eval(const GridView<K>& g, K key) {
   return e.x + grid_lin(off, e.y - e.x, sh);
 }
 
+// Smallest key whose grid bucket is >= target (the largest key when no key's is): the
+// inverse of the monotone grid function, for the key range of a bucket.  A
+// binary search over the cells' first buckets (and over the sub-cells of a
+// split cell) finds the cell that holds the answer, and the cell's integer
+// interpolation is inverted in closed form: the smallest offset with
+// floor(off' * span / 2^s) >= t is off' = ceil(t * 2^s / span).  The result is
+// checked with grid_eval at the key and the key before it; should the check
+// fail, a binary search over all keys answers, so the result is exact either way.
+template <typename K>
+__device__ K grid_inv(const GridView<K>& g, uint32_t ncell, uint32_t target) {
+  if (grid_eval<K>(g, (K)0) >= target) return (K)0;
+  if (grid_eval<K>(g, g.gmax) < target) return (K)~(K)0;
+  auto cstart = [&](uint32_t c) -> uint32_t {  // bucket of the cell's first key
+    const uint2 e = g.t1[c];
+    return (e.x & GRID_SPLIT) ? g.t2[e.y].x : e.x;
+  };
+  uint32_t lo = 0, hi = ncell - 1u;  // the last cell whose first bucket is below target
+  while (lo < hi) {
+    const uint32_t m = (lo + hi + 1u) >> 1;
+    if (cstart(m) < target) lo = m; else hi = m - 1u;
+  }
+  uint2 e = g.t1[lo];
+  uint32_t sh = g.sh1;
+  K first = (K)(g.origin + ((K)lo << g.sh1));
+  if (e.x & GRID_SPLIT) {
+    const uint32_t sb = (e.x >> 16) & 31u;
+    sh = g.sh1 - sb;
+    uint32_t l2 = 0, h2 = (1u << sb) - 1u;
+    while (l2 < h2) {
+      const uint32_t m = (l2 + h2 + 1u) >> 1;
+      if (g.t2[e.y + m].x < target) l2 = m; else h2 = m - 1u;
+    }
+    first = (K)(first + ((K)l2 << sh));
+    e = g.t2[e.y + l2];
+  }
+  const uint32_t span = e.y - e.x, t = target - e.x;  // t >= 1: the cell starts below target
+  K cand;
+  if (t >= span) {  // every key of the cell is below target: the next cell's first key
+    cand = (K)(first + ((K)1 << sh));
+  } else {
+    const uint32_t s = min(sh, 32u);  // grid_lin interpolates on the top 32 bits of the offset
+    const uint64_t top = (((uint64_t)t << s) + span - 1u) / span;
+    cand = (K)(first + ((K)top << (sh - s)));
+  }
+  if (cand != (K)0 && grid_eval<K>(g, cand) >= target && grid_eval<K>(g, (K)(cand - 1u)) < target) return cand;
+#ifdef GGMS_SETUP_TRACE
+  atomicAdd(&ggms_trace_buf[63], 1ull);  // fallbacks, read by the trace reader
+#endif
+  K a = 0, b = (K)~(K)0;
+  while (a < b) {
+    const K mid = a + ((b - a) >> 1);
+    if (grid_eval<K>(g, mid) >= target) b = mid; else a = mid + 1u;
+  }
+  return a;
+}
+
 // ------------------------------------------------------------------ refinement levels
 // A segment of candidates.  Every key of the segment lies in [lo, hi]; its bin
 // is (key - lo) >> shift, shift chosen so that bins < NBIN.

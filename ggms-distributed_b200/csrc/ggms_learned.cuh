@@ -327,9 +327,10 @@ __device__ void learned_finish(const K* sorted, uint32_t S, uint32_t B, uint32_t
 // bases -> grid -> occupancy -> choice (grid 1 if within the bound, else the
 // sampled grid 0 stays in use).
 // Knots of the learned PL model (one CTA): mreq segments requested (0: the
-// default, min(PL_M, B / 4)).  With window_z >= 0 the bucket focus is built
-// here too, from the ks (krank: their ascending ranks among n keys), and
-// stored in L for setup_learned_pl; L == null: no focus.
+// default, min(PL_M, B / 4)).  Launched with two CTAs: CTA 0 places the knots
+// while CTA 1 builds the bucket focus from the ks (krank: their ascending ranks
+// among n keys; window_z < 0: none) and stores it in L for setup_learned_pl
+// (L == null: not stored).
 template <typename K>
 __global__ __launch_bounds__(SETUP_NT) void setup_pl_knots(const K* __restrict__ sorted, uint32_t S,
                                                           uint32_t B, Assigner<K>* A, uint32_t mreq,
@@ -341,16 +342,20 @@ __global__ __launch_bounds__(SETUP_NT) void setup_pl_knots(const K* __restrict__
   __shared__ Warp wsh;
   __shared__ uint32_t wred[33];
   GGMS_TRACE(5);
-  if (L && window_z >= 0.0f) {
-    // the statistics' space is unused here: it holds the focus bins
-    build_warp(krank, nk, n, S, window_z, L0_WIN, reinterpret_cast<uint32_t*>(sm.st), wred, &wsh);
-  } else if (threadIdx.x == 0) {
-    wsh.n = 2;
-    wsh.p[0] = wsh.w[0] = 0.0f;
-    wsh.p[1] = wsh.w[1] = 1.0f;
+  if (blockIdx.x == 1) {
+    if (!L) return;
+    if (window_z >= 0.0f) {
+      // the statistics' space is unused in this CTA: it holds the focus bins
+      build_warp(krank, nk, n, S, window_z, L0_WIN, reinterpret_cast<uint32_t*>(sm.st), wred, &wsh);
+    } else if (threadIdx.x == 0) {
+      wsh.n = 2;
+      wsh.p[0] = wsh.w[0] = 0.0f;
+      wsh.p[1] = wsh.w[1] = 1.0f;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) L->warp = wsh;
+    return;
   }
-  __syncthreads();
-  if (L && threadIdx.x == 0) L->warp = wsh;
   pl_knots<K>(sorted, S, B, GGMS_ASSIGNER_LEARNED_PL, A, sm, mreq);
   GGMS_TRACE(6);
 }
@@ -442,8 +447,8 @@ static int learn_and_choose(int kind, const K* sorted, uint32_t S, uint32_t B, i
                                     sampled_done, pl_knots);
     if (rc) return rc;
   } else {
-    const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 4u;
-    if (launch_pdl(setup_pl_knots<K>, 1, SETUP_NT, sizeof(LearnSmem<K>), st, sorted, S, B, &As[1], pl_knots, krank,
+    const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 2u;
+    if (launch_pdl(setup_pl_knots<K>, 2, SETUP_NT, sizeof(LearnSmem<K>), st, sorted, S, B, &As[1], pl_knots, krank,
                    nk, n, window_z, L) != cudaSuccess ||
         launch_pdl(pl_stats_grid<K>, (PL_M + 31) / 32, 1024, 0, st, sorted, S, (const Assigner<K>*)&As[1], L) !=
             cudaSuccess)
