@@ -41,6 +41,9 @@ int ggms_multiselect_segmented_f32(ggms_context* ctx, const float* d_in, const i
 GGMS_API int ggms_trace_read_f32(unsigned long long* out) {
   return cudaMemcpyFromSymbol(out, ggms_trace_buf, sizeof(ggms_trace_buf)) == cudaSuccess ? 0 : 4;
 }
+GGMS_API int ggms_trace_read_cta_f32(unsigned long long* out) {
+  return cudaMemcpyFromSymbol(out, ggms_trace_cta, sizeof(ggms_trace_cta)) == cudaSuccess ? 0 : 4;
+}
 #endif
 
 }  // extern "C"

@@ -38,9 +38,23 @@ static __device__ unsigned long long ggms_trace_buf[64];
       ggms_trace_buf[(i)] = t_;                                        \
     }                                                                  \
   } while (0)
+// Per-CTA points of the two passes: thread 0 of every block stores its
+// %globaltimer in row i (0/1 PASS 1 start/end, 2/3 PASS 2 start/end).
+static __device__ unsigned long long ggms_trace_cta[4][1024];
+#define GGMS_TRACE_CTA(i)                                              \
+  do {                                                                 \
+    if (threadIdx.x == 0 && blockIdx.x < 1024) {                       \
+      unsigned long long t_;                                           \
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_));           \
+      ggms_trace_cta[(i)][blockIdx.x] = t_;                            \
+    }                                                                  \
+  } while (0)
 #else
 #define GGMS_TRACE(i) \
   do {                \
+  } while (0)
+#define GGMS_TRACE_CTA(i) \
+  do {                    \
   } while (0)
 #endif
 

@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(CS_NT) asg_sort_cluster(const K* __restrict__ 
       off[r] = base + __popc(peers & lt);
     }
     __syncthreads();
-    if (sh < 32) GGMS_TRACE(46 + (sh >> 3) * 4);
+    if (sh < 24) GGMS_TRACE(46 + (sh >> 3) * 4);
     // per digit: exclusive prefix over the warps (in place) and this CTA's total
     {
       const uint32_t d = tid >> 2, q = tid & 3u;       // 4 threads per digit, 8 warps each
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(CS_NT) asg_sort_cluster(const K* __restrict__ 
       if (tot == S) sm.skip = 1u;  // every key has this digit: nothing moves
     }
     __syncthreads();
-    if (sh < 32) GGMS_TRACE(47 + (sh >> 3) * 4);
+    if (sh < 24) GGMS_TRACE(47 + (sh >> 3) * 4);
     const bool skip = sm.skip != 0u;
     if (!skip) {
 #pragma unroll
@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(CS_NT) asg_sort_cluster(const K* __restrict__ 
       }
     }
     __syncthreads();  // b is complete (the cluster's a was read into registers before (1))
-    if (sh < 32) GGMS_TRACE(48 + (sh >> 3) * 4);
+    if (sh < 24) GGMS_TRACE(48 + (sh >> 3) * 4);
     if (!skip) {
       for (uint32_t i = tid; i < per; i += CS_NT) {
         const K k = sm.b[i];
@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(CS_NT) asg_sort_cluster(const K* __restrict__ 
       }
     }
     cluster.sync();  // (2) the next order is complete; the counts have been read
-    if (sh < 32) GGMS_TRACE(49 + (sh >> 3) * 4);
+    if (sh < 24) GGMS_TRACE(49 + (sh >> 3) * 4);
   }
   K* out = sorted + (size_t)me * per;
   for (uint32_t i = tid; i < per; i += CS_NT) out[i] = A[i];
@@ -900,6 +900,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_count(const T* __res
   uint2* s2 = s1 + GRID_T1;
   uint32_t* hs = (uint32_t*)(smem + GRID_SMEM);
   GGMS_TRACE(24);
+  GGMS_TRACE_CTA(0);
   const GridView<K> gv = grid_to_smem<K>(G, s1, s2);
   const uint32_t B = gv.B;
   K* wq = reinterpret_cast<K*>(hs + B) + (threadIdx.x >> 5) * WQ_DEPTH;
@@ -1050,6 +1051,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_count(const T* __res
     if (v) atomicAdd(&hist0[i], v);
   }
   GGMS_TRACE(25);
+  GGMS_TRACE_CTA(1);
 }
 
 // Inclusive scan of the level-0 counts (one CTA) + the largest bucket.  The
@@ -1134,65 +1136,14 @@ __global__ void lvl_locate_rows(const uint32_t* __restrict__ rows, uint32_t row_
 // one warp (tiny_select), a larger small one by one CTA.
 constexpr uint32_t TS_SORT_ABOVE = 8;
 
-// Level-0 child of bucket (or group) b, which holds a k; I: inclusive counts of
-// the buckets (or, coarse, of the groups).
-template <typename K>
-__device__ __forceinline__ void l0_child_make(uint32_t b, bool coarse, uint32_t gsh, uint32_t B,
-                                              const uint32_t* I, const GridView<K>& gv, uint32_t ncell,
-                                              const Windows<K>& W,
-                                              Counters* C, uint32_t* cmap0, Seg<K>* segs1, uint32_t* cursor1,
-                                              TileRef* tiles1, K* points, uint32_t* khead1, uint32_t* smalls,
-                                              uint32_t* bigs1, const Caps& caps, const uint32_t* kcnt0,
-                                              uint32_t tiny_keys, uint32_t* tinies) {
-  const uint32_t start = b ? I[b - 1] : 0u;
-  const uint32_t cnt = I[b] - start;
-  // key range of bucket b: [L(b), L(b+1) - 1], L(x) = smallest key with eval >= x
-  auto L = [&](uint32_t target) -> K { return grid_inv<K>(gv, ncell, target); };
-  // a gap bucket (windows) stands for its whole gap: up to the gap's last bucket;
-  // a group, for its buckets [b << gsh, (b + 1) << gsh)
-  const uint32_t b0 = coarse ? b << gsh : b;
-  const uint32_t e = coarse ? ((b + 1u) << gsh) - 1u : win_end<K>(W, b);
-  const K lo = (b0 == 0) ? (K)0 : L(b0);
-  const K hi = (e >= B - 1) ? key_max<K>() : (K)(L(e + 1) - 1);
-  atomicAdd(&C->active0, 1u);
-  if (lo == hi) {
-    uint32_t pid = atomicAdd(&C->npoints, 1u);
-    if (pid >= caps.points) { set_status(C, GGMS_E_INTERNAL); cmap0[b] = CM_NONE; return; }
-    points[pid] = lo;
-    cmap0[b] = CM_POINT | pid;
-    atomicAdd(&C->point0, 1u);
-    return;
-  }
-  const uint32_t id = atomicAdd(&C->nsegs[1], 1u);
-  if (id >= caps.segs) { set_status(C, GGMS_E_INTERNAL); cmap0[b] = CM_NONE; return; }
-  Seg<K> s;
-  s.off = start;
-  s.cnt = cnt;
-  s.lo = lo;
-  s.hi = hi;
-  s.shift = (uint32_t)max(0, bitlen((K)(hi - lo)) - RADIX_BITS);
-  s.small = cnt <= caps.small_keys ? 1u : 0u;
-  s.pad = b;  // the level-0 bucket or group (l0_bases needs it)
-  segs1[id] = s;
-  cursor1[id] = 0u;
-  khead1[id] = K_NIL;
-  cmap0[b] = id;
-  atomicAdd(&C->cand0, (unsigned long long)cnt);
-  if (s.small) {
-    const bool tiny = !coarse && cnt <= tiny_keys && kcnt0[b] <= TS_SORT_ABOVE;
-    const uint32_t si = atomicAdd(tiny ? &C->ntiny : &C->nsmall, 1u);
-    if (si < caps.segs) (tiny ? tinies : smalls)[si] = id; else set_status(C, GGMS_E_INTERNAL);
-    return;
-  }
-  const uint32_t bi = atomicAdd(&C->nbig[1], 1u);
-  if (bi < caps.segs) bigs1[bi] = id; else set_status(C, GGMS_E_INTERNAL);
-  const uint32_t nt = (cnt + TILE - 1) / TILE;
-  const uint32_t t0 = atomicAdd(&C->ntiles[1], nt);
-  if (t0 + nt > caps.tiles || t0 + nt < t0) { set_status(C, GGMS_E_INTERNAL); return; }
-  for (uint32_t t = 0; t < nt; ++t) tiles1[t0 + t] = TileRef{id, t};
-}
-
-// One thread per bucket (or group).
+// Level-0 children: one thread per bucket (or, coarse, per group) holding a k.
+// A child is a point (a single key: answered from `points`) or a segment with
+// its key range [L(b), L(b+1) - 1], L(x) = smallest key with bucket >= x (a gap
+// bucket of the windows stands for its whole gap; a group for its buckets),
+// finished by the warp or CTA selects or refined by a level.  Ids in the
+// shared lists are reserved per block: shared atomics inside the block, then
+// one global atomic per counter -- a global counter bumped by every active
+// bucket serialises ~10^3 same-address atomics in L2.
 template <typename K>
 __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __restrict__ aflag,
                             uint32_t B, const Grid<K>* __restrict__ Gs, Counters* C,
@@ -1206,6 +1157,11 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
   // it in shared memory (every thread helps load it before any returns)
   __shared__ uint2 s1[GRID_T1];
   __shared__ uint2 s2[GRID_SUBCAP];
+  enum { N_ACT, N_PT, N_SEG, N_TINY, N_SMALL, N_BIG, N_TILE, N_CTR };
+  __shared__ uint32_t ctr[N_CTR], cbase[N_CTR];
+  __shared__ unsigned long long cand_s;
+  if (threadIdx.x < N_CTR) ctr[threadIdx.x] = 0u;
+  if (threadIdx.x == 0) cand_s = 0ull;
   GGMS_TRACE(28);
   const Grid<K>* G = Gs + C->asg_choice;
   const GridView<K> gv = grid_to_smem<K>(G, s1, s2);
@@ -1215,13 +1171,95 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   const bool coarse = C->coarse != 0u;
   const uint32_t gsh = coarse_shift(B);
-  if (b >= (coarse ? NGRP : B)) return;
-  if (!(((coarse ? aflagc : aflag)[b >> 5] >> (b & 31)) & 1u)) {
-    cmap0[b] = CM_NONE;
+  const uint32_t* Ib = coarse ? ic : I;
+  // 1. classify this thread's bucket and take its block-local slots
+  enum { C_NONE, C_POINT, C_TINY, C_SMALL, C_BIG };
+  uint32_t kind = C_NONE, start = 0, cnt = 0, li = 0, lt = 0, nt = 0, ls = 0;
+  K lo = 0, hi = 0;
+  if (b < (coarse ? NGRP : B)) {
+    if (!(((coarse ? aflagc : aflag)[b >> 5] >> (b & 31)) & 1u)) {
+      cmap0[b] = CM_NONE;
+    } else {
+      start = b ? Ib[b - 1] : 0u;
+      cnt = Ib[b] - start;
+      const uint32_t b0 = coarse ? b << gsh : b;
+      const uint32_t e = coarse ? ((b + 1u) << gsh) - 1u : win_end<K>(*Wg, b);
+      lo = (b0 == 0) ? (K)0 : grid_inv<K>(gv, ncell, b0);
+      hi = (e >= B - 1) ? key_max<K>() : (K)(grid_inv<K>(gv, ncell, e + 1u) - 1u);
+      atomicAdd(&ctr[N_ACT], 1u);
+      if (lo == hi) {
+        kind = C_POINT;
+        li = atomicAdd(&ctr[N_PT], 1u);
+      } else {
+        ls = atomicAdd(&ctr[N_SEG], 1u);
+        atomicAdd(&cand_s, (unsigned long long)cnt);
+        if (cnt <= caps.small_keys) {
+          kind = (!coarse && cnt <= tiny_keys && kcnt0[b] <= TS_SORT_ABOVE) ? C_TINY : C_SMALL;
+          li = atomicAdd(&ctr[kind == C_TINY ? N_TINY : N_SMALL], 1u);
+        } else {
+          kind = C_BIG;
+          li = atomicAdd(&ctr[N_BIG], 1u);
+          nt = (cnt + TILE - 1) / TILE;
+          lt = atomicAdd(&ctr[N_TILE], nt);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  GGMS_TRACE(58);
+  // 2. the block's ranges in the shared lists
+  if (threadIdx.x == 0 && ctr[N_ACT]) {
+    atomicAdd(&C->active0, ctr[N_ACT]);
+    if (ctr[N_PT]) {
+      atomicAdd(&C->point0, ctr[N_PT]);
+      cbase[N_PT] = atomicAdd(&C->npoints, ctr[N_PT]);
+    }
+    if (ctr[N_SEG]) {
+      cbase[N_SEG] = atomicAdd(&C->nsegs[1], ctr[N_SEG]);
+      atomicAdd(&C->cand0, cand_s);
+    }
+    if (ctr[N_TINY]) cbase[N_TINY] = atomicAdd(&C->ntiny, ctr[N_TINY]);
+    if (ctr[N_SMALL]) cbase[N_SMALL] = atomicAdd(&C->nsmall, ctr[N_SMALL]);
+    if (ctr[N_BIG]) {
+      cbase[N_BIG] = atomicAdd(&C->nbig[1], ctr[N_BIG]);
+      cbase[N_TILE] = atomicAdd(&C->ntiles[1], ctr[N_TILE]);
+    }
+  }
+  __syncthreads();
+  GGMS_TRACE(59);
+  // 3. write this thread's child
+  if (kind == C_NONE) return;
+  if (kind == C_POINT) {
+    const uint32_t pid = cbase[N_PT] + li;
+    if (pid >= caps.points) { set_status(C, GGMS_E_INTERNAL); cmap0[b] = CM_NONE; return; }
+    points[pid] = lo;
+    cmap0[b] = CM_POINT | pid;
     return;
   }
-  l0_child_make<K>(b, coarse, gsh, B, coarse ? ic : I, gv, ncell, *Wg, C, cmap0, segs1, cursor1, tiles1, points, khead1,
-                   smalls, bigs1, caps, kcnt0, tiny_keys, tinies);
+  const uint32_t id = cbase[N_SEG] + ls;
+  if (id >= caps.segs) { set_status(C, GGMS_E_INTERNAL); cmap0[b] = CM_NONE; return; }
+  Seg<K> sg;
+  sg.off = start;
+  sg.cnt = cnt;
+  sg.lo = lo;
+  sg.hi = hi;
+  sg.shift = (uint32_t)max(0, bitlen((K)(hi - lo)) - RADIX_BITS);
+  sg.small = kind != C_BIG ? 1u : 0u;
+  sg.pad = b;  // the level-0 bucket or group (l0_bases needs it)
+  segs1[id] = sg;
+  cursor1[id] = 0u;
+  khead1[id] = K_NIL;
+  cmap0[b] = id;
+  if (kind != C_BIG) {
+    const uint32_t si = cbase[kind == C_TINY ? N_TINY : N_SMALL] + li;
+    if (si < caps.segs) (kind == C_TINY ? tinies : smalls)[si] = id; else set_status(C, GGMS_E_INTERNAL);
+    return;
+  }
+  const uint32_t bi = cbase[N_BIG] + li;
+  if (bi < caps.segs) bigs1[bi] = id; else set_status(C, GGMS_E_INTERNAL);
+  const uint32_t t0 = cbase[N_TILE] + lt;
+  if (t0 + nt > caps.tiles || t0 + nt < t0) { set_status(C, GGMS_E_INTERNAL); return; }
+  for (uint32_t t = 0; t < nt; ++t) tiles1[t0 + t] = TileRef{id, t};
 }
 
 // ks follow their bin: resolved (single key) or the id of the next segment.
@@ -1408,12 +1446,14 @@ __global__ void l0_relabel_bases(const uint32_t* __restrict__ cmap0, uint32_t nk
                                  uint32_t* khead1, uint32_t* knext, uint32_t* crow, uint32_t B, uint32_t ncta,
                                  Caps caps, cudaGraphConditionalHandle lev1) {
   pdl_entry();
+  GGMS_TRACE(60);
   if (lev1 && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(lev1, C->nbig[1] ? 1u : 0u);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nk; i += gridDim.x * blockDim.x) {
     const uint32_t s = k_seg[i];
     if (s == K_DONE) continue;
     relabel_one<K>(i, cmap0[k_bin[i]], k_seg, k_key, points, C, segs1, khead1, knext);
   }
+  GGMS_TRACE(61);
   bases_body<K>(crow, B, ncta, segs1, C, caps);
 }
 
@@ -1450,6 +1490,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
   constexpr int EPV = Vec16<T>::N;
   if (C->coarse) return;  // l0_compact_coarse copies this call's groups
   GGMS_TRACE(32);
+  GGMS_TRACE_CTA(2);
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ Windows<K> W;
   __shared__ RingBars rbars;
@@ -1681,6 +1722,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
       if (in_hot(key)) bucket_and_put(key);
     }
   }
+  GGMS_TRACE_CTA(3);
   if (overflow) set_status(C, GGMS_E_INTERNAL);
 }
 

@@ -148,10 +148,11 @@ __global__ __launch_bounds__(CNT_NT) void na_count(const float* __restrict__ in,
         }
         if (hit) idx = s * NBIN + ((u >> (24 - 8 * L)) & 255u);
       }
-      const uint32_t peers = __match_any_sync(FULL, idx);
-      if (idx != NONE && lane == (uint32_t)(__ffs(peers) - 1)) {
-        if (in_smem) atomicAdd(&shist[idx], (uint32_t)__popc(peers));
-        else atomicAdd(&ghist[idx], (uint32_t)__popc(peers));
+      if (in_smem) {  // shared atomics without a return value cost less than a match instruction
+        if (idx != NONE) atomicAdd(&shist[idx], 1u);
+      } else {  // global atomics: one per distinct counter of the warp
+        const uint32_t peers = __match_any_sync(FULL, idx);
+        if (idx != NONE && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&ghist[idx], (uint32_t)__popc(peers));
       }
     }
   }
