@@ -76,31 +76,32 @@ __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
 template <typename K> __host__ __device__ constexpr K key_max() { return (K)~(K)0; }
 
 // ------------------------------------------------------------------ block scan (1024 threads)
-// Inclusive scan of `cnt` (multiple of 1024) uint32 values in global memory, in place.
-// Returns (to thread 0) the maximum element.
+// Inclusive scan of `cnt` (multiple of NT) uint32 values in shared or global
+// memory, in place.  Returns (to thread 0) the maximum element.  Warp w scans
+// the contiguous chunk [w * cnt/32, (w + 1) * cnt/32) row by row (lane l holds
+// element 32 i + l of row i), so every access of a warp is 32 consecutive
+// words: no bank conflicts in shared memory, coalesced in global memory.
 template <int NT>
 __device__ void block_inclusive_scan_global(uint32_t* data, uint32_t cnt, uint32_t* smem_warp,
                                             uint32_t* max_out) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint32_t ipt = cnt / NT;
-  uint32_t* mine = data + (size_t)tid * ipt;
+  const uint32_t rows = cnt / NT;  // rows of 32 per warp
+  uint32_t* chunk = data + (size_t)warp * rows * 32u;
   uint32_t sum = 0, mx = 0;
-  for (uint32_t i = 0; i < ipt; ++i) {
-    uint32_t v = mine[i];
+  for (uint32_t i = 0; i < rows; ++i) {
+    const uint32_t v = chunk[i * 32u + lane];
     mx = max(mx, v);
     sum += v;
   }
-  // warp inclusive scan of thread sums
-  uint32_t inc = sum;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t t = __shfl_up_sync(FULL, inc, o);
-    if (lane >= o) inc += t;
+  for (int o = 16; o > 0; o >>= 1) {
+    sum += __shfl_xor_sync(FULL, sum, o);
+    mx = max(mx, __shfl_xor_sync(FULL, mx, o));
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(FULL, mx, o));
-  if (lane == 31) smem_warp[warp] = inc;
-  if (lane == 0) smem_warp[32 + warp] = mx;
+  if (lane == 0) {
+    smem_warp[warp] = sum;
+    smem_warp[32 + warp] = mx;
+  }
   __syncthreads();
   if (warp == 0) {
     uint32_t w = (lane < NT / 32) ? smem_warp[lane] : 0u;
@@ -116,10 +117,11 @@ __device__ void block_inclusive_scan_global(uint32_t* data, uint32_t cnt, uint32
     if (lane == 0) smem_warp[64] = wm;
   }
   __syncthreads();
-  uint32_t run = inc - sum + (warp > 0 ? smem_warp[warp - 1] : 0u);
-  for (uint32_t i = 0; i < ipt; ++i) {
-    run += mine[i];
-    mine[i] = run;
+  uint32_t carry = warp > 0 ? smem_warp[warp - 1] : 0u;
+  for (uint32_t i = 0; i < rows; ++i) {
+    const uint32_t inc = warp_incl_scan_u32(chunk[i * 32u + lane], lane);
+    chunk[i * 32u + lane] = carry + inc;
+    carry += __shfl_sync(FULL, inc, 31);
   }
   if (tid == 0 && max_out) *max_out = smem_warp[64];
   __syncthreads();

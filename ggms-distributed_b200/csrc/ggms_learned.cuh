@@ -447,7 +447,7 @@ static int learn_and_choose(int kind, const K* sorted, uint32_t S, uint32_t B, i
                                     sampled_done, pl_knots);
     if (rc) return rc;
   } else {
-    const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 2u;
+    const uint32_t steps = steps_opt > 0 ? (uint32_t)steps_opt : 1u;
     if (launch_pdl(setup_pl_knots<K>, 2, SETUP_NT, sizeof(LearnSmem<K>), st, sorted, S, B, &As[1], pl_knots, krank,
                    nk, n, window_z, L) != cudaSuccess ||
         launch_pdl(pl_stats_grid<K>, (PL_M + 31) / 32, 1024, 0, st, sorted, S, (const Assigner<K>*)&As[1], L) !=

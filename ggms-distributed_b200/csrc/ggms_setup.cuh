@@ -614,10 +614,11 @@ __device__ void build_warp(const uint32_t* __restrict__ krank, uint32_t nk, uint
 // Occupancy of the grid's buckets on the (sorted) sample, over 256 groups of
 // buckets: max / mean.
 // At most GRID_MEASURE_N samples are used (a strided subsample of the sorted
-// sample, still sorted): 32 per group on average, enough to see imbalance
-// against the bound (3.0: a group holding three times its share), and all of
-// a thread's samples are loaded at once.
-constexpr uint32_t GRID_MEASURE_N = 8192;
+// sample, still sorted): 16 per group on average, enough to see imbalance
+// against the bound (3.0: a group holding three times its share; a model that
+// fits the sample exactly reads about 1.8 from the sampling noise alone), and
+// all of a thread's samples are loaded at once.
+constexpr uint32_t GRID_MEASURE_N = 4096;
 
 template <typename K>
 __device__ float grid_measure(const GridView<K>& g, const K* sorted_all, uint32_t S_all, uint32_t* hist256,
