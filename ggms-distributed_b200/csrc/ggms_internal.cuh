@@ -71,6 +71,12 @@ __device__ __forceinline__ void pdl_entry() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
+// The two halves, for kernels that read data older than their predecessor's
+// output before waiting: a kernel's CTAs start only after its predecessor has
+// passed its own wait, i.e. after the kernel before that has completed, so
+// anything written two or more kernels back may be read before pdl_wait().
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // ------------------------------------------------------------------ key traits
 template <typename T> struct KeyOf;

@@ -890,7 +890,9 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_count(const T* __res
                                               const Windows<typename KeyOf<T>::K>* __restrict__ Wg,
                                               uint32_t* __restrict__ hist0, uint32_t* __restrict__ crow,
                                               uint32_t ring_st) {
-  pdl_entry();
+  // the grid (final since the assigner, two or more kernels back) is loaded
+  // while the predecessor, which zeroes hist0 and possibly the windows, ends
+  pdl_trigger();
   using K = typename KeyOf<T>::K;
   constexpr int EPV = Vec16<T>::N;
   extern __shared__ __align__(128) uint8_t smem[];
@@ -906,9 +908,10 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_count(const T* __res
   const GridView<K> gv = grid_to_smem<K>(G, s1, s2);
   const uint32_t B = gv.B;
   K* wq = reinterpret_cast<K*>(hs + B) + (threadIdx.x >> 5) * WQ_DEPTH;
+  for (uint32_t i = threadIdx.x; i < B; i += NT) hs[i] = 0u;
+  pdl_wait();
   if (threadIdx.x == 0) W = *Wg;
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&C->passes, 1u);
-  for (uint32_t i = threadIdx.x; i < B; i += NT) hs[i] = 0u;
   __syncthreads();
   const uint32_t lane = threadIdx.x & 31;
 
@@ -1154,7 +1157,7 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
                             K* points, uint32_t* khead1, uint32_t* smalls, uint32_t* bigs1, Caps caps,
                             const uint32_t* __restrict__ ic, const uint32_t* __restrict__ aflagc,
                             const uint32_t* __restrict__ kcnt0, uint32_t tiny_keys, uint32_t* tinies) {
-  pdl_entry();
+  pdl_trigger();  // the grid is loaded before the wait (it is older than the predecessor's output)
   // the key-range searches read the grid a few dozen times per bucket: keep
   // it in shared memory (every thread helps load it before any returns)
   __shared__ uint2 s1[GRID_T1];
@@ -1168,6 +1171,7 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
   const Grid<K>* G = Gs + C->asg_choice;
   const GridView<K> gv = grid_to_smem<K>(G, s1, s2);
   const uint32_t ncell = G->ncell;
+  pdl_wait();
   __syncthreads();
   GGMS_TRACE(29);
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1487,17 +1491,22 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
                                                 const uint32_t* __restrict__ crow,
                                                 typename KeyOf<T>::K* dst, uint64_t dst_cap,
                                                 uint32_t ring_st, const uint32_t* __restrict__ I0) {
-  pdl_entry();
+  // Before the wait: the grid, the windows, the child map and the counts (all
+  // from two or more kernels back); after it: the write cursors (crow), which
+  // the predecessor (l0_relabel_bases) forms.
+  pdl_trigger();
   using K = typename KeyOf<T>::K;
   constexpr int EPV = Vec16<T>::N;
-  if (C->coarse) return;  // l0_compact_coarse copies this call's groups
+  if (C->coarse) {  // l0_compact_coarse copies this call's groups
+    pdl_wait();
+    return;
+  }
   GGMS_TRACE(32);
   GGMS_TRACE_CTA(2);
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ Windows<K> W;
   __shared__ RingBars rbars;
   if (threadIdx.x == 0) W = *Wg;
-  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&C->passes, 1u);
   const Grid<K>* G = Gs + C->asg_choice;
   uint2* s1 = (uint2*)smem;
   uint2* s2 = s1 + GRID_T1;
@@ -1512,13 +1521,17 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
   const uint32_t* myrow = crow + (size_t)blockIdx.x * B;
   for (uint32_t w = warp; w < B / 32; w += NT / 32) {
     const uint32_t b = w * 32 + lane;
-    const bool copied = cmap0[b] < CM_POINT;
-    if (copied) cur[b] = myrow[b];
-    const uint32_t bits = __ballot_sync(FULL, copied);
+    const uint32_t bits = __ballot_sync(FULL, cmap0[b] < CM_POINT);
     if (lane == 0) {
       amask[w] = bits;
       wpre[w] = __popc(bits);
     }
+  }
+  pdl_wait();
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&C->passes, 1u);
+  for (uint32_t w = warp; w < B / 32; w += NT / 32) {
+    const uint32_t b = w * 32 + lane;
+    if (cmap0[b] < CM_POINT) cur[b] = myrow[b];
   }
   __shared__ unsigned long long hot_mass_s;
   __shared__ K run_lo[L0_RUNS], run_span[L0_RUNS];
