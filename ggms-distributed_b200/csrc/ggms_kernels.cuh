@@ -1150,7 +1150,8 @@ constexpr uint32_t TS_SORT_ABOVE = 8;
 // one global atomic per counter -- a global counter bumped by every active
 // bucket serialises ~10^3 same-address atomics in L2.
 template <typename K>
-__global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __restrict__ aflag,
+__global__ __launch_bounds__(1024) void l0_children(const uint32_t* __restrict__ I,
+                                                    const uint32_t* __restrict__ aflag,
                             uint32_t B, const Grid<K>* __restrict__ Gs, Counters* C,
                             const Windows<K>* __restrict__ Wg,
                             uint32_t* cmap0, Seg<K>* segs1, uint32_t* cursor1, TileRef* tiles1,
@@ -1213,23 +1214,16 @@ __global__ void l0_children(const uint32_t* __restrict__ I, const uint32_t* __re
   }
   __syncthreads();
   GGMS_TRACE(58);
-  // 2. the block's ranges in the shared lists
-  if (threadIdx.x == 0 && ctr[N_ACT]) {
-    atomicAdd(&C->active0, ctr[N_ACT]);
-    if (ctr[N_PT]) {
-      atomicAdd(&C->point0, ctr[N_PT]);
-      cbase[N_PT] = atomicAdd(&C->npoints, ctr[N_PT]);
-    }
-    if (ctr[N_SEG]) {
-      cbase[N_SEG] = atomicAdd(&C->nsegs[1], ctr[N_SEG]);
-      atomicAdd(&C->cand0, cand_s);
-    }
-    if (ctr[N_TINY]) cbase[N_TINY] = atomicAdd(&C->ntiny, ctr[N_TINY]);
-    if (ctr[N_SMALL]) cbase[N_SMALL] = atomicAdd(&C->nsmall, ctr[N_SMALL]);
-    if (ctr[N_BIG]) {
-      cbase[N_BIG] = atomicAdd(&C->nbig[1], ctr[N_BIG]);
-      cbase[N_TILE] = atomicAdd(&C->ntiles[1], ctr[N_TILE]);
-    }
+  // 2. the block's ranges in the shared lists: one lane per counter, so the
+  //    global atomics (each an L2 round trip) are in flight together
+  if (threadIdx.x < 32u && ctr[N_ACT]) {
+    const uint32_t t = threadIdx.x;
+    uint32_t* const cp = t == N_ACT ? &C->active0 : t == N_PT ? &C->npoints : t == N_SEG ? &C->nsegs[1]
+                         : t == N_TINY ? &C->ntiny : t == N_SMALL ? &C->nsmall : t == N_BIG ? &C->nbig[1]
+                                                                                            : &C->ntiles[1];
+    if (t < N_CTR && ctr[t]) cbase[t] = atomicAdd(cp, ctr[t]);
+    if (t == N_CTR && ctr[N_PT]) atomicAdd(&C->point0, ctr[N_PT]);
+    if (t == N_CTR + 1u && ctr[N_SEG]) atomicAdd(&C->cand0, cand_s);
   }
   __syncthreads();
   GGMS_TRACE(59);

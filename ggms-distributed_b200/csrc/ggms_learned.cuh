@@ -200,10 +200,13 @@ __device__ float pl_fb(float theta, const PLStats* st, uint32_t M, double S, PLR
   return (float)(L / S);
 }
 
-// Adam on theta (thread j owns theta_j).  Returns the final loss.
+// Adam on theta (thread j owns theta_j).  Returns the best loss seen.  Every
+// evaluation writes its CDF at the knots, alternating between cdf_out and
+// cdf_alt so that the best one is never overwritten: no final evaluation is
+// needed; thread 0 stores 1 in *in_alt when the best CDF is in cdf_alt.
 __device__ float pl_train_block(const PLStats* st, uint32_t M, uint32_t S, uint32_t steps, float lr,
-                                PLRed& red, float* cdf_out, float* loss0_out, float* theta_out,
-                                float* grad_out) {
+                                PLRed& red, float* cdf_out, float* cdf_alt, uint32_t* in_alt,
+                                float* loss0_out, float* theta_out, float* grad_out) {
   // start from the sample's own CDF: increments proportional to each segment's
   // sample count (for knots at uniform quantiles, all 1: softplus^-1(1))
   float theta;
@@ -215,28 +218,30 @@ __device__ float pl_train_block(const PLStats* st, uint32_t M, uint32_t S, uint3
   float m1 = 0.0f, m2 = 0.0f, g = 0.0f;
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
   float b1t = 1.0f, b2t = 1.0f;
-  float loss = pl_fb(theta, st, M, (double)S, red, &g, nullptr);
+  float loss = pl_fb(theta, st, M, (double)S, red, &g, cdf_out);
   if (loss0_out && threadIdx.x == 0) *loss0_out = loss;
-  // keep the best parameters seen: the quantile init is already close to the
+  // keep the best parameters seen: the initialisation is already close to the
   // optimum, so a step can overshoot; the result never loses to the init
-  float best = loss, best_theta = theta;
+  float best = loss, best_theta = theta, best_g = g;
+  bool alt = false;  // the best CDF is in cdf_alt
   for (uint32_t it = 0; it < steps; ++it) {
     b1t *= b1;
     b2t *= b2;
     m1 = b1 * m1 + (1.0f - b1) * g;
     m2 = b2 * m2 + (1.0f - b2) * g * g;
     theta -= lr * (m1 / (1.0f - b1t)) / (sqrtf(m2 / (1.0f - b2t)) + eps);
-    loss = pl_fb(theta, st, M, (double)S, red, &g, nullptr);
+    loss = pl_fb(theta, st, M, (double)S, red, &g, alt ? cdf_out : cdf_alt);
     if (loss < best) {  // the loss is block-uniform: every thread takes the same branch
       best = loss;
       best_theta = theta;
+      best_g = g;
+      alt = !alt;
     }
   }
-  theta = best_theta;
-  loss = pl_fb(theta, st, M, (double)S, red, &g, cdf_out);
-  if (theta_out && threadIdx.x < M) theta_out[threadIdx.x] = theta;
-  if (grad_out && threadIdx.x < M) grad_out[threadIdx.x] = g;
-  return loss;
+  if (theta_out && threadIdx.x < M) theta_out[threadIdx.x] = best_theta;
+  if (grad_out && threadIdx.x < M) grad_out[threadIdx.x] = best_g;
+  if (threadIdx.x == 0) *in_alt = alt ? 1u : 0u;
+  return best;
 }
 
 // New bases (strictly increasing) and slopes of a PL assigner from CDF values
@@ -380,9 +385,11 @@ __global__ __launch_bounds__(SETUP_NT) void setup_learned_pl(const K* __restrict
   GGMS_TRACE(9);
   pl_stats_load(L, M, sm.st);
   GGMS_TRACE(10);
+  __shared__ uint32_t in_alt;
   if (threadIdx.x < PL_NT) {
-    const float loss = pl_train_block(sm.st, M, S, steps, lr, sm.red, sm.cdf, &L->loss_init,
-                                      L->theta, L->grad);
+    // sm.qcdf (the knot placement's scratch) is free here: the second CDF buffer
+    const float loss = pl_train_block(sm.st, M, S, steps, lr, sm.red, sm.cdf, sm.qcdf, &in_alt,
+                                      &L->loss_init, L->theta, L->grad);
     if (threadIdx.x == 0) {
       L->loss = loss;
       L->M = M;
@@ -390,6 +397,10 @@ __global__ __launch_bounds__(SETUP_NT) void setup_learned_pl(const K* __restrict
     }
   }
   __syncthreads();
+  if (in_alt) {
+    for (uint32_t j = threadIdx.x; j <= M; j += blockDim.x) sm.cdf[j] = sm.qcdf[j];
+    __syncthreads();
+  }
   GGMS_TRACE(11);
   if (threadIdx.x == 0) wsh = L->warp;  // built with the knots (setup_pl_knots)
   __syncthreads();

@@ -48,6 +48,7 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
   const uint32_t tid = threadIdx.x;
   GGMS_TRACE(17);
   const GridView<K> gv = grid_to_smem<K>(Gs + C->asg_choice, s1, s2);
+  const uint32_t ncell = Gs[C->asg_choice].ncell;
   const uint32_t B = gv.B;
   int32_t* cnt = reinterpret_cast<int32_t*>(bm + B / 32u);  // difference array [B + 1]
   const uint32_t nidx = (S + WIN_IDX - 1u) / WIN_IDX;  // S <= 65536
@@ -155,12 +156,8 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
       v = (K)0;
     } else if (upper && target >= B) {
       v = key_max<K>();
-    } else {
-      K lo = 0, hi = key_max<K>();
-      while (lo < hi) {
-        const K mid = lo + ((hi - lo) >> 1);
-        if (min(grid_eval<K>(gv, mid), B - 1u) >= target) hi = mid; else lo = mid + 1;
-      }
+    } else {  // target <= B - 1: the clamp to B - 1 does not change the answer
+      const K lo = grid_inv<K>(gv, ncell, target);
       v = upper ? (lo == 0 ? (K)0 : (K)(lo - 1u)) : lo;
     }
     if (upper) sw.hi[r] = v; else sw.lo[r] = v;
