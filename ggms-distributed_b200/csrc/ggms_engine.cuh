@@ -340,21 +340,16 @@ static int launch_small_select(Context* ctx, const InT* src, const Seg<K>* segs_
                                  (int)sm));
     attr = true;
   }
-  // the warp finisher (its own list of segments) runs on the side stream,
-  // next to the CTA finisher
-  if (caps.tiny_keys) {
-    if (const int r_ = ensure_side(ctx)) return r_;
-    GGMS_CU(cudaEventRecord(ctx->fork2, st));
-    GGMS_CU(cudaStreamWaitEvent(ctx->side, ctx->fork2, 0));
-    ++ctx->launches;
-    tiny_select<InT, TS_NT><<<ctx->sms * 8, TS_NT, 0, ctx->side>>>(src, segs_q, w.tinies, w.C, khead_q, w.knext,
-                                                                   k_off, w.krank, w.kseg, w.kkey, caps);
-    GGMS_CU(cudaEventRecord(ctx->join2, ctx->side));
-  }
   ++ctx->launches;
   GGMS_CU(launch_pdl(small_select<InT, SS_NT>, ctx->sms * 2, SS_NT, sm, st, src, segs_q, w.smalls, w.C, khead_q,
                      w.knext, k_off, w.krank, w.kseg, w.kkey, caps.small_keys, caps));
-  if (caps.tiny_keys) GGMS_CU(cudaStreamWaitEvent(st, ctx->join2, 0));
+  // the warp finisher (its own list of segments) runs beside the CTA finisher:
+  // it does not wait for it before its work (tiny_select)
+  if (caps.tiny_keys) {
+    ++ctx->launches;
+    GGMS_CU(launch_pdl(tiny_select<InT, TS_NT>, ctx->sms * 8, TS_NT, 0, st, src, segs_q, w.tinies, w.C, khead_q,
+                       w.knext, k_off, w.krank, w.kseg, w.kkey, caps));
+  }
   return GGMS_OK;
 }
 

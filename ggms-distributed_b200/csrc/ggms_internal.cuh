@@ -39,8 +39,9 @@ static __device__ unsigned long long ggms_trace_buf[64];
     }                                                                  \
   } while (0)
 // Per-CTA points of the two passes: thread 0 of every block stores its
-// %globaltimer in row i (0/1 PASS 1 start/end, 2/3 PASS 2 start/end).
-static __device__ unsigned long long ggms_trace_cta[4][1024];
+// %globaltimer in row i (0/1 PASS 1 start/end, 2/3 PASS 2 start/end, 4/5 end of
+// the CTA and warp finishers).
+static __device__ unsigned long long ggms_trace_cta[6][1024];
 #define GGMS_TRACE_CTA(i)                                              \
   do {                                                                 \
     if (threadIdx.x == 0 && blockIdx.x < 1024) {                       \
@@ -336,7 +337,12 @@ __device__ K grid_inv(const GridView<K>& g, uint32_t ncell, uint32_t target) {
     cand = (K)(first + ((K)1 << sh));
   } else {
     const uint32_t s = min(sh, 32u);  // grid_lin interpolates on the top 32 bits of the offset
-    const uint64_t top = (((uint64_t)t << s) + span - 1u) / span;
+    // ceil(t * 2^s / span): the quotient (< 2^48) from a double division, then
+    // corrected to the exact integer ceiling with two multiplications
+    const uint64_t num = (uint64_t)t << s;
+    uint64_t top = (uint64_t)ceil(__ddiv_rn((double)num, (double)span));
+    if (top * span < num) ++top;
+    else if (top > 0u && (top - 1u) * span >= num) --top;
     cand = (K)(first + ((K)top << (sh - s)));
   }
   if (cand != (K)0 && grid_eval<K>(g, cand) >= target && grid_eval<K>(g, (K)(cand - 1u)) < target) return cand;

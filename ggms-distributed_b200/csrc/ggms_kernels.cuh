@@ -2510,6 +2510,7 @@ __global__ __launch_bounds__(NT) void small_select(const InT* __restrict__ src,
     __syncthreads();
   }
   GGMS_TRACE(36);
+  GGMS_TRACE_CTA(4);
 }
 
 // One warp finishes a whole tiny segment (at most tiny_keys<K>() keys, as
@@ -2586,7 +2587,10 @@ __global__ __launch_bounds__(NT) void tiny_select(const InT* __restrict__ src,
                                                  const int64_t* __restrict__ k_off,
                                                  const uint32_t* __restrict__ k_rank, uint32_t* k_seg,
                                                  typename KeyOf<InT>::K* k_key, Caps caps) {
-  pdl_entry();
+  // Launched right after small_select, whose output it does not read: it lets
+  // its successor launch and runs beside small_select, and waits for it only
+  // at its end (so that it completes after its predecessor).
+  pdl_trigger();
   using K = typename KeyOf<InT>::K;
   constexpr uint32_t TK = tiny_keys<K>();
   constexpr int NW = NT / 32;
@@ -2695,6 +2699,8 @@ __global__ __launch_bounds__(NT) void tiny_select(const InT* __restrict__ src,
     if (lane == 0) atomicAdd(&C->small_segs, nb);
   }
   GGMS_TRACE(40);
+  GGMS_TRACE_CTA(5);
+  pdl_wait();
 }
 
 // ------------------------------------------------------------------ batched segments
