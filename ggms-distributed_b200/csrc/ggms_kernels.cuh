@@ -2646,7 +2646,44 @@ __global__ __launch_bounds__(NT) void tiny_select(const InT* __restrict__ src,
       }
       __syncwarp();
       const int bits = bitlen((K)(s.hi - s.lo));
-      if (k_off) {
+      // Up to 64 keys: every key's rank by comparing it with all the others (ties
+      // broken by position), once for all of the segment's ks; a k is then one
+      // ballot.  Cheaper than 8-bit radix rounds, whose 256-bin histograms cost
+      // the same however few keys there are.
+      const bool by_rank = cnt <= 64u;
+      uint32_t ra = 0xFFFFFFFFu, rb = 0xFFFFFFFFu;
+      K ka = 0, kb = 0;
+      if (by_rank) {
+        ka = lane < cnt ? v[lane] : (K)0;
+        kb = lane + 32u < cnt ? v[lane + 32u] : (K)0;
+        uint32_t ca = 0, cb = 0;
+        for (uint32_t j = 0; j < cnt; ++j) {
+          const K x = v[j];
+          ca += (x < ka || (x == ka && j < lane)) ? 1u : 0u;
+          cb += (x < kb || (x == kb && j < lane + 32u)) ? 1u : 0u;
+        }
+        if (lane < cnt) ra = ca;
+        if (lane + 32u < cnt) rb = cb;
+      }
+      auto rank_pick = [&](uint32_t r, bool* ok) -> K {
+        const uint32_t ma = __ballot_sync(FULL, ra == r), mb = __ballot_sync(FULL, rb == r);
+        *ok = (ma | mb) != 0u;
+        const K xa = __shfl_sync(FULL, ka, ma ? __ffs(ma) - 1 : 0);
+        const K xb = __shfl_sync(FULL, kb, mb ? __ffs(mb) - 1 : 0);
+        return ma ? xa : xb;
+      };
+      if (k_off && by_rank) {
+        const int64_t k0 = k_off[id], k1 = k_off[id + 1];
+        for (int64_t k = k0; k < k1; ++k) {
+          if (k_seg[k] == K_DONE) continue;  // warp-uniform
+          bool ok = false;
+          const K pre = rank_pick(k_rank[k], &ok);
+          if (lane == 0) {
+            if (ok) k_key[k] = (K)(s.lo + pre); else set_status(C, GGMS_E_INTERNAL);
+            k_seg[k] = K_DONE;
+          }
+        }
+      } else if (k_off) {
         const int64_t k0 = k_off[id], k1 = k_off[id + 1];
         if ((uint64_t)(k1 - k0) > TS_SORT_ABOVE) {
           uint32_t N = 32;
@@ -2687,7 +2724,8 @@ __global__ __launch_bounds__(NT) void tiny_select(const InT* __restrict__ src,
         for (uint32_t k = khead; k != K_NIL; k = knext[k]) {
           bool ok = false;
           const uint32_t r = k_rank[k];
-          const K pre = r < cnt ? warp_radix_select<K>(v, cnt, bits, r, h, lane, &ok) : (K)0;
+          const K pre = by_rank ? rank_pick(r, &ok)
+                                : (r < cnt ? warp_radix_select<K>(v, cnt, bits, r, h, lane, &ok) : (K)0);
           if (lane == 0) {
             if (ok) k_key[k] = (K)(s.lo + pre); else set_status(C, GGMS_E_INTERNAL);
             k_seg[k] = K_DONE;
