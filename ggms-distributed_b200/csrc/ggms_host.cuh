@@ -249,7 +249,7 @@ static int make_plan(Plan* p, uint64_t n, uint32_t nk, const ggms_opts& o) {
   p->cap_tiles = (uint32_t)((n + TILE - 1) / TILE) + p->cap_seg;
   p->train_steps = o.train_steps > 0 ? o.train_steps : 0;
   p->bound = o.imbalance_bound > 0.0f ? o.imbalance_bound : 3.0f;
-  p->window_z = o.window_z == 0.0f ? 8.0f : o.window_z;
+  p->window_z = o.window_z == 0.0f ? 6.0f : o.window_z;
   p->seed = o.seed;
   p->cap_q = 0;
   if (o.pl_knots != 0 && (o.pl_knots < 16 || o.pl_knots > 1024)) return GGMS_E_INVALID_ARG;

@@ -292,8 +292,16 @@ __device__ __forceinline__ uint32_t grid_eval(const GridView<K>& g, K key) {
     sh = g.sh1 - sb;
     e = g.t2[e.y + ((uint32_t)(d >> sh) & ((1u << sb) - 1u))];
   }
-  const K off = d & (K)(((K)1 << sh) - 1);
-  return e.x + grid_lin(off, e.y - e.x, sh);
+  if constexpr (sizeof(K) == 4) {
+    // floor(off * span / 2^sh) with off = d mod 2^sh: shifting d left by 32 - sh
+    // drops the bits above the offset and scales it by 2^(32 - sh), so the high
+    // word of the product with span is the same floor.  The clamped funnel
+    // shift gives 0 for sh = 0 (a one-key cell, offset 0).
+    return e.x + __umulhi(__funnelshift_lc(0u, (uint32_t)d, 32u - sh), e.y - e.x);
+  } else {
+    const K off = d & (K)(((K)1 << sh) - 1);
+    return e.x + grid_lin(off, e.y - e.x, sh);
+  }
 }
 
 // Smallest key whose grid bucket is >= target (the largest key when no key's is): the

@@ -411,8 +411,24 @@ __device__ __forceinline__ GridView<K> grid_view_global(const Grid<K>* G) {
 template <typename K>
 __device__ __forceinline__ GridView<K> grid_to_smem(const Grid<K>* __restrict__ G, uint2* s1, uint2* s2) {
   const uint32_t nc = G->ncell, ns = G->nsubent;
-  for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) s1[i] = G->t1[i];
-  for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x) s2[i] = G->t2[i];
+  // both tables as one index range, 8 loads in flight per thread
+  const uint32_t tot = nc + ns, nt = blockDim.x;
+  for (uint32_t i0 = threadIdx.x; i0 < tot; i0 += 8u * nt) {
+    uint2 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const uint32_t i = i0 + (uint32_t)u * nt;
+      if (i < tot) v[u] = i < nc ? G->t1[i] : G->t2[i - nc];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const uint32_t i = i0 + (uint32_t)u * nt;
+      if (i < tot) {
+        if (i < nc) s1[i] = v[u];
+        else s2[i - nc] = v[u];
+      }
+    }
+  }
   GridView<K> v;
   v.t1 = s1; v.t2 = s2; v.origin = G->origin; v.gmax = G->gmax;
   v.sh1 = G->sh1; v.B = G->B;
@@ -1332,14 +1348,24 @@ __global__ __launch_bounds__(1024) void l0_between(uint32_t* hist0, uint32_t B, 
   // 1. inclusive scan of the counts (and the largest bucket outside the gap buckets)
   const bool on = W.on != 0u;
   uint32_t m = 0;
-  for (uint32_t i = tid; i < B; i += 1024) {
-    const uint32_t v = hist0[i];
-    I[i] = v;
-    if (on) {
-      bool gap = false;
+  for (uint32_t i0 = tid; i0 < B; i0 += 8u * 1024u) {  // 8 loads in flight per thread
+    uint32_t v[8];
 #pragma unroll
-      for (uint32_t g = 0; g <= L0_WIN; ++g) gap = gap || (g <= W.R && i == W.gb0[g]);
-      if (!gap) m = max(m, v);
+    for (int u = 0; u < 8; ++u) {
+      const uint32_t i = i0 + (uint32_t)u * 1024u;
+      v[u] = i < B ? hist0[i] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const uint32_t i = i0 + (uint32_t)u * 1024u;
+      if (i >= B) break;
+      I[i] = v[u];
+      if (on) {
+        bool gap = false;
+#pragma unroll
+        for (uint32_t g = 0; g <= L0_WIN; ++g) gap = gap || (g <= W.R && i == W.gb0[g]);
+        if (!gap) m = max(m, v[u]);
+      }
     }
   }
   __syncthreads();
@@ -1406,23 +1432,33 @@ __device__ __forceinline__ void bases_body(uint32_t* crow, uint32_t B, uint32_t 
     // group, whose column then holds the group's cursors)
     const uint32_t b = coarse ? s.pad << gsh : s.pad;
     uint64_t run = s.off;
-    for (uint32_t g0 = 0; g0 < ncta; g0 += 32) {
-      const uint32_t g = g0 + lane;
-      uint32_t v = 0u;
-      if (g < ncta) {
-        if (coarse)
-          for (uint32_t j = 0; j < (1u << gsh); ++j) v += crow[(size_t)g * B + b + j];
-        else
-          v = crow[(size_t)g * B + b];
-      }
-      uint32_t inc = v;
+    // a column of up to 256 CTAs' counts per batch, all loads in flight at once
+    constexpr int BB = 8;
+    for (uint32_t g0 = 0; g0 < ncta; g0 += 32u * BB) {
+      uint32_t v[BB];
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(FULL, inc, o);
-        if ((int)lane >= o) inc += t;
+      for (int u = 0; u < BB; ++u) {
+        const uint32_t g = g0 + (uint32_t)u * 32u + lane;
+        v[u] = 0u;
+        if (g < ncta) {
+          if (coarse)
+            for (uint32_t j = 0; j < (1u << gsh); ++j) v[u] += crow[(size_t)g * B + b + j];
+          else
+            v[u] = crow[(size_t)g * B + b];
+        }
       }
-      if (g < ncta) crow[(size_t)g * B + b] = (uint32_t)(run + inc - v);
-      run += __shfl_sync(FULL, inc, 31);
+#pragma unroll
+      for (int u = 0; u < BB; ++u) {
+        const uint32_t g = g0 + (uint32_t)u * 32u + lane;
+        uint32_t inc = v[u];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t t = __shfl_up_sync(FULL, inc, o);
+          if ((int)lane >= o) inc += t;
+        }
+        if (g < ncta) crow[(size_t)g * B + b] = (uint32_t)(run + inc - v[u]);
+        run += __shfl_sync(FULL, inc, 31);
+      }
     }
   }
 }
@@ -1521,12 +1557,9 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
       wpre[w] = __popc(bits);
     }
   }
-  pdl_wait();
-  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&C->passes, 1u);
-  for (uint32_t w = warp; w < B / 32; w += NT / 32) {
-    const uint32_t b = w * 32 + lane;
-    if (cmap0[b] < CM_POINT) cur[b] = myrow[b];
-  }
+  // The cell bitmasks and runs below read only what kernels two or more back
+  // wrote (the grid, windows, child map and counts), so they are built before
+  // the dependency wait, while the write cursors are still being formed.
   __shared__ unsigned long long hot_mass_s;
   __shared__ K run_lo[L0_RUNS], run_span[L0_RUNS];
   __shared__ uint32_t nruns_s, ncopied_s;
@@ -1625,6 +1658,22 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
       }
       if (in_run) record(start, ncell - 1u);
       nruns_s = nr;
+    }
+  }
+  pdl_wait();
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&C->passes, 1u);
+  // the write cursors, 8 loads in flight per thread (this is on the critical path)
+  for (uint32_t b0 = threadIdx.x; b0 < B; b0 += 8u * NT) {
+    uint32_t v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const uint32_t b = b0 + (uint32_t)u * NT;
+      v[u] = (b < B && ((amask[b >> 5] >> (b & 31)) & 1u)) ? myrow[b] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const uint32_t b = b0 + (uint32_t)u * NT;
+      if (b < B) cur[b] = v[u];
     }
   }
   __syncthreads();

@@ -5,8 +5,8 @@
 // Here the sorted sample already says roughly where each k lies: if the k-th
 // key has ascending rank r, the number of sample keys below it is binomial
 // (S, q = (r + 1/2) / n), so the key lies between the sample keys at positions
-// S q -+ m, m = z sqrt(S q (1 - q)) + z + 2, except with a probability far
-// below 10^-12 for z = 8.  Every k thus gets a range of level-0 buckets; their
+// S q -+ m, m = z sqrt(S q (1 - q)) + z + 2, except with a probability below
+// 10^-9 for the default z = 6 (a miss costs time, never exactness).  Every k thus gets a range of level-0 buckets; their
 // union, merged across gaps that hold under 1/256 of the sample into at most
 // L0_WIN runs holding at most a quarter of it, is the only place PASS 1 computes
 // buckets.  Keys elsewhere are counted per gap between runs (a few compares),

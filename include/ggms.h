@@ -95,13 +95,14 @@ typedef struct ggms_opts {
                                    thread with cp.async into its own shared-memory slots, three chunks
                                    ahead (-1 and -2: pass_threads 1024 only); 0 = the default (4) */
   float window_z;               /* PASS 1 windows: safety margin of the predicted k positions in
-                                   binomial standard deviations; 0 = 8; < 0 = no windows */
+                                   binomial standard deviations; 0 = 6; < 0 = no windows */
   int32_t autotune;             /* 1: when num_buckets and the pass shape are left at 0, the first call of a
                                    shape class times the candidates on the caller's data and the context
                                    keeps the fastest (the batched path tunes its level kernels' CTAs) */
   ggms_stats* stats;            /* optional host pointer */
   int32_t pl_knots;             /* segments of the learned piecewise-linear CDF model: 16..1024;
-                                   0 = auto (min(1024, num_buckets / 4)).  Appended last: a caller
+                                   0 = auto (PL: min(512, num_buckets / 4); MLP: min(1024,
+                                   num_buckets / 4)).  Appended last: a caller
                                    built against the layout without it (struct_size = its offset)
                                    is still accepted and gets the default */
   int32_t pad0;
