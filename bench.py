@@ -80,8 +80,8 @@ WORKLOADS = {
 # capture of the same kernels on the same half-normal workload at n = 2^26
 # (profiles/l0_passes_half_normal_f32_n26.md); both passes read the input once,
 # so the traffic of a launch grows in proportion to n.
-PASS_TRAFFIC_PER_ELEM = {"l0_count": (268580096 + 3641344) / 2**26,
-                         "l0_compact": (271806720 + 3763712) / 2**26}
+PASS_TRAFFIC_PER_ELEM = {"l0_count": (268612096 + 3892224) / 2**26,
+                         "l0_compact": (271976960 + 3587840) / 2**26}
 
 
 def peaks():
