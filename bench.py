@@ -647,8 +647,23 @@ def run_kernels_only(args):
     import ggms_b200 as G
     torch.cuda.set_device(0)
     w = dict(WORKLOADS[args.workload])
-    if w["kind"] != "single":
-        raise SystemExit("--kernels-only runs the single-vector workloads")
+    if w["kind"] != "single":  # the batched workloads at their stated shape, default options
+        vals, seg_off, ks, k_off = segmented_inputs(w)
+        view = {np.dtype(np.uint32): np.int32}.get(vals.dtype)
+        d_v = torch.from_numpy(vals.view(view) if view else vals).cuda()
+        d_so, d_ko = torch.from_numpy(seg_off).cuda(), torch.from_numpy(k_off).cuda()
+        d_k = torch.from_numpy(ks.view(np.int32)).cuda()
+        d_out = torch.empty(len(ks), dtype=torch.int32, device="cuda")
+        ctx = G.Context(0)
+        for _ in range(args.steps):
+            rc = G.segmented(ctx, d_v.data_ptr(), d_so.data_ptr(), len(seg_off) - 1, d_k.data_ptr(),
+                             d_ko.data_ptr(), d_out.data_ptr(), vals.dtype)
+            if rc:
+                raise G.GGMSError(rc, "segmented")
+        torch.cuda.synchronize()
+        ctx.close()
+        print("kernels-only run done", int(seg_off[-1]), args.steps)
+        return
     w["n"] = 1 << args.n_log2
     v, ks = single_inputs(w)
     d_v = torch.from_numpy(v).cuda()

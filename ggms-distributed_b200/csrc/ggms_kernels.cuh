@@ -2154,17 +2154,38 @@ __global__ __launch_bounds__(NT) void lvl_count(const InT* __restrict__ src,
   const uint32_t nt = min(C->ntiles[p], caps.tiles);
   const uint32_t ns = min(C->nsegs[p], caps.segs);
   if (Q && nt && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&C->passes, 1u);  // level 0 reads the input
-  uint32_t loaded = 0xFFFFFFFFu;  // quantile table in shared memory
-  for (uint32_t t = blockIdx.x; t < nt; t += gridDim.x) {
+  // Each CTA takes a contiguous range of the tile list, where a segment's tiles
+  // are consecutive: the histogram of one segment's run of tiles stays in
+  // shared memory and is added to the segment's row once per run, not once
+  // per tile (a row holds NBIN bins for TILE keys), and the quantile table is
+  // loaded once per run.
+  const uint32_t per = (nt + gridDim.x - 1) / gridDim.x;
+  const uint32_t t_beg = min(blockIdx.x * per, nt), t_end = min(t_beg + per, nt);
+  uint32_t open = 0xFFFFFFFFu;  // segment whose counts the shared histogram holds
+  unsigned long long open_keys = 0;
+  auto flush = [&]() {  // all threads, after a barrier
+    uint32_t* row = rows + (size_t)open * NBIN;
+    for (uint32_t i = threadIdx.x; i < NBIN; i += NT) {
+      const uint32_t v = h[i];
+      if (v) atomicAdd(&row[i], v);
+    }
+    if (threadIdx.x == 0) atomicAdd(&C->refine_elems, open_keys);
+  };
+  for (uint32_t t = t_beg; t < t_end; ++t) {
     const TileRef tr = tiles[t];
     if (tr.seg >= ns) continue;  // only after a capacity error (status already set)
     const Seg<K> s = segs[tr.seg];
-    if (Q && s.pad != loaded) {  // the previous tile ended with a barrier
-      qtab_to_smem<K>(qtab, qdir, s.pad, qb, qd);
-      loaded = s.pad;
+    if (tr.seg != open) {  // the previous tile ended with a barrier
+      if (open != 0xFFFFFFFFu) {
+        flush();
+        __syncthreads();
+      }
+      if (Q) qtab_to_smem<K>(qtab, qdir, s.pad, qb, qd);
+      for (uint32_t i = threadIdx.x; i < NBIN; i += NT) h[i] = 0u;
+      open = tr.seg;
+      open_keys = 0;
+      __syncthreads();
     }
-    for (uint32_t i = threadIdx.x; i < NBIN; i += NT) h[i] = 0u;
-    __syncthreads();
     const uint64_t beg = s.off + (uint64_t)tr.no * TILE;
     const uint64_t end = min(beg + TILE, s.off + s.cnt);
     constexpr int U = 8;  // independent loads in flight per thread
@@ -2184,15 +2205,10 @@ __global__ __launch_bounds__(NT) void lvl_count(const InT* __restrict__ src,
         atomicAdd(&h[bin], 1u);
       }
     }
-    __syncthreads();
-    uint32_t* row = rows + (size_t)tr.seg * NBIN;
-    for (uint32_t i = threadIdx.x; i < NBIN; i += NT) {
-      uint32_t v = h[i];
-      if (v) atomicAdd(&row[i], v);
-    }
-    if (threadIdx.x == 0) atomicAdd(&C->refine_elems, (unsigned long long)(end - beg));
+    open_keys += end - beg;
     __syncthreads();
   }
+  if (open != 0xFFFFFFFFu) flush();  // the last tile ended with a barrier
 }
 
 __global__ __launch_bounds__(1024) void lvl_scan(uint32_t* rows, const uint32_t* __restrict__ bigs,
@@ -2288,6 +2304,9 @@ __global__ __launch_bounds__(NT) void lvl_children(uint32_t* rows, const uint32_
 }
 
 // Copies each key whose bin became a child segment into that child's region.
+// Tiles go to CTAs grid-stride, so the CTAs running at one time fill the same
+// children side by side and L2 merges their partial sectors (contiguous tile
+// ranges per CTA measured 24 % slower on the 4096-segment batch).
 template <typename InT, int NT, bool Q = false>
 __global__ __launch_bounds__(NT) void lvl_compact(const InT* __restrict__ src,
                                                  const Seg<typename KeyOf<InT>::K>* __restrict__ segs,
@@ -2331,28 +2350,41 @@ __global__ __launch_bounds__(NT) void lvl_compact(const InT* __restrict__ src,
         const uint64_t i = beg + o + (uint64_t)u * NT;
         kk[u] = i < end ? KeyOf<InT>::to(src[i]) : (K)0;
       }
+      // 1. each key's child (CM_NONE when its bin is not copied)
+      uint32_t cc[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const bool valid = beg + o + (uint64_t)u * NT < end;
-        const K key = kk[u];
-        uint32_t c = CM_NONE;
-        if (valid) {
+        cc[u] = CM_NONE;
+        if (beg + o + (uint64_t)u * NT < end) {
           uint32_t bin;
-          if (Q) bin = qbin<K>(key, s.lo, s.shift, qb, qd);
-          else bin = min((uint32_t)((K)(key - s.lo) >> s.shift), (uint32_t)NBIN - 1u);
-          c = cm[bin];
+          if (Q) bin = qbin<K>(kk[u], s.lo, s.shift, qb, qd);
+          else bin = min((uint32_t)((K)(kk[u] - s.lo) >> s.shift), (uint32_t)NBIN - 1u);
+          cc[u] = cm[bin];
         }
-        const bool hit = valid && c < CM_POINT;
+      }
+      // 2. one cursor reservation per group of lanes with the same child, for
+      // all U keys before any result is used: the U global atomics of a warp
+      // are in flight together instead of one round trip after another
+      uint32_t peers[U], base[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const bool hit = cc[u] < CM_POINT;
         const uint32_t hm = __ballot_sync(FULL, hit);
-        if (hm && hit) {
-          const uint32_t peers = __match_any_sync(hm, c);
-          const int leader = __ffs(peers) - 1;
-          uint32_t basepos = 0;
-          if ((int)lane == leader) basepos = atomicAdd(&cursor_q[c], (uint32_t)__popc(peers));
-          basepos = __shfl_sync(peers, basepos, leader);
-          const uint32_t slot = basepos + __popc(peers & lanemask_lt());
-          const Seg<K>& sg = segs_q[c];
-          if (slot < sg.cnt) dst[sg.off + slot] = key;
+        peers[u] = 0u;
+        base[u] = 0u;
+        if (hit) {
+          peers[u] = __match_any_sync(hm, cc[u]);
+          if ((int)lane == __ffs(peers[u]) - 1) base[u] = atomicAdd(&cursor_q[cc[u]], (uint32_t)__popc(peers[u]));
+        }
+      }
+      // 3. the stores
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (peers[u]) {
+          const uint32_t b0 = __shfl_sync(peers[u], base[u], __ffs(peers[u]) - 1);
+          const uint32_t slot = b0 + __popc(peers[u] & lanemask_lt());
+          const Seg<K>& sg = segs_q[cc[u]];
+          if (slot < sg.cnt) dst[sg.off + slot] = kk[u];
           else set_status(const_cast<Counters*>(C), GGMS_E_INTERNAL);
         }
       }
