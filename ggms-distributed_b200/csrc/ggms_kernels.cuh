@@ -868,6 +868,51 @@ __device__ __forceinline__ void stream_keys(Src& src, typename KeyOf<T>::K* wq, 
   });
 }
 
+// Float input: the run tests on the raw bits.  The key of a float is its bits
+// with the sign bit flipped (non-negative values) or all bits flipped
+// (negative ones), so a key run [lo, lo + sp] that lies within one sign is the
+// raw range [lo ^ 2^31, ... + sp] (non-negative) or [~(lo + sp), ... + sp]
+// (negative), of the same span; the unsigned test (raw - rlo) <= sp rejects
+// every float of the other sign by wrap-around (rlo + sp stays below 2^31, or
+// the range ends at 2^32 - 1 - lo).  NaN and +-Inf keep their places.  Returns
+// false for a run that holds keys of both signs.
+__device__ __forceinline__ bool run_to_raw(uint32_t lo, uint32_t sp, uint32_t& rlo) {
+  const uint32_t hi = lo + sp;
+  if (lo >= 0x80000000u) { rlo = lo ^ 0x80000000u; return true; }
+  if (hi < 0x80000000u) { rlo = ~hi; return true; }
+  return false;
+}
+__device__ __forceinline__ uint32_t float_key_of_bits(uint32_t u) {
+  return u ^ ((u >> 31) ? 0xFFFFFFFFu : 0x80000000u);
+}
+
+// stream_keys for float input with a raw-bit test (run_to_raw): a key is
+// formed only for the values that pass, as the queue hands them out; the
+// queue's leftovers are turned into keys at the end, so the caller sees keys.
+template <typename Src, typename Test, typename Take>
+__device__ __forceinline__ void stream_raw_f32(Src& src, uint32_t* wq, uint32_t& qn, uint32_t lane, Test& test,
+                                               Take&& take) {
+  src.run([&](const uint4& qv) {
+    const uint32_t e[4] = {qv.x, qv.y, qv.z, qv.w};
+    bool hh[4];
+    bool any = false;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      hh[t] = test(e[t]);
+      any = any || hh[t];
+    }
+    if (!__any_sync(FULL, any)) return;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      uint32_t r0;
+      if (wq_push(wq, qn, hh[t], e[t], lane, &r0)) take(float_key_of_bits(r0));
+    }
+  });
+  __syncwarp();
+  if (lane < qn) wq[lane] = float_key_of_bits(wq[lane]);
+  __syncwarp();
+}
+
 // PASS 1 over windows with R runs (compile-time): the run tests, the per-run
 // counts (CNT) into below[0..R), the keys inside a run to take().
 template <typename T, uint32_t R, bool CNT, typename Src, typename Take>
@@ -875,6 +920,19 @@ __device__ __forceinline__ void count_runs(const Windows<typename KeyOf<T>::K>& 
                                            typename KeyOf<T>::K* wq, uint32_t& qn, uint32_t lane,
                                            uint32_t (&below)[L0_WIN], Take&& take) {
   using K = typename KeyOf<T>::K;
+  if constexpr (std::is_same<T, float>::value && !CNT) {
+    RunTest<K, R, false> tr;
+    bool raw = true;
+#pragma unroll
+    for (uint32_t r = 0; r < R; ++r) {
+      tr.sp[r] = (K)(W.hi[r] - W.lo[r]);
+      raw = raw && run_to_raw(W.lo[r], tr.sp[r], tr.lo[r]);
+    }
+    if (raw) {  // the same for every thread (W is the CTA's copy)
+      stream_raw_f32(src, wq, qn, lane, tr, take);
+      return;
+    }
+  }
   RunTest<K, R, CNT> t;
 #pragma unroll
   for (uint32_t r = 0; r < R; ++r) {
@@ -1716,6 +1774,19 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
     for (uint32_t r = 0; r < R; ++r) {
       t.lo[r] = win ? W.lo[r] : run_lo[r];
       t.sp[r] = win ? (K)(W.hi[r] - W.lo[r]) : run_span[r];
+    }
+    if constexpr (std::is_same<T, float>::value) {
+      RunTest<K, R, false> tr;
+      bool raw = true;
+#pragma unroll
+      for (uint32_t r = 0; r < R; ++r) {
+        tr.sp[r] = t.sp[r];
+        raw = raw && run_to_raw(t.lo[r], t.sp[r], tr.lo[r]);
+      }
+      if (raw) {  // the same for every thread of the CTA
+        stream_raw_f32(src, wq, qn, lane, tr, bucket_and_put);
+        return;
+      }
     }
     stream_keys<T>(src, wq, qn, lane, t, bucket_and_put);
   };
