@@ -874,12 +874,19 @@ __device__ __forceinline__ void stream_keys(Src& src, typename KeyOf<T>::K* wq, 
 // raw range [lo ^ 2^31, ... + sp] (non-negative) or [~(lo + sp), ... + sp]
 // (negative), of the same span; the unsigned test (raw - rlo) <= sp rejects
 // every float of the other sign by wrap-around (rlo + sp stays below 2^31, or
-// the range ends at 2^32 - 1 - lo).  NaN and +-Inf keep their places.  Returns
-// false for a run that holds keys of both signs.
-__device__ __forceinline__ bool run_to_raw(uint32_t lo, uint32_t sp, uint32_t& rlo) {
+// the range ends at 2^32 - 1 - lo).  NaN and +-Inf keep their places.  A run
+// over both signs is still one cyclic raw range when it reaches an end of the
+// key space: from key 0 it holds every negative float (raw 2^31 .. 2^32 - 1)
+// and the non-negative ones up to hi (raw 0 .. hi ^ 2^31); up to the largest
+// key it holds every non-negative float and the negative ones down to lo (raw
+// 0 .. ~lo).  Returns false for a run over both signs that reaches neither end.
+__device__ __forceinline__ bool run_to_raw(uint32_t lo, uint32_t sp, uint32_t& rlo, uint32_t& rsp) {
   const uint32_t hi = lo + sp;
+  rsp = sp;
   if (lo >= 0x80000000u) { rlo = lo ^ 0x80000000u; return true; }
   if (hi < 0x80000000u) { rlo = ~hi; return true; }
+  if (lo == 0u) { rlo = 0x80000000u; rsp = 0x80000000u + (hi ^ 0x80000000u); return true; }
+  if (hi == 0xFFFFFFFFu) { rlo = 0u; rsp = ~lo; return true; }
   return false;
 }
 __device__ __forceinline__ uint32_t float_key_of_bits(uint32_t u) {
@@ -924,10 +931,7 @@ __device__ __forceinline__ void count_runs(const Windows<typename KeyOf<T>::K>& 
     RunTest<K, R, false> tr;
     bool raw = true;
 #pragma unroll
-    for (uint32_t r = 0; r < R; ++r) {
-      tr.sp[r] = (K)(W.hi[r] - W.lo[r]);
-      raw = raw && run_to_raw(W.lo[r], tr.sp[r], tr.lo[r]);
-    }
+    for (uint32_t r = 0; r < R; ++r) raw = raw && run_to_raw(W.lo[r], (K)(W.hi[r] - W.lo[r]), tr.lo[r], tr.sp[r]);
     if (raw) {  // the same for every thread (W is the CTA's copy)
       stream_raw_f32(src, wq, qn, lane, tr, take);
       return;
@@ -1779,10 +1783,7 @@ __global__ __launch_bounds__(NT, PASS_MIN_CTAS(NT)) void l0_compact(const T* __r
       RunTest<K, R, false> tr;
       bool raw = true;
 #pragma unroll
-      for (uint32_t r = 0; r < R; ++r) {
-        tr.sp[r] = t.sp[r];
-        raw = raw && run_to_raw(t.lo[r], t.sp[r], tr.lo[r]);
-      }
+      for (uint32_t r = 0; r < R; ++r) raw = raw && run_to_raw(t.lo[r], t.sp[r], tr.lo[r], tr.sp[r]);
       if (raw) {  // the same for every thread of the CTA
         stream_raw_f32(src, wq, qn, lane, tr, bucket_and_put);
         return;
