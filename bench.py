@@ -80,8 +80,8 @@ WORKLOADS = {
 # capture of the same kernels on the same half-normal workload at n = 2^26
 # (profiles/l0_passes_half_normal_f32_n26.md); both passes read the input once,
 # so the traffic of a launch grows in proportion to n.
-PASS_TRAFFIC_PER_ELEM = {"l0_count": (268612096 + 3892224) / 2**26,
-                         "l0_compact": (271976960 + 3587840) / 2**26}
+PASS_TRAFFIC_PER_ELEM = {"l0_count": (268579072 + 3161088) / 2**26,
+                         "l0_compact": (272013824 + 3980544) / 2**26}
 
 
 def peaks():
@@ -647,7 +647,8 @@ def run_kernels_only(args):
     import ggms_b200 as G
     torch.cuda.set_device(0)
     w = dict(WORKLOADS[args.workload])
-    if w["kind"] != "single":  # the batched workloads at their stated shape, default options
+    if w["kind"] != "single":  # the batched workloads (4096 segments; 2^30 keys unless --total-log2)
+        w["total"] = 1 << args.total_log2
         vals, seg_off, ks, k_off = segmented_inputs(w)
         view = {np.dtype(np.uint32): np.int32}.get(vals.dtype)
         d_v = torch.from_numpy(vals.view(view) if view else vals).cuda()
@@ -692,6 +693,8 @@ def main():
     ap.add_argument("--backend", default="auto")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--n-log2", type=int, default=28, help="vector length (--kernels-only runs only)")
+    ap.add_argument("--total-log2", type=int, default=30,
+                    help="keys of a batched workload in all (--kernels-only runs only)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="a few device-resident calls and exit (for profilers); no JSON line")
     args = ap.parse_args()
