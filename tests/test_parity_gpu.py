@@ -238,7 +238,7 @@ def test_config3_adversarial(ctx, gen):
 @pytest.mark.parametrize("gen,seed", [("mixture8_f32", 31), ("lognormal_f32", 32)])
 def test_config4_learned(ctx, gen, seed):
     """The learned-assigner benchmark as configured: 2^28 keys, 2^14 random ks;
-    the sampled pivots, the 256-knot PL-CDF model, the default (1024-knot) PL
+    the sampled pivots, the 256-knot PL-CDF model, the default (512-knot) PL
     model, the 1-32-32-1 MLP and AUTO, every answer exact."""
     n = 1 << 28
     v = D.VALUE_GENERATORS[gen](n, seed)
