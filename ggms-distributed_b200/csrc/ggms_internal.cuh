@@ -365,6 +365,19 @@ __device__ K grid_inv(const GridView<K>& g, uint32_t ncell, uint32_t target) {
   return a;
 }
 
+// Largest key whose bucket is <= e (the last key of the bucket range ending at
+// e).  When no key reaches bucket e + 1 -- e is the last bucket, or the model
+// maps even the largest key below e + 1, as a learned model whose buckets are
+// focused on the ks can -- that is the largest key itself; grid_inv's answer
+// (the largest key as "none") minus one would drop it from the range.
+template <typename K>
+__device__ K grid_last_key(const GridView<K>& g, uint32_t ncell, uint32_t e) {
+  const K kmax = (K)~(K)0;
+  if (e >= g.B - 1u || min(grid_eval<K>(g, kmax), g.B - 1u) <= e) return kmax;
+  const K first_above = grid_inv<K>(g, ncell, e + 1u);
+  return first_above ? (K)(first_above - 1u) : (K)0;  // 0: even key 0 lies above e (an empty range)
+}
+
 // ------------------------------------------------------------------ refinement levels
 // A segment of candidates.  Every key of the segment lies in [lo, hi]; its bin
 // is (key - lo) >> shift, shift chosen so that bins < NBIN.

@@ -1270,7 +1270,7 @@ __global__ __launch_bounds__(1024) void l0_children(const uint32_t* __restrict__
       const uint32_t b0 = coarse ? b << gsh : b;
       const uint32_t e = coarse ? ((b + 1u) << gsh) - 1u : win_end<K>(*Wg, b);
       lo = (b0 == 0) ? (K)0 : grid_inv<K>(gv, ncell, b0);
-      hi = (e >= B - 1) ? key_max<K>() : (K)(grid_inv<K>(gv, ncell, e + 1u) - 1u);
+      hi = grid_last_key<K>(gv, ncell, e);
       atomicAdd(&ctr[N_ACT], 1u);
       if (lo == hi) {
         kind = C_POINT;

@@ -146,19 +146,16 @@ __global__ __launch_bounds__(WIN_NT) void l0_window(const K* __restrict__ sorted
   }
   __syncthreads();
   GGMS_TRACE(22);
-  // 5. key range of each run: [L(rb0), L(rb1 + 1) - 1], L(x) = smallest key with bucket >= x
+  // 5. key range of each run: [L(rb0), L(rb1 + 1) - 1], L(x) = smallest key with
+  //    bucket >= x; the upper end is the largest key when no key reaches rb1 + 1
   if (sw.on && tid < 2u * sw.R) {
     const uint32_t r = tid >> 1;
     const bool upper = tid & 1u;
-    const uint32_t target = upper ? sw.rb1[r] + 1u : sw.rb0[r];
     K v;
-    if (!upper && target == 0u) {
-      v = (K)0;
-    } else if (upper && target >= B) {
-      v = key_max<K>();
-    } else {  // target <= B - 1: the clamp to B - 1 does not change the answer
-      const K lo = grid_inv<K>(gv, ncell, target);
-      v = upper ? (lo == 0 ? (K)0 : (K)(lo - 1u)) : lo;
+    if (upper) {
+      v = grid_last_key<K>(gv, ncell, sw.rb1[r]);
+    } else {  // rb0 <= B - 1: the clamp to B - 1 does not change the answer
+      v = sw.rb0[r] == 0u ? (K)0 : grid_inv<K>(gv, ncell, sw.rb0[r]);
     }
     if (upper) sw.hi[r] = v; else sw.lo[r] = v;
   }

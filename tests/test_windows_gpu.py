@@ -98,3 +98,43 @@ def test_focused_buckets_cut_candidates(ctx):
         res[z] = st
     assert res[0.0]["window_runs"] >= 1
     assert res[0.0]["candidates"] * 3 < res[-1.0]["candidates"], res
+
+
+def _f32_bits(u):
+    return np.array(u, dtype=np.uint32).view(np.float32)
+
+
+@pytest.mark.parametrize("case", ["specials", "all_negative", "signed_zeros"])
+@pytest.mark.parametrize("window_z", [0.0, 0.001])
+def test_windows_raw_bit_runs(ctx, case, window_z):
+    """fp32 window runs are tested on the raw bits of the input, not on keys:
+    runs within one sign, runs over both signs from the smallest key or up to
+    the largest (one cyclic range of raw bits), and runs over +-0 in the middle
+    (which keep the key test).  NaNs of both signs, +-Inf, +-0 and subnormals are
+    among the values, and ks sit at both ends, in the top 1 % and at the sign
+    boundary."""
+    g = np.random.default_rng({"specials": 31, "all_negative": 32, "signed_zeros": 33}[case])
+    n = N
+    if case == "all_negative":
+        v = -np.abs(g.standard_normal(n)).astype(np.float32)
+        v[g.integers(0, n, 50)] = -0.0
+    elif case == "signed_zeros":
+        v = (1e-3 * g.standard_normal(n)).astype(np.float32)
+        z = g.random(n)
+        v[z < 0.05] = 0.0
+        v[(z >= 0.05) & (z < 0.10)] = -0.0
+    else:
+        v = g.standard_normal(n).astype(np.float32)
+        specials = _f32_bits([0x7FC00000, 0xFFC00000, 0x7F800000, 0xFF800000, 0x00000000, 0x80000000,
+                              0x00000001, 0x80000001, 0x007FFFFF, 0x807FFFFF, 0x7FFFFFFF, 0xFFFFFFFF])
+        for s in specials:
+            v[g.integers(0, n, 40)] = s
+    neg = int(np.count_nonzero(v.view(np.uint32) >> 31))  # keys below +0.0
+    ks = np.concatenate([D.ks_top1pct(n, 1024, 7),
+                         np.clip(n - neg + np.arange(-3, 4), 1, n),
+                         [2, 3, n - 1, n - 2]]).astype(np.uint32)
+    d = to_device(v)
+    out, st = G.select(ctx, d.data_ptr(), n, ks, np.float32, stats=True, window_z=window_z)
+    np.testing.assert_array_equal(orc.bits(out), orc.bits(orc.select(v, ks)))
+    out_s = G.select(ctx, d.data_ptr(), n, ks, np.float32, assigner=G.ASSIGNER_SAMPLED, window_z=window_z)
+    np.testing.assert_array_equal(orc.bits(out_s), orc.bits(orc.select(v, ks)))
