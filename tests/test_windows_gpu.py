@@ -138,3 +138,20 @@ def test_windows_raw_bit_runs(ctx, case, window_z):
     np.testing.assert_array_equal(orc.bits(out), orc.bits(orc.select(v, ks)))
     out_s = G.select(ctx, d.data_ptr(), n, ks, np.float32, assigner=G.ASSIGNER_SAMPLED, window_z=window_z)
     np.testing.assert_array_equal(orc.bits(out_s), orc.bits(orc.select(v, ks)))
+
+
+@pytest.mark.parametrize("assigner", [G.ASSIGNER_AUTO, G.ASSIGNER_SAMPLED])
+def test_windows_extreme_keys_f64(ctx, assigner):
+    """fp64 with the NaN payloads whose keys are 0 and the largest 64-bit key,
+    +-Inf and +-0, windows on: every bucket range of the windows and of the
+    level-0 children keeps the largest key, whichever bucket the model gives it."""
+    g = np.random.default_rng(34)
+    n = N
+    v = g.standard_normal(n)
+    for s in [0x7FFFFFFFFFFFFFFF, 0xFFFFFFFFFFFFFFFF, 0x7FF8000000000000, 0xFFF8000000000000,
+              0x7FF0000000000000, 0xFFF0000000000000, 0x0000000000000000, 0x8000000000000000]:
+        v[g.integers(0, n, 40)] = np.array([s], dtype=np.uint64).view(np.float64)[0]
+    ks = np.concatenate([D.ks_top1pct(n, 1024, 8), [2, 3, n - 1, n - 2]]).astype(np.uint32)
+    d = to_device(v)
+    out = G.select(ctx, d.data_ptr(), n, ks, np.float64, assigner=assigner)
+    np.testing.assert_array_equal(orc.bits(out), orc.bits(orc.select(v, ks)))
