@@ -155,3 +155,37 @@ def test_windows_extreme_keys_f64(ctx, assigner):
     d = to_device(v)
     out = G.select(ctx, d.data_ptr(), n, ks, np.float64, assigner=assigner)
     np.testing.assert_array_equal(orc.bits(out), orc.bits(orc.select(v, ks)))
+
+
+@pytest.mark.parametrize("shape,buckets,offset", [((256, 4), 0, 0), ((256, 8), 0, 0), ((512, 2), 0, 0),
+                                                  ((512, 8), 0, 0), ((1024, 2), 0, 0), ((1024, -1), 0, 0),
+                                                  ((1024, -2), 0, 0), ((1024, 4), 32768, 0),
+                                                  ((1024, 4), 4096, 0), ((1024, 4), 0, 1), ((1024, -1), 0, 3)])
+def test_windows_raw_bit_pass_shapes(ctx, shape, buckets, offset):
+    """The windowed passes in every streaming shape (register loads of 2-8
+    vectors, the TMA ring, per-thread async copies), other bucket counts, and a
+    vector starting 4 or 12 bytes past a 16-byte boundary (its head and tail go
+    through the key test, the body through the raw-bit test): mixed-sign fp32
+    with NaNs, +-Inf and +-0, ks at both ends, in the top 1 % and at the sign
+    boundary; AUTO and sampled, bit-exact."""
+    import torch
+
+    g = np.random.default_rng(35)
+    n = N
+    v = g.standard_normal(n + offset).astype(np.float32)
+    for s in [0x7FC00000, 0xFFC00000, 0x7F800000, 0xFF800000, 0x00000000, 0x80000000, 0x7FFFFFFF, 0xFFFFFFFF]:
+        v[g.integers(0, n + offset, 40)] = np.array([s], dtype=np.uint32).view(np.float32)[0]
+    w = v[offset:]
+    neg = int(np.count_nonzero(w.view(np.uint32) >> 31))
+    ks = np.concatenate([D.ks_top1pct(n, 1024, 9), np.clip(n - neg + np.arange(-2, 3), 1, n),
+                         [2, n - 1]]).astype(np.uint32)
+    exp = orc.select(w, ks)
+    base = to_device(v)
+    ptr = base.data_ptr() + 4 * offset
+    kw = dict(pass_threads=shape[0], pass_unroll=shape[1])
+    if buckets:
+        kw["num_buckets"] = buckets
+    for a in (G.ASSIGNER_AUTO, G.ASSIGNER_SAMPLED):
+        out = G.select(ctx, ptr, n, ks, np.float32, assigner=a, **kw)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(orc.bits(out), orc.bits(exp))
