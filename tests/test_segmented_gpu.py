@@ -116,3 +116,30 @@ def test_segmented_size_classes(ctx, dtype):
     ks = np.concatenate(ks_l).astype(np.uint32)
     got = run_segmented(ctx, vals, seg_off, ks, k_off)
     np.testing.assert_array_equal(orc.bits(got), orc.bits(orc.select_segmented(vals, seg_off, ks, k_off)))
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.uint32])
+def test_segmented_extreme_keys(ctx, dtype):
+    """Segments of every finishing class holding the smallest and largest keys
+    (fp32: the NaN payloads 0xFFFFFFFF and 0x7FFFFFFF, +-Inf, +-0; uint32: 0 and
+    2^32 - 1), each with its extreme ks and a run of ks."""
+    g = np.random.default_rng(18)
+    lens = [100, 3000, 5000, 70000, 1 << 20]
+    parts, ks_l = [], []
+    for ln in lens:
+        if dtype == np.float32:
+            v = g.standard_normal(ln).astype(np.float32)
+            sp = np.array([0x7FFFFFFF, 0xFFFFFFFF, 0x7F800000, 0xFF800000, 0x80000000, 0x00000000], np.uint32)
+            v[g.integers(0, ln, 12)] = sp[g.integers(0, len(sp), 12)].view(np.float32)
+        else:
+            v = g.integers(0, 1 << 32, size=ln, dtype=np.uint64).astype(np.uint32)
+            v[g.integers(0, ln, 12)] = np.array([0, 0xFFFFFFFF], np.uint32)[g.integers(0, 2, 12)]
+        parts.append(v)
+        k = np.concatenate([[1, 2, ln - 1, ln, (ln + 1) // 2], g.integers(1, ln + 1, size=20)])
+        ks_l.append(k.astype(np.uint32))
+    vals = np.concatenate(parts).astype(dtype)
+    seg_off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    k_off = np.concatenate([[0], np.cumsum([len(k) for k in ks_l])]).astype(np.int64)
+    ks = np.concatenate(ks_l).astype(np.uint32)
+    got = run_segmented(ctx, vals, seg_off, ks, k_off)
+    np.testing.assert_array_equal(orc.bits(got), orc.bits(orc.select_segmented(vals, seg_off, ks, k_off)))
