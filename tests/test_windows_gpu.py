@@ -189,3 +189,24 @@ def test_windows_raw_bit_pass_shapes(ctx, shape, buckets, offset):
         out = G.select(ctx, ptr, n, ks, np.float32, assigner=a, **kw)
         torch.cuda.synchronize()
         np.testing.assert_array_equal(orc.bits(out), orc.bits(exp))
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_windows_topk_extreme_keys(ctx, dtype):
+    """Top-k with the largest keys in the data (+NaN with the largest payload,
+    other +NaNs, +Inf): the ks 1..K form one window run at the top of the key
+    space, which must keep the largest key whatever bucket the model gives it."""
+    g = np.random.default_rng(36)
+    n = N
+    v = g.standard_normal(n).astype(dtype)
+    if dtype == np.float32:
+        sp = np.array([0x7FFFFFFF, 0x7FC00000, 0x7F800000], np.uint32).view(np.float32)
+    else:
+        sp = np.array([0x7FFFFFFFFFFFFFFF, 0x7FF8000000000000, 0x7FF0000000000000], np.uint64).view(np.float64)
+    for s in sp:
+        v[g.integers(0, n, 30)] = s
+    d = to_device(v)
+    K = 4096
+    for a in (G.ASSIGNER_AUTO, G.ASSIGNER_SAMPLED):
+        out = G.topk(ctx, d.data_ptr(), n, K, dtype, assigner=a)
+        np.testing.assert_array_equal(orc.bits(out), orc.bits(orc.select(v, np.arange(1, K + 1, dtype=np.uint32))))
